@@ -1,0 +1,299 @@
+#!/usr/bin/env python
+"""Benchmark of the UW shallow-cumulus driver compute_uwshcu on B200.
+
+Workload: 259,200 independent columns (a 720 x 360 grid) x 30 levels, 5 tracers (qv, ql, qi, nl,
+ni), dt = 1800 s, seeded synthetic soundings (hpc-and-climate-model_b200/soundings.py) with the
+PBL relative humidity drawn from U(0.675, 0.93) so that about 40 % of the columns convect.
+A step is one compute_uwshcu call over all columns.  Metric: columns per second.
+
+  value : device-resident throughput (inputs already in HBM, uwshcu_compute_device), CUDA events
+          on the launching stream around exactly K steps; inputs (1.2 GB) exceed the 126 MB L2.
+  e2e   : the same metric through the reference-facing C ABI compute_uwshcu_ with host arrays:
+          the timed region includes the host->device copy of each step's inputs and the
+          device->host copy of its outputs.
+  --impl reference : the reference algorithm's CPU implementation (the C restatement in
+          oracle/, compiled with -O2 -ffp-contract=off, OpenMP over all host cores) on a bounded
+          sample of the same workload.
+
+Multi-GPU (torchrun): every rank processes its own 259,200 columns (different seeds); columns are
+independent, so there is no collective on the data path ("scaling": "weak").  Timing is the max
+over ranks of the device time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "hpc-and-climate-model_b200")
+sys.path.insert(0, PKG)
+
+NCOL = 259_200
+PVER = 30
+NCNST = 5
+RH_PBL = (0.675, 0.93)
+METRIC = "columns/s (compute_uwshcu, FP64, 259,200 x 30 levels)"
+
+
+def bytes_per_column(mkx=PVER, ncnst=NCNST):
+    """Algorithmic bytes of one column: inputs read + outputs written (FP64)."""
+    n_in = 3 * (mkx + 1) + 10 * mkx + ncnst * mkx + 2
+    n_out = 6 * (mkx + 1) + 14 * mkx + ncnst * mkx + 7
+    return 8 * n_in, 8 * n_out
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def run_reference(args):
+    """CPU arm: the oracle (C restatement of the reference algorithm) on host cores."""
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+    import soundings
+    oracle.init_default()
+    cores = os.cpu_count() or 1
+    sample = int(args.cpu_sample)
+    s = soundings.make_soundings(sample, PVER, seed=1, rh_pbl=RH_PBL)
+    for _ in range(args.warmup if args.warmup < 1 else 1):
+        oracle.compute(s, nthreads=cores, diag=False)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        oracle.compute(s, nthreads=cores, diag=False)
+        times.append(time.perf_counter() - t0)
+    sec = float(np.median(times))
+    val = sample / sec
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": "columns/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded soundings)",
+        "config": {"workload": "compute_uwshcu 259,200 x 30 levels, 5 tracers, dt=1800 s; each "
+                               "step a %d-column sample" % sample,
+                   "ncol_sample": sample, "pver": PVER, "ncnst": NCNST},
+        "cpu_baseline": {"value": val, "unit": "columns/s", "cores": cores, "kind": "port",
+                         "sample": "%d columns of the 259,200-column workload per step" % sample},
+        "e2e": {"value": val, "unit": "columns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_leg(seconds=10.0):
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+    import soundings
+    oracle.init_default()
+    cores = os.cpu_count() or 1
+    n = 32768
+    s = soundings.make_soundings(n, PVER, seed=3, rh_pbl=RH_PBL)
+    oracle.compute(s, nthreads=cores, diag=False)
+    done, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        oracle.compute(s, nthreads=cores, diag=False)
+        done += n
+    sec = time.perf_counter() - t0
+    return {"value": done / sec, "unit": "columns/s", "cores": cores, "kind": "port",
+            "sample": "%d passes over a %d-column slice of the workload (%.1f s)" % (done // n, n, sec)}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ncol", type=int, default=NCOL)
+    ap.add_argument("--cpu-sample", type=int, default=32768)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import soundings
+    import uwshcu_b200 as uw
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    assert uw.init_default() == 0
+    n = args.ncol
+    s = soundings.make_soundings(n, PVER, seed=1 + rank, rh_pbl=RH_PBL)
+    case = uw.DeviceCase(s)
+    stream = torch.cuda.Stream()
+    nbytes_in, nbytes_out = bytes_per_column()
+
+    def step():
+        case.out["cush"].copy_(case.cush0, non_blocking=True)
+        rc = case.launch(stream=stream)
+        if rc != 0:
+            raise RuntimeError("uwshcu_compute_device: %d %s" % (rc, uw.last_cuda_error()))
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(args.warmup, 3)):
+            step()
+    stream.synchronize()
+    st = case.status(stream)
+    trig = float((case.out["cush"] != -1.0).float().mean().item())
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+            for _ in range(args.steps):
+                step()
+            ev1.record(stream)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if pg:
+        t = torch.tensor([ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * n / (ms * 1e-3)
+    kernel_ms = ms
+
+    # end-to-end through compute_uwshcu_ with host arrays
+    e2e = None
+    if not args.no_e2e:
+        out = uw.alloc_outputs(PVER, NCNST, n, s["cush"])
+        for _ in range(2):
+            out["cush"][:] = s["cush"]
+            rc, _ = uw.compute_host(s, out=out)
+        if pg:
+            pg.barrier()
+        ksteps = max(1, min(args.steps, 5))
+        t0 = time.perf_counter()
+        for _ in range(ksteps):
+            out["cush"][:] = s["cush"]
+            rc, _ = uw.compute_host(s, out=out)
+        sec = (time.perf_counter() - t0) / ksteps
+        if pg:
+            t = torch.tensor([sec], device="cuda")
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            sec = float(t.item())
+        e2e = {"value": world * n / sec, "unit": "columns/s",
+               "h2d_bytes_per_step": int(n * (nbytes_in + 8 * PVER)),
+               "d2h_bytes_per_step": int(n * nbytes_out), "ms_per_step": sec * 1e3,
+               "status": int(rc)}
+
+    peak, peak_kind = peaks()
+    alg = n * (nbytes_in + nbytes_out)
+    achieved = alg / (kernel_ms * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "columns/s", "n_gpus": world,
+        "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded soundings, PCG64 seed 1+rank)",
+        "config": {"workload": "compute_uwshcu 259,200 columns (720x360) x 30 levels, 5 tracers, "
+                               "dt=1800 s, ~40%% convecting", "ncol_per_gpu": n, "pver": PVER,
+                   "ncnst": NCNST, "trigger_fraction": trig, "l2": "inputs (1.2 GB) larger than L2",
+                   "parallelism": "column shards, %d rank(s), no collective" % world},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                     "note": "FP64 column physics is compute-bound; algorithmic bytes = "
+                             "%d B/column" % (nbytes_in + nbytes_out)},
+        "gpu_launches": args.steps,
+        "status": st,
+    }
+    if e2e is not None:
+        line["e2e"] = e2e
+    if clk is not None:
+        line["clocks"] = clk.summary()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_leg()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

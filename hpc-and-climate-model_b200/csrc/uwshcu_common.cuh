@@ -1,0 +1,96 @@
+// uwshcu_common.cuh -- data shared by the UW shallow-cumulus kernels and the host library.
+//
+// Layout conventions (the Fortran compute_uwshcu argument layout, uwshcu.F90:529-580):
+//   interface fields (mix, 0:mkx) -> a[k*mix + i],            k = 0 .. mkx, k = 0 at the surface
+//   layer fields     (mix, mkx)   -> a[(k-1)*mix + i],        k = 1 .. mkx
+//   tracer fields    (mix, mkx, ncnst) -> a[((m-1)*mkx + k-1)*mix + i]
+// with i the 0-based column index.  Column index fastest means a warp of consecutive columns reads
+// and writes 32 consecutive doubles for every (k, m): level-major structure of arrays.
+#pragma once
+#include <cstdint>
+
+#define UW_NCMAX 32      // largest tracer count the kernels accept
+#define UW_TBL 250       // saturation-vapour-pressure table length (wv_saturation.F90:43)
+
+// Per-column integer diagnostics, array (UW_NDI, mix).
+#define UW_DI_EXIT 0     // bitmask of the exit_* flags (uwshcu.F90:889-899); 0 = convection ran
+#define UW_DI_LIMIT 1    // bitmask of the limit_* flags and ind_delcin (uwshcu.F90:901-910)
+#define UW_DI_KINV 2
+#define UW_DI_KLCL 3
+#define UW_DI_KLFC 4
+#define UW_DI_KREL 5
+#define UW_DI_KBUP 6
+#define UW_DI_KPEN 7
+#define UW_NDI 8
+// Per-column real diagnostics, array (UW_NDR, mix).
+#define UW_DR_CIN 0
+#define UW_DR_CINLCL 1
+#define UW_DR_PLCL 2
+#define UW_DR_PLFC 3
+#define UW_DR_PINV 4
+#define UW_DR_PBUP 5
+#define UW_DR_PPEN 6
+#define UW_DR_TKEAVG 7
+#define UW_NDR 8
+
+// exit_* bits
+#define UW_X_UWCU (1 << 0)
+#define UW_X_CONDEN (1 << 1)
+#define UW_X_KLCLMKX (1 << 2)
+#define UW_X_KLFCMKX (1 << 3)
+#define UW_X_UFRC (1 << 4)
+#define UW_X_WTW (1 << 5)
+#define UW_X_DRYCORE (1 << 6)
+#define UW_X_WU (1 << 7)
+#define UW_X_CUFILTER (1 << 8)
+#define UW_X_KINV1 (1 << 9)
+#define UW_X_REI (1 << 10)
+// limit_* bits
+#define UW_L_SHCU (1 << 0)
+#define UW_L_NEGCON (1 << 1)
+#define UW_L_UFRC (1 << 2)
+#define UW_L_PPEN (1 << 3)
+#define UW_L_EMF (1 << 4)
+#define UW_L_CINLCL (1 << 5)
+#define UW_L_CIN (1 << 6)
+#define UW_L_CBMF (1 << 7)
+#define UW_L_REI (1 << 8)
+#define UW_L_DELCIN (1 << 9)
+
+// Device error word bits (set with atomicOr, read back by the host and mapped to status codes).
+#define UW_ERRBIT_MU 1        // 'Critical error in mu calculation' (uwshcu.F90:2119-2122)
+#define UW_ERRBIT_FINDSP 2    // findsp did not converge (uwshcu.F90:5423-5431)
+#define UW_ERRBIT_ENTHALPY 4  // findsp enthalpy not conserved (uwshcu.F90:5435-5447)
+
+// Physical constants and tables, set once by uwshcu_init and copied to __constant__ memory.
+struct UwConst {
+    // uwshcu module (uwshcu.F90:25-37)
+    double xlv, xlf, xls, cp, zvir, r, g, ep2, p00, rovcp, rpen;
+    // wv_saturation module (wv_saturation.F90:48-59)
+    double tmin, tmax, ttrice, epsqs, rgasv, hlatf, hlatv, cpws, tmelt;
+    double pcf[6];
+    double omeps, trinv;   // 1 - epsqs and 1/ttrice, as vqsatd computes them on every call
+    int icephs;
+    // constituents
+    int ncnst, ixnumliq, ixnumice;
+    double qmin[UW_NCMAX];
+    int wet[UW_NCMAX];
+};
+
+// Pointers of one compute_uwshcu call (device addresses), in the Fortran argument order.
+struct UwArgs {
+    int mix, mkx, iend, ncnst;
+    int inv;             // 1: level order of compute_uwshcu_inv (top-down), 0: bottom-up
+    double dt;
+    const double *ps0, *zs0, *p0, *z0, *dp0, *u0, *v0, *qv0, *ql0, *qi0, *t0, *s0, *tr0, *tke;
+    const double *pblh;
+    double *cush;
+    double *umf, *slflx, *qtflx, *flxprc1, *flxsnow1, *qvten, *qlten, *qiten, *sten, *uten, *vten,
+        *trten, *qrten, *qsten, *precip, *snow, *evapc, *cufrc, *qcu, *qlu, *qiu, *cbmf, *qc, *rliq;
+    double *cnt, *cnb;
+    const double *dpdry0;
+    double *wu;
+    int *diag_int;       // optional (UW_NDI, mix)
+    double *diag_real;   // optional (UW_NDR, mix)
+    unsigned int *err;   // device error word
+};

@@ -1,0 +1,1767 @@
+// uwshcu_fp64.cu -- FP64 sm_100a kernel of compute_uwshcu (uwshcu.F90:478-4664), one thread per column.
+//
+// Each thread owns one column.  The inputs are read directly in the Fortran (mix, k) layout, so a warp
+// of 32 consecutive columns issues 32 consecutive 8-byte loads for every level (level-major SoA).
+// Read-only inputs stay in global memory (read through the non-coherent path); the profiles the scheme
+// updates live in thread-private arrays sized by the template bound KP >= mkx + 1.  The saturation
+// table (wv_saturation.F90 estbl) is staged once per block in shared memory, where the data-dependent
+// lookups of neighbouring threads do not serialise the way __constant__ reads would.
+//
+// Numerics: every expression keeps the Fortran evaluation order, the file is built with -fmad=false
+// (no FMA contraction) and IEEE division/sqrt, so the only differences to the CPU restatement are the
+// last-bit differences of pow/exp/log/erfc between CUDA's libdevice and glibc.  exnf(p) = (p/p00)**rovcp
+// is evaluated once per distinct pressure and passed into conden: conden at p = ps0(k), p0(k), pe,
+// prel, plcl or the cloud top recomputes exactly these values in the Fortran, so the result is the
+// same bit for bit and the per-call pow disappears from the Newton loop.
+//
+// Structure relative to the Fortran: the iteration-1 results that the Fortran keeps in *_s arrays
+// (uwshcu.F90:4177-4277) are written straight into this column's output slots, which hold exactly
+// those values if iteration 2 falls back to explicit CIN (uwshcu.F90:1891-2011); the *_o copies of the
+// inputs (:1306-1327) are re-read from the input arrays, and the derived profiles are recomputed
+// from them with the same operations.  No loop has a data-dependent trip count beyond the fixed
+// Fortran bounds (conden 10, qsinvert 10, compute_alpha 10, compute_mumin2 10, compute_ppen 5,
+// findsp 8), and every level index the scheme derives (kinv, klcl, klfc, krel, kbup, kpen) comes
+// from a loop over 0..mkx, so all array accesses stay inside the column.
+#include <cuda_runtime.h>
+#include <math.h>
+#include "uwshcu_common.cuh"
+
+namespace {
+
+__constant__ UwConst c;
+__constant__ double c_estbl[UW_TBL];
+
+#define MX(a, b) ((a) > (b) ? (a) : (b))
+#define MN(a, b) ((a) < (b) ? (a) : (b))
+
+// estblf (wv_saturation.F90:64-80).  e is clamped to [tmin, tmax] first (a NaN argument ends at
+// tmax), so i stays in 1..203 and i+1 inside the 204 filled entries.
+__device__ __forceinline__ double estblf(double td, const double* __restrict__ tbl)
+{
+    double e = MX(MN(td, c.tmax), c.tmin);
+    int i = (int)(e - c.tmin) + 1;
+    double ai = trunc(e - c.tmin);
+    return (c.tmin + ai - e + 1.0) * tbl[i - 1] - (c.tmin + ai - e) * tbl[i];
+}
+
+// vqsatd with len = 1 (wv_saturation.F90:482-609) returning es, qs and gam.
+__device__ __forceinline__ void qsat3(double t, double p, double& es, double& qs, double& gam,
+                                      const double* __restrict__ tbl)
+{
+    es = estblf(t, tbl);
+    qs = c.epsqs * es / (p - c.omeps * es);
+    qs = MN(1.0, qs);
+    if (qs < 0.0) {
+        qs = 1.0;
+        es = p;
+    }
+    double hltalt, desdt;
+    if (c.icephs && c.ttrice != 0.0) {
+        double tc = t - c.tmelt;
+        bool lflg = (tc >= -c.ttrice && tc < 0.0);
+        double weight = MN(-tc * c.trinv, 1.0);
+        double hlatsb = c.hlatv + weight * c.hlatf;
+        double hlatvp = c.hlatv - 2369.0 * tc;
+        hltalt = (t < c.tmelt) ? hlatsb : hlatvp;
+        double tterm = lflg ? c.pcf[0] + tc * (c.pcf[1] + tc * (c.pcf[2] + tc * (c.pcf[3] + tc * c.pcf[4]))) : 0.0;
+        desdt = hltalt * es / (c.rgasv * t * t) + tterm * c.trinv;
+    } else {
+        double hlatvp = c.hlatv - 2369.0 * (t - c.tmelt);
+        double hlatsb = c.icephs ? c.hlatv + c.hlatf : c.hlatv;
+        hltalt = (t < c.tmelt) ? hlatsb : hlatvp;
+        desdt = hltalt * es / (c.rgasv * t * t);
+    }
+    gam = hltalt * qs * p * desdt / (c.cpws * es * (p - c.omeps * es));
+    if (qs == 1.0) gam = 0.0;
+}
+
+// The qs of vqsatd only (what conden and the buoyancy sorting consume).
+__device__ __forceinline__ double qsat_qs(double t, double p, const double* __restrict__ tbl)
+{
+    double es = estblf(t, tbl);
+    double qs = c.epsqs * es / (p - c.omeps * es);
+    qs = MN(1.0, qs);
+    if (qs < 0.0) qs = 1.0;
+    return qs;
+}
+
+__device__ __forceinline__ double exnf(double p) { return pow(p / c.p00, c.rovcp); }
+
+// conden (uwshcu.F90:4718-4785) with ex = exnf(p) supplied by the caller.
+__device__ __forceinline__ int conden(double p, double ex, double thl, double qt, double& th, double& qv,
+                                      double& ql, double& qi, const double* __restrict__ tbl)
+{
+    double tc = thl * ex;
+    double nu = MX(MN((268.0 - tc) / 20.0, 1.0), 0.0);
+    double leff = (1.0 - nu) * c.xlv + nu * c.xls;
+    double temps = tc;
+    double rvls = qsat_qs(temps, p, tbl);
+    if (rvls >= qt) {
+        qv = qt;
+        ql = 0.0;
+        qi = 0.0;
+        th = tc / ex;
+        return 0;
+    }
+    double qs = rvls;
+#pragma unroll 1
+    for (int it = 0; it < 10; it++) {
+        temps = temps + ((tc - temps) * c.cp / leff + qt - rvls) /
+                            (c.cp / leff + c.ep2 * leff * rvls / c.r / temps / temps);
+        qs = qsat_qs(temps, p, tbl);
+        rvls = qs;
+    }
+    double qc = MX(qt - qs, 0.0);
+    qv = qt - qc;
+    ql = qc * (1.0 - nu);
+    qi = nu * qc;
+    th = temps / ex;
+    return (fabs((temps - (leff / c.cp) * qc) - tc) >= 1.0) ? 1 : 0;
+}
+
+// roots (uwshcu.F90:4787-4829); r1/r2 keep the caller's values on the failure branches.
+__device__ __forceinline__ int roots(double a, double b, double cc, double& r1, double& r2)
+{
+    int status = 0;
+    if (a == 0.0) {
+        if (b == 0.0) status = 1;
+        else r1 = -cc / b;
+        r2 = r1;
+    } else {
+        if (b == 0.0) {
+            if (a * cc > 0.0) status = 2;
+            else r1 = sqrt(-cc / a);
+            r2 = -r1;
+        } else {
+            if ((b * b - 4.0 * a * cc) < 0.0) {
+                status = 3;
+            } else {
+                double q = -0.5 * (b + copysign(1.0, b) * sqrt(b * b - 4.0 * a * cc));
+                r1 = q / a;
+                r2 = cc / q;
+            }
+        }
+    }
+    return status;
+}
+
+// slope (uwshcu.F90:4831-4861); field/p0/sl are 1-based local arrays.
+template <int KP>
+__device__ __forceinline__ void slope(int mkx, const double* field, const double* p0, double* sl)
+{
+    double below = (field[2] - field[1]) / (p0[2] - p0[1]);
+#pragma unroll 1
+    for (int k = 2; k <= mkx; k++) {
+        double above = (field[k] - field[k - 1]) / (p0[k] - p0[k - 1]);
+        if (above > 0.0) sl[k - 1] = MX(0.0, MN(above, below));
+        else sl[k - 1] = MN(0.0, MX(above, below));
+        below = above;
+    }
+    sl[mkx] = sl[mkx - 1];
+}
+
+// qsinvert (uwshcu.F90:4863-4929) with exsfc = exnf(psfc).
+__device__ double qsinvert(double qt, double thl, double psfc, double exsfc, const double* __restrict__ tbl)
+{
+    const double psmin = 100.0 * 100.0, dpsmax = 1.0;
+    double es, qs, gam;
+    double Ti = thl * exsfc;
+    qsat3(Ti, psfc, es, qs, gam, tbl);
+    double rhi = qt / qs;
+    if (rhi <= 0.01) return psmin;
+    double TLCL = 55.0 + 1.0 / (1.0 / (Ti - 55.0) - log(rhi) / 2840.0);
+    double PiLCL = TLCL / thl;
+    double ps = c.p00 * pow(PiLCL, 1.0 / c.rovcp);
+#pragma unroll 1
+    for (int i = 1; i <= 10; i++) {
+        double Pis = pow(ps / c.p00, c.rovcp);
+        double Ts = thl * Pis;
+        qsat3(Ts, ps, es, qs, gam, tbl);
+        double err = qt - qs;
+        double nu = MX(MN((268.0 - Ts) / 20.0, 1.0), 0.0);
+        double leff = (1.0 - nu) * c.xlv + nu * c.xls;
+        double dlnqsdT = gam * (c.cp / leff) / qs;
+        double dTdPis = thl;
+        double dPisdps = c.rovcp * Pis / ps;
+        double dlnqsdps = -1.0 / (ps - (1.0 - c.ep2) * es);
+        double derrdps = -qs * (dlnqsdT * dTdPis * dPisdps + dlnqsdps);
+        double dps = -err / derrdps;
+        ps = ps + dps;
+        if (ps < 0.0) return psmin;
+        if (fabs(dps) <= dpsmax) return ps;
+    }
+    return psmin;
+}
+
+// compute_alpha (uwshcu.F90:4931-4950)
+__device__ double compute_alpha(double del_CIN, double ke)
+{
+    double x0 = 0.0;
+#pragma unroll 1
+    for (int it = 0; it < 10; it++) {
+        double x1 = x0 - (exp(-x0 * ke * del_CIN) - x0) / (-ke * del_CIN * exp(-x0 * ke * del_CIN) - 1.0);
+        x0 = x1;
+    }
+    return x0;
+}
+
+// compute_mumin2 (uwshcu.F90:4952-4979)
+__device__ double compute_mumin2(double mulcl, double rmaxfrac, double mulow)
+{
+    double x0 = mulow;
+#pragma unroll 1
+    for (int it = 0; it < 10; it++) {
+        double ex = exp(-(x0 * x0));
+        double ef = erfc(x0);
+        double exf = ex / ef;
+        double t1 = ex / 2.0 / rmaxfrac;
+        double t2 = mulcl * 2.5066 / 2.0;
+        double f = 0.5 * (exf * exf) - 0.5 * (t1 * t1) - (t2 * t2);
+        double fs = (2.0 * (exf * exf)) * (exf / sqrt(3.141592) - x0) + (0.5 * x0 * (ex * ex)) / (rmaxfrac * rmaxfrac);
+        double x1 = x0 - f / fs;
+        x0 = x1;
+    }
+    return x0;
+}
+
+// compute_ppen (uwshcu.F90:4981-5028); the 1.e-8 at :4998 is a default-real literal.
+__device__ double compute_ppen(double wtwb, double D, double bogbot, double bogtop, double rho0j, double dpen)
+{
+    double x0;
+    double SB = (bogtop - bogbot) / dpen;
+    double s00 = bogbot / rho0j - D * wtwb;
+    if (D * dpen < (double)1.e-8f) {
+        if (s00 >= 0.0) x0 = dpen;
+        else x0 = MX(0.0, MN(dpen, -0.5 * wtwb / s00));
+    } else {
+        if (s00 >= 0.0) x0 = dpen;
+        else x0 = 0.0;
+#pragma unroll 1
+        for (int it = 0; it < 5; it++) {
+            double f = exp(-2.0 * D * x0) * (wtwb - (bogbot - SB / (2.0 * D)) / (D * rho0j)) +
+                       (SB * x0 + bogbot - SB / (2.0 * D)) / (D * rho0j);
+            double fs = -2.0 * D * exp(-2.0 * D * x0) * (wtwb - (bogbot - SB / (2.0 * D)) / (D * rho0j)) +
+                        (SB) / (D * rho0j);
+            if (fs >= 0.0) fs = MX(fs, 1.e-10);
+            else fs = MN(fs, -1.e-10);
+            double x1 = x0 - f / fs;
+            x0 = x1;
+        }
+    }
+    return -MX(0.0, MN(dpen, x0));
+}
+
+// single_cin (uwshcu.F90:4704-4715) with the exner values of pbot/ptop supplied.
+__device__ __forceinline__ double single_cin(double pbot, double exb, double thv0bot, double ptop, double ext,
+                                             double thv0top, double thvubot, double thvutop)
+{
+    return ((1.0 - thvubot / thv0bot) + (1.0 - thvutop / thv0top)) * (pbot - ptop) /
+           (pbot / (c.r * thv0bot * exb) + ptop / (c.r * thv0top * ext));
+}
+
+// getbuoy (uwshcu.F90:4672-4702) with the exner values supplied.
+__device__ __forceinline__ void getbuoy(double pbot, double exb, double thv0bot, double ptop, double ext,
+                                        double thv0top, double thvubot, double thvutop, double& plfc, double& cin)
+{
+    if (thvubot > thv0bot && thvutop > thv0top) {
+        plfc = pbot;
+    } else if (thvubot <= thv0bot && thvutop <= thv0top) {
+        cin = cin - ((thvubot / thv0bot - 1.0) + (thvutop / thv0top - 1.0)) * (pbot - ptop) /
+                        (pbot / (c.r * thv0bot * exb) + ptop / (c.r * thv0top * ext));
+    } else if (thvubot > thv0bot && thvutop <= thv0top) {
+        double frc = (thvutop / thv0top - 1.0) / ((thvutop / thv0top - 1.0) - (thvubot / thv0bot - 1.0));
+        cin = cin - (thvutop / thv0top - 1.0) * ((ptop + frc * (pbot - ptop)) - ptop) /
+                        (pbot / (c.r * thv0bot * exb) + ptop / (c.r * thv0top * ext));
+    } else {
+        double frc = (thvubot / thv0bot - 1.0) / ((thvubot / thv0bot - 1.0) - (thvutop / thv0top - 1.0));
+        plfc = pbot - frc * (pbot - ptop);
+        cin = cin - (thvubot / thv0bot - 1.0) * (pbot - plfc) /
+                        (pbot / (c.r * thv0bot * exb) + ptop / (c.r * thv0top * ext));
+    }
+}
+
+// fluxbelowinv (uwshcu.F90:5030-5094).  Writes xflx(0:kinv-1); the Fortran zeroes xflx(kinv:mkx)
+// too, but the caller only reads 0..kinv-1.
+__device__ __forceinline__ void fluxbelowinv(double cbmf, const double* ps0, int kinv, double dt, double xsrc,
+                                             double xmean, double xtopin, double xbotin, double* xflx)
+{
+    double xtop, xbot;
+    double dp = ps0[kinv - 1] - ps0[kinv];
+    if (fabs(xbotin - xtopin) <= 1.e-13) {
+        xbot = xbotin - 1.e-13;
+        xtop = xtopin + 1.e-13;
+    } else {
+        xbot = xbotin;
+        xtop = xtopin;
+    }
+    double xtop_ori = xtop, xbot_ori = xbot;
+    double rcbmf = (cbmf * c.g * dt) / dp;
+    double rpeff = (xmean - xtop) / (xbot - xtop);
+    rpeff = MN(MX(0.0, rpeff), 1.0);
+    if (rpeff == 0.0 || rpeff == 1.0) {
+        xbot = xmean;
+        xtop = xmean;
+    }
+    double rr = rpeff / rcbmf;
+    double pinv = ps0[kinv - 1] - rpeff * dp;
+#pragma unroll 1
+    for (int k = 0; k <= kinv - 1; k++) xflx[k] = cbmf * (xsrc - xbot) * (ps0[0] - ps0[k]) / (ps0[0] - pinv);
+    if (rr <= 1.0) xflx[kinv - 1] = xflx[kinv - 1] - (1.0 - rr) * cbmf * (xtop_ori - xbot_ori);
+}
+
+// findsp (uwshcu.F90:5164-5454) for one point; returns the wet-bulb qsp and ORs error bits.
+__device__ double findsp_point(double q, double t, double p, unsigned int& errbits, const double* __restrict__ tbl)
+{
+    const double omeps = 1.0 - c.epsqs, trinv = 1.0 / c.ttrice, a1 = 7.5 * log(10.0), rair = 287.04;
+    const double c3 = rair * a1 / c.cpws, dttol = 1.e-4, dqtol = 1.e-4, tt0 = 273.15;
+    double dtt = 0.0, dq = 0.0, enin, enout = 1.0, tsp, qsp, hltalt = 0.0;
+    int doit = 0;
+    double tlim = MN(MX(t, 173.0), 373.0);
+    double es = estblf(tlim, tbl);
+    double denom = p - omeps * es;
+    double qs = c.epsqs * es / denom;
+    if (p > 5.0 * es && qs > 0.0 && qs < 0.5) {
+        qs = MN(c.epsqs * es / denom, 1.0);
+        double tc = tlim - tt0;
+        double weight = MN(-tc * trinv, 1.0);
+        double hlatsb = c.hlatv + weight * c.hlatf;
+        double hlatvp = c.hlatv - 2369.0 * tc;
+        hltalt = (tlim < tt0) ? hlatsb : hlatvp;
+        enin = c.cpws * tlim + hltalt * q;
+        double tmp = q - qs;
+        double c1 = hltalt * c3;
+        double c2 = (tlim + 36.0) * (tlim + 36.0);
+        double r1b = c2 / (c2 + c1 * qs);
+        double qvd = r1b * tmp;
+        tsp = tlim + ((hltalt / c.cpws) * qvd);
+        es = estblf(tsp, tbl);
+        qsp = MN(c.epsqs * es / (p - omeps * es), 1.0);
+    } else {
+        doit = 1;
+        tsp = tlim;
+        qsp = q;
+        enin = 1.0;
+    }
+#pragma unroll 1
+    for (int l = 1; l <= 8 && doit == 0; l++) {
+        es = estblf(tsp, tbl);
+        qs = MN(c.epsqs * es / (p - omeps * es), 1.0);
+        double tc = tsp - tt0;
+        bool lflg = (tc >= -c.ttrice && tc < 0.0);
+        double weight = MN(-tc * trinv, 1.0);
+        double hlatsb = c.hlatv + weight * c.hlatf;
+        double hlatvp = c.hlatv - 2369.0 * tc;
+        hltalt = (tsp < tt0) ? hlatsb : hlatvp;
+        double tterm = lflg ? c.pcf[0] + tc * (c.pcf[1] + tc * (c.pcf[2] + tc * (c.pcf[3] + tc * c.pcf[4]))) : 0.0;
+        double desdt = hltalt * es / (c.rgasv * tsp * tsp) + tterm * trinv;
+        double dqsdt = (c.epsqs + omeps * qs) / (p - omeps * es) * desdt;
+        double gg = enin - (c.cpws * tsp + hltalt * qsp);
+        double dgdt = -(c.cpws + hltalt * dqsdt);
+        double t1 = tsp - gg / dgdt;
+        dtt = fabs(t1 - tsp) / t1;
+        tsp = MX(t1, c.tmin);
+        es = estblf(tsp, tbl);
+        double q1 = MN(c.epsqs * es / (p - omeps * es), 1.0);
+        dq = fabs(q1 - qsp) / MX(q1, 1.e-12);
+        qsp = q1;
+        if (dtt < dttol && dq < dqtol) doit = 2;
+        enout = c.cpws * tsp + hltalt * qsp;
+        if (tsp < 174.16) doit = 4;
+    }
+    if (doit == 0 && (dtt > dttol || dq > dqtol)) errbits |= UW_ERRBIT_FINDSP;
+    if (doit == 2 && fabs((enin - enout) / (enin + enout)) > 1.e-4) errbits |= UW_ERRBIT_ENTHALPY;
+    return qsp;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------------
+// The column kernel.  KP bounds the level arrays (mkx + 1 <= KP), NC the tracer count.
+template <int KP, int NC>
+__global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A)
+{
+    __shared__ double tbl[UW_TBL];
+    for (int t = threadIdx.x; t < UW_TBL; t += blockDim.x) tbl[t] = c_estbl[t];
+    __syncthreads();
+
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.iend) return;
+
+    const int mix = A.mix, mkx = A.mkx, ncnst = A.ncnst;
+    const double dt = A.dt;
+    const double xlv = c.xlv, xls = c.xls, cp = c.cp, zvir = c.zvir, r = c.r, g = c.g, p00 = c.p00,
+                 rovcp = c.rovcp, rpen = c.rpen;
+    const double rle = 0.1, rkm = 14.0, rkfre = 1.0, rmaxfrac = 0.10, mumin1 = 0.906, rbuoy = 1.0,
+                 rdrag = 1.0, epsvarw = 5.e-4, PGFc = 0.7, criqc = 0.7e-3, frc_rasn = 1.0, kevp = 2.e-6;
+    const int ixnumliq = c.ixnumliq, ixnumice = c.ixnumice;
+
+    // Row of level k in the caller's arrays: bottom-up (compute_uwshcu) or CAM's top-down order
+    // (compute_uwshcu_inv, uwshcu.F90:380-469, where interface k and layer k both sit at row mkx-k).
+    const int inv = A.inv;
+#define RI(k) (inv ? (mkx - (k)) : (k))
+#define RL(k) (inv ? (mkx - (k)) : ((k) - 1))
+#define GI(a, k) __ldg(&A.a[(size_t)RI(k) * mix + i])
+#define GL(a, k) __ldg(&A.a[(size_t)RL(k) * mix + i])
+#define GT(m, k) __ldg(&A.tr0[((size_t)((m) - 1) * mkx + RL(k)) * mix + i])
+#define OI(a, k) A.a[(size_t)RI(k) * mix + i]
+#define OL(a, k) A.a[(size_t)RL(k) * mix + i]
+#define OT(m, k) A.trten[((size_t)((m) - 1) * mkx + RL(k)) * mix + i]
+#define CNT(x) (inv ? (double)(mkx + 1) - (x) : (x))
+
+    // ---- thread-private profiles ---------------------------------------------------------------
+    double ps0[KP], p0[KP], dp0[KP], zs0[KP], exn0[KP], exns0[KP];
+    double qv0[KP], ql0[KP], qi0[KP], t0[KP], s0[KP], qt0[KP], thl0[KP];
+    double ssthl0[KP], ssqt0[KP], ssu0[KP], ssv0[KP], sstr0[NC][KP];
+    double thv0bot[KP], thv0top[KP], thvl0bot[KP], thvl0top[KP];
+    double thv0bot_o[KP], thv0top_o[KP], thvl0bot_o[KP], thvl0top_o[KP];
+    double umf[KP], emf[KP], thlu[KP], qtu[KP], uu[KP], vu[KP], thvu[KP], wu[KP], ufrc[KP], rei[KP];
+    double fer[KP], fdr[KP], dwten[KP], diten[KP], tru[NC][KP];
+    double thlu_emf[KP], qtu_emf[KP], uu_emf[KP], vu_emf[KP], tru_emf[NC][KP];
+    double slflx[KP], qtflx[KP], uflx[KP], vflx[KP], trflx[NC][KP], xflx[KP];
+    double qlten_sink[KP], qiten_sink[KP], nlten_sink[KP], niten_sink[KP];
+    double uten[KP], vten[KP], uf[KP], vf[KP], qrten[KP], qsten[KP], slten[KP], qtten[KP];
+    double qlten[KP], qiten[KP], qvten[KP], sten[KP], qc[KP], qc_l[KP], qc_i[KP], evapc[KP];
+    double flxrain[KP], flxsnow[KP], cufrc[KP], qcu[KP], qlu[KP], qiu[KP], trten[NC][KP];
+    double qw0[KP], trflx_d[KP], trflx_u[KP];
+    double trsrc[NC], tre[NC];
+
+    unsigned int errbits = 0;
+    int xflags = 0, lflags = 0;
+    bool id_exit = false;
+    int kinv = 0, klcl = 0, klfc = 0, krel = 0, kbup = 0, kpen = 0;
+    int kinv_s = 0, klcl_s = 0, klfc_s = 0, krel_s = 0, kbup_s = 0, kpen_s = 0;
+    double cin = 0, cinlcl = 0, plcl = 0, plfc = 0, prel = 0, exlcl = 1.0, exprel = 1.0, tkeavg = 0,
+           thvlmin = 0, qtsrc = 0, thlsrc = 0, thvlsrc = 0, usrc = 0, vsrc = 0, thv0lcl = 0, thv0rel = 0;
+    double cin_i = 0, cinlcl_i = 0, ke = 0, kinv_o_d = 0;
+    int kinv_o = 0, klcl_o = 0, klfc_o = 0;
+    double plcl_o = 0, plfc_o = 0, tkeavg_o = 0, thvlmin_o = 0, qtsrc_o = 0, thvlsrc_o = 0, thlsrc_o = 0,
+           usrc_o = 0, vsrc_o = 0, thv0lcl_o = 0, trsrc_o[NC];
+    double cin_s = -1.0, cinlcl_s = -1.0, plcl_s = 0, plfc_s = 0, pinv_s = 0, pbup_s = 0, ppen_s = 0,
+           tkeavg_s = 0;
+    double cbmf = 0, wlcl = 0, ufrclcl = 0, ppen = 0, precip = 0, snow = 0, rliq = 0, cush, cnt, cnb;
+    double thlu_top = 0, qtu_top = 0, exntop = 1.0, drage = 0, bogbot = 0, bogtop = 0, rho0j = 0,
+           wtwb = 0, wtw = 0, xs1 = 0, xs2 = 0, xc1 = 0, xc2 = 0;
+    double thj, qvj, qlj, qij;
+    double rainflx = 0, snowflx = 0;
+    (void)kinv_o_d;
+
+    // ---- output initialisation (uwshcu.F90:1087-1124) ------------------------------------------
+    for (int k = 0; k <= mkx; k++) {
+        OI(umf, k) = 0.0;
+        OI(slflx, k) = 0.0;
+        OI(qtflx, k) = 0.0;
+        OI(flxprc1, k) = 0.0;
+        OI(flxsnow1, k) = 0.0;
+        OI(wu, k) = 0.0;
+    }
+    for (int k = 1; k <= mkx; k++) {
+        OL(qvten, k) = 0.0; OL(qlten, k) = 0.0; OL(qiten, k) = 0.0; OL(sten, k) = 0.0;
+        OL(uten, k) = 0.0; OL(vten, k) = 0.0; OL(qrten, k) = 0.0; OL(qsten, k) = 0.0;
+        OL(evapc, k) = 0.0; OL(cufrc, k) = 0.0; OL(qcu, k) = 0.0; OL(qlu, k) = 0.0;
+        OL(qiu, k) = 0.0; OL(qc, k) = 0.0;
+        for (int m = 1; m <= ncnst; m++) OT(m, k) = 0.0;
+    }
+    A.precip[i] = 0.0;
+    A.snow[i] = 0.0;
+    A.cbmf[i] = 0.0;
+    A.rliq[i] = 0.0;
+    A.cnt[i] = CNT((double)mkx);
+    A.cnb[i] = CNT(0.0);
+
+    // ---- inputs and findsp (uwshcu.F90:1216-1259) ----------------------------------------------
+    for (int k = 0; k <= mkx; k++) {
+        ps0[k] = GI(ps0, k);
+        zs0[k] = GI(zs0, k);
+        exns0[k] = pow(ps0[k] / p00, rovcp);
+    }
+    for (int k = 1; k <= mkx; k++) {
+        p0[k] = GL(p0, k);
+        dp0[k] = GL(dp0, k);
+        qv0[k] = GL(qv0, k);
+        ql0[k] = GL(ql0, k);
+        qi0[k] = GL(qi0, k);
+        t0[k] = GL(t0, k);
+        s0[k] = GL(s0, k);
+        exn0[k] = pow(p0[k] / p00, rovcp);
+        qt0[k] = (qv0[k] + ql0[k] + qi0[k]);
+        thl0[k] = (t0[k] - xlv * ql0[k] / cp - xls * qi0[k] / cp) / exn0[k];
+        qw0[k] = findsp_point(qv0[k], t0[k], p0[k], errbits, tbl);
+    }
+    const double pblh = __ldg(&A.pblh[i]);
+    cush = A.cush[i];
+    {
+        double tmpf[KP];
+        slope<KP>(mkx, thl0, p0, ssthl0);
+        slope<KP>(mkx, qt0, p0, ssqt0);
+        for (int k = 1; k <= mkx; k++) tmpf[k] = GL(u0, k);
+        slope<KP>(mkx, tmpf, p0, ssu0);
+        for (int k = 1; k <= mkx; k++) tmpf[k] = GL(v0, k);
+        slope<KP>(mkx, tmpf, p0, ssv0);
+        for (int m = 1; m <= ncnst; m++) {
+            for (int k = 1; k <= mkx; k++) tmpf[k] = GT(m, k);
+            slope<KP>(mkx, tmpf, p0, sstr0[m - 1]);
+        }
+    }
+    // thv0 at layer bottom/top (:1275-1299)
+    for (int k = 1; k <= mkx; k++) {
+        double thl0bot = thl0[k] + ssthl0[k] * (ps0[k - 1] - p0[k]);
+        double qt0bot = qt0[k] + ssqt0[k] * (ps0[k - 1] - p0[k]);
+        if (conden(ps0[k - 1], exns0[k - 1], thl0bot, qt0bot, thj, qvj, qlj, qij, tbl)) {
+            xflags |= UW_X_CONDEN;
+            id_exit = true;
+            goto l333;
+        }
+        thv0bot[k] = thj * (1.0 + zvir * qvj - qlj - qij);
+        thvl0bot[k] = thl0bot * (1.0 + zvir * qt0bot);
+        double thl0top = thl0[k] + ssthl0[k] * (ps0[k] - p0[k]);
+        double qt0top = qt0[k] + ssqt0[k] * (ps0[k] - p0[k]);
+        if (conden(ps0[k], exns0[k], thl0top, qt0top, thj, qvj, qlj, qij, tbl)) {
+            xflags |= UW_X_CONDEN;
+            id_exit = true;
+            goto l333;
+        }
+        thv0top[k] = thj * (1.0 + zvir * qvj - qlj - qij);
+        thvl0top[k] = thl0top * (1.0 + zvir * qt0top);
+        thv0bot_o[k] = thv0bot[k];
+        thv0top_o[k] = thv0top[k];
+        thvl0bot_o[k] = thvl0bot[k];
+        thvl0top_o[k] = thvl0top[k];
+    }
+    // per-column initialisation (:1333-1408)
+    for (int k = 0; k <= mkx; k++) {
+        umf[k] = 0.0; emf[k] = 0.0; slflx[k] = 0.0; qtflx[k] = 0.0; uflx[k] = 0.0; vflx[k] = 0.0;
+        ufrc[k] = 0.0; thlu[k] = 0.0; qtu[k] = 0.0; uu[k] = 0.0; vu[k] = 0.0; wu[k] = 0.0;
+        thvu[k] = 0.0; thlu_emf[k] = 0.0; qtu_emf[k] = 0.0; uu_emf[k] = 0.0; vu_emf[k] = 0.0;
+        for (int m = 0; m < ncnst; m++) {
+            trflx[m][k] = 0.0;
+            tru[m][k] = 0.0;
+            tru_emf[m][k] = 0.0;
+        }
+    }
+    for (int k = 1; k <= mkx; k++) {
+        qvten[k] = 0.0; qlten[k] = 0.0; qiten[k] = 0.0; sten[k] = 0.0; uten[k] = 0.0; vten[k] = 0.0;
+        qrten[k] = 0.0; qsten[k] = 0.0; dwten[k] = 0.0; diten[k] = 0.0; evapc[k] = 0.0;
+        cufrc[k] = 0.0; qcu[k] = 0.0; qlu[k] = 0.0; qiu[k] = 0.0; fer[k] = 0.0; fdr[k] = 0.0;
+        qc[k] = 0.0; qc_l[k] = 0.0; qc_i[k] = 0.0; qtten[k] = 0.0; slten[k] = 0.0;
+        qlten_sink[k] = 0.0; qiten_sink[k] = 0.0; nlten_sink[k] = 0.0; niten_sink[k] = 0.0;
+        rei[k] = 0.0; uf[k] = 0.0; vf[k] = 0.0;
+        for (int m = 0; m < ncnst; m++) trten[m][k] = 0.0;
+    }
+    cnt = (double)mkx;
+    cnb = 0.0;
+
+    // ---- implicit-CIN loop (uwshcu.F90:1421-4331) --------------------------------------------
+    for (int iter = 1; iter <= 2; iter++) {
+        double tscaleh = cush;
+        cush = -1.0;
+
+        // kinv (:1455-1468)
+        kinv = 1;
+        for (int k = mkx - 1; k >= 1; k--) {
+            if ((pblh + 5.0 - zs0[k]) * (pblh + 5.0 - zs0[k + 1]) < 0.0) {
+                kinv = k + 1;
+                break;
+            }
+        }
+        if (kinv <= 1) {
+            xflags |= UW_X_KINV1;
+            id_exit = true;
+            goto l333;
+        }
+        // tkeavg, thvlmin (:1484-1499)
+        {
+            double dpsum = 0.0;
+            tkeavg = 0.0;
+            thvlmin = 1000.0;
+            for (int k = 0; k <= kinv - 1; k++) {
+                double dpi;
+                if (k == 0) dpi = ps0[0] - p0[1];
+                else if (k == (kinv - 1)) dpi = p0[kinv - 1] - ps0[kinv - 1];
+                else dpi = p0[k] - p0[k + 1];
+                dpsum = dpsum + dpi;
+                tkeavg = tkeavg + dpi * GI(tke, k);
+                if (k != 0) thvlmin = MN(thvlmin, MN(thvl0bot[k], thvl0top[k]));
+            }
+            tkeavg = tkeavg / dpsum;
+        }
+        // source air (:1509-1516)
+        qtsrc = qt0[1];
+        thvlsrc = thvlmin;
+        thlsrc = thvlsrc / (1.0 + zvir * qtsrc);
+        usrc = GL(u0, kinv - 1) + ssu0[kinv - 1] * (ps0[kinv - 1] - p0[kinv - 1]);
+        vsrc = GL(v0, kinv - 1) + ssv0[kinv - 1] * (ps0[kinv - 1] - p0[kinv - 1]);
+        for (int m = 1; m <= ncnst; m++) trsrc[m - 1] = GT(m, 1);
+        // LCL (:1533-1549)
+        plcl = qsinvert(qtsrc, thlsrc, ps0[0], exns0[0], tbl);
+        klcl = mkx;
+        for (int k = 0; k <= mkx; k++) {
+            if (ps0[k] < plcl) {
+                klcl = k;
+                break;
+            }
+        }
+        klcl = MX(1, klcl);
+        if (plcl < 30000.0) {
+            xflags |= UW_X_KLCLMKX;
+            id_exit = true;
+            goto l333;
+        }
+        exlcl = exnf(plcl);
+        {
+            double thl0lcl = thl0[klcl] + ssthl0[klcl] * (plcl - p0[klcl]);
+            double qt0lcl = qt0[klcl] + ssqt0[klcl] * (plcl - p0[klcl]);
+            if (conden(plcl, exlcl, thl0lcl, qt0lcl, thj, qvj, qlj, qij, tbl)) {
+                xflags |= UW_X_CONDEN;
+                id_exit = true;
+                goto l333;
+            }
+            thv0lcl = thj * (1.0 + zvir * qvj - qlj - qij);
+        }
+        // CIN (:1592-1685)
+        cin = 0.0;
+        cinlcl = 0.0;
+        plfc = 0.0;
+        klfc = mkx;
+        {
+            double thvubot, thvutop = 0.0;
+            if (klcl >= kinv) {
+                for (int k = kinv; k <= mkx - 1; k++) {
+                    if (k < klcl) {
+                        thvubot = thvlsrc;
+                        thvutop = thvlsrc;
+                        cin = cin + single_cin(ps0[k - 1], exns0[k - 1], thv0bot[k], ps0[k], exns0[k], thv0top[k], thvubot, thvutop);
+                    } else if (k == klcl) {
+                        thvubot = thvlsrc;
+                        thvutop = thvlsrc;
+                        cin = cin + single_cin(ps0[k - 1], exns0[k - 1], thv0bot[k], plcl, exlcl, thv0lcl, thvubot, thvutop);
+                        if (cin < 0.0) lflags |= UW_L_CINLCL;
+                        cinlcl = MX(cin, 0.0);
+                        cin = cinlcl;
+                        thvubot = thvlsrc;
+                        if (conden(ps0[k], exns0[k], thlsrc, qtsrc, thj, qvj, qlj, qij, tbl)) {
+                            xflags |= UW_X_CONDEN;
+                            id_exit = true;
+                            goto l333;
+                        }
+                        thvutop = thj * (1.0 + zvir * qvj - qlj - qij);
+                        getbuoy(plcl, exlcl, thv0lcl, ps0[k], exns0[k], thv0top[k], thvubot, thvutop, plfc, cin);
+                        if (plfc > 0.0) {
+                            klfc = k;
+                            break;
+                        }
+                    } else {
+                        thvubot = thvutop;
+                        if (conden(ps0[k], exns0[k], thlsrc, qtsrc, thj, qvj, qlj, qij, tbl)) {
+                            xflags |= UW_X_CONDEN;
+                            id_exit = true;
+                            goto l333;
+                        }
+                        thvutop = thj * (1.0 + zvir * qvj - qlj - qij);
+                        getbuoy(ps0[k - 1], exns0[k - 1], thv0bot[k], ps0[k], exns0[k], thv0top[k], thvubot, thvutop, plfc, cin);
+                        if (plfc > 0.0) {
+                            klfc = k;
+                            break;
+                        }
+                    }
+                }
+            } else {
+                cinlcl = 0.0;
+                for (int k = kinv; k <= mkx - 1; k++) {
+                    if (conden(ps0[k - 1], exns0[k - 1], thlsrc, qtsrc, thj, qvj, qlj, qij, tbl)) {
+                        xflags |= UW_X_CONDEN;
+                        id_exit = true;
+                        goto l333;
+                    }
+                    thvubot = thj * (1.0 + zvir * qvj - qlj - qij);
+                    if (conden(ps0[k], exns0[k], thlsrc, qtsrc, thj, qvj, qlj, qij, tbl)) {
+                        xflags |= UW_X_CONDEN;
+                        id_exit = true;
+                        goto l333;
+                    }
+                    thvutop = thj * (1.0 + zvir * qvj - qlj - qij);
+                    getbuoy(ps0[k - 1], exns0[k - 1], thv0bot[k], ps0[k], exns0[k], thv0top[k], thvubot, thvutop, plfc, cin);
+                    if (plfc > 0.0) {
+                        klfc = k;
+                        break;
+                    }
+                }
+            }
+        }
+        // (label 35, :1676-1685)
+        if (cin < 0.0) lflags |= UW_L_CIN;
+        cin = MX(0.0, cin);
+        if (klfc >= mkx) {
+            klfc = mkx;
+            xflags |= UW_X_KLFCMKX;
+            id_exit = true;
+            goto l333;
+        }
+        if (iter == 1) {
+            cin_i = cin;
+            cinlcl_i = cinlcl;
+            ke = rbuoy / (rkfre * tkeavg + epsvarw);
+            kinv_o = kinv; klcl_o = klcl; klfc_o = klfc; plcl_o = plcl; plfc_o = plfc;
+            tkeavg_o = tkeavg; thvlmin_o = thvlmin; qtsrc_o = qtsrc; thvlsrc_o = thvlsrc;
+            thlsrc_o = thlsrc; usrc_o = usrc; vsrc_o = vsrc; thv0lcl_o = thv0lcl;
+            for (int m = 0; m < ncnst; m++) trsrc_o[m] = trsrc[m];
+        } else {
+            double del_CIN = cin - cin_i;
+            if (del_CIN > 0.0) {
+                // implicit CIN: restore the iteration-1 state (:1759-1889)
+                double alpha = compute_alpha(del_CIN, ke);
+                cin = cin_i + alpha * del_CIN;
+                cinlcl = cinlcl_i;
+                kinv = kinv_o; klcl = klcl_o; klfc = klfc_o; plcl = plcl_o; plfc = plfc_o;
+                tkeavg = tkeavg_o; thvlmin = thvlmin_o; qtsrc = qtsrc_o; thvlsrc = thvlsrc_o;
+                thlsrc = thlsrc_o; usrc = usrc_o; vsrc = vsrc_o; thv0lcl = thv0lcl_o;
+                for (int m = 0; m < ncnst; m++) trsrc[m] = trsrc_o[m];
+                exlcl = exnf(plcl);
+                for (int k = 1; k <= mkx; k++) {
+                    qv0[k] = GL(qv0, k);
+                    ql0[k] = GL(ql0, k);
+                    qi0[k] = GL(qi0, k);
+                    t0[k] = GL(t0, k);
+                    s0[k] = GL(s0, k);
+                    qt0[k] = (qv0[k] + ql0[k] + qi0[k]);
+                    thl0[k] = (t0[k] - xlv * ql0[k] / cp - xls * qi0[k] / cp) / exn0[k];
+                    thv0bot[k] = thv0bot_o[k];
+                    thv0top[k] = thv0top_o[k];
+                    thvl0bot[k] = thvl0bot_o[k];
+                    thvl0top[k] = thvl0top_o[k];
+                }
+                slope<KP>(mkx, thl0, p0, ssthl0);
+                slope<KP>(mkx, qt0, p0, ssqt0);
+                for (int k = 0; k <= mkx; k++) {
+                    umf[k] = 0.0; emf[k] = 0.0; slflx[k] = 0.0; qtflx[k] = 0.0; uflx[k] = 0.0;
+                    vflx[k] = 0.0; ufrc[k] = 0.0; thlu[k] = 0.0; qtu[k] = 0.0; uu[k] = 0.0;
+                    vu[k] = 0.0; wu[k] = 0.0; thvu[k] = 0.0; thlu_emf[k] = 0.0; qtu_emf[k] = 0.0;
+                    uu_emf[k] = 0.0; vu_emf[k] = 0.0;
+                    for (int m = 0; m < ncnst; m++) {
+                        trflx[m][k] = 0.0;
+                        tru[m][k] = 0.0;
+                        tru_emf[m][k] = 0.0;
+                    }
+                }
+                for (int k = 1; k <= mkx; k++) {
+                    qvten[k] = 0.0; qlten[k] = 0.0; qiten[k] = 0.0; sten[k] = 0.0; uten[k] = 0.0;
+                    vten[k] = 0.0; qrten[k] = 0.0; qsten[k] = 0.0; dwten[k] = 0.0; diten[k] = 0.0;
+                    evapc[k] = 0.0; cufrc[k] = 0.0; qcu[k] = 0.0; qlu[k] = 0.0; qiu[k] = 0.0;
+                    fer[k] = 0.0; fdr[k] = 0.0; qc[k] = 0.0; qc_l[k] = 0.0; qc_i[k] = 0.0;
+                    qtten[k] = 0.0; slten[k] = 0.0;
+                    for (int m = 0; m < ncnst; m++) trten[m][k] = 0.0;
+                }
+                precip = 0.0; snow = 0.0; rliq = 0.0; cbmf = 0.0;
+                cnt = (double)mkx; cnb = 0.0; ufrclcl = 0.0; wlcl = 0.0;
+            } else {
+                // explicit CIN: the iteration-1 outputs already sit in the output slots (:1891-2011);
+                // flxprc1/flxsnow1 keep their initial zeros on this path, wu_out gets wu.
+                lflags |= UW_L_DELCIN;
+                for (int k = 0; k <= mkx; k++) OI(wu, k) = wu[k];
+                if (A.diag_real) {
+                    A.diag_real[UW_DR_CIN * (size_t)mix + i] = cin_s;
+                    A.diag_real[UW_DR_CINLCL * (size_t)mix + i] = cinlcl_s;
+                    A.diag_real[UW_DR_PLCL * (size_t)mix + i] = plcl_s;
+                    A.diag_real[UW_DR_PLFC * (size_t)mix + i] = plfc_s;
+                    A.diag_real[UW_DR_PINV * (size_t)mix + i] = pinv_s;
+                    A.diag_real[UW_DR_PBUP * (size_t)mix + i] = pbup_s;
+                    A.diag_real[UW_DR_PPEN * (size_t)mix + i] = ppen_s;
+                    A.diag_real[UW_DR_TKEAVG * (size_t)mix + i] = tkeavg_s;
+                }
+                kinv = kinv_s; klcl = klcl_s; klfc = klfc_s; krel = krel_s; kbup = kbup_s; kpen = kpen_s;
+                id_exit = false;
+                goto l333;
+            }
+        }
+
+        // ---- release level and closure (:2035-2184) ------------------------------------------
+        if (klcl < kinv) {
+            krel = kinv;
+            prel = ps0[krel - 1];
+            exprel = exns0[krel - 1];
+            thv0rel = thv0bot[krel];
+        } else {
+            krel = klcl;
+            prel = plcl;
+            exprel = exlcl;
+            thv0rel = thv0lcl;
+        }
+        {
+            double wcrit = sqrt(2.0 * cin * rbuoy);
+            double sigmaw = sqrt(rkfre * tkeavg + epsvarw);
+            double mu = wcrit / sigmaw / 1.4142;
+            if (mu >= 3.0) {
+                id_exit = true;
+                goto l333;
+            }
+            double rho0inv = ps0[kinv - 1] / (r * thv0top[kinv - 1] * exns0[kinv - 1]);
+            cbmf = (rho0inv * sigmaw / 2.5066) * exp(-(mu * mu));
+            double cbmflimit = 0.9 * dp0[kinv - 1] / g / dt;
+            double mumin0 = 0.0;
+            if (cbmf > cbmflimit) mumin0 = sqrt(-log(2.5066 * cbmflimit / rho0inv / sigmaw));
+            mu = MX(MX(mu, mumin0), mumin1);
+            double mulcl = sqrt(2.0 * cinlcl * rbuoy) / 1.4142 / sigmaw;
+            double ta = exp(-(mu * mu)) / 2.5066, te = erfc(mu);
+            double mulclstar = sqrt(MX(0.0, 2.0 * (ta * ta) * (1.0 / (te * te) - 0.25 / (rmaxfrac * rmaxfrac))));
+            if (mulcl > 1.e-8 && mulcl > mulclstar) {
+                double mumin2 = compute_mumin2(mulcl, rmaxfrac, mu);
+                if (mu > mumin2) errbits |= UW_ERRBIT_MU;
+                mu = MX(mu, mumin2);
+                if (mu == mumin2) lflags |= UW_L_UFRC;
+            }
+            if (mu == mumin0) lflags |= UW_L_CBMF;
+            if (mu == mumin1) lflags |= UW_L_UFRC;
+            cbmf = (rho0inv * sigmaw / 2.5066) * exp(-(mu * mu));
+            double winv = sigmaw * (2.0 / 2.5066) * exp(-(mu * mu)) / erfc(mu);
+            wtw = winv * winv - 2.0 * cinlcl * rbuoy;
+            if (wtw <= 0.0) {
+                xflags |= UW_X_WTW;
+                id_exit = true;
+                goto l333;
+            }
+            wlcl = sqrt(wtw);
+            ufrclcl = cbmf / wlcl / rho0inv;
+            if (ufrclcl <= 0.0001) {
+                xflags |= UW_X_UFRC;
+                id_exit = true;
+                goto l333;
+            }
+            ufrc[krel - 1] = ufrclcl;
+            for (int k = kinv - 1; k <= krel - 1; k++) {
+                umf[k] = cbmf;
+                wu[k] = winv;
+            }
+        }
+        // updraft at the release level (:2205-2236)
+        emf[krel - 1] = 0.0;
+        umf[krel - 1] = cbmf;
+        wu[krel - 1] = wlcl;
+        thlu[krel - 1] = thlsrc;
+        qtu[krel - 1] = qtsrc;
+        if (conden(prel, exprel, thlsrc, qtsrc, thj, qvj, qlj, qij, tbl)) {
+            xflags |= UW_X_CONDEN;
+            id_exit = true;
+            goto l333;
+        }
+        thvu[krel - 1] = thj * (1.0 + zvir * qvj - qlj - qij);
+        {
+            double uplus = 0.0, vplus = 0.0;
+            if (krel == kinv) {
+                uplus = PGFc * ssu0[kinv] * (prel - ps0[kinv - 1]);
+                vplus = PGFc * ssv0[kinv] * (prel - ps0[kinv - 1]);
+            } else {
+                for (int k = kinv; k <= MX(krel - 1, kinv); k++) {
+                    uplus = uplus + PGFc * ssu0[k] * (ps0[k] - ps0[k - 1]);
+                    vplus = vplus + PGFc * ssv0[k] * (ps0[k] - ps0[k - 1]);
+                }
+                uplus = uplus + PGFc * ssu0[krel] * (prel - ps0[krel - 1]);
+                vplus = vplus + PGFc * ssv0[krel] * (prel - ps0[krel - 1]);
+            }
+            uu[krel - 1] = usrc + uplus;
+            vu[krel - 1] = vsrc + vplus;
+        }
+        for (int m = 0; m < ncnst; m++) tru[m][krel - 1] = trsrc[m];
+
+        {
+            double scaleh = tscaleh;
+            if (tscaleh < 0.0) scaleh = 1000.0;
+            // ---- buoyancy-sorting updraft, iter_scaleh loop (:2306-2952) ----------------------
+            for (int iter_scaleh = 1; iter_scaleh <= 3; iter_scaleh++) {
+                kbup = krel;
+                kpen = krel;
+                wtw = wlcl * wlcl;
+                double pe = 0.5 * (prel + ps0[krel]);
+                double dpe = prel - ps0[krel];
+                double exne = exnf(pe);
+                double thvebot = thv0rel;
+                double thle = thl0[krel] + ssthl0[krel] * (pe - p0[krel]);
+                double qte = qt0[krel] + ssqt0[krel] * (pe - p0[krel]);
+                double ue = GL(u0, krel) + ssu0[krel] * (pe - p0[krel]);
+                double ve = GL(v0, krel) + ssv0[krel] * (pe - p0[krel]);
+                for (int m = 0; m < ncnst; m++) tre[m] = GT(m + 1, krel) + sstr0[m][krel] * (pe - p0[krel]);
+
+                for (int k = krel; k <= mkx - 1; k++) {
+                    const int km1 = k - 1;
+                    double thlue = thlu[km1];
+                    double qtue = qtu[km1];
+                    double wue = wu[km1];
+                    wtwb = wtw;
+                    for (int iter_xc = 1; iter_xc <= 2; iter_xc++) {
+                        wtw = wu[km1] * wu[km1];
+                        if (conden(pe, exne, thle, qte, thj, qvj, qlj, qij, tbl)) {
+                            xflags |= UW_X_CONDEN;
+                            id_exit = true;
+                            goto l333;
+                        }
+                        double thv0j = thj * (1.0 + zvir * qvj - qlj - qij);
+                        rho0j = pe / (r * thv0j * exne);
+                        double excess0 = qte - qsat_qs(thle * exne, pe, tbl);
+                        if (conden(pe, exne, thlue, qtue, thj, qvj, qlj, qij, tbl)) {
+                            xflags |= UW_X_CONDEN;
+                            id_exit = true;
+                            goto l333;
+                        }
+                        if ((qlj + qij) > criqc) {
+                            double exql = ((qlj + qij) - criqc) * qlj / (qlj + qij);
+                            double exqi = ((qlj + qij) - criqc) * qij / (qlj + qij);
+                            qtue = qtue - exql - exqi;
+                            thlue = thlue + (xlv / cp / exne) * exql + (xls / cp / exne) * exqi;
+                        }
+                        if (conden(pe, exne, thlue, qtue, thj, qvj, qlj, qij, tbl)) {
+                            xflags |= UW_X_CONDEN;
+                            id_exit = true;
+                            goto l333;
+                        }
+                        double thvj = thj * (1.0 + zvir * qvj - qlj - qij);
+                        double excessu = qtue - qsat_qs(thlue * exne, pe, tbl);
+                        double cridis = rle * scaleh;
+                        double xc;
+                        if ((excessu <= 0.0 && excess0 <= 0.0) || (excessu >= 0.0 && excess0 >= 0.0)) {
+                            xc = MN(1.0, MX(0.0, 1.0 - 2.0 * rbuoy * g * cridis / (wue * wue) * (1.0 - thvj / thv0j)));
+                        } else {
+                            double xsat = excessu / (excessu - excess0);
+                            double thlxsat = thlue + xsat * (thle - thlue);
+                            double qtxsat = qtue + xsat * (qte - qtue);
+                            if (conden(pe, exne, thlxsat, qtxsat, thj, qvj, qlj, qij, tbl)) {
+                                xflags |= UW_X_CONDEN;
+                                id_exit = true;
+                                goto l333;
+                            }
+                            double thvxsat = thj * (1.0 + zvir * qvj - qlj - qij);
+                            double x_cu = 0.0, x_en = 0.0;
+                            for (int kk = 1; kk <= 2; kk++) {
+                                double thv_x0, thv_x1;
+                                if (kk == 1) {
+                                    thv_x0 = thvj;
+                                    thv_x1 = (1.0 - 1.0 / xsat) * thvj + (1.0 / xsat) * thvxsat;
+                                } else {
+                                    thv_x1 = thv0j;
+                                    thv_x0 = (xsat / (xsat - 1.0)) * thv0j + (1.0 / (1.0 - xsat)) * thvxsat;
+                                }
+                                double aquad = wue * wue;
+                                double bquad = 2.0 * rbuoy * g * cridis * (thv_x1 - thv_x0) / thv0j - 2.0 * (wue * wue);
+                                double cquad = 2.0 * rbuoy * g * cridis * (thv_x0 - thv0j) / thv0j + (wue * wue);
+                                if (kk == 1) {
+                                    if ((bquad * bquad - 4.0 * aquad * cquad) >= 0.0) {
+                                        roots(aquad, bquad, cquad, xs1, xs2);
+                                        x_cu = MN(1.0, MX(0.0, MN(xsat, MN(xs1, xs2))));
+                                    } else {
+                                        x_cu = xsat;
+                                    }
+                                } else {
+                                    if ((bquad * bquad - 4.0 * aquad * cquad) >= 0.0) {
+                                        roots(aquad, bquad, cquad, xs1, xs2);
+                                        x_en = MN(1.0, MX(0.0, MX(xsat, MN(xs1, xs2))));
+                                    } else {
+                                        x_en = 1.0;
+                                    }
+                                }
+                            }
+                            if (x_cu == xsat) xc = MX(x_cu, x_en);
+                            else xc = x_cu;
+                        }
+                        double ee2 = xc * xc;
+                        double ud2 = 1.0 - 2.0 * xc + xc * xc;
+                        rei[k] = (0.5 * rkm / GL(z0, k) / g / rho0j);
+                        if (xc > 0.5) rei[k] = MN(rei[k], 0.9 * log(dp0[k] / g / dt / umf[km1] + 1.0) / dpe / (2.0 * xc - 1.0));
+                        fer[k] = rei[k] * ee2;
+                        fdr[k] = rei[k] * ud2;
+                        umf[k] = umf[km1] * exp(dpe * (fer[k] - fdr[k]));
+                        emf[k] = 0.0;
+                        if (fer[k] * dpe < 1.e-4) {
+                            thlu[k] = thlu[km1] + (thle + ssthl0[k] * dpe / 2.0 - thlu[km1]) * fer[k] * dpe;
+                            qtu[k] = qtu[km1] + (qte + ssqt0[k] * dpe / 2.0 - qtu[km1]) * fer[k] * dpe;
+                            uu[k] = uu[km1] + (ue + ssu0[k] * dpe / 2.0 - uu[km1]) * fer[k] * dpe - PGFc * ssu0[k] * dpe;
+                            vu[k] = vu[km1] + (ve + ssv0[k] * dpe / 2.0 - vu[km1]) * fer[k] * dpe - PGFc * ssv0[k] * dpe;
+                            for (int m = 0; m < ncnst; m++)
+                                tru[m][k] = tru[m][km1] + (tre[m] + sstr0[m][k] * dpe / 2.0 - tru[m][km1]) * fer[k] * dpe;
+                        } else {
+                            const double ef = exp(-fer[k] * dpe);
+                            thlu[k] = (thle + ssthl0[k] / fer[k] - ssthl0[k] * dpe / 2.0) -
+                                      (thle + ssthl0[k] * dpe / 2.0 - thlu[km1] + ssthl0[k] / fer[k]) * ef;
+                            qtu[k] = (qte + ssqt0[k] / fer[k] - ssqt0[k] * dpe / 2.0) -
+                                     (qte + ssqt0[k] * dpe / 2.0 - qtu[km1] + ssqt0[k] / fer[k]) * ef;
+                            uu[k] = (ue + (1.0 - PGFc) * ssu0[k] / fer[k] - ssu0[k] * dpe / 2.0) -
+                                    (ue + ssu0[k] * dpe / 2.0 - uu[km1] + (1.0 - PGFc) * ssu0[k] / fer[k]) * ef;
+                            vu[k] = (ve + (1.0 - PGFc) * ssv0[k] / fer[k] - ssv0[k] * dpe / 2.0) -
+                                    (ve + ssv0[k] * dpe / 2.0 - vu[km1] + (1.0 - PGFc) * ssv0[k] / fer[k]) * ef;
+                            for (int m = 0; m < ncnst; m++)
+                                tru[m][k] = (tre[m] + sstr0[m][k] / fer[k] - sstr0[m][k] * dpe / 2.0) -
+                                            (tre[m] + sstr0[m][k] * dpe / 2.0 - tru[m][km1] + sstr0[m][k] / fer[k]) * ef;
+                        }
+                        if (conden(ps0[k], exns0[k], thlu[k], qtu[k], thj, qvj, qlj, qij, tbl)) {
+                            xflags |= UW_X_CONDEN;
+                            id_exit = true;
+                            goto l333;
+                        }
+                        if ((qlj + qij) > criqc) {
+                            double exql = ((qlj + qij) - criqc) * qlj / (qlj + qij);
+                            double exqi = ((qlj + qij) - criqc) * qij / (qlj + qij);
+                            qtu[k] = qtu[k] - exql - exqi;
+                            thlu[k] = thlu[k] + (xlv / cp / exns0[k]) * exql + (xls / cp / exns0[k]) * exqi;
+                            dwten[k] = exql;
+                            diten[k] = exqi;
+                        } else {
+                            dwten[k] = 0.0;
+                            diten[k] = 0.0;
+                        }
+                        if (conden(ps0[k], exns0[k], thlu[k], qtu[k], thj, qvj, qlj, qij, tbl)) {
+                            xflags |= UW_X_CONDEN;
+                            id_exit = true;
+                            goto l333;
+                        }
+                        thvu[k] = thj * (1.0 + zvir * qvj - qlj - qij);
+                        bogbot = rbuoy * (thvu[km1] / thvebot - 1.0);
+                        bogtop = rbuoy * (thvu[k] / thv0top[k] - 1.0);
+                        double delbog = bogtop - bogbot;
+                        drage = fer[k] * (1.0 + rdrag);
+                        double expfac = exp(-2.0 * drage * dpe);
+                        wtwb = wtw;
+                        if (drage * dpe > 1.e-3)
+                            wtw = wtw * expfac + (delbog + (1.0 - expfac) * (bogbot + delbog / (-2.0 * drage * dpe))) / (rho0j * drage);
+                        else
+                            wtw = wtw + dpe * (bogbot + bogtop) / rho0j;
+                        if (wtw > 0.0) {
+                            thlue = 0.5 * (thlu[km1] + thlu[k]);
+                            qtue = 0.5 * (qtu[km1] + qtu[k]);
+                            wue = 0.5 * sqrt(MX(wtwb + wtw, 0.0));
+                        } else {
+                            break;   // go to 111
+                        }
+                    }
+                    // (label 111, :2726-2793)
+                    if (umf[k] == 0.0) wtw = -1.0;
+                    if (bogtop > 0.0 && wtw > 0.0) kbup = k;
+                    if (wtw <= 0.0) {
+                        kpen = k;
+                        break;   // go to 45
+                    }
+                    wu[k] = sqrt(wtw);
+                    if (wu[k] > 100.0) {
+                        xflags |= UW_X_WU;
+                        id_exit = true;
+                        goto l333;
+                    }
+                    {
+                        double rhos0j = ps0[k] / (r * 0.5 * (thv0bot[k + 1] + thv0top[k]) * exns0[k]);
+                        ufrc[k] = umf[k] / (rhos0j * wu[k]);
+                        if (ufrc[k] > rmaxfrac) {
+                            lflags |= UW_L_UFRC;
+                            ufrc[k] = rmaxfrac;
+                            umf[k] = rmaxfrac * rhos0j * wu[k];
+                            fdr[k] = fer[k] - log(umf[k] / umf[km1]) / dpe;
+                        }
+                    }
+                    pe = p0[k + 1];
+                    dpe = dp0[k + 1];
+                    exne = exn0[k + 1];
+                    thvebot = thv0bot[k + 1];
+                    thle = thl0[k + 1];
+                    qte = qt0[k + 1];
+                    ue = GL(u0, k + 1);
+                    ve = GL(v0, k + 1);
+                    for (int m = 0; m < ncnst; m++) tre[m] = GT(m + 1, k + 1);
+                }
+                // (label 45) penetration depth (:2884-2907)
+                if (drage == 0.0) {
+                    double aquad = (bogtop - bogbot) / (ps0[kpen] - ps0[kpen - 1]);
+                    double bquad = 2.0 * bogbot;
+                    double cquad = -(wu[kpen - 1] * wu[kpen - 1]) * rho0j;
+                    int status = roots(aquad, bquad, cquad, xc1, xc2);
+                    if (status == 0) {
+                        if (xc1 <= 0.0 && xc2 <= 0.0) {
+                            ppen = MX(xc1, xc2);
+                            ppen = MN(0.0, MX(-dp0[kpen], ppen));
+                        } else if (xc1 > 0.0 && xc2 > 0.0) {
+                            ppen = -dp0[kpen];
+                        } else {
+                            ppen = MN(xc1, xc2);
+                            ppen = MN(0.0, MX(-dp0[kpen], ppen));
+                        }
+                    } else {
+                        ppen = -dp0[kpen];
+                    }
+                } else {
+                    ppen = compute_ppen(wtwb, drage, bogbot, bogtop, rho0j, dp0[kpen]);
+                }
+                if (ppen == -dp0[kpen] || ppen == 0.0) lflags |= UW_L_PPEN;
+                // condensate at the cumulus top (:2917-2942)
+                if (fer[kpen] * (-ppen) < 1.e-4) {
+                    thlu_top = thlu[kpen - 1] + (thl0[kpen] + ssthl0[kpen] * (-ppen) / 2.0 - thlu[kpen - 1]) * fer[kpen] * (-ppen);
+                    qtu_top = qtu[kpen - 1] + (qt0[kpen] + ssqt0[kpen] * (-ppen) / 2.0 - qtu[kpen - 1]) * fer[kpen] * (-ppen);
+                } else {
+                    const double ef = exp(-fer[kpen] * (-ppen));
+                    thlu_top = (thl0[kpen] + ssthl0[kpen] / fer[kpen] - ssthl0[kpen] * (-ppen) / 2.0) -
+                               (thl0[kpen] + ssthl0[kpen] * (-ppen) / 2.0 - thlu[kpen - 1] + ssthl0[kpen] / fer[kpen]) * ef;
+                    qtu_top = (qt0[kpen] + ssqt0[kpen] / fer[kpen] - ssqt0[kpen] * (-ppen) / 2.0) -
+                              (qt0[kpen] + ssqt0[kpen] * (-ppen) / 2.0 - qtu[kpen - 1] + ssqt0[kpen] / fer[kpen]) * ef;
+                }
+                exntop = pow((ps0[kpen - 1] + ppen) / p00, rovcp);
+                if (conden(ps0[kpen - 1] + ppen, exntop, thlu_top, qtu_top, thj, qvj, qlj, qij, tbl)) {
+                    xflags |= UW_X_CONDEN;
+                    id_exit = true;
+                    goto l333;
+                }
+                if ((qlj + qij) > criqc) {
+                    dwten[kpen] = ((qlj + qij) - criqc) * qlj / (qlj + qij);
+                    diten[kpen] = ((qlj + qij) - criqc) * qij / (qlj + qij);
+                    qtu_top = qtu_top - dwten[kpen] - diten[kpen];
+                    thlu_top = thlu_top + (xlv / cp / exntop) * dwten[kpen] + (xls / cp / exntop) * diten[kpen];
+                } else {
+                    dwten[kpen] = 0.0;
+                    diten[kpen] = 0.0;
+                }
+                {
+                    double rhos0j = ps0[kpen - 1] / (r * 0.5 * (thv0bot[kpen] + thv0top[kpen - 1]) * exns0[kpen - 1]);
+                    cush = zs0[kpen - 1] - ppen / rhos0j / g;
+                }
+                scaleh = cush;
+            }
+        }
+        // forcedCu filter (:2964-2992)
+        if (kbup == krel) {
+            lflags |= UW_L_SHCU;
+            xflags |= UW_X_CUFILTER;
+            id_exit = true;
+            goto l333;
+        }
+        lflags &= ~UW_L_SHCU;
+        for (int k = kpen; k <= mkx; k++) {
+            umf[k] = 0.0;
+            emf[k] = 0.0;
+            ufrc[k] = 0.0;
+        }
+        for (int k = kpen + 1; k <= mkx; k++) {
+            dwten[k] = 0.0;
+            diten[k] = 0.0;
+            fer[k] = 0.0;
+            fdr[k] = 0.0;
+        }
+        // penetrative entrainment (:3055-3183)
+        for (int k = 0; k <= mkx; k++) {
+            thlu_emf[k] = thlu[k];
+            qtu_emf[k] = qtu[k];
+            uu_emf[k] = uu[k];
+            vu_emf[k] = vu[k];
+            for (int m = 0; m < ncnst; m++) tru_emf[m][k] = tru[m][k];
+        }
+        for (int k = kpen - 1; k >= kbup; k--) {
+            double rhos0j = ps0[k] / (r * 0.5 * (thv0bot[k + 1] + thv0top[k]) * exns0[k]);
+            if (k == kpen - 1) {
+                if ((umf[k] * ppen * rei[kpen] * rpen) < -0.1 * rhos0j) lflags |= UW_L_EMF;
+                if ((umf[k] * ppen * rei[kpen] * rpen) < -0.9 * dp0[kpen] / g / dt) lflags |= UW_L_EMF;
+                emf[k] = MX(MX(umf[k] * ppen * rei[kpen] * rpen, -0.1 * rhos0j), -0.9 * dp0[kpen] / g / dt);
+                thlu_emf[k] = thl0[kpen] + ssthl0[kpen] * (ps0[k] - p0[kpen]);
+                qtu_emf[k] = qt0[kpen] + ssqt0[kpen] * (ps0[k] - p0[kpen]);
+                uu_emf[k] = GL(u0, kpen) + ssu0[kpen] * (ps0[k] - p0[kpen]);
+                vu_emf[k] = GL(v0, kpen) + ssv0[kpen] * (ps0[k] - p0[kpen]);
+                for (int m = 0; m < ncnst; m++) tru_emf[m][k] = GT(m + 1, kpen) + sstr0[m][kpen] * (ps0[k] - p0[kpen]);
+            } else {
+                if ((emf[k + 1] - umf[k] * dp0[k + 1] * rei[k + 1] * rpen) < -0.1 * rhos0j) lflags |= UW_L_EMF;
+                if ((emf[k + 1] - umf[k] * dp0[k + 1] * rei[k + 1] * rpen) < -0.9 * dp0[k + 1] / g / dt) lflags |= UW_L_EMF;
+                emf[k] = MX(MX(emf[k + 1] - umf[k] * dp0[k + 1] * rei[k + 1] * rpen, -0.1 * rhos0j), -0.9 * dp0[k + 1] / g / dt);
+                if (fabs(emf[k]) > fabs(emf[k + 1])) {
+                    thlu_emf[k] = (thlu_emf[k + 1] * emf[k + 1] + thl0[k + 1] * (emf[k] - emf[k + 1])) / emf[k];
+                    qtu_emf[k] = (qtu_emf[k + 1] * emf[k + 1] + qt0[k + 1] * (emf[k] - emf[k + 1])) / emf[k];
+                    uu_emf[k] = (uu_emf[k + 1] * emf[k + 1] + GL(u0, k + 1) * (emf[k] - emf[k + 1])) / emf[k];
+                    vu_emf[k] = (vu_emf[k + 1] * emf[k + 1] + GL(v0, k + 1) * (emf[k] - emf[k + 1])) / emf[k];
+                    for (int m = 0; m < ncnst; m++)
+                        tru_emf[m][k] = (tru_emf[m][k + 1] * emf[k + 1] + GT(m + 1, k + 1) * (emf[k] - emf[k + 1])) / emf[k];
+                } else {
+                    thlu_emf[k] = thl0[k + 1];
+                    qtu_emf[k] = qt0[k + 1];
+                    uu_emf[k] = GL(u0, k + 1);
+                    vu_emf[k] = GL(v0, k + 1);
+                    for (int m = 0; m < ncnst; m++) tru_emf[m][k] = GT(m + 1, k + 1);
+                }
+            }
+        }
+        // 1. PBL fluxes (:3255-3290)
+        {
+            double xsrc = qtsrc, xmean = qt0[kinv];
+            double xtop = qt0[kinv + 1] + ssqt0[kinv + 1] * (ps0[kinv] - p0[kinv + 1]);
+            double xbot = qt0[kinv - 1] + ssqt0[kinv - 1] * (ps0[kinv - 1] - p0[kinv - 1]);
+            fluxbelowinv(cbmf, ps0, kinv, dt, xsrc, xmean, xtop, xbot, xflx);
+            for (int k = 0; k <= kinv - 1; k++) qtflx[k] = xflx[k];
+            xsrc = thlsrc;
+            xmean = thl0[kinv];
+            xtop = thl0[kinv + 1] + ssthl0[kinv + 1] * (ps0[kinv] - p0[kinv + 1]);
+            xbot = thl0[kinv - 1] + ssthl0[kinv - 1] * (ps0[kinv - 1] - p0[kinv - 1]);
+            fluxbelowinv(cbmf, ps0, kinv, dt, xsrc, xmean, xtop, xbot, xflx);
+            for (int k = 0; k <= kinv - 1; k++) slflx[k] = cp * exns0[k] * xflx[k];
+            xsrc = usrc;
+            xmean = GL(u0, kinv);
+            xtop = GL(u0, kinv + 1) + ssu0[kinv + 1] * (ps0[kinv] - p0[kinv + 1]);
+            xbot = GL(u0, kinv - 1) + ssu0[kinv - 1] * (ps0[kinv - 1] - p0[kinv - 1]);
+            fluxbelowinv(cbmf, ps0, kinv, dt, xsrc, xmean, xtop, xbot, xflx);
+            for (int k = 0; k <= kinv - 1; k++) uflx[k] = xflx[k];
+            xsrc = vsrc;
+            xmean = GL(v0, kinv);
+            xtop = GL(v0, kinv + 1) + ssv0[kinv + 1] * (ps0[kinv] - p0[kinv + 1]);
+            xbot = GL(v0, kinv - 1) + ssv0[kinv - 1] * (ps0[kinv - 1] - p0[kinv - 1]);
+            fluxbelowinv(cbmf, ps0, kinv, dt, xsrc, xmean, xtop, xbot, xflx);
+            for (int k = 0; k <= kinv - 1; k++) vflx[k] = xflx[k];
+            for (int m = 0; m < ncnst; m++) {
+                xsrc = trsrc[m];
+                xmean = GT(m + 1, kinv);
+                xtop = GT(m + 1, kinv + 1) + sstr0[m][kinv + 1] * (ps0[kinv] - p0[kinv + 1]);
+                xbot = GT(m + 1, kinv - 1) + sstr0[m][kinv - 1] * (ps0[kinv - 1] - p0[kinv - 1]);
+                fluxbelowinv(cbmf, ps0, kinv, dt, xsrc, xmean, xtop, xbot, xflx);
+                for (int k = 0; k <= kinv - 1; k++) trflx[m][k] = xflx[k];
+            }
+        }
+        // 2. non-buoyancy-sorting fluxes (:3300-3313)
+        {
+            double uplus = 0.0, vplus = 0.0;
+            for (int k = kinv; k <= krel - 1; k++) {
+                const int kp1 = k + 1;
+                qtflx[k] = cbmf * (qtsrc - (qt0[kp1] + ssqt0[kp1] * (ps0[k] - p0[kp1])));
+                slflx[k] = cbmf * (thlsrc - (thl0[kp1] + ssthl0[kp1] * (ps0[k] - p0[kp1]))) * cp * exns0[k];
+                uplus = uplus + PGFc * ssu0[k] * (ps0[k] - ps0[k - 1]);
+                vplus = vplus + PGFc * ssv0[k] * (ps0[k] - ps0[k - 1]);
+                uflx[k] = cbmf * (usrc + uplus - (GL(u0, kp1) + ssu0[kp1] * (ps0[k] - p0[kp1])));
+                vflx[k] = cbmf * (vsrc + vplus - (GL(v0, kp1) + ssv0[kp1] * (ps0[k] - p0[kp1])));
+                for (int m = 0; m < ncnst; m++)
+                    trflx[m][k] = cbmf * (trsrc[m] - (GT(m + 1, kp1) + sstr0[m][kp1] * (ps0[k] - p0[kp1])));
+            }
+        }
+        // 3. buoyancy-sorting fluxes (:3322-3331)
+        for (int k = krel; k <= kbup - 1; k++) {
+            const int kp1 = k + 1;
+            slflx[k] = cp * exns0[k] * umf[k] * (thlu[k] - (thl0[kp1] + ssthl0[kp1] * (ps0[k] - p0[kp1])));
+            qtflx[k] = umf[k] * (qtu[k] - (qt0[kp1] + ssqt0[kp1] * (ps0[k] - p0[kp1])));
+            uflx[k] = umf[k] * (uu[k] - (GL(u0, kp1) + ssu0[kp1] * (ps0[k] - p0[kp1])));
+            vflx[k] = umf[k] * (vu[k] - (GL(v0, kp1) + ssv0[kp1] * (ps0[k] - p0[kp1])));
+            for (int m = 0; m < ncnst; m++)
+                trflx[m][k] = umf[k] * (tru[m][k] - (GT(m + 1, kp1) + sstr0[m][kp1] * (ps0[k] - p0[kp1])));
+        }
+        // 4. penetrative-entrainment fluxes (:3392-3401)
+        for (int k = kbup; k <= kpen - 1; k++) {
+            slflx[k] = cp * exns0[k] * emf[k] * (thlu_emf[k] - (thl0[k] + ssthl0[k] * (ps0[k] - p0[k])));
+            qtflx[k] = emf[k] * (qtu_emf[k] - (qt0[k] + ssqt0[k] * (ps0[k] - p0[k])));
+            uflx[k] = emf[k] * (uu_emf[k] - (GL(u0, k) + ssu0[k] * (ps0[k] - p0[k])));
+            vflx[k] = emf[k] * (vu_emf[k] - (GL(v0, k) + ssv0[k] * (ps0[k] - p0[k])));
+            for (int m = 0; m < ncnst; m++)
+                trflx[m][k] = emf[k] * (tru_emf[m][k] - (GT(m + 1, k) + sstr0[m][k] * (ps0[k] - p0[k])));
+        }
+        // condensate tendency by compensating subsidence (:3416-3476)
+        {
+            // uemf(k), evaluated on demand with the same expressions as :3416-3422
+#define UEMF(kk)                                                                                          \
+    ((kk) <= kinv - 2 ? cbmf * (ps0[0] - ps0[(kk)]) / (ps0[0] - ps0[kinv - 1])                             \
+                      : ((kk) <= krel - 1 ? cbmf : ((kk) <= kbup - 1 ? umf[(kk)] : ((kk) <= kpen - 1 ? emf[(kk)] : 0.0))))
+            for (int k = 1; k <= kpen; k++) {
+                double comsub = 0.5 * (UEMF(k) + UEMF(k - 1));
+                double thlten_sub, qtten_sub, qlten_sub, qiten_sub, nlten_sub, niten_sub;
+                if (comsub >= 0.0) {
+                    if (k == mkx) {
+                        thlten_sub = 0.0; qtten_sub = 0.0; qlten_sub = 0.0; qiten_sub = 0.0;
+                        nlten_sub = 0.0; niten_sub = 0.0;
+                    } else {
+                        thlten_sub = g * comsub * (thl0[k + 1] - thl0[k]) / (p0[k] - p0[k + 1]);
+                        qtten_sub = g * comsub * (qt0[k + 1] - qt0[k]) / (p0[k] - p0[k + 1]);
+                        qlten_sub = g * comsub * (ql0[k + 1] - ql0[k]) / (p0[k] - p0[k + 1]);
+                        qiten_sub = g * comsub * (qi0[k + 1] - qi0[k]) / (p0[k] - p0[k + 1]);
+                        nlten_sub = g * comsub * (GT(ixnumliq, k + 1) - GT(ixnumliq, k)) / (p0[k] - p0[k + 1]);
+                        niten_sub = g * comsub * (GT(ixnumice, k + 1) - GT(ixnumice, k)) / (p0[k] - p0[k + 1]);
+                    }
+                } else {
+                    if (k == 1) {
+                        thlten_sub = 0.0; qtten_sub = 0.0; qlten_sub = 0.0; qiten_sub = 0.0;
+                        nlten_sub = 0.0; niten_sub = 0.0;
+                    } else {
+                        thlten_sub = g * comsub * (thl0[k] - thl0[k - 1]) / (p0[k - 1] - p0[k]);
+                        qtten_sub = g * comsub * (qt0[k] - qt0[k - 1]) / (p0[k - 1] - p0[k]);
+                        qlten_sub = g * comsub * (ql0[k] - ql0[k - 1]) / (p0[k - 1] - p0[k]);
+                        qiten_sub = g * comsub * (qi0[k] - qi0[k - 1]) / (p0[k - 1] - p0[k]);
+                        nlten_sub = g * comsub * (GT(ixnumliq, k) - GT(ixnumliq, k - 1)) / (p0[k - 1] - p0[k]);
+                        niten_sub = g * comsub * (GT(ixnumice, k) - GT(ixnumice, k - 1)) / (p0[k - 1] - p0[k]);
+                    }
+                }
+                double thl_prog = thl0[k] + thlten_sub * dt;
+                double qt_prog = MX(qt0[k] + qtten_sub * dt, 1.e-12);
+                if (conden(p0[k], exn0[k], thl_prog, qt_prog, thj, qvj, qlj, qij, tbl)) {
+                    id_exit = true;
+                    goto l333;
+                }
+                qlten_sink[k] = MX(qlten_sub, -ql0[k] / dt);
+                qiten_sink[k] = MX(qiten_sub, -qi0[k] / dt);
+                nlten_sink[k] = MX(nlten_sub, -GT(ixnumliq, k) / dt);
+                niten_sink[k] = MX(niten_sub, -GT(ixnumice, k) / dt);
+            }
+#undef UEMF
+        }
+        // momentum tendency (:3488-3501)
+        for (int k = 1; k <= kpen; k++) {
+            uten[k] = (uflx[k - 1] - uflx[k]) * g / dp0[k];
+            vten[k] = (vflx[k - 1] - vflx[k]) * g / dp0[k];
+            uf[k] = GL(u0, k) + uten[k] * dt;
+            vf[k] = GL(v0, k) + vten[k] * dt;
+        }
+        // thermodynamic tendencies (:3511-3791)
+        rliq = 0.0;
+        rainflx = 0.0;
+        snowflx = 0.0;
+        {
+            double qlubelow = 0.0, qiubelow = 0.0;
+            for (int k = 1; k <= kpen; k++) {
+                const int km1 = k - 1;
+                dwten[k] = dwten[k] * 0.5 * (umf[k - 1] + umf[k]) * g / dp0[k];
+                diten[k] = diten[k] * 0.5 * (umf[k - 1] + umf[k]) * g / dp0[k];
+                qrten[k] = frc_rasn * dwten[k];
+                qsten[k] = frc_rasn * diten[k];
+                rainflx = rainflx + qrten[k] * dp0[k] / g;
+                snowflx = snowflx + qsten[k] * dp0[k] / g;
+                slten[k] = (slflx[km1] - slflx[k]) * g / dp0[k];
+                if (k == 1) {
+                    const double u1 = GL(u0, k), u2 = GL(u0, k + 1), v1 = GL(v0, k), v2 = GL(v0, k + 1);
+                    slten[k] = slten[k] - g / 4.0 / dp0[k] *
+                                              (uflx[k] * (uf[k + 1] - uf[k] + u2 - u1) +
+                                               vflx[k] * (vf[k + 1] - vf[k] + v2 - v1));
+                } else if (k >= 2 && k <= kpen - 1) {
+                    const double um = GL(u0, k - 1), u1 = GL(u0, k), u2 = GL(u0, k + 1);
+                    const double vm = GL(v0, k - 1), v1 = GL(v0, k), v2 = GL(v0, k + 1);
+                    slten[k] = slten[k] - g / 4.0 / dp0[k] *
+                                              (uflx[k] * (uf[k + 1] - uf[k] + u2 - u1) +
+                                               uflx[k - 1] * (uf[k] - uf[k - 1] + u1 - um) +
+                                               vflx[k] * (vf[k + 1] - vf[k] + v2 - v1) +
+                                               vflx[k - 1] * (vf[k] - vf[k - 1] + v1 - vm));
+                } else if (k == kpen) {
+                    const double um = GL(u0, k - 1), u1 = GL(u0, k), vm = GL(v0, k - 1), v1 = GL(v0, k);
+                    slten[k] = slten[k] - g / 4.0 / dp0[k] *
+                                              (uflx[k - 1] * (uf[k] - uf[k - 1] + u1 - um) +
+                                               vflx[k - 1] * (vf[k] - vf[k - 1] + v1 - vm));
+                }
+                qtten[k] = (qtflx[km1] - qtflx[k]) * g / dp0[k];
+
+                double qlu_mid, qiu_mid;
+                if (k < krel || k > kpen) {
+                    qlu_mid = 0.0;
+                    qiu_mid = 0.0;
+                    qlj = 0.0;
+                    qij = 0.0;
+                } else if (k == krel) {
+                    if (conden(prel, exprel, thlu[krel - 1], qtu[krel - 1], thj, qvj, qlj, qij, tbl)) {
+                        xflags |= UW_X_CONDEN;
+                        id_exit = true;
+                        goto l333;
+                    }
+                    qlubelow = qlj;
+                    qiubelow = qij;
+                    if (conden(ps0[k], exns0[k], thlu[k], qtu[k], thj, qvj, qlj, qij, tbl)) {
+                        xflags |= UW_X_CONDEN;
+                        id_exit = true;
+                        goto l333;
+                    }
+                    qlu_mid = 0.5 * (qlubelow + qlj) * (prel - ps0[k]) / (ps0[k - 1] - ps0[k]);
+                    qiu_mid = 0.5 * (qiubelow + qij) * (prel - ps0[k]) / (ps0[k - 1] - ps0[k]);
+                } else if (k == kpen) {
+                    if (conden(ps0[k - 1] + ppen, exntop, thlu_top, qtu_top, thj, qvj, qlj, qij, tbl)) {
+                        xflags |= UW_X_CONDEN;
+                        id_exit = true;
+                        goto l333;
+                    }
+                    qlu_mid = 0.5 * (qlubelow + qlj) * (-ppen) / (ps0[k - 1] - ps0[k]);
+                    qiu_mid = 0.5 * (qiubelow + qij) * (-ppen) / (ps0[k - 1] - ps0[k]);
+                } else {
+                    if (conden(ps0[k], exns0[k], thlu[k], qtu[k], thj, qvj, qlj, qij, tbl)) {
+                        xflags |= UW_X_CONDEN;
+                        id_exit = true;
+                        goto l333;
+                    }
+                    qlu_mid = 0.5 * (qlubelow + qlj);
+                    qiu_mid = 0.5 * (qiubelow + qij);
+                }
+                qlubelow = qlj;
+                qiubelow = qij;
+
+                double qc_lm, qc_im, nc_lm, nc_im;
+                qc_l[k] = (1.0 - frc_rasn) * dwten[k];
+                qc_i[k] = (1.0 - frc_rasn) * diten[k];
+                const double trl = GT(ixnumliq, k), tri = GT(ixnumice, k);
+                if (k <= kbup) {
+                    qc_l[k] = qc_l[k] + g * 0.5 * (umf[k - 1] + umf[k]) * fdr[k] * qlu_mid;
+                    qc_i[k] = qc_i[k] + g * 0.5 * (umf[k - 1] + umf[k]) * fdr[k] * qiu_mid;
+                    qc_lm = -g * 0.5 * (umf[k - 1] + umf[k]) * fdr[k] * ql0[k];
+                    qc_im = -g * 0.5 * (umf[k - 1] + umf[k]) * fdr[k] * qi0[k];
+                    nc_lm = -g * 0.5 * (umf[k - 1] + umf[k]) * fdr[k] * trl;
+                    nc_im = -g * 0.5 * (umf[k - 1] + umf[k]) * fdr[k] * tri;
+                } else {
+                    qc_lm = 0.0;
+                    qc_im = 0.0;
+                    nc_lm = 0.0;
+                    nc_im = 0.0;
+                }
+                if (k == kbup) {
+                    qc_l[k] = qc_l[k] + g * umf[k] * qlj / (ps0[k - 1] - ps0[k]);
+                    qc_i[k] = qc_i[k] + g * umf[k] * qij / (ps0[k - 1] - ps0[k]);
+                    qc_lm = qc_lm - g * umf[k] * ql0[k] / (ps0[k - 1] - ps0[k]);
+                    qc_im = qc_im - g * umf[k] * qi0[k] / (ps0[k - 1] - ps0[k]);
+                    nc_lm = nc_lm - g * umf[k] * trl / (ps0[k - 1] - ps0[k]);
+                    nc_im = nc_im - g * umf[k] * tri / (ps0[k - 1] - ps0[k]);
+                    double ql_emf_kbup, qi_emf_kbup, thjj, qvjj;
+                    if (conden(p0[k], exn0[k], thlu_emf[k], qtu_emf[k], thjj, qvjj, ql_emf_kbup, qi_emf_kbup, tbl)) {
+                        id_exit = true;
+                        goto l333;
+                    }
+                    double nl_emf_kbup = (ql_emf_kbup > 0.0) ? tru_emf[ixnumliq - 1][k] : 0.0;
+                    double ni_emf_kbup = (qi_emf_kbup > 0.0) ? tru_emf[ixnumice - 1][k] : 0.0;
+                    qc_lm = qc_lm - g * emf[k] * (ql_emf_kbup - ql0[k]) / (ps0[k - 1] - ps0[k]);
+                    qc_im = qc_im - g * emf[k] * (qi_emf_kbup - qi0[k]) / (ps0[k - 1] - ps0[k]);
+                    nc_lm = nc_lm - g * emf[k] * (nl_emf_kbup - trl) / (ps0[k - 1] - ps0[k]);
+                    nc_im = nc_im - g * emf[k] * (ni_emf_kbup - tri) / (ps0[k - 1] - ps0[k]);
+                }
+                qlten[k] = qc_l[k] + frc_rasn * dwten[k] + (MX(0.0, ql0[k] + (qc_lm + qlten_sink[k]) * dt) - ql0[k]) / dt;
+                qiten[k] = qc_i[k] + frc_rasn * diten[k] + (MX(0.0, qi0[k] + (qc_im + qiten_sink[k]) * dt) - qi0[k]) / dt;
+                trten[ixnumliq - 1][k] = MX(nc_lm + nlten_sink[k], -trl / dt);
+                trten[ixnumice - 1][k] = MX(nc_im + niten_sink[k], -tri / dt);
+                qvten[k] = qtten[k] - qlten[k] - qiten[k];
+                sten[k] = slten[k] + xlv * qlten[k] + xls * qiten[k];
+                qc[k] = qc_l[k] + qc_i[k];
+                rliq = rliq + qc[k] * dp0[k] / g / 1000.0;
+            }
+        }
+        // evaporation and melting of precipitation (:3808-3934)
+        {
+            double evpint_rain = 0.0, evpint_snow = 0.0;
+            for (int k = 0; k <= mkx; k++) {
+                flxrain[k] = 0.0;
+                flxsnow[k] = 0.0;
+            }
+            for (int k = mkx; k >= 1; k--) {
+                double snowmlt;
+                if (t0[k] > 273.16) snowmlt = MX(0.0, flxsnow[k] * g / dp0[k]);
+                else snowmlt = 0.0;
+                double qs1 = qsat_qs(t0[k], p0[k], tbl);
+                double subsat = MX((1.0 - qv0[k] / qs1), 0.0);
+                double evprain = kevp * subsat * sqrt(flxrain[k] + snowmlt * dp0[k] / g);
+                double evpsnow = kevp * subsat * sqrt(MX(flxsnow[k] - snowmlt * dp0[k] / g, 0.0));
+                double evplimit = MX(0.0, (qw0[k] - qv0[k]) / dt);
+                double evplimit_rain = MN(evplimit, (flxrain[k] + snowmlt * dp0[k] / g) * g / dp0[k]);
+                evplimit_rain = MN(evplimit_rain, (rainflx - evpint_rain) * g / dp0[k]);
+                evprain = MX(0.0, MN(evplimit_rain, evprain));
+                double evplimit_snow = MN(evplimit, MX(flxsnow[k] - snowmlt * dp0[k] / g, 0.0) * g / dp0[k]);
+                evplimit_snow = MN(evplimit_snow, (snowflx - evpint_snow) * g / dp0[k]);
+                evpsnow = MX(0.0, MN(evplimit_snow, evpsnow));
+                if ((evprain + evpsnow) > evplimit) {
+                    double tmp1 = evprain * evplimit / (evprain + evpsnow);
+                    double tmp2 = evpsnow * evplimit / (evprain + evpsnow);
+                    evprain = tmp1;
+                    evpsnow = tmp2;
+                }
+                evapc[k] = evprain + evpsnow;
+                evpint_rain = evpint_rain + evprain * dp0[k] / g;
+                evpint_snow = evpint_snow + evpsnow * dp0[k] / g;
+                double ntraprd = qrten[k] - evprain + snowmlt;
+                double ntsnprd = qsten[k] - evpsnow - snowmlt;
+                flxrain[k - 1] = flxrain[k] + ntraprd * dp0[k] / g;
+                flxsnow[k - 1] = flxsnow[k] + ntsnprd * dp0[k] / g;
+                flxrain[k - 1] = MX(flxrain[k - 1], 0.0);
+                flxsnow[k - 1] = MX(flxsnow[k - 1], 0.0);
+                qlten[k] = qlten[k] - qrten[k];
+                qiten[k] = qiten[k] - qsten[k];
+                qvten[k] = qvten[k] + evprain + evpsnow;
+                qtten[k] = qlten[k] + qiten[k] + qvten[k];
+                if ((qv0[k] + qvten[k] * dt) < c.qmin[0] || (ql0[k] + qlten[k] * dt) < c.qmin[1] ||
+                    (qi0[k] + qiten[k] * dt) < c.qmin[2])
+                    lflags |= UW_L_NEGCON;
+                sten[k] = sten[k] - xlv * evprain - xls * evpsnow - (xls - xlv) * snowmlt;
+                slten[k] = sten[k] - xlv * qlten[k] - xls * qiten[k];
+            }
+            precip = (flxrain[0] + flxsnow[0]) / 1000.0;
+            snow = flxsnow[0] / 1000.0;
+        }
+        // remove detrained condensate (:3966-3981)
+        for (int k = 1; k <= kpen; k++) {
+            qtten[k] = qtten[k] - qc[k];
+            qlten[k] = qlten[k] - qc_l[k];
+            qiten[k] = qiten[k] - qc_i[k];
+            slten[k] = slten[k] + (xlv * qc_l[k] + xls * qc_i[k]);
+            sten[k] = sten[k] - (xls - xlv) * qc_i[k];
+        }
+        // positive_moisture_single (uwshcu.F90:5096-5162 via :3995-4001); state after the tendencies
+        {
+            const double qvmin = c.qmin[0], qlmin = c.qmin[1], qimin = c.qmin[2];
+            double qvs[KP];
+            for (int k = 1; k <= mkx; k++) qvs[k] = qv0[k] + qvten[k] * dt;
+            double dqv = 0.0;
+            for (int k = mkx; k >= 1; k--) {
+                double qlk = ql0[k] + qlten[k] * dt;
+                double qik = qi0[k] + qiten[k] * dt;
+                double dql = MX(0.0, 1.0 * qlmin - qlk);
+                double dqi = MX(0.0, 1.0 * qimin - qik);
+                qlten[k] = qlten[k] + dql / dt;
+                qiten[k] = qiten[k] + dqi / dt;
+                qvten[k] = qvten[k] - (dql + dqi) / dt;
+                sten[k] = sten[k] + xlv * (dql / dt) + xls * (dqi / dt);
+                qvs[k] = qvs[k] - dql - dqi;
+                dqv = MX(0.0, 1.0 * qvmin - qvs[k]);
+                qvten[k] = qvten[k] + dqv / dt;
+                qvs[k] = qvs[k] + dqv;
+                if (k != 1) {
+                    qvs[k - 1] = qvs[k - 1] - dqv * dp0[k] / dp0[k - 1];
+                    qvten[k - 1] = qvten[k - 1] - dqv * dp0[k] / dp0[k - 1] / dt;
+                }
+                qvs[k] = MX(qvs[k], qvmin);
+            }
+            if (dqv > 1.e-20) {
+                double sum = 0.0;
+                for (int k = 1; k <= mkx; k++)
+                    if (qvs[k] > 2.0 * qvmin) sum = sum + qvs[k] * dp0[k];
+                double aa = dqv * dp0[1] / MX(1.e-20, sum);
+                if (aa < 0.5) {
+                    for (int k = 1; k <= mkx; k++) {
+                        if (qvs[k] > 2.0 * qvmin) {
+                            double dum = aa * qvs[k];
+                            qvs[k] = qvs[k] - dum;
+                            qvten[k] = qvten[k] - dum / dt;
+                        }
+                    }
+                }
+            }
+        }
+        for (int k = 1; k <= mkx; k++) {
+            qtten[k] = qvten[k] + qlten[k] + qiten[k];
+            slten[k] = sten[k] - xlv * qlten[k] - xls * qiten[k];
+        }
+        // tracer tendencies (:4007-4076)
+        for (int m = 4; m <= ncnst; m++) {
+            if (m != ixnumliq && m != ixnumice) {
+                const double trmin = c.qmin[m - 1];
+                const bool wet = c.wet[m - 1] != 0;
+                for (int k = 0; k <= mkx; k++) {
+                    trflx_d[k] = 0.0;
+                    trflx_u[k] = 0.0;
+                }
+                for (int k = 1; k <= mkx - 1; k++) {
+                    double pdelx = wet ? dp0[k] : GL(dpdry0, k);
+                    double dum = (GT(m, k) - trmin) * pdelx / g / dt + trflx[m - 1][k - 1] - trflx[m - 1][k] + trflx_d[k - 1];
+                    trflx_d[k] = MN(0.0, dum);
+                }
+                for (int k = mkx; k >= 2; k--) {
+                    double pdelx = wet ? dp0[k] : GL(dpdry0, k);
+                    double dum = (GT(m, k) - trmin) * pdelx / g / dt + trflx[m - 1][k - 1] - trflx[m - 1][k] +
+                                 trflx_d[k - 1] - trflx_d[k] - trflx_u[k];
+                    trflx_u[k - 1] = MX(0.0, -dum);
+                }
+                for (int k = 1; k <= mkx; k++) {
+                    double pdelx = wet ? dp0[k] : GL(dpdry0, k);
+                    trten[m - 1][k] = (trflx[m - 1][k - 1] - trflx[m - 1][k] + trflx_d[k - 1] - trflx_d[k] +
+                                       trflx_u[k - 1] - trflx_u[k]) * g / pdelx;
+                }
+            }
+        }
+        // in-cloud diagnostics (:4092-4158)
+        if (conden(prel, exprel, thlu[krel - 1], qtu[krel - 1], thj, qvj, qlj, qij, tbl)) {
+            xflags |= UW_X_CONDEN;
+            id_exit = true;
+            goto l333;
+        }
+        {
+            double qcubelow = qlj + qij, qlubelow = qlj, qiubelow = qij;
+            for (int k = krel; k <= kpen; k++) {
+                int idc;
+                if (k == kpen) idc = conden(ps0[k - 1] + ppen, exntop, thlu_top, qtu_top, thj, qvj, qlj, qij, tbl);
+                else idc = conden(ps0[k], exns0[k], thlu[k], qtu[k], thj, qvj, qlj, qij, tbl);
+                if (idc) {
+                    xflags |= UW_X_CONDEN;
+                    id_exit = true;
+                    goto l333;
+                }
+                qcu[k] = 0.5 * (qcubelow + qlj + qij);
+                qlu[k] = 0.5 * (qlubelow + qlj);
+                qiu[k] = 0.5 * (qiubelow + qij);
+                cufrc[k] = (ufrc[k - 1] + ufrc[k]);
+                if (k == krel) {
+                    cufrc[k] = (ufrclcl + ufrc[k]) * (prel - ps0[k]) / (ps0[k - 1] - ps0[k]);
+                } else if (k == kpen) {
+                    cufrc[k] = (ufrc[k - 1] + 0.0) * (-ppen) / (ps0[k - 1] - ps0[k]);
+                    if ((qlj + qij) > criqc) {
+                        qcu[k] = 0.5 * (qcubelow + criqc);
+                        qlu[k] = 0.5 * (qlubelow + criqc * qlj / (qlj + qij));
+                        qiu[k] = 0.5 * (qiubelow + criqc * qij / (qlj + qij));
+                    }
+                }
+                qcubelow = qlj + qij;
+                qlubelow = qlj;
+                qiubelow = qij;
+            }
+        }
+        cnt = (double)kpen;
+        cnb = (double)(krel - 1);
+
+        if (iter == 1) {
+            // Save the iteration-1 outputs into the output slots (the Fortran *_s copies, :4177-4277)
+            for (int k = 0; k <= mkx; k++) {
+                OI(umf, k) = umf[k];
+                OI(slflx, k) = slflx[k];
+                OI(qtflx, k) = qtflx[k];
+            }
+            for (int k = 1; k <= mkx; k++) {
+                OL(qvten, k) = qvten[k]; OL(qlten, k) = qlten[k]; OL(qiten, k) = qiten[k];
+                OL(sten, k) = sten[k]; OL(uten, k) = uten[k]; OL(vten, k) = vten[k];
+                OL(qrten, k) = qrten[k]; OL(qsten, k) = qsten[k]; OL(evapc, k) = evapc[k];
+                OL(cufrc, k) = cufrc[k]; OL(qcu, k) = qcu[k]; OL(qlu, k) = qlu[k];
+                OL(qiu, k) = qiu[k]; OL(qc, k) = qc[k];
+                for (int m = 1; m <= ncnst; m++) OT(m, k) = trten[m - 1][k];
+            }
+            A.precip[i] = precip;
+            A.snow[i] = snow;
+            A.cush[i] = cush;
+            A.cbmf[i] = cbmf;
+            A.rliq[i] = rliq;
+            A.cnt[i] = CNT(cnt);
+            A.cnb[i] = CNT(cnb);
+            cin_s = cin; cinlcl_s = cinlcl; plcl_s = plcl; pinv_s = ps0[kinv - 1]; plfc_s = plfc;
+            pbup_s = ps0[kbup]; ppen_s = ps0[kpen - 1] + ppen; tkeavg_s = tkeavg;
+            kinv_s = kinv; klcl_s = klcl; klfc_s = klfc; krel_s = krel; kbup_s = kbup; kpen_s = kpen;
+            // advance the state for the second CIN estimate (:4177-4184, :4285-4327)
+            for (int k = 1; k <= mkx; k++) {
+                double qv0s = qv0[k] + qvten[k] * dt;
+                double ql0s = ql0[k] + qlten[k] * dt;
+                double qi0s = qi0[k] + qiten[k] * dt;
+                double s0s = s0[k] + sten[k] * dt;
+                double t0s = t0[k] + sten[k] * dt / cp;
+                qv0[k] = qv0s;
+                ql0[k] = ql0s;
+                qi0[k] = qi0s;
+                s0[k] = s0s;
+                t0[k] = t0s;
+                qt0[k] = (qv0[k] + ql0[k] + qi0[k]);
+                thl0[k] = (t0[k] - xlv * ql0[k] / cp - xls * qi0[k] / cp) / exn0[k];
+            }
+            slope<KP>(mkx, thl0, p0, ssthl0);
+            slope<KP>(mkx, qt0, p0, ssqt0);
+            for (int k = 1; k <= mkx; k++) {
+                double thl0bot = thl0[k] + ssthl0[k] * (ps0[k - 1] - p0[k]);
+                double qt0bot = qt0[k] + ssqt0[k] * (ps0[k - 1] - p0[k]);
+                if (conden(ps0[k - 1], exns0[k - 1], thl0bot, qt0bot, thj, qvj, qlj, qij, tbl)) {
+                    xflags |= UW_X_CONDEN;
+                    id_exit = true;
+                    goto l333;
+                }
+                thv0bot[k] = thj * (1.0 + zvir * qvj - qlj - qij);
+                thvl0bot[k] = thl0bot * (1.0 + zvir * qt0bot);
+                double thl0top = thl0[k] + ssthl0[k] * (ps0[k] - p0[k]);
+                double qt0top = qt0[k] + ssqt0[k] * (ps0[k] - p0[k]);
+                if (conden(ps0[k], exns0[k], thl0top, qt0top, thj, qvj, qlj, qij, tbl)) {
+                    xflags |= UW_X_CONDEN;
+                    id_exit = true;
+                    goto l333;
+                }
+                thv0top[k] = thj * (1.0 + zvir * qvj - qlj - qij);
+                thvl0top[k] = thl0top * (1.0 + zvir * qt0top);
+            }
+        }
+    }
+
+    // ---- final outputs (uwshcu.F90:4337-4370) --------------------------------------------------
+    for (int k = 0; k <= mkx; k++) {
+        OI(umf, k) = umf[k];
+        OI(wu, k) = wu[k];
+        OI(slflx, k) = slflx[k];
+        OI(qtflx, k) = qtflx[k];
+        OI(flxprc1, k) = flxrain[k] + flxsnow[k];
+        OI(flxsnow1, k) = flxsnow[k];
+    }
+    for (int k = 1; k <= mkx; k++) {
+        OL(qvten, k) = qvten[k]; OL(qlten, k) = qlten[k]; OL(qiten, k) = qiten[k];
+        OL(sten, k) = sten[k]; OL(uten, k) = uten[k]; OL(vten, k) = vten[k];
+        OL(qrten, k) = qrten[k]; OL(qsten, k) = qsten[k]; OL(evapc, k) = evapc[k];
+        OL(cufrc, k) = cufrc[k]; OL(qcu, k) = qcu[k]; OL(qlu, k) = qlu[k];
+        OL(qiu, k) = qiu[k]; OL(qc, k) = qc[k];
+        for (int m = 1; m <= ncnst; m++) OT(m, k) = trten[m - 1][k];
+    }
+    A.precip[i] = precip;
+    A.snow[i] = snow;
+    A.cush[i] = cush;
+    A.cbmf[i] = cbmf;
+    A.rliq[i] = rliq;
+    A.cnt[i] = CNT(cnt);
+    A.cnb[i] = CNT(cnb);
+    if (A.diag_real) {
+        A.diag_real[UW_DR_CIN * (size_t)mix + i] = cin;
+        A.diag_real[UW_DR_CINLCL * (size_t)mix + i] = cinlcl;
+        A.diag_real[UW_DR_PLCL * (size_t)mix + i] = plcl;
+        A.diag_real[UW_DR_PLFC * (size_t)mix + i] = plfc;
+        A.diag_real[UW_DR_PINV * (size_t)mix + i] = ps0[kinv - 1];
+        A.diag_real[UW_DR_PBUP * (size_t)mix + i] = ps0[kbup];
+        A.diag_real[UW_DR_PPEN * (size_t)mix + i] = ps0[kpen - 1] + ppen;
+        A.diag_real[UW_DR_TKEAVG * (size_t)mix + i] = tkeavg;
+    }
+
+l333:
+    if (id_exit) {
+        xflags |= UW_X_UWCU;
+        for (int k = 0; k <= mkx; k++) {
+            OI(umf, k) = 0.0;
+            OI(wu, k) = 0.0;
+            OI(slflx, k) = 0.0;
+            OI(qtflx, k) = 0.0;
+            OI(flxprc1, k) = 0.0;
+            OI(flxsnow1, k) = 0.0;
+        }
+        for (int k = 1; k <= mkx; k++) {
+            OL(qvten, k) = 0.0; OL(qlten, k) = 0.0; OL(qiten, k) = 0.0; OL(sten, k) = 0.0;
+            OL(uten, k) = 0.0; OL(vten, k) = 0.0; OL(qrten, k) = 0.0; OL(qsten, k) = 0.0;
+            OL(evapc, k) = 0.0; OL(cufrc, k) = 0.0; OL(qcu, k) = 0.0; OL(qlu, k) = 0.0;
+            OL(qiu, k) = 0.0; OL(qc, k) = 0.0;
+            for (int m = 1; m <= ncnst; m++) OT(m, k) = 0.0;
+        }
+        A.precip[i] = 0.0;
+        A.snow[i] = 0.0;
+        A.cush[i] = -1.0;
+        A.cbmf[i] = 0.0;
+        A.rliq[i] = 0.0;
+        A.cnt[i] = CNT(1.0);
+        A.cnb[i] = CNT((double)mkx);
+        if (A.diag_real) {
+            A.diag_real[UW_DR_CIN * (size_t)mix + i] = -1.0;
+            A.diag_real[UW_DR_CINLCL * (size_t)mix + i] = -1.0;
+            for (int j = UW_DR_PLCL; j < UW_NDR; j++) A.diag_real[j * (size_t)mix + i] = 0.0;
+        }
+        kinv = klcl = klfc = krel = kbup = kpen = 0;
+    }
+    if (A.diag_int) {
+        A.diag_int[UW_DI_EXIT * (size_t)mix + i] = xflags;
+        A.diag_int[UW_DI_LIMIT * (size_t)mix + i] = lflags;
+        A.diag_int[UW_DI_KINV * (size_t)mix + i] = kinv;
+        A.diag_int[UW_DI_KLCL * (size_t)mix + i] = klcl;
+        A.diag_int[UW_DI_KLFC * (size_t)mix + i] = klfc;
+        A.diag_int[UW_DI_KREL * (size_t)mix + i] = krel;
+        A.diag_int[UW_DI_KBUP * (size_t)mix + i] = kbup;
+        A.diag_int[UW_DI_KPEN * (size_t)mix + i] = kpen;
+    }
+    if (errbits) atomicOr(A.err, errbits);
+#undef RI
+#undef RL
+#undef CNT
+#undef GI
+#undef GL
+#undef GT
+#undef OI
+#undef OL
+#undef OT
+}
+
+// ------------------------------------------------------------------------------------------------
+// Host-side hooks of this translation unit.
+extern "C" cudaError_t uw_fp64_set_constants(const UwConst* h, const double* tbl)
+{
+    cudaError_t e = cudaMemcpyToSymbol(c, h, sizeof(UwConst));
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyToSymbol(c_estbl, tbl, sizeof(double) * UW_TBL);
+}
+
+// Launch one thread per column.  Returns cudaErrorInvalidValue for shapes outside the
+// instantiated bounds (the host validates first).
+extern "C" cudaError_t uw_fp64_launch(const UwArgs* a, int block, cudaStream_t stream)
+{
+    if (a->iend <= 0) return cudaSuccess;
+    if (block <= 0) block = 128;
+    dim3 grid((unsigned)((a->iend + block - 1) / block));
+    if (a->mkx + 1 <= 32 && a->ncnst <= 5) uwshcu_fp64_kernel<32, 5><<<grid, block, 0, stream>>>(*a);
+    else if (a->mkx + 1 <= 64 && a->ncnst <= 5) uwshcu_fp64_kernel<64, 5><<<grid, block, 0, stream>>>(*a);
+    else if (a->mkx + 1 <= 64 && a->ncnst <= UW_NCMAX) uwshcu_fp64_kernel<64, UW_NCMAX><<<grid, block, 0, stream>>>(*a);
+    else return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}

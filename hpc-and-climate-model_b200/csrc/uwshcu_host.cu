@@ -1,0 +1,623 @@
+// uwshcu_host.cu -- host side of libuwshcu_b200.so: constants, saturation table, device arena,
+// pinned staging and the C ABI declared in include/uwshcu.h.
+//
+// The reference drop-in (src/physics/bxcompute_uwshcu_inv.cpp:6195-6496, 6887-7043) allocates and
+// frees ~50 device arrays and ~35 pinned arrays on every call and runs findsp on the CPU.  Here the
+// device arena and the pinned staging area are allocated once per device and grown on demand,
+// every column-physics step (findsp included) runs on the GPU, and a call costs one H2D copy of the
+// packed inputs, one kernel launch and one D2H copy of the packed outputs.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "uwshcu.h"
+#include "uwshcu_common.cuh"
+
+extern "C" cudaError_t uw_fp64_set_constants(const UwConst* h, const double* tbl);
+extern "C" cudaError_t uw_fp64_launch(const UwArgs* a, int block, cudaStream_t stream);
+
+namespace {
+
+constexpr int kMaxDev = 16;
+
+struct DeviceState {
+    unsigned uploaded_gen = 0;   // generation of the constants in this device's __constant__ bank
+    unsigned int* d_err = nullptr;
+    cudaStream_t stream = nullptr;
+    double* d_buf = nullptr;     // device arena (doubles)
+    size_t d_cap = 0;
+    double* h_buf = nullptr;     // pinned staging (doubles)
+    size_t h_cap = 0;
+};
+
+struct State {
+    std::mutex mu;
+    bool init = false;
+    unsigned gen = 0;            // bumped by every uwshcu_init / uwshcu_set_rpen
+    UwConst k{};
+    double tbl[UW_TBL];
+    int precision = UWSHCU_PREC_FP64;
+    int block = 128;
+    DeviceState dev[kMaxDev];
+    char lasterr[256] = "";
+};
+
+State& S()
+{
+    static State s;
+    return s;
+}
+
+// ---- saturation table: gffgch (gffgch.F90:1-127) tabulated by gestbl (wv_saturation.F90:82-204)
+double gffgch(double t, int itype, double tmelt)
+{
+    double tr, es, eswtr = 0.0;
+    int itp = itype;
+    if (itp < 0) {
+        tr = std::fabs((double)itp);
+        itp = 1;
+    } else {
+        tr = 0.0;
+    }
+    if (!(t < (tmelt - tr) && itp == 1)) {
+        const double ps = 1013.246, ts = 373.16;
+        double e1 = 11.344 * (1.0 - t / ts);
+        double e2 = -3.49149 * (ts / t - 1.0);
+        double f1 = -7.90298 * (ts / t - 1.0);
+        double f2 = 5.02808 * std::log10(ts / t);
+        double f3 = -1.3816 * (std::pow(10.0, e1) - 1.0) / 10000000.0;
+        double f4 = 8.1328 * (std::pow(10.0, e2) - 1.0) / 1000.0;
+        double f5 = std::log10(ps);
+        double f = f1 + f2 + f3 + f4 + f5;
+        es = (std::pow(10.0, f)) * 100.0;
+        eswtr = es;
+        if (t >= tmelt || itp == 0) return es;
+    }
+    double t0 = tmelt;
+    double term1 = 2.01889049 / (t0 / t);
+    double term2 = 3.56654 * std::log(t0 / t);
+    double term3 = 20.947031 * (t0 / t);
+    es = 575.185606e10 * std::exp(-(term1 + term2 + term3));
+    if (t < (tmelt - tr)) return es;
+    double weight = std::min((tmelt - t) / tr, 1.0);
+    return weight * es + (1.0 - weight) * eswtr;
+}
+
+void build_table(double* tbl, double tmin, double tmax, double ttrice, int icephs, double tmelt)
+{
+    int lentbl = (int)(tmax - tmin + 2.000001);
+    if (lentbl > UW_TBL) lentbl = UW_TBL;
+    int itype = icephs ? (ttrice != 0.0 ? (int)(-ttrice) : 1) : 0;
+    double t = tmin - 1.0;
+    for (int n = 0; n < lentbl; n++) {
+        t = t + 1.0;
+        tbl[n] = gffgch(t, itype, tmelt);
+    }
+    for (int n = lentbl; n < UW_TBL; n++) tbl[n] = -99999.0;
+}
+
+int cuda_fail(cudaError_t e)
+{
+    std::snprintf(S().lasterr, sizeof(S().lasterr), "%s", cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? UWSHCU_ERR_ALLOC : UWSHCU_ERR_CUDA;
+}
+
+int status_from_bits(unsigned bits)
+{
+    if (bits & UW_ERRBIT_ENTHALPY) return UWSHCU_ERR_FINDSP_ENTHALPY;
+    if (bits & UW_ERRBIT_FINDSP) return UWSHCU_ERR_FINDSP_NONCONVERGED;
+    if (bits & UW_ERRBIT_MU) return UWSHCU_ERR_MU_INCONSISTENT;
+    return UWSHCU_OK;
+}
+
+// Make the current device ready: constants uploaded, error word and stream created.
+int ensure_device(DeviceState** out)
+{
+    State& s = S();
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev <= 0) {
+        std::snprintf(s.lasterr, sizeof(s.lasterr), "%s", e != cudaSuccess ? cudaGetErrorString(e) : "no device");
+        return UWSHCU_ERR_NO_DEVICE;
+    }
+    int dev = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return cuda_fail(e);
+    if (dev < 0 || dev >= kMaxDev) return UWSHCU_ERR_NO_DEVICE;
+    DeviceState& d = s.dev[dev];
+    if (!d.d_err) {
+        if ((e = cudaMalloc(&d.d_err, sizeof(unsigned int))) != cudaSuccess) return cuda_fail(e);
+        if ((e = cudaMemset(d.d_err, 0, sizeof(unsigned int))) != cudaSuccess) return cuda_fail(e);
+    }
+    if (!d.stream) {
+        if ((e = cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking)) != cudaSuccess) return cuda_fail(e);
+    }
+    if (d.uploaded_gen != s.gen) {
+        if ((e = uw_fp64_set_constants(&s.k, s.tbl)) != cudaSuccess) return cuda_fail(e);
+        d.uploaded_gen = s.gen;
+    }
+    *out = &d;
+    return UWSHCU_OK;
+}
+
+int grow(DeviceState& d, size_t ndev_doubles, size_t nhost_doubles)
+{
+    cudaError_t e;
+    if (ndev_doubles > d.d_cap) {
+        if (d.d_buf) cudaFree(d.d_buf);
+        d.d_buf = nullptr;
+        d.d_cap = 0;
+        if ((e = cudaMalloc(&d.d_buf, ndev_doubles * sizeof(double))) != cudaSuccess) return cuda_fail(e);
+        d.d_cap = ndev_doubles;
+    }
+    if (nhost_doubles > d.h_cap) {
+        if (d.h_buf) cudaFreeHost(d.h_buf);
+        d.h_buf = nullptr;
+        d.h_cap = 0;
+        if ((e = cudaMallocHost(&d.h_buf, nhost_doubles * sizeof(double))) != cudaSuccess) return cuda_fail(e);
+        d.h_cap = nhost_doubles;
+    }
+    return UWSHCU_OK;
+}
+
+// A strided copy between a caller array (rows of `ld` doubles) and the compact staging area (rows
+// of n doubles), split over a few host threads for the large calls.
+struct Plane {
+    const double* src;
+    double* dst;
+    size_t rows;
+    size_t src_ld, dst_ld, n;
+};
+
+void copy_planes(const std::vector<Plane>& planes)
+{
+    size_t total = 0;
+    for (const Plane& p : planes) total += p.rows * p.n;
+    unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    unsigned nth = (unsigned)std::min<size_t>(std::min(hw, 16u), std::max<size_t>(1, total / (1u << 20)));
+    // flatten to (plane, row) work items
+    std::vector<std::pair<size_t, size_t>> items;
+    for (size_t p = 0; p < planes.size(); p++)
+        for (size_t r = 0; r < planes[p].rows; r++) items.emplace_back(p, r);
+    auto work = [&](unsigned t) {
+        for (size_t w = t; w < items.size(); w += nth) {
+            const Plane& p = planes[items[w].first];
+            size_t r = items[w].second;
+            std::memcpy(p.dst + r * p.dst_ld, p.src + r * p.src_ld, p.n * sizeof(double));
+        }
+    };
+    if (nth <= 1) {
+        work(0);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < nth; t++) th.emplace_back(work, t);
+    work(0);
+    for (auto& t : th) t.join();
+}
+
+bool bad_dims(int mix, int mkx, int iend, int ncnst)
+{
+    return mix < 1 || mkx < 3 || mkx > UWSHCU_MAX_LEVELS || iend < 0 || iend > mix || ncnst < 3 ||
+           ncnst > UWSHCU_MAX_TRACERS || ncnst != S().k.ncnst;
+}
+
+// Host-pointer call shared by compute_uwshcu_ (inv = 0) and compute_uwshcu_inv_ (inv = 1).
+// Column arrays use leading dimension mix on the host and n = iend on the device.
+int host_call(int inv, int mix, int mkx, int iend, int ncnst, double dt, const double* ps0,
+              const double* zs0, const double* p0, const double* z0, const double* dp0,
+              const double* u0, const double* v0, const double* qv0, const double* ql0,
+              const double* qi0, const double* t0, const double* s0, const double* tr0,
+              const double* tke, const double* pblh, double* cush, double* umf, double* slflx,
+              double* qtflx, double* flxprc1, double* flxsnow1, double* qvten, double* qlten,
+              double* qiten, double* sten, double* uten, double* vten, double* trten,
+              double* qrten, double* qsten, double* precip, double* snow, double* evapc,
+              double* cufrc, double* qcu, double* qlu, double* qiu, double* cbmf, double* qc,
+              double* rliq, double* cnt, double* cnb, const double* dpdry0, double* wu)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    if (!s.init) return UWSHCU_ERR_NOT_INITIALIZED;
+    if (bad_dims(mix, mkx, iend, ncnst)) return UWSHCU_ERR_BAD_ARGS;
+    const void* need[] = {ps0, zs0, p0, z0, dp0, u0, v0, qv0, ql0, qi0, t0, s0, tr0, tke, pblh, cush,
+                          umf, slflx, qtflx, flxprc1, flxsnow1, qvten, qlten, qiten, sten, uten, vten,
+                          trten, qrten, qsten, precip, snow, evapc, cufrc, qcu, qlu, qiu, cbmf, qc, rliq,
+                          cnt, cnb, dpdry0, wu};
+    for (const void* p : need)
+        if (!p) return UWSHCU_ERR_BAD_ARGS;
+    if (iend == 0) return UWSHCU_OK;
+    DeviceState* d = nullptr;
+    int rc = ensure_device(&d);
+    if (rc != UWSHCU_OK) return rc;
+
+    const size_t n = (size_t)iend, ld = (size_t)mix, KI = (size_t)mkx + 1, KL = (size_t)mkx;
+    const size_t KT = KL * (size_t)ncnst;
+    // packed input block: 3 interface fields, 11 layer fields, tracers, pblh, cush
+    const size_t nin = (3 * KI + 11 * KL + KT + 2) * n;
+    // packed output block: 6 interface fields, 14 layer fields, tracers, 7 column fields
+    const size_t nout = (6 * KI + 14 * KL + KT + 7) * n;
+    if ((rc = grow(*d, nin + nout, nin + nout)) != UWSHCU_OK) return rc;
+
+    double* hin = d->h_buf;
+    double* hout = d->h_buf + nin;
+    double* din = d->d_buf;
+    double* dout = d->d_buf + nin;
+    // input planes
+    std::vector<Plane> in;
+    size_t off = 0;
+    auto add_in = [&](const double* a, size_t rows) -> const double* {
+        in.push_back(Plane{a, hin + off, rows, ld, n, n});
+        const double* dp = din + off;
+        off += rows * n;
+        return dp;
+    };
+    UwArgs A{};
+    A.mix = (int)n;
+    A.mkx = mkx;
+    A.iend = iend;
+    A.ncnst = ncnst;
+    A.inv = inv;
+    A.dt = dt;
+    A.ps0 = add_in(ps0, KI);
+    A.zs0 = add_in(zs0, KI);
+    A.tke = add_in(tke, KI);
+    A.p0 = add_in(p0, KL);
+    A.z0 = add_in(z0, KL);
+    A.dp0 = add_in(dp0, KL);
+    A.u0 = add_in(u0, KL);
+    A.v0 = add_in(v0, KL);
+    A.qv0 = add_in(qv0, KL);
+    A.ql0 = add_in(ql0, KL);
+    A.qi0 = add_in(qi0, KL);
+    A.t0 = add_in(t0, KL);
+    A.s0 = add_in(s0, KL);
+    A.dpdry0 = add_in(dpdry0, KL);
+    A.tr0 = add_in(tr0, KT);   // (mix, mkx, ncnst) rows of mix: mkx*ncnst rows
+    A.pblh = add_in(pblh, 1);
+    double* d_cush = const_cast<double*>(add_in(cush, 1));
+    A.cush = d_cush;
+    copy_planes(in);
+
+    std::vector<Plane> out;
+    size_t oo = 0;
+    auto add_out = [&](double* a, size_t rows) -> double* {
+        out.push_back(Plane{hout + oo, a, rows, n, ld, n});
+        double* dp = dout + oo;
+        oo += rows * n;
+        return dp;
+    };
+    A.umf = add_out(umf, KI);
+    A.slflx = add_out(slflx, KI);
+    A.qtflx = add_out(qtflx, KI);
+    A.flxprc1 = add_out(flxprc1, KI);
+    A.flxsnow1 = add_out(flxsnow1, KI);
+    A.wu = add_out(wu, KI);
+    A.qvten = add_out(qvten, KL);
+    A.qlten = add_out(qlten, KL);
+    A.qiten = add_out(qiten, KL);
+    A.sten = add_out(sten, KL);
+    A.uten = add_out(uten, KL);
+    A.vten = add_out(vten, KL);
+    A.qrten = add_out(qrten, KL);
+    A.qsten = add_out(qsten, KL);
+    A.evapc = add_out(evapc, KL);
+    A.cufrc = add_out(cufrc, KL);
+    A.qcu = add_out(qcu, KL);
+    A.qlu = add_out(qlu, KL);
+    A.qiu = add_out(qiu, KL);
+    A.qc = add_out(qc, KL);
+    A.trten = add_out(trten, KT);
+    A.precip = add_out(precip, 1);
+    A.snow = add_out(snow, 1);
+    A.cbmf = add_out(cbmf, 1);
+    A.rliq = add_out(rliq, 1);
+    A.cnt = add_out(cnt, 1);
+    A.cnb = add_out(cnb, 1);
+    // cush is in/out: the kernel reads and rewrites it in place in the input block
+    out.push_back(Plane{hin + (A.cush - din), cush, 1, n, ld, n});
+    A.err = d->d_err;
+    A.diag_int = nullptr;
+    A.diag_real = nullptr;
+
+    cudaError_t e;
+    cudaStream_t st = d->stream;
+    unsigned int hbits = 0;
+    if ((e = cudaMemsetAsync(d->d_err, 0, sizeof(unsigned int), st)) != cudaSuccess) return cuda_fail(e);
+    if ((e = cudaMemcpyAsync(din, hin, nin * sizeof(double), cudaMemcpyHostToDevice, st)) != cudaSuccess) return cuda_fail(e);
+    if ((e = uw_fp64_launch(&A, s.block, st)) != cudaSuccess) return cuda_fail(e);
+    if ((e = cudaMemcpyAsync(hout, dout, nout * sizeof(double), cudaMemcpyDeviceToHost, st)) != cudaSuccess) return cuda_fail(e);
+    if ((e = cudaMemcpyAsync(hin + (A.cush - din), A.cush, n * sizeof(double), cudaMemcpyDeviceToHost, st)) != cudaSuccess) return cuda_fail(e);
+    if ((e = cudaMemcpyAsync(&hbits, d->d_err, sizeof(unsigned int), cudaMemcpyDeviceToHost, st)) != cudaSuccess) return cuda_fail(e);
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e);
+    copy_planes(out);
+    return status_from_bits(hbits);
+}
+
+}  // namespace
+
+// ================================================================================== C ABI ======
+
+extern "C" {
+
+int uwshcu_init(double xlv, double cp, double xlf, double zvir, double r, double g, double ep2,
+                double tmin, double tmax, double ttrice, int icephs, double epsqs, double rgasv,
+                double tmelt, int ncnst, const double* qmin, const int* cnst_wet, int ixnumliq,
+                int ixnumice)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    if (ncnst < 3 || ncnst > UWSHCU_MAX_TRACERS || !qmin || !cnst_wet || ixnumliq < 1 ||
+        ixnumliq > ncnst || ixnumice < 1 || ixnumice > ncnst || !(cp > 0.0) || !(tmax > tmin) ||
+        (int)(tmax - tmin + 2.000001) > UW_TBL)
+        return UWSHCU_ERR_BAD_ARGS;
+    double rpen = s.init ? s.k.rpen : 10.0;
+    UwConst k{};
+    // init_uwshcu (uwshcu.F90:230-239)
+    k.xlv = xlv;
+    k.xlf = xlf;
+    k.xls = k.xlv + k.xlf;
+    k.cp = cp;
+    k.zvir = zvir;
+    k.r = r;
+    k.g = g;
+    k.ep2 = ep2;
+    k.p00 = 1.e5;
+    k.rovcp = k.r / k.cp;
+    k.rpen = rpen;
+    // gestbl (wv_saturation.F90:129-138, 181-185); esinti passes latvap, latice, rh2o, cpair
+    k.tmin = tmin;
+    k.tmax = tmax;
+    k.ttrice = ttrice;
+    k.icephs = icephs ? 1 : 0;
+    k.epsqs = epsqs;
+    k.hlatv = xlv;
+    k.hlatf = xlf;
+    k.rgasv = rgasv;
+    k.cpws = cp;
+    k.tmelt = tmelt;
+    k.pcf[0] = 5.04469588506e-01;
+    k.pcf[1] = -5.47288442819e+00;
+    k.pcf[2] = -3.67471858735e-01;
+    k.pcf[3] = -8.95963532403e-03;
+    k.pcf[4] = -7.78053686625e-05;
+    k.pcf[5] = 0.0;
+    k.omeps = 1.0 - k.epsqs;
+    k.trinv = (ttrice != 0.0) ? 1.0 / ttrice : 0.0;
+    k.ncnst = ncnst;
+    k.ixnumliq = ixnumliq;
+    k.ixnumice = ixnumice;
+    for (int m = 0; m < ncnst; m++) {
+        k.qmin[m] = qmin[m];
+        k.wet[m] = cnst_wet[m] != 0;
+    }
+    build_table(s.tbl, tmin, tmax, ttrice, k.icephs, tmelt);
+    s.k = k;
+    s.init = true;
+    s.gen++;
+    return UWSHCU_OK;
+}
+
+int uwshcu_set_rpen(double rpen)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    if (!s.init) return UWSHCU_ERR_NOT_INITIALIZED;
+    s.k.rpen = rpen;
+    s.gen++;
+    return UWSHCU_OK;
+}
+
+int uwshcu_init_default(void)
+{
+    // CESM shr_const values (rair = R/mwdair, rh2o = R/mwwv, zvir = rh2o/rair - 1, epsilo = mwwv/mwdair)
+    const double boltz = 1.38065e-23, avogad = 6.02214e26, rgas = avogad * boltz;
+    const double mwdair = 28.966, mwwv = 18.016;
+    const double rdair = rgas / mwdair, rwv = rgas / mwwv, zv = (rwv / rdair) - 1.0;
+    const double qmin[5] = {1.e-12, 0.0, 0.0, 0.0, 0.0};
+    const int wet[5] = {1, 1, 1, 1, 1};
+    int rc = uwshcu_init(2.501e6, 1.00464e3, 3.337e5, zv, rdair, 9.80616, mwwv / mwdair, 173.16, 375.16,
+                         20.0, 1, mwwv / mwdair, rwv, 273.15, 5, qmin, wet, 4, 5);
+    if (rc != UWSHCU_OK) return rc;
+    return uwshcu_set_rpen(10.0);
+}
+
+int uwshcu_set_precision(int mode)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    if (mode != UWSHCU_PREC_FP64) return UWSHCU_ERR_BAD_ARGS;
+    s.precision = mode;
+    return UWSHCU_OK;
+}
+
+int uwshcu_set_block(int threads)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    if (threads == 0) threads = 128;
+    if (threads < 32 || threads > 128 || threads % 32) return UWSHCU_ERR_BAD_ARGS;
+    s.block = threads;
+    return UWSHCU_OK;
+}
+
+int uwshcu_get_estbl(double* out250)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    if (!s.init) return UWSHCU_ERR_NOT_INITIALIZED;
+    if (!out250) return UWSHCU_ERR_BAD_ARGS;
+    std::memcpy(out250, s.tbl, sizeof(s.tbl));
+    return UWSHCU_OK;
+}
+
+int uwshcu_finalize(void)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    int cur = 0;
+    bool have = cudaGetDevice(&cur) == cudaSuccess;
+    for (int dv = 0; dv < kMaxDev; dv++) {
+        DeviceState& d = s.dev[dv];
+        if (!d.d_err && !d.d_buf && !d.h_buf && !d.stream) continue;
+        cudaSetDevice(dv);
+        if (d.d_buf) cudaFree(d.d_buf);
+        if (d.h_buf) cudaFreeHost(d.h_buf);
+        if (d.d_err) cudaFree(d.d_err);
+        if (d.stream) cudaStreamDestroy(d.stream);
+        d = DeviceState{};
+    }
+    if (have) cudaSetDevice(cur);
+    return UWSHCU_OK;
+}
+
+const char* uwshcu_last_cuda_error(void) { return S().lasterr; }
+
+int compute_uwshcu_(const int* mix, const int* mkx, const int* iend, const int* ncnst, const double* dt,
+                    const double* ps0_in, const double* zs0_in, const double* p0_in, const double* z0_in,
+                    const double* dp0_in, const double* u0_in, const double* v0_in, const double* qv0_in,
+                    const double* ql0_in, const double* qi0_in, const double* t0_in, const double* s0_in,
+                    const double* tr0_in, const double* tke_in, const double* cldfrct_in,
+                    const double* concldfrct_in, const double* pblh_in, double* cush_inout,
+                    double* umf_out, double* slflx_out, double* qtflx_out, double* flxprc1_out,
+                    double* flxsnow1_out, double* qvten_out, double* qlten_out, double* qiten_out,
+                    double* sten_out, double* uten_out, double* vten_out, double* trten_out,
+                    double* qrten_out, double* qsten_out, double* precip_out, double* snow_out,
+                    double* evapc_out, double* cufrc_out, double* qcu_out, double* qlu_out,
+                    double* qiu_out, double* cbmf_out, double* qc_out, double* rliq_out,
+                    const double* massflx_sh, double* cnt_out, double* cnb_out, void* qsat,
+                    const int* lchnk, const double* dpdry0_in, double* wu_out)
+{
+    (void)cldfrct_in;
+    (void)concldfrct_in;
+    (void)massflx_sh;
+    (void)qsat;
+    (void)lchnk;
+    if (!mix || !mkx || !iend || !ncnst || !dt) return UWSHCU_ERR_BAD_ARGS;
+    return host_call(0, *mix, *mkx, *iend, *ncnst, *dt, ps0_in, zs0_in, p0_in, z0_in, dp0_in, u0_in, v0_in,
+                     qv0_in, ql0_in, qi0_in, t0_in, s0_in, tr0_in, tke_in, pblh_in, cush_inout, umf_out,
+                     slflx_out, qtflx_out, flxprc1_out, flxsnow1_out, qvten_out, qlten_out, qiten_out,
+                     sten_out, uten_out, vten_out, trten_out, qrten_out, qsten_out, precip_out, snow_out,
+                     evapc_out, cufrc_out, qcu_out, qlu_out, qiu_out, cbmf_out, qc_out, rliq_out,
+                     cnt_out, cnb_out, dpdry0_in, wu_out);
+}
+
+int compute_uwshcu_inv_(const int* mix, const int* mkx, const int* iend, const int* ncnst, const double* dt,
+                        const double* ps0_inv, const double* zs0_inv, const double* p0_inv,
+                        const double* z0_inv, const double* dp0_inv, const double* u0_inv,
+                        const double* v0_inv, const double* qv0_inv, const double* ql0_inv,
+                        const double* qi0_inv, const double* t0_inv, const double* s0_inv,
+                        const double* tr0_inv, const double* tke_inv, const double* cldfrct_inv,
+                        const double* concldfrct_inv, const double* pblh, double* cush,
+                        const double* tpert2, const double* qpert2, const double* massflx_sh,
+                        double* umf_inv, double* slflx_inv, double* qtflx_inv, double* flxprc1_inv,
+                        double* flxsnow1_inv, double* qvten_inv, double* qlten_inv, double* qiten_inv,
+                        double* sten_inv, double* uten_inv, double* vten_inv, double* trten_inv,
+                        double* qrten_inv, double* qsten_inv, double* precip, double* snow,
+                        double* evapc_inv, double* cufrc_inv, double* qcu_inv, double* qlu_inv,
+                        double* qiu_inv, double* cbmf, double* qc_inv, double* rliq, double* cnt_inv,
+                        double* cnb_inv, void* qsat, const int* lchnk, const double* dpdry0_inv,
+                        double* wu_inv)
+{
+    (void)cldfrct_inv;
+    (void)concldfrct_inv;
+    (void)tpert2;
+    (void)qpert2;
+    (void)massflx_sh;
+    (void)qsat;
+    (void)lchnk;
+    if (!mix || !mkx || !iend || !ncnst || !dt) return UWSHCU_ERR_BAD_ARGS;
+    return host_call(1, *mix, *mkx, *iend, *ncnst, *dt, ps0_inv, zs0_inv, p0_inv, z0_inv, dp0_inv, u0_inv,
+                     v0_inv, qv0_inv, ql0_inv, qi0_inv, t0_inv, s0_inv, tr0_inv, tke_inv, pblh, cush,
+                     umf_inv, slflx_inv, qtflx_inv, flxprc1_inv, flxsnow1_inv, qvten_inv, qlten_inv,
+                     qiten_inv, sten_inv, uten_inv, vten_inv, trten_inv, qrten_inv, qsten_inv, precip,
+                     snow, evapc_inv, cufrc_inv, qcu_inv, qlu_inv, qiu_inv, cbmf, qc_inv, rliq, cnt_inv,
+                     cnb_inv, dpdry0_inv, wu_inv);
+}
+
+int bxcompute_uwshcu_inv_(const int* pcols, const int* pver, const int* ncol, const int* pcnst,
+                          const double* ztodt, const double* ps0_inv, const double* zs0_inv,
+                          const double* p0_inv, const double* z0_inv, const double* dp0_inv,
+                          const double* u0_inv, const double* v0_inv, const double* qv0_inv,
+                          const double* ql0_inv, const double* qi0_inv, const double* t0_inv,
+                          const double* s0_inv, const double* tr0_inv, const double* tke_inv,
+                          const double* cldfrct_inv, const double* concldfrct_inv, const double* pblh,
+                          double* cush, double* umf_inv, double* slflx_inv, double* qtflx_inv,
+                          double* flxprc1_inv, double* flxsnow1_inv, double* qvten_inv,
+                          double* qlten_inv, double* qiten_inv, double* sten_inv, double* uten_inv,
+                          double* vten_inv, double* trten_inv, double* qrten_inv, double* qsten_inv,
+                          double* precip, double* snow, double* evapc_inv, double* cufrc_inv,
+                          double* qcu_inv, double* qlu_inv, double* qiu_inv, double* cbmf,
+                          double* qc_inv, double* rliq, double* cnt_inv, double* cnb_inv,
+                          const int* lchnk, const double* dpdry0_inv, double* wu_inv)
+{
+    return compute_uwshcu_inv_(pcols, pver, ncol, pcnst, ztodt, ps0_inv, zs0_inv, p0_inv, z0_inv, dp0_inv,
+                               u0_inv, v0_inv, qv0_inv, ql0_inv, qi0_inv, t0_inv, s0_inv, tr0_inv, tke_inv,
+                               cldfrct_inv, concldfrct_inv, pblh, cush, nullptr, nullptr, nullptr, umf_inv,
+                               slflx_inv, qtflx_inv, flxprc1_inv, flxsnow1_inv, qvten_inv, qlten_inv,
+                               qiten_inv, sten_inv, uten_inv, vten_inv, trten_inv, qrten_inv, qsten_inv,
+                               precip, snow, evapc_inv, cufrc_inv, qcu_inv, qlu_inv, qiu_inv, cbmf, qc_inv,
+                               rliq, cnt_inv, cnb_inv, nullptr, lchnk, dpdry0_inv, wu_inv);
+}
+
+int uwshcu_compute_device(int mix, int mkx, int iend, int ncnst, double dt, int inv, const double* ps0,
+                          const double* zs0, const double* p0, const double* z0, const double* dp0,
+                          const double* u0, const double* v0, const double* qv0, const double* ql0,
+                          const double* qi0, const double* t0, const double* s0, const double* tr0,
+                          const double* tke, const double* pblh, double* cush, double* umf,
+                          double* slflx, double* qtflx, double* flxprc1, double* flxsnow1,
+                          double* qvten, double* qlten, double* qiten, double* sten, double* uten,
+                          double* vten, double* trten, double* qrten, double* qsten, double* precip,
+                          double* snow, double* evapc, double* cufrc, double* qcu, double* qlu,
+                          double* qiu, double* cbmf, double* qc, double* rliq, double* cnt,
+                          double* cnb, const double* dpdry0, double* wu, int* diag_int,
+                          double* diag_real, void* stream)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    if (!s.init) return UWSHCU_ERR_NOT_INITIALIZED;
+    if (bad_dims(mix, mkx, iend, ncnst) || (inv != 0 && inv != 1)) return UWSHCU_ERR_BAD_ARGS;
+    const void* need[] = {ps0, zs0, p0, z0, dp0, u0, v0, qv0, ql0, qi0, t0, s0, tr0, tke, pblh, cush,
+                          umf, slflx, qtflx, flxprc1, flxsnow1, qvten, qlten, qiten, sten, uten, vten,
+                          trten, qrten, qsten, precip, snow, evapc, cufrc, qcu, qlu, qiu, cbmf, qc, rliq,
+                          cnt, cnb, dpdry0, wu};
+    for (const void* p : need)
+        if (!p) return UWSHCU_ERR_BAD_ARGS;
+    DeviceState* d = nullptr;
+    int rc = ensure_device(&d);
+    if (rc != UWSHCU_OK) return rc;
+    UwArgs A{};
+    A.mix = mix; A.mkx = mkx; A.iend = iend; A.ncnst = ncnst; A.inv = inv; A.dt = dt;
+    A.ps0 = ps0; A.zs0 = zs0; A.p0 = p0; A.z0 = z0; A.dp0 = dp0; A.u0 = u0; A.v0 = v0; A.qv0 = qv0;
+    A.ql0 = ql0; A.qi0 = qi0; A.t0 = t0; A.s0 = s0; A.tr0 = tr0; A.tke = tke; A.pblh = pblh; A.cush = cush;
+    A.umf = umf; A.slflx = slflx; A.qtflx = qtflx; A.flxprc1 = flxprc1; A.flxsnow1 = flxsnow1;
+    A.qvten = qvten; A.qlten = qlten; A.qiten = qiten; A.sten = sten; A.uten = uten; A.vten = vten;
+    A.trten = trten; A.qrten = qrten; A.qsten = qsten; A.precip = precip; A.snow = snow; A.evapc = evapc;
+    A.cufrc = cufrc; A.qcu = qcu; A.qlu = qlu; A.qiu = qiu; A.cbmf = cbmf; A.qc = qc; A.rliq = rliq;
+    A.cnt = cnt; A.cnb = cnb; A.dpdry0 = dpdry0; A.wu = wu; A.diag_int = diag_int; A.diag_real = diag_real;
+    A.err = d->d_err;
+    cudaError_t e = uw_fp64_launch(&A, s.block, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e);
+    return UWSHCU_OK;
+}
+
+int uwshcu_device_status(void* stream)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    DeviceState* d = nullptr;
+    int rc = ensure_device(&d);
+    if (rc != UWSHCU_OK) return rc;
+    cudaError_t e;
+    unsigned int bits = 0;
+    if ((e = cudaStreamSynchronize((cudaStream_t)stream)) != cudaSuccess) return cuda_fail(e);
+    if ((e = cudaMemcpy(&bits, d->d_err, sizeof(bits), cudaMemcpyDeviceToHost)) != cudaSuccess) return cuda_fail(e);
+    if ((e = cudaMemset(d->d_err, 0, sizeof(unsigned int))) != cudaSuccess) return cuda_fail(e);
+    return status_from_bits(bits);
+}
+
+}  // extern "C"

@@ -1,0 +1,202 @@
+"""Python binding of libuwshcu_b200.so (ctypes over the C ABI of include/uwshcu.h).
+
+This is the interface tests and the benchmark use.  It adds nothing to the computation: every call
+goes to a C entry point with the Fortran argument list (compute_uwshcu_, compute_uwshcu_inv_,
+bxcompute_uwshcu_inv_) or to the device-resident entry uwshcu_compute_device.  If the shared
+library is missing, importing this module raises: there is no CPU fallback.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libuwshcu_b200.so")
+
+OUT_IFACE = ("umf", "slflx", "qtflx", "flxprc1", "flxsnow1", "wu")
+OUT_LAYER = ("qvten", "qlten", "qiten", "sten", "uten", "vten", "qrten", "qsten", "evapc",
+             "cufrc", "qcu", "qlu", "qiu", "qc")
+OUT_COL = ("precip", "snow", "cbmf", "rliq", "cnt", "cnb", "cush")
+IN_IFACE = ("ps0", "zs0", "tke")
+IN_LAYER = ("p0", "z0", "dp0", "u0", "v0", "qv0", "ql0", "qi0", "t0", "s0", "cldfrct",
+            "concldfrct", "dpdry0")
+
+OK = 0
+ERR_MU_INCONSISTENT = 1
+ERR_FINDSP_NONCONVERGED = 2
+ERR_FINDSP_ENTHALPY = 3
+ERR_BAD_ARGS = -1
+ERR_NOT_INITIALIZED = -2
+ERR_CUDA = -3
+ERR_NO_DEVICE = -4
+ERR_ALLOC = -5
+
+EXPORTS = ("uwshcu_init", "uwshcu_set_rpen", "uwshcu_init_default", "uwshcu_set_precision",
+           "uwshcu_set_block", "uwshcu_get_estbl", "uwshcu_finalize", "uwshcu_last_cuda_error",
+           "compute_uwshcu_", "compute_uwshcu_inv_", "bxcompute_uwshcu_inv_",
+           "uwshcu_compute_device", "uwshcu_device_status")
+
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libuwshcu_b200.so is not built (%s); run build.py" % LIB_PATH)
+        L = ctypes.CDLL(LIB_PATH)
+        for name in EXPORTS:
+            getattr(L, name).restype = ctypes.c_int
+        L.uwshcu_last_cuda_error.restype = ctypes.c_char_p
+        _lib = L
+    return _lib
+
+
+def init_default():
+    return lib().uwshcu_init_default()
+
+
+def init(xlv, cp, xlf, zvir, r, g, ep2, tmin, tmax, ttrice, icephs, epsqs, rgasv, tmelt, qmin,
+         cnst_wet, ixnumliq, ixnumice):
+    qmin = np.ascontiguousarray(qmin, dtype=np.float64)
+    wet = np.ascontiguousarray(cnst_wet, dtype=np.int32)
+    f = ctypes.c_double
+    return lib().uwshcu_init(f(xlv), f(cp), f(xlf), f(zvir), f(r), f(g), f(ep2), f(tmin), f(tmax),
+                             f(ttrice), ctypes.c_int(icephs), f(epsqs), f(rgasv), f(tmelt),
+                             ctypes.c_int(len(qmin)), qmin.ctypes.data_as(_D),
+                             wet.ctypes.data_as(_I), ctypes.c_int(ixnumliq),
+                             ctypes.c_int(ixnumice))
+
+
+def set_rpen(rpen):
+    return lib().uwshcu_set_rpen(ctypes.c_double(rpen))
+
+
+def set_block(threads):
+    return lib().uwshcu_set_block(ctypes.c_int(threads))
+
+
+def estbl():
+    t = np.zeros(250)
+    rc = lib().uwshcu_get_estbl(t.ctypes.data_as(_D))
+    if rc != 0:
+        raise RuntimeError("uwshcu_get_estbl: %d" % rc)
+    return t
+
+
+def last_cuda_error():
+    return lib().uwshcu_last_cuda_error().decode()
+
+
+def _p(a):
+    return a.ctypes.data_as(_D)
+
+
+def alloc_outputs(mkx, ncnst, mix, cush_in):
+    out = {k: np.zeros((mkx + 1, mix)) for k in OUT_IFACE}
+    out.update({k: np.zeros((mkx, mix)) for k in OUT_LAYER})
+    out["trten"] = np.zeros((ncnst, mkx, mix))
+    out.update({k: np.zeros(mix) for k in OUT_COL})
+    out["cush"][:] = cush_in
+    return out
+
+
+def compute_host(s, entry="compute_uwshcu_", out=None, iend=None):
+    """Call a host entry point on a sounding dict (numpy arrays in the Fortran layout; mix = ncol).
+    entry: 'compute_uwshcu_' (bottom-up arrays), 'compute_uwshcu_inv_' or 'bxcompute_uwshcu_inv_'
+    (CAM top-down arrays, e.g. soundings.to_inv(s)).  Returns (status, outputs)."""
+    L = lib()
+    mkx, ncnst, n = s["mkx"], s["ncnst"], s["ncol"]
+    if out is None:
+        out = alloc_outputs(mkx, ncnst, n, s["cush"])
+    o = out
+    ci = lambda v: ctypes.byref(ctypes.c_int(int(v)))
+    cd = lambda v: ctypes.byref(ctypes.c_double(float(v)))
+    ie = n if iend is None else iend
+    common_in = (_p(s["ps0"]), _p(s["zs0"]), _p(s["p0"]), _p(s["z0"]), _p(s["dp0"]), _p(s["u0"]),
+                 _p(s["v0"]), _p(s["qv0"]), _p(s["ql0"]), _p(s["qi0"]), _p(s["t0"]), _p(s["s0"]),
+                 _p(s["tr0"]), _p(s["tke"]), _p(s["cldfrct"]), _p(s["concldfrct"]), _p(s["pblh"]),
+                 _p(o["cush"]))
+    outs1 = (_p(o["umf"]), _p(o["slflx"]), _p(o["qtflx"]), _p(o["flxprc1"]), _p(o["flxsnow1"]),
+             _p(o["qvten"]), _p(o["qlten"]), _p(o["qiten"]), _p(o["sten"]), _p(o["uten"]),
+             _p(o["vten"]), _p(o["trten"]), _p(o["qrten"]), _p(o["qsten"]), _p(o["precip"]),
+             _p(o["snow"]), _p(o["evapc"]), _p(o["cufrc"]), _p(o["qcu"]), _p(o["qlu"]),
+             _p(o["qiu"]), _p(o["cbmf"]), _p(o["qc"]), _p(o["rliq"]))
+    lchnk = ci(0)
+    if entry == "compute_uwshcu_":
+        rc = L.compute_uwshcu_(ci(n), ci(mkx), ci(ie), ci(ncnst), cd(s["dt"]), *common_in, *outs1,
+                               _p(s["massflx_sh"]), _p(o["cnt"]), _p(o["cnb"]), None, lchnk,
+                               _p(s["dpdry0"]), _p(o["wu"]))
+    elif entry == "compute_uwshcu_inv_":
+        z = np.zeros(n)
+        rc = L.compute_uwshcu_inv_(ci(n), ci(mkx), ci(ie), ci(ncnst), cd(s["dt"]), *common_in,
+                                   _p(z), _p(z), _p(s["massflx_sh"]), *outs1, _p(o["cnt"]),
+                                   _p(o["cnb"]), None, lchnk, _p(s["dpdry0"]), _p(o["wu"]))
+    elif entry == "bxcompute_uwshcu_inv_":
+        rc = L.bxcompute_uwshcu_inv_(ci(n), ci(mkx), ci(ie), ci(ncnst), cd(s["dt"]), *common_in,
+                                     *outs1, _p(o["cnt"]), _p(o["cnb"]), lchnk, _p(s["dpdry0"]),
+                                     _p(o["wu"]))
+    else:
+        raise ValueError(entry)
+    return rc, o
+
+
+class DeviceCase:
+    """Inputs and outputs of one workload resident in device memory (torch tensors used only as
+    allocations), for uwshcu_compute_device."""
+
+    def __init__(self, s, device="cuda", diag=False, inputs=None):
+        import torch
+        self.torch = torch
+        self.mkx, self.ncnst, self.n = s["mkx"], s["ncnst"], s["ncol"]
+        self.dt = s["dt"]
+        self.inp = inputs if inputs is not None else {
+            k: torch.from_numpy(np.ascontiguousarray(s[k])).to(device)
+            for k in IN_IFACE + IN_LAYER + ("tr0", "pblh")}
+        self.cush0 = torch.from_numpy(np.ascontiguousarray(s["cush"])).to(device)
+        n, mkx, nc = self.n, self.mkx, self.ncnst
+        self.out = {k: torch.zeros((mkx + 1, n), dtype=torch.float64, device=device) for k in OUT_IFACE}
+        self.out.update({k: torch.zeros((mkx, n), dtype=torch.float64, device=device) for k in OUT_LAYER})
+        self.out["trten"] = torch.zeros((nc, mkx, n), dtype=torch.float64, device=device)
+        self.out.update({k: torch.zeros(n, dtype=torch.float64, device=device) for k in OUT_COL})
+        self.out["cush"].copy_(self.cush0)
+        self.diag_int = torch.zeros((8, n), dtype=torch.int32, device=device) if diag else None
+        self.diag_real = torch.zeros((8, n), dtype=torch.float64, device=device) if diag else None
+
+    def reset_cush(self):
+        self.out["cush"].copy_(self.cush0)
+
+    def launch(self, inv=0, stream=None):
+        """Enqueue one call on `stream` (torch stream or None for the current stream)."""
+        torch = self.torch
+        st = stream if stream is not None else torch.cuda.current_stream()
+        P = lambda t: ctypes.c_void_p(t.data_ptr())
+        i, o = self.inp, self.out
+        return lib().uwshcu_compute_device(
+            ctypes.c_int(self.n), ctypes.c_int(self.mkx), ctypes.c_int(self.n),
+            ctypes.c_int(self.ncnst), ctypes.c_double(self.dt), ctypes.c_int(inv),
+            P(i["ps0"]), P(i["zs0"]), P(i["p0"]), P(i["z0"]), P(i["dp0"]), P(i["u0"]), P(i["v0"]),
+            P(i["qv0"]), P(i["ql0"]), P(i["qi0"]), P(i["t0"]), P(i["s0"]), P(i["tr0"]),
+            P(i["tke"]), P(i["pblh"]), P(o["cush"]), P(o["umf"]), P(o["slflx"]), P(o["qtflx"]),
+            P(o["flxprc1"]), P(o["flxsnow1"]), P(o["qvten"]), P(o["qlten"]), P(o["qiten"]),
+            P(o["sten"]), P(o["uten"]), P(o["vten"]), P(o["trten"]), P(o["qrten"]),
+            P(o["qsten"]), P(o["precip"]), P(o["snow"]), P(o["evapc"]), P(o["cufrc"]),
+            P(o["qcu"]), P(o["qlu"]), P(o["qiu"]), P(o["cbmf"]), P(o["qc"]), P(o["rliq"]),
+            P(o["cnt"]), P(o["cnb"]), P(i["dpdry0"]), P(o["wu"]),
+            P(self.diag_int) if self.diag_int is not None else None,
+            P(self.diag_real) if self.diag_real is not None else None,
+            ctypes.c_void_p(st.cuda_stream))
+
+    def status(self, stream=None):
+        torch = self.torch
+        st = stream if stream is not None else torch.cuda.current_stream()
+        return lib().uwshcu_device_status(ctypes.c_void_p(st.cuda_stream))
+
+    def outputs_numpy(self):
+        o = {k: v.cpu().numpy() for k, v in self.out.items()}
+        if self.diag_int is not None:
+            o["diag_int"] = self.diag_int.cpu().numpy()
+            o["diag_real"] = self.diag_real.cpu().numpy()
+        return o

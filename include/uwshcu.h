@@ -1,0 +1,170 @@
+/*
+ * uwshcu.h -- C ABI of the B200 UW shallow-cumulus library (libuwshcu_b200.so).
+ *
+ * Drop-in for the per-column driver of the UW shallow convection scheme of CAM / CAS-ESM
+ * (guirenbenxin/HPC-and-climate-model, src/physics/uwshcu.F90).  Every entry point takes plain
+ * pointers and sizes.  Host entry points follow Fortran calling conventions (all arguments by
+ * reference, trailing underscore) so a Fortran caller binds them with an iso_c_binding interface
+ * block; arrays are column-major with the column index fastest and leading dimension `mix`, exactly
+ * as the Fortran routines declare them.
+ *
+ * All entry points return an int status: 0 on success, > 0 for the conditions on which the
+ * reference stops the model with endrun (the outputs are still produced), < 0 for errors that
+ * prevented the computation.  Nothing in the library prints or aborts.
+ */
+#ifndef UWSHCU_B200_H
+#define UWSHCU_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define UWSHCU_OK 0
+#define UWSHCU_ERR_MU_INCONSISTENT 1     /* uwshcu.F90:2119-2122 'Critical error in mu calculation' */
+#define UWSHCU_ERR_FINDSP_NONCONVERGED 2 /* uwshcu.F90:5423-5431 'findsp not converging'           */
+#define UWSHCU_ERR_FINDSP_ENTHALPY 3     /* uwshcu.F90:5435-5447 'enthalpy is not conserved'       */
+#define UWSHCU_ERR_BAD_ARGS (-1)         /* null pointer or dimension out of range                 */
+#define UWSHCU_ERR_NOT_INITIALIZED (-2)  /* uwshcu_init was not called                             */
+#define UWSHCU_ERR_CUDA (-3)             /* CUDA runtime error (uwshcu_last_cuda_error names it)   */
+#define UWSHCU_ERR_NO_DEVICE (-4)        /* no CUDA device visible                                 */
+#define UWSHCU_ERR_ALLOC (-5)            /* device or pinned host allocation failed                */
+
+#define UWSHCU_MAX_LEVELS 63             /* mkx limit of the compiled kernels                      */
+#define UWSHCU_MAX_TRACERS 32            /* ncnst limit of the compiled kernels                    */
+
+/* Precision modes of the device path (uwshcu_set_precision). */
+#define UWSHCU_PREC_FP64 0               /* FP64 throughout, Fortran evaluation order, no FMA      */
+
+/* ---- set-up -------------------------------------------------------------------------------- */
+
+/* Replaces init_uwshcu (uwshcu.F90:102-249) + esinti/gestbl (esinti.F90:38-51,
+ * wv_saturation.F90:82-204) + the constituent metadata compute_uwshcu reads (qmin,
+ * constituents.F90:54; cnst_get_type_byind; cnst_get_ind NUMLIQ/NUMICE, uwshcu.F90:1076-1077).
+ * Host-only: builds the saturation table and stores the constants; the device copy is made on the
+ * first compute call.  ixnumliq/ixnumice are 1-based; cnst_wet[m] != 0 marks a 'wet' tracer. */
+int uwshcu_init(double xlv, double cp, double xlf, double zvir, double r, double g, double ep2,
+                double tmin, double tmax, double ttrice, int icephs, double epsqs, double rgasv,
+                double tmelt, int ncnst, const double *qmin, const int *cnst_wet, int ixnumliq,
+                int ixnumice);
+
+/* Replaces uwshcu_readnl (uwshcu.F90:58-98): the penetrative-entrainment efficiency rpen. */
+int uwshcu_set_rpen(double rpen);
+
+/* uwshcu_init + uwshcu_set_rpen with the CESM shr_const values CAM passes (convect_shallow.F90:280,
+ * physpkg.F90:638), rpen = 10, five tracers (Q, CLDLIQ, CLDICE, NUMLIQ, NUMICE) with
+ * qmin = {1e-12, 0, 0, 0, 0}. */
+int uwshcu_init_default(void);
+
+/* Precision of the device path: UWSHCU_PREC_FP64. */
+int uwshcu_set_precision(int mode);
+
+/* Threads per block of the column kernel (0 = built-in default). */
+int uwshcu_set_block(int threads);
+
+/* Copy of the 250-entry saturation-vapour-pressure table (wv_saturation.F90 estbl). */
+int uwshcu_get_estbl(double *out250);
+
+/* Release the device arena and pinned staging buffers. */
+int uwshcu_finalize(void);
+
+/* Text of the last CUDA error seen by the library ("" if none). */
+const char *uwshcu_last_cuda_error(void);
+
+/* ---- host entry points (Fortran conventions) --------------------------------------------------- */
+
+/* compute_uwshcu (uwshcu.F90:478-492), argument list unchanged.  Arrays (mix, 0:mkx), (mix, mkx),
+ * (mix, mkx, ncnst) with k = 1 the surface layer; columns 1..iend are computed.  `qsat` (the
+ * fqsatd function pointer) and `lchnk` are accepted and ignored: the library evaluates the
+ * saturation functions of wv_saturation itself.  cldfrct/concldfrct/massflx_sh are accepted and
+ * unused, as in the Fortran with shallow_closure_scheme = 'cam'. */
+int compute_uwshcu_(const int *mix, const int *mkx, const int *iend, const int *ncnst,
+                    const double *dt, const double *ps0_in, const double *zs0_in,
+                    const double *p0_in, const double *z0_in, const double *dp0_in,
+                    const double *u0_in, const double *v0_in, const double *qv0_in,
+                    const double *ql0_in, const double *qi0_in, const double *t0_in,
+                    const double *s0_in, const double *tr0_in, const double *tke_in,
+                    const double *cldfrct_in, const double *concldfrct_in, const double *pblh_in,
+                    double *cush_inout, double *umf_out, double *slflx_out, double *qtflx_out,
+                    double *flxprc1_out, double *flxsnow1_out, double *qvten_out,
+                    double *qlten_out, double *qiten_out, double *sten_out, double *uten_out,
+                    double *vten_out, double *trten_out, double *qrten_out, double *qsten_out,
+                    double *precip_out, double *snow_out, double *evapc_out, double *cufrc_out,
+                    double *qcu_out, double *qlu_out, double *qiu_out, double *cbmf_out,
+                    double *qc_out, double *rliq_out, const double *massflx_sh, double *cnt_out,
+                    double *cnb_out, void *qsat, const int *lchnk, const double *dpdry0_in,
+                    double *wu_out);
+
+/* compute_uwshcu_inv (uwshcu.F90:251-265, called from convect_shallow.F90:585-600): the same
+ * computation on CAM's top-down level order.  The level reversal is folded into the kernel's
+ * loads and stores instead of being copied.  tpert2/qpert2 are unused (shallow_zmh_pert =
+ * .false., uwshcu.F90:40). */
+int compute_uwshcu_inv_(const int *mix, const int *mkx, const int *iend, const int *ncnst,
+                        const double *dt, const double *ps0_inv, const double *zs0_inv,
+                        const double *p0_inv, const double *z0_inv, const double *dp0_inv,
+                        const double *u0_inv, const double *v0_inv, const double *qv0_inv,
+                        const double *ql0_inv, const double *qi0_inv, const double *t0_inv,
+                        const double *s0_inv, const double *tr0_inv, const double *tke_inv,
+                        const double *cldfrct_inv, const double *concldfrct_inv,
+                        const double *pblh, double *cush, const double *tpert2,
+                        const double *qpert2, const double *massflx_sh, double *umf_inv,
+                        double *slflx_inv, double *qtflx_inv, double *flxprc1_inv,
+                        double *flxsnow1_inv, double *qvten_inv, double *qlten_inv,
+                        double *qiten_inv, double *sten_inv, double *uten_inv, double *vten_inv,
+                        double *trten_inv, double *qrten_inv, double *qsten_inv, double *precip,
+                        double *snow, double *evapc_inv, double *cufrc_inv, double *qcu_inv,
+                        double *qlu_inv, double *qiu_inv, double *cbmf, double *qc_inv,
+                        double *rliq, double *cnt_inv, double *cnb_inv, void *qsat,
+                        const int *lchnk, const double *dpdry0_inv, double *wu_inv);
+
+/* bxcompute_uwshcu_inv_ (src/physics/bxcompute_uwshcu_inv.cpp:6172-6184): the entry of the
+ * reference's own GPU drop-in, same argument list (pcols, pver, ncol, pcnst, ztodt, ..., lchnk,
+ * dpdry0_inv, wu_inv).  Runs compute_uwshcu_inv_; unlike the reference it honours pcols as the
+ * leading dimension when ncol < pcols and computes every column (no ncol/32 tail drop). */
+int bxcompute_uwshcu_inv_(const int *pcols, const int *pver, const int *ncol, const int *pcnst,
+                          const double *ztodt, const double *ps0_inv, const double *zs0_inv,
+                          const double *p0_inv, const double *z0_inv, const double *dp0_inv,
+                          const double *u0_inv, const double *v0_inv, const double *qv0_inv,
+                          const double *ql0_inv, const double *qi0_inv, const double *t0_inv,
+                          const double *s0_inv, const double *tr0_inv, const double *tke_inv,
+                          const double *cldfrct_inv, const double *concldfrct_inv,
+                          const double *pblh, double *cush, double *umf_inv, double *slflx_inv,
+                          double *qtflx_inv, double *flxprc1_inv, double *flxsnow1_inv,
+                          double *qvten_inv, double *qlten_inv, double *qiten_inv,
+                          double *sten_inv, double *uten_inv, double *vten_inv, double *trten_inv,
+                          double *qrten_inv, double *qsten_inv, double *precip, double *snow,
+                          double *evapc_inv, double *cufrc_inv, double *qcu_inv, double *qlu_inv,
+                          double *qiu_inv, double *cbmf, double *qc_inv, double *rliq,
+                          double *cnt_inv, double *cnb_inv, const int *lchnk,
+                          const double *dpdry0_inv, double *wu_inv);
+
+/* ---- device-resident entry point -------------------------------------------------------------- */
+
+/* The computation of compute_uwshcu (inv = 0) or compute_uwshcu_inv (inv = 1) on arrays that
+ * already live in device memory, in the same layouts with leading dimension mix.  Enqueued on
+ * `stream` (a cudaStream_t, 0 = legacy default stream) and returns without synchronising;
+ * diag_int (8, mix) and diag_real (8, mix) are optional per-column diagnostics (exit/limit flags,
+ * kinv, klcl, klfc, krel, kbup, kpen; cin, cinlcl, plcl, plfc, pinv, pbup, ppen, tkeavg).
+ * The endrun conditions of the call are collected on the device; uwshcu_device_status(stream)
+ * waits for the stream and returns them. */
+int uwshcu_compute_device(int mix, int mkx, int iend, int ncnst, double dt, int inv,
+                          const double *ps0, const double *zs0, const double *p0,
+                          const double *z0, const double *dp0, const double *u0, const double *v0,
+                          const double *qv0, const double *ql0, const double *qi0,
+                          const double *t0, const double *s0, const double *tr0,
+                          const double *tke, const double *pblh, double *cush, double *umf,
+                          double *slflx, double *qtflx, double *flxprc1, double *flxsnow1,
+                          double *qvten, double *qlten, double *qiten, double *sten, double *uten,
+                          double *vten, double *trten, double *qrten, double *qsten,
+                          double *precip, double *snow, double *evapc, double *cufrc, double *qcu,
+                          double *qlu, double *qiu, double *cbmf, double *qc, double *rliq,
+                          double *cnt, double *cnb, const double *dpdry0, double *wu,
+                          int *diag_int, double *diag_real, void *stream);
+
+/* Wait for `stream` and return the status collected by the device calls enqueued on it since the
+ * previous uwshcu_device_status call. */
+int uwshcu_device_status(void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

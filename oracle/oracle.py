@@ -1,0 +1,136 @@
+"""ctypes front end of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Loads oracle/_build/libuwshcu_oracle.so (built by oracle/Makefile) and exposes
+compute_uwshcu / compute_uwshcu_inv on the sounding dicts produced by
+hpc-and-climate-model_b200/soundings.py.  Only tests, the smoke check and the CPU-baseline leg of
+bench.py use this module; it is the checker, not the product.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libuwshcu_oracle.so")
+
+OUT_IFACE = ("umf", "slflx", "qtflx", "flxprc1", "flxsnow1", "wu")
+OUT_LAYER = ("qvten", "qlten", "qiten", "sten", "uten", "vten", "qrten", "qsten", "evapc",
+             "cufrc", "qcu", "qlu", "qiu", "qc")
+OUT_COL = ("precip", "snow", "cbmf", "rliq", "cnt", "cnb", "cush")
+NDI, NDR = 8, 8
+
+_lib = None
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        _lib = ctypes.CDLL(LIB_PATH)
+        _lib.uwo_init_default.restype = ctypes.c_int
+        _lib.uwo_compute_uwshcu.restype = ctypes.c_int
+        _lib.uwo_compute_uwshcu_inv.restype = ctypes.c_int
+        for name in ("uwo_exnf", "uwo_estblf", "uwo_qsinvert", "uwo_compute_alpha",
+                     "uwo_compute_mumin2", "uwo_compute_ppen", "uwo_single_cin"):
+            getattr(_lib, name).restype = ctypes.c_double
+        rc = _lib.uwo_init_default()
+        if rc != 0:
+            raise RuntimeError("uwo_init_default failed: %d" % rc)
+    return _lib
+
+
+def init(xlv, cp, xlf, zvir, r, g, ep2, rpen, tmn, tmx, trice, icephs, epsqs, rgasv, tmelt,
+         qmin, cnst_wet, ixnumliq, ixnumice):
+    L = lib()
+    qmin = np.ascontiguousarray(qmin, dtype=np.float64)
+    wet = np.ascontiguousarray(cnst_wet, dtype=np.int32)
+    f = ctypes.c_double
+    rc = L.uwo_init(f(xlv), f(cp), f(xlf), f(zvir), f(r), f(g), f(ep2), f(rpen), f(tmn), f(tmx),
+                    f(trice), ctypes.c_int(icephs), f(epsqs), f(rgasv), f(tmelt),
+                    ctypes.c_int(len(qmin)), _p(qmin), wet.ctypes.data_as(_I),
+                    ctypes.c_int(ixnumliq), ctypes.c_int(ixnumice))
+    if rc != 0:
+        raise RuntimeError("uwo_init failed: %d" % rc)
+
+
+def init_default():
+    rc = lib().uwo_init_default()
+    if rc != 0:
+        raise RuntimeError("uwo_init_default failed: %d" % rc)
+
+
+def _p(a):
+    return a.ctypes.data_as(_D)
+
+
+def alloc_outputs(mkx, ncnst, mix, cush_in):
+    out = {k: np.zeros((mkx + 1, mix)) for k in OUT_IFACE}
+    out.update({k: np.zeros((mkx, mix)) for k in OUT_LAYER})
+    out["trten"] = np.zeros((ncnst, mkx, mix))
+    out.update({k: np.zeros(mix) for k in OUT_COL})
+    out["cush"][:] = cush_in
+    return out
+
+
+def compute(s, nthreads=0, diag=True, inv=False):
+    """Run the oracle on a sounding dict (all columns, mix = iend = ncol).  Returns the output
+    dict; with diag=True also 'diag_int' (8, ncol) and 'diag_real' (8, ncol)."""
+    L = lib()
+    mkx, ncnst, n = s["mkx"], s["ncnst"], s["ncol"]
+    o = alloc_outputs(mkx, ncnst, n, s["cush"])
+    di = np.zeros((NDI, n), dtype=np.int32)
+    dr = np.zeros((NDR, n))
+    ci, cd = ctypes.c_int, ctypes.c_double
+    if not inv:
+        rc = L.uwo_compute_uwshcu(
+            ci(n), ci(mkx), ci(n), ci(ncnst), cd(s["dt"]),
+            _p(s["ps0"]), _p(s["zs0"]), _p(s["p0"]), _p(s["z0"]), _p(s["dp0"]), _p(s["u0"]),
+            _p(s["v0"]), _p(s["qv0"]), _p(s["ql0"]), _p(s["qi0"]), _p(s["t0"]), _p(s["s0"]),
+            _p(s["tr0"]), _p(s["tke"]), _p(s["cldfrct"]), _p(s["concldfrct"]), _p(s["pblh"]),
+            _p(o["cush"]), _p(o["umf"]), _p(o["slflx"]), _p(o["qtflx"]), _p(o["flxprc1"]),
+            _p(o["flxsnow1"]), _p(o["qvten"]), _p(o["qlten"]), _p(o["qiten"]), _p(o["sten"]),
+            _p(o["uten"]), _p(o["vten"]), _p(o["trten"]), _p(o["qrten"]), _p(o["qsten"]),
+            _p(o["precip"]), _p(o["snow"]), _p(o["evapc"]), _p(o["cufrc"]), _p(o["qcu"]),
+            _p(o["qlu"]), _p(o["qiu"]), _p(o["cbmf"]), _p(o["qc"]), _p(o["rliq"]),
+            _p(s["massflx_sh"]), _p(o["cnt"]), _p(o["cnb"]), _p(s["dpdry0"]), _p(o["wu"]),
+            di.ctypes.data_as(_I) if diag else None, _p(dr) if diag else None, ci(nthreads))
+    else:
+        z = np.zeros(n)
+        rc = L.uwo_compute_uwshcu_inv(
+            ci(n), ci(mkx), ci(n), ci(ncnst), cd(s["dt"]),
+            _p(s["ps0"]), _p(s["zs0"]), _p(s["p0"]), _p(s["z0"]), _p(s["dp0"]), _p(s["u0"]),
+            _p(s["v0"]), _p(s["qv0"]), _p(s["ql0"]), _p(s["qi0"]), _p(s["t0"]), _p(s["s0"]),
+            _p(s["tr0"]), _p(s["tke"]), _p(s["cldfrct"]), _p(s["concldfrct"]), _p(s["pblh"]),
+            _p(o["cush"]), _p(z), _p(z), _p(s["massflx_sh"]),
+            _p(o["umf"]), _p(o["slflx"]), _p(o["qtflx"]), _p(o["flxprc1"]), _p(o["flxsnow1"]),
+            _p(o["qvten"]), _p(o["qlten"]), _p(o["qiten"]), _p(o["sten"]), _p(o["uten"]),
+            _p(o["vten"]), _p(o["trten"]), _p(o["qrten"]), _p(o["qsten"]), _p(o["precip"]),
+            _p(o["snow"]), _p(o["evapc"]), _p(o["cufrc"]), _p(o["qcu"]), _p(o["qlu"]),
+            _p(o["qiu"]), _p(o["cbmf"]), _p(o["qc"]), _p(o["rliq"]), _p(o["cnt"]), _p(o["cnb"]),
+            _p(s["dpdry0"]), _p(o["wu"]), ci(nthreads))
+        diag = False
+    o["status"] = rc
+    if diag:
+        o["diag_int"] = di
+        o["diag_real"] = dr
+    return o
+
+
+def estbl():
+    t = np.zeros(250)
+    lib().uwo_get_estbl(_p(t))
+    return t
+
+
+def consts():
+    c = np.zeros(22)
+    lib().uwo_get_consts(_p(c))
+    return c
