@@ -22,7 +22,10 @@ LIB = os.path.join(LIBDIR, "libuwshcu_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "-I", CSRC, "-I", INCLUDE]
 UNITS = {
-    "uwshcu_fp64.cu": ["-fmad=false"],
+    "uwshcu_fp64_k32n5.cu": ["-fmad=false"],
+    "uwshcu_fp64_k64n5.cu": ["-fmad=false"],
+    "uwshcu_fp64_k32n32.cu": ["-fmad=false"],
+    "uwshcu_fp64_k64n32.cu": ["-fmad=false"],
     "uwshcu_host.cu": [],
 }
 
@@ -47,17 +50,23 @@ def build(verbose=False, force=False):
     os.makedirs(BUILD, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
     hdr = _headers_mtime()
-    objs, relink = [], force or not os.path.exists(LIB)
+    objs, relink, jobs = [], force or not os.path.exists(LIB), []
     for unit, flags in UNITS.items():
         src = os.path.join(CSRC, unit)
         obj = os.path.join(BUILD, unit.replace(".cu", ".o"))
         objs.append(obj)
         if force or not os.path.exists(obj) or os.path.getmtime(obj) < max(os.path.getmtime(src), hdr):
-            cmd = [nvcc()] + ARCH + COMMON + flags + ["-c", src, "-o", obj]
+            jobs.append([nvcc()] + ARCH + COMMON + flags + ["-c", src, "-o", obj])
+    if jobs:
+        relink = True
+        procs = []
+        for cmd in jobs:
             if verbose:
                 print(" ".join(cmd), flush=True)
-            subprocess.run(cmd, check=True)
-            relink = True
+            procs.append(subprocess.Popen(cmd))
+        bad = [p.wait() for p in procs]
+        if any(bad):
+            raise RuntimeError("nvcc failed")
     if relink or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
         cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lpthread"]
         if verbose:

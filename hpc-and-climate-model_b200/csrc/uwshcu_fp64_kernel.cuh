@@ -1,4 +1,8 @@
-// uwshcu_fp64.cu -- FP64 sm_100a kernel of compute_uwshcu (uwshcu.F90:478-4664), one thread per column.
+// uwshcu_fp64_kernel.cuh -- FP64 sm_100a kernel of compute_uwshcu (uwshcu.F90:478-4664), one thread per column.
+//
+// Included by the uwshcu_fp64_k*.cu translation units, each instantiating the kernel for one
+// (level bound, tracer bound) pair so the instantiations compile in parallel; every unit carries its
+// own copy of the constant bank.
 //
 // Each thread owns one column.  The inputs are read directly in the Fortran (mix, k) layout, so a warp
 // of 32 consecutive columns issues 32 consecutive 8-byte loads for every level (level-major SoA).
@@ -22,6 +26,7 @@
 // Fortran bounds (conden 10, qsinvert 10, compute_alpha 10, compute_mumin2 10, compute_ppen 5,
 // findsp 8), and every level index the scheme derives (kinv, klcl, klfc, krel, kbup, kpen) comes
 // from a loop over 0..mkx, so all array accesses stay inside the column.
+#pragma once
 #include <cuda_runtime.h>
 #include <math.h>
 #include "uwshcu_common.cuh"
@@ -377,15 +382,39 @@ __device__ double findsp_point(double q, double t, double p, unsigned int& errbi
 
 // ------------------------------------------------------------------------------------------------
 // The column kernel.  KP bounds the level arrays (mkx + 1 <= KP), NC the tracer count.
-template <int KP, int NC>
-__global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A)
+//
+// MODE selects what a launch does:
+//   UW_MODE_ALL      every column 0..iend-1 runs the whole scheme (single pass);
+//   UW_MODE_TRIGGER  every column runs up to the end of the iteration-1 closure (uwshcu.F90:2184).
+//                    Columns that leave the scheme on the way write their final outputs (the
+//                    label-333 zeroes); the others are appended to the worklist `wl` (warp ballot,
+//                    one atomicAdd per warp) and write nothing;
+//   UW_MODE_LIST     thread t runs the whole scheme for column wl[t], t < *wl_count.
+// The worklist path recomputes the phase-1 part of a convecting column instead of storing it: the
+// heavy buoyancy-sorting work then runs in warps made only of convecting columns.
+#define UW_MODE_ALL 0
+#define UW_MODE_TRIGGER 1
+#define UW_MODE_LIST 2
+
+template <int KP, int NC, int MODE>
+__global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restrict__ wl, int* __restrict__ wl_count)
 {
     __shared__ double tbl[UW_TBL];
     for (int t = threadIdx.x; t < UW_TBL; t += blockDim.x) tbl[t] = c_estbl[t];
     __syncthreads();
 
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.iend) return;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    int i;
+    bool active;
+    if (MODE == UW_MODE_LIST) {
+        active = tid < *wl_count;
+        i = active ? wl[tid] : 0;
+    } else {
+        active = tid < A.iend;
+        i = tid;
+    }
+    bool cand = false;
+    if (active) {
 
     const int mix = A.mix, mkx = A.mkx, ncnst = A.ncnst;
     const double dt = A.dt;
@@ -446,6 +475,7 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A)
     (void)kinv_o_d;
 
     // ---- output initialisation (uwshcu.F90:1087-1124) ------------------------------------------
+    if (MODE != UW_MODE_TRIGGER) {
     for (int k = 0; k <= mkx; k++) {
         OI(umf, k) = 0.0;
         OI(slflx, k) = 0.0;
@@ -467,6 +497,7 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A)
     A.rliq[i] = 0.0;
     A.cnt[i] = CNT((double)mkx);
     A.cnb[i] = CNT(0.0);
+    }
 
     // ---- inputs and findsp (uwshcu.F90:1216-1259) ----------------------------------------------
     for (int k = 0; k <= mkx; k++) {
@@ -830,6 +861,11 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A)
                 umf[k] = cbmf;
                 wu[k] = winv;
             }
+        }
+        if (MODE == UW_MODE_TRIGGER) {
+            // the column convects past the closure: hand it to the worklist pass
+            cand = true;
+            goto l_done;
         }
         // updraft at the release level (:2205-2236)
         emf[krel - 1] = 0.0;
@@ -1731,7 +1767,21 @@ l333:
         A.diag_int[UW_DI_KBUP * (size_t)mix + i] = kbup;
         A.diag_int[UW_DI_KPEN * (size_t)mix + i] = kpen;
     }
+l_done:
     if (errbits) atomicOr(A.err, errbits);
+    }  // active
+    if (MODE == UW_MODE_TRIGGER) {
+        // warp-aggregated append of this warp's candidates
+        const unsigned lane = threadIdx.x & 31u;
+        const unsigned mask = __ballot_sync(0xffffffffu, cand);
+        if (mask) {
+            const int leader = __ffs(mask) - 1;
+            int base = 0;
+            if ((int)lane == leader) base = atomicAdd(wl_count, __popc(mask));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (cand) wl[base + __popc(mask & ((1u << lane) - 1u))] = i;
+        }
+    }
 #undef RI
 #undef RL
 #undef CNT
@@ -1743,25 +1793,3 @@ l333:
 #undef OT
 }
 
-// ------------------------------------------------------------------------------------------------
-// Host-side hooks of this translation unit.
-extern "C" cudaError_t uw_fp64_set_constants(const UwConst* h, const double* tbl)
-{
-    cudaError_t e = cudaMemcpyToSymbol(c, h, sizeof(UwConst));
-    if (e != cudaSuccess) return e;
-    return cudaMemcpyToSymbol(c_estbl, tbl, sizeof(double) * UW_TBL);
-}
-
-// Launch one thread per column.  Returns cudaErrorInvalidValue for shapes outside the
-// instantiated bounds (the host validates first).
-extern "C" cudaError_t uw_fp64_launch(const UwArgs* a, int block, cudaStream_t stream)
-{
-    if (a->iend <= 0) return cudaSuccess;
-    if (block <= 0) block = 128;
-    dim3 grid((unsigned)((a->iend + block - 1) / block));
-    if (a->mkx + 1 <= 32 && a->ncnst <= 5) uwshcu_fp64_kernel<32, 5><<<grid, block, 0, stream>>>(*a);
-    else if (a->mkx + 1 <= 64 && a->ncnst <= 5) uwshcu_fp64_kernel<64, 5><<<grid, block, 0, stream>>>(*a);
-    else if (a->mkx + 1 <= 64 && a->ncnst <= UW_NCMAX) uwshcu_fp64_kernel<64, UW_NCMAX><<<grid, block, 0, stream>>>(*a);
-    else return cudaErrorInvalidValue;
-    return cudaGetLastError();
-}

@@ -19,12 +19,39 @@
 #include "uwshcu.h"
 #include "uwshcu_common.cuh"
 
-extern "C" cudaError_t uw_fp64_set_constants(const UwConst* h, const double* tbl);
-extern "C" cudaError_t uw_fp64_launch(const UwArgs* a, int block, cudaStream_t stream);
+#define UW_DECL(KP, NC)                                                                              \
+    extern "C" cudaError_t uw_fp64_set_constants_k##KP##n##NC(const UwConst* h, const double* tbl); \
+    extern "C" cudaError_t uw_fp64_launch_k##KP##n##NC(const UwArgs* a, int mode, int* wl, int* wl_count, \
+                                                       int nthreads, int block, cudaStream_t stream);
+UW_DECL(32, 5)
+UW_DECL(64, 5)
+UW_DECL(32, 32)
+UW_DECL(64, 32)
+#undef UW_DECL
 
 namespace {
 
 constexpr int kMaxDev = 16;
+constexpr int kModeAll = 0, kModeTrigger = 1, kModeList = 2;
+
+cudaError_t set_constants_all(const UwConst* k, const double* tbl)
+{
+    cudaError_t e;
+    if ((e = uw_fp64_set_constants_k32n5(k, tbl)) != cudaSuccess) return e;
+    if ((e = uw_fp64_set_constants_k64n5(k, tbl)) != cudaSuccess) return e;
+    if ((e = uw_fp64_set_constants_k32n32(k, tbl)) != cudaSuccess) return e;
+    return uw_fp64_set_constants_k64n32(k, tbl);
+}
+
+cudaError_t launch_mode(const UwArgs* a, int mode, int* wl, int* wl_count, int nthreads, int block,
+                        cudaStream_t st)
+{
+    if (a->mkx + 1 <= 32 && a->ncnst <= 5) return uw_fp64_launch_k32n5(a, mode, wl, wl_count, nthreads, block, st);
+    if (a->mkx + 1 <= 64 && a->ncnst <= 5) return uw_fp64_launch_k64n5(a, mode, wl, wl_count, nthreads, block, st);
+    if (a->mkx + 1 <= 32 && a->ncnst <= UW_NCMAX) return uw_fp64_launch_k32n32(a, mode, wl, wl_count, nthreads, block, st);
+    if (a->mkx + 1 <= 64 && a->ncnst <= UW_NCMAX) return uw_fp64_launch_k64n32(a, mode, wl, wl_count, nthreads, block, st);
+    return cudaErrorInvalidValue;
+}
 
 struct DeviceState {
     unsigned uploaded_gen = 0;   // generation of the constants in this device's __constant__ bank
@@ -34,6 +61,12 @@ struct DeviceState {
     size_t d_cap = 0;
     double* h_buf = nullptr;     // pinned staging (doubles)
     size_t h_cap = 0;
+    int* d_wl = nullptr;         // worklist of convecting columns: [0] = count, [1..] = column ids
+    size_t wl_cap = 0;
+    // opt-in per-launch timing: events around the trigger and worklist launches of each call
+    static constexpr int kSlots = 256;
+    cudaEvent_t ev[kSlots][3] = {};
+    int nrec = 0;                // calls recorded since the last read (capped at kSlots)
 };
 
 struct State {
@@ -43,7 +76,9 @@ struct State {
     UwConst k{};
     double tbl[UW_TBL];
     int precision = UWSHCU_PREC_FP64;
+    int schedule = UWSHCU_SCHED_TWO_PHASE;
     int block = 128;
+    bool profiling = false;
     DeviceState dev[kMaxDev];
     char lasterr[256] = "";
 };
@@ -138,7 +173,7 @@ int ensure_device(DeviceState** out)
         if ((e = cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking)) != cudaSuccess) return cuda_fail(e);
     }
     if (d.uploaded_gen != s.gen) {
-        if ((e = uw_fp64_set_constants(&s.k, s.tbl)) != cudaSuccess) return cuda_fail(e);
+        if ((e = set_constants_all(&s.k, s.tbl)) != cudaSuccess) return cuda_fail(e);
         d.uploaded_gen = s.gen;
     }
     *out = &d;
@@ -199,6 +234,47 @@ void copy_planes(const std::vector<Plane>& planes)
     for (unsigned t = 1; t < nth; t++) th.emplace_back(work, t);
     work(0);
     for (auto& t : th) t.join();
+}
+
+int grow_worklist(DeviceState& d, size_t ncol)
+{
+    if (ncol + 1 <= d.wl_cap) return UWSHCU_OK;
+    if (d.d_wl) cudaFree(d.d_wl);
+    d.d_wl = nullptr;
+    d.wl_cap = 0;
+    cudaError_t e = cudaMalloc(&d.d_wl, (ncol + 1) * sizeof(int));
+    if (e != cudaSuccess) return cuda_fail(e);
+    d.wl_cap = ncol + 1;
+    return UWSHCU_OK;
+}
+
+// Enqueue the column computation for A on st with the selected schedule.
+int enqueue(DeviceState& d, const UwArgs& A, cudaStream_t st)
+{
+    State& s = S();
+    cudaError_t e;
+    if (s.schedule == UWSHCU_SCHED_SINGLE_PASS) {
+        if ((e = launch_mode(&A, kModeAll, nullptr, nullptr, A.iend, s.block, st)) != cudaSuccess) return cuda_fail(e);
+        return UWSHCU_OK;
+    }
+    int rc = grow_worklist(d, (size_t)A.iend);
+    if (rc != UWSHCU_OK) return rc;
+    int* count = d.d_wl;
+    int* list = d.d_wl + 1;
+    cudaEvent_t* ev = nullptr;
+    if (s.profiling && d.nrec < DeviceState::kSlots) {
+        ev = d.ev[d.nrec];
+        for (int j = 0; j < 3; j++)
+            if (!ev[j] && (e = cudaEventCreate(&ev[j])) != cudaSuccess) return cuda_fail(e);
+        d.nrec++;
+    }
+    if ((e = cudaMemsetAsync(count, 0, sizeof(int), st)) != cudaSuccess) return cuda_fail(e);
+    if (ev && (e = cudaEventRecord(ev[0], st)) != cudaSuccess) return cuda_fail(e);
+    if ((e = launch_mode(&A, kModeTrigger, list, count, A.iend, s.block, st)) != cudaSuccess) return cuda_fail(e);
+    if (ev && (e = cudaEventRecord(ev[1], st)) != cudaSuccess) return cuda_fail(e);
+    if ((e = launch_mode(&A, kModeList, list, count, A.iend, s.block, st)) != cudaSuccess) return cuda_fail(e);
+    if (ev && (e = cudaEventRecord(ev[2], st)) != cudaSuccess) return cuda_fail(e);
+    return UWSHCU_OK;
 }
 
 bool bad_dims(int mix, int mkx, int iend, int ncnst)
@@ -329,7 +405,7 @@ int host_call(int inv, int mix, int mkx, int iend, int ncnst, double dt, const d
     unsigned int hbits = 0;
     if ((e = cudaMemsetAsync(d->d_err, 0, sizeof(unsigned int), st)) != cudaSuccess) return cuda_fail(e);
     if ((e = cudaMemcpyAsync(din, hin, nin * sizeof(double), cudaMemcpyHostToDevice, st)) != cudaSuccess) return cuda_fail(e);
-    if ((e = uw_fp64_launch(&A, s.block, st)) != cudaSuccess) return cuda_fail(e);
+    if ((rc = enqueue(*d, A, st)) != UWSHCU_OK) return rc;
     if ((e = cudaMemcpyAsync(hout, dout, nout * sizeof(double), cudaMemcpyDeviceToHost, st)) != cudaSuccess) return cuda_fail(e);
     if ((e = cudaMemcpyAsync(hin + (A.cush - din), A.cush, n * sizeof(double), cudaMemcpyDeviceToHost, st)) != cudaSuccess) return cuda_fail(e);
     if ((e = cudaMemcpyAsync(&hbits, d->d_err, sizeof(unsigned int), cudaMemcpyDeviceToHost, st)) != cudaSuccess) return cuda_fail(e);
@@ -435,6 +511,54 @@ int uwshcu_set_precision(int mode)
     return UWSHCU_OK;
 }
 
+int uwshcu_set_schedule(int schedule)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    if (schedule != UWSHCU_SCHED_SINGLE_PASS && schedule != UWSHCU_SCHED_TWO_PHASE) return UWSHCU_ERR_BAD_ARGS;
+    s.schedule = schedule;
+    return UWSHCU_OK;
+}
+
+int uwshcu_set_profiling(int on)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    s.profiling = on != 0;
+    for (int dv = 0; dv < kMaxDev; dv++) s.dev[dv].nrec = 0;
+    return UWSHCU_OK;
+}
+
+int uwshcu_profile_read(int* calls, double* trigger_ms, double* list_ms, int* list_columns)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    if (!calls || !trigger_ms || !list_ms) return UWSHCU_ERR_BAD_ARGS;
+    *calls = 0;
+    *trigger_ms = 0.0;
+    *list_ms = 0.0;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev) return UWSHCU_ERR_NO_DEVICE;
+    DeviceState& d = s.dev[dev];
+    cudaError_t e;
+    for (int n = 0; n < d.nrec; n++) {
+        float a = 0.f, b = 0.f;
+        if ((e = cudaEventSynchronize(d.ev[n][2])) != cudaSuccess) return cuda_fail(e);
+        if ((e = cudaEventElapsedTime(&a, d.ev[n][0], d.ev[n][1])) != cudaSuccess) return cuda_fail(e);
+        if ((e = cudaEventElapsedTime(&b, d.ev[n][1], d.ev[n][2])) != cudaSuccess) return cuda_fail(e);
+        *trigger_ms += a;
+        *list_ms += b;
+    }
+    *calls = d.nrec;
+    if (list_columns) {
+        int cnt = 0;
+        if (d.d_wl && (e = cudaMemcpy(&cnt, d.d_wl, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess) return cuda_fail(e);
+        *list_columns = cnt;
+    }
+    d.nrec = 0;
+    return UWSHCU_OK;
+}
+
 int uwshcu_set_block(int threads)
 {
     State& s = S();
@@ -468,6 +592,10 @@ int uwshcu_finalize(void)
         if (d.d_buf) cudaFree(d.d_buf);
         if (d.h_buf) cudaFreeHost(d.h_buf);
         if (d.d_err) cudaFree(d.d_err);
+        if (d.d_wl) cudaFree(d.d_wl);
+        for (int n = 0; n < DeviceState::kSlots; n++)
+            for (int j = 0; j < 3; j++)
+                if (d.ev[n][j]) cudaEventDestroy(d.ev[n][j]);
         if (d.stream) cudaStreamDestroy(d.stream);
         d = DeviceState{};
     }
@@ -600,9 +728,7 @@ int uwshcu_compute_device(int mix, int mkx, int iend, int ncnst, double dt, int 
     A.cufrc = cufrc; A.qcu = qcu; A.qlu = qlu; A.qiu = qiu; A.cbmf = cbmf; A.qc = qc; A.rliq = rliq;
     A.cnt = cnt; A.cnb = cnb; A.dpdry0 = dpdry0; A.wu = wu; A.diag_int = diag_int; A.diag_real = diag_real;
     A.err = d->d_err;
-    cudaError_t e = uw_fp64_launch(&A, s.block, (cudaStream_t)stream);
-    if (e != cudaSuccess) return cuda_fail(e);
-    return UWSHCU_OK;
+    return enqueue(*d, A, (cudaStream_t)stream);
 }
 
 int uwshcu_device_status(void* stream)

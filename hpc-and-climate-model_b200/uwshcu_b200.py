@@ -32,7 +32,8 @@ ERR_NO_DEVICE = -4
 ERR_ALLOC = -5
 
 EXPORTS = ("uwshcu_init", "uwshcu_set_rpen", "uwshcu_init_default", "uwshcu_set_precision",
-           "uwshcu_set_block", "uwshcu_get_estbl", "uwshcu_finalize", "uwshcu_last_cuda_error",
+           "uwshcu_set_block", "uwshcu_set_schedule", "uwshcu_set_profiling",
+           "uwshcu_profile_read", "uwshcu_get_estbl", "uwshcu_finalize", "uwshcu_last_cuda_error",
            "compute_uwshcu_", "compute_uwshcu_inv_", "bxcompute_uwshcu_inv_",
            "uwshcu_compute_device", "uwshcu_device_status")
 
@@ -72,6 +73,27 @@ def init(xlv, cp, xlf, zvir, r, g, ep2, tmin, tmax, ttrice, icephs, epsqs, rgasv
 
 def set_rpen(rpen):
     return lib().uwshcu_set_rpen(ctypes.c_double(rpen))
+
+
+SCHED_SINGLE_PASS = 0
+SCHED_TWO_PHASE = 1
+
+
+def set_schedule(schedule):
+    return lib().uwshcu_set_schedule(ctypes.c_int(schedule))
+
+
+def set_profiling(on):
+    return lib().uwshcu_set_profiling(ctypes.c_int(1 if on else 0))
+
+
+def profile_read():
+    """(calls, trigger_ms, list_ms, worklist length of the last call) since the previous read."""
+    n, a, b, c = ctypes.c_int(), ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+    rc = lib().uwshcu_profile_read(ctypes.byref(n), ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+    if rc != 0:
+        raise RuntimeError("uwshcu_profile_read: %d" % rc)
+    return n.value, a.value, b.value, c.value
 
 
 def set_block(threads):

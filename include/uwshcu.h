@@ -58,6 +58,22 @@ int uwshcu_init_default(void);
 /* Precision of the device path: UWSHCU_PREC_FP64. */
 int uwshcu_set_precision(int mode);
 
+/* Kernel schedules (uwshcu_set_schedule). */
+#define UWSHCU_SCHED_SINGLE_PASS 0       /* one launch, every column runs the whole scheme          */
+#define UWSHCU_SCHED_TWO_PHASE 1         /* default: trigger pass over all columns, then the
+                                            convecting columns from a device worklist             */
+
+/* Select the kernel schedule; both give identical results. */
+int uwshcu_set_schedule(int schedule);
+
+/* Opt-in timing of the two-phase schedule: when on, every call records CUDA events on its stream
+ * around the trigger launch and the worklist launch (up to 256 calls between reads). */
+int uwshcu_set_profiling(int on);
+
+/* Wait for the recorded calls and return their number, the summed device time of the trigger and
+ * worklist launches in milliseconds and (optional) the worklist length of the last call; resets. */
+int uwshcu_profile_read(int *calls, double *trigger_ms, double *list_ms, int *list_columns);
+
 /* Threads per block of the column kernel (0 = built-in default). */
 int uwshcu_set_block(int threads);
 

@@ -90,3 +90,20 @@ def test_repeat_calls_are_deterministic(uw, cuda):
     assert rc1 == rc2 == 0
     for f in FIELDS:
         assert np.array_equal(o1[f], o2[f]), f
+
+
+def test_schedules_agree_bit_for_bit(uw, cuda):
+    """The single-pass and the two-phase (trigger pass + worklist) schedules compute the same
+    column code on the same inputs."""
+    s = soundings.make_soundings(5000, 30, seed=61)
+    outs = []
+    try:
+        for sched in (uw.SCHED_SINGLE_PASS, uw.SCHED_TWO_PHASE):
+            assert uw.set_schedule(sched) == 0
+            rc, o = uw.compute_host(s)
+            assert rc == 0
+            outs.append(o)
+    finally:
+        uw.set_schedule(uw.SCHED_TWO_PHASE)
+    for f in FIELDS:
+        assert np.array_equal(outs[0][f], outs[1][f]), f
