@@ -26,6 +26,8 @@ UNITS = {
     "uwshcu_fp64_k64n5.cu": ["-fmad=false"],
     "uwshcu_fp64_k32n32.cu": ["-fmad=false"],
     "uwshcu_fp64_k64n32.cu": ["-fmad=false"],
+    "uwshcu_mixed_k32n5.cu": [],
+    "uwshcu_mixed_k64n5.cu": [],
     "uwshcu_host.cu": [],
 }
 

@@ -12,8 +12,9 @@
 // lookups of neighbouring threads do not serialise the way __constant__ reads would.
 //
 // Numerics: every expression keeps the Fortran evaluation order, the file is built with -fmad=false
-// (no FMA contraction) and IEEE division/sqrt, so the only differences to the CPU restatement are the
-// last-bit differences of pow/exp/log/erfc between CUDA's libdevice and glibc.  exnf(p) = (p/p00)**rovcp
+// (no FMA contraction) and IEEE division/sqrt, and pow/exp/log/erfc are the routines of uw_math.h,
+// which give the same bits on the host and the device; the CPU restatement built with the same
+// routines therefore computes the same bits as this kernel.  exnf(p) = (p/p00)**rovcp
 // is evaluated once per distinct pressure and passed into conden: conden at p = ps0(k), p0(k), pe,
 // prel, plcl or the cloud top recomputes exactly these values in the Fortran, so the result is the
 // same bit for bit and the per-call pow disappears from the Newton loop.
@@ -30,6 +31,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include "uwshcu_common.cuh"
+#include "uw_math.h"
 
 namespace {
 
@@ -90,7 +92,7 @@ __device__ __forceinline__ double qsat_qs(double t, double p, const double* __re
     return qs;
 }
 
-__device__ __forceinline__ double exnf(double p) { return pow(p / c.p00, c.rovcp); }
+__device__ __forceinline__ double exnf(double p) { return uw_pow(p / c.p00, c.rovcp); }
 
 // conden (uwshcu.F90:4718-4785) with ex = exnf(p) supplied by the caller.
 __device__ __forceinline__ int conden(double p, double ex, double thl, double qt, double& th, double& qv,
@@ -174,12 +176,12 @@ __device__ double qsinvert(double qt, double thl, double psfc, double exsfc, con
     qsat3(Ti, psfc, es, qs, gam, tbl);
     double rhi = qt / qs;
     if (rhi <= 0.01) return psmin;
-    double TLCL = 55.0 + 1.0 / (1.0 / (Ti - 55.0) - log(rhi) / 2840.0);
+    double TLCL = 55.0 + 1.0 / (1.0 / (Ti - 55.0) - uw_log(rhi) / 2840.0);
     double PiLCL = TLCL / thl;
-    double ps = c.p00 * pow(PiLCL, 1.0 / c.rovcp);
+    double ps = c.p00 * uw_pow(PiLCL, 1.0 / c.rovcp);
 #pragma unroll 1
     for (int i = 1; i <= 10; i++) {
-        double Pis = pow(ps / c.p00, c.rovcp);
+        double Pis = uw_pow(ps / c.p00, c.rovcp);
         double Ts = thl * Pis;
         qsat3(Ts, ps, es, qs, gam, tbl);
         double err = qt - qs;
@@ -204,7 +206,7 @@ __device__ double compute_alpha(double del_CIN, double ke)
     double x0 = 0.0;
 #pragma unroll 1
     for (int it = 0; it < 10; it++) {
-        double x1 = x0 - (exp(-x0 * ke * del_CIN) - x0) / (-ke * del_CIN * exp(-x0 * ke * del_CIN) - 1.0);
+        double x1 = x0 - (uw_exp(-x0 * ke * del_CIN) - x0) / (-ke * del_CIN * uw_exp(-x0 * ke * del_CIN) - 1.0);
         x0 = x1;
     }
     return x0;
@@ -216,8 +218,8 @@ __device__ double compute_mumin2(double mulcl, double rmaxfrac, double mulow)
     double x0 = mulow;
 #pragma unroll 1
     for (int it = 0; it < 10; it++) {
-        double ex = exp(-(x0 * x0));
-        double ef = erfc(x0);
+        double ex = uw_exp(-(x0 * x0));
+        double ef = uw_erfc(x0);
         double exf = ex / ef;
         double t1 = ex / 2.0 / rmaxfrac;
         double t2 = mulcl * 2.5066 / 2.0;
@@ -243,9 +245,9 @@ __device__ double compute_ppen(double wtwb, double D, double bogbot, double bogt
         else x0 = 0.0;
 #pragma unroll 1
         for (int it = 0; it < 5; it++) {
-            double f = exp(-2.0 * D * x0) * (wtwb - (bogbot - SB / (2.0 * D)) / (D * rho0j)) +
+            double f = uw_exp(-2.0 * D * x0) * (wtwb - (bogbot - SB / (2.0 * D)) / (D * rho0j)) +
                        (SB * x0 + bogbot - SB / (2.0 * D)) / (D * rho0j);
-            double fs = -2.0 * D * exp(-2.0 * D * x0) * (wtwb - (bogbot - SB / (2.0 * D)) / (D * rho0j)) +
+            double fs = -2.0 * D * uw_exp(-2.0 * D * x0) * (wtwb - (bogbot - SB / (2.0 * D)) / (D * rho0j)) +
                         (SB) / (D * rho0j);
             if (fs >= 0.0) fs = MX(fs, 1.e-10);
             else fs = MN(fs, -1.e-10);
@@ -317,7 +319,7 @@ __device__ __forceinline__ void fluxbelowinv(double cbmf, const double* ps0, int
 // findsp (uwshcu.F90:5164-5454) for one point; returns the wet-bulb qsp and ORs error bits.
 __device__ double findsp_point(double q, double t, double p, unsigned int& errbits, const double* __restrict__ tbl)
 {
-    const double omeps = 1.0 - c.epsqs, trinv = 1.0 / c.ttrice, a1 = 7.5 * log(10.0), rair = 287.04;
+    const double omeps = 1.0 - c.epsqs, trinv = 1.0 / c.ttrice, a1 = 7.5 * uw_log(10.0), rair = 287.04;
     const double c3 = rair * a1 / c.cpws, dttol = 1.e-4, dqtol = 1.e-4, tt0 = 273.15;
     double dtt = 0.0, dq = 0.0, enin, enout = 1.0, tsp, qsp, hltalt = 0.0;
     int doit = 0;
@@ -503,7 +505,7 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
     for (int k = 0; k <= mkx; k++) {
         ps0[k] = GI(ps0, k);
         zs0[k] = GI(zs0, k);
-        exns0[k] = pow(ps0[k] / p00, rovcp);
+        exns0[k] = uw_pow(ps0[k] / p00, rovcp);
     }
     for (int k = 1; k <= mkx; k++) {
         p0[k] = GL(p0, k);
@@ -513,7 +515,7 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
         qi0[k] = GL(qi0, k);
         t0[k] = GL(t0, k);
         s0[k] = GL(s0, k);
-        exn0[k] = pow(p0[k] / p00, rovcp);
+        exn0[k] = uw_pow(p0[k] / p00, rovcp);
         qt0[k] = (qv0[k] + ql0[k] + qi0[k]);
         thl0[k] = (t0[k] - xlv * ql0[k] / cp - xls * qi0[k] / cp) / exn0[k];
         qw0[k] = findsp_point(qv0[k], t0[k], p0[k], errbits, tbl);
@@ -825,13 +827,13 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                 goto l333;
             }
             double rho0inv = ps0[kinv - 1] / (r * thv0top[kinv - 1] * exns0[kinv - 1]);
-            cbmf = (rho0inv * sigmaw / 2.5066) * exp(-(mu * mu));
+            cbmf = (rho0inv * sigmaw / 2.5066) * uw_exp(-(mu * mu));
             double cbmflimit = 0.9 * dp0[kinv - 1] / g / dt;
             double mumin0 = 0.0;
-            if (cbmf > cbmflimit) mumin0 = sqrt(-log(2.5066 * cbmflimit / rho0inv / sigmaw));
+            if (cbmf > cbmflimit) mumin0 = sqrt(-uw_log(2.5066 * cbmflimit / rho0inv / sigmaw));
             mu = MX(MX(mu, mumin0), mumin1);
             double mulcl = sqrt(2.0 * cinlcl * rbuoy) / 1.4142 / sigmaw;
-            double ta = exp(-(mu * mu)) / 2.5066, te = erfc(mu);
+            double ta = uw_exp(-(mu * mu)) / 2.5066, te = uw_erfc(mu);
             double mulclstar = sqrt(MX(0.0, 2.0 * (ta * ta) * (1.0 / (te * te) - 0.25 / (rmaxfrac * rmaxfrac))));
             if (mulcl > 1.e-8 && mulcl > mulclstar) {
                 double mumin2 = compute_mumin2(mulcl, rmaxfrac, mu);
@@ -841,8 +843,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
             }
             if (mu == mumin0) lflags |= UW_L_CBMF;
             if (mu == mumin1) lflags |= UW_L_UFRC;
-            cbmf = (rho0inv * sigmaw / 2.5066) * exp(-(mu * mu));
-            double winv = sigmaw * (2.0 / 2.5066) * exp(-(mu * mu)) / erfc(mu);
+            cbmf = (rho0inv * sigmaw / 2.5066) * uw_exp(-(mu * mu));
+            double winv = sigmaw * (2.0 / 2.5066) * uw_exp(-(mu * mu)) / uw_erfc(mu);
             wtw = winv * winv - 2.0 * cinlcl * rbuoy;
             if (wtw <= 0.0) {
                 xflags |= UW_X_WTW;
@@ -998,10 +1000,10 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                         double ee2 = xc * xc;
                         double ud2 = 1.0 - 2.0 * xc + xc * xc;
                         rei[k] = (0.5 * rkm / GL(z0, k) / g / rho0j);
-                        if (xc > 0.5) rei[k] = MN(rei[k], 0.9 * log(dp0[k] / g / dt / umf[km1] + 1.0) / dpe / (2.0 * xc - 1.0));
+                        if (xc > 0.5) rei[k] = MN(rei[k], 0.9 * uw_log(dp0[k] / g / dt / umf[km1] + 1.0) / dpe / (2.0 * xc - 1.0));
                         fer[k] = rei[k] * ee2;
                         fdr[k] = rei[k] * ud2;
-                        umf[k] = umf[km1] * exp(dpe * (fer[k] - fdr[k]));
+                        umf[k] = umf[km1] * uw_exp(dpe * (fer[k] - fdr[k]));
                         emf[k] = 0.0;
                         if (fer[k] * dpe < 1.e-4) {
                             thlu[k] = thlu[km1] + (thle + ssthl0[k] * dpe / 2.0 - thlu[km1]) * fer[k] * dpe;
@@ -1011,7 +1013,7 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                             for (int m = 0; m < ncnst; m++)
                                 tru[m][k] = tru[m][km1] + (tre[m] + sstr0[m][k] * dpe / 2.0 - tru[m][km1]) * fer[k] * dpe;
                         } else {
-                            const double ef = exp(-fer[k] * dpe);
+                            const double ef = uw_exp(-fer[k] * dpe);
                             thlu[k] = (thle + ssthl0[k] / fer[k] - ssthl0[k] * dpe / 2.0) -
                                       (thle + ssthl0[k] * dpe / 2.0 - thlu[km1] + ssthl0[k] / fer[k]) * ef;
                             qtu[k] = (qte + ssqt0[k] / fer[k] - ssqt0[k] * dpe / 2.0) -
@@ -1050,7 +1052,7 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                         bogtop = rbuoy * (thvu[k] / thv0top[k] - 1.0);
                         double delbog = bogtop - bogbot;
                         drage = fer[k] * (1.0 + rdrag);
-                        double expfac = exp(-2.0 * drage * dpe);
+                        double expfac = uw_exp(-2.0 * drage * dpe);
                         wtwb = wtw;
                         if (drage * dpe > 1.e-3)
                             wtw = wtw * expfac + (delbog + (1.0 - expfac) * (bogbot + delbog / (-2.0 * drage * dpe))) / (rho0j * drage);
@@ -1084,7 +1086,7 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                             lflags |= UW_L_UFRC;
                             ufrc[k] = rmaxfrac;
                             umf[k] = rmaxfrac * rhos0j * wu[k];
-                            fdr[k] = fer[k] - log(umf[k] / umf[km1]) / dpe;
+                            fdr[k] = fer[k] - uw_log(umf[k] / umf[km1]) / dpe;
                         }
                     }
                     pe = p0[k + 1];
@@ -1125,13 +1127,13 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                     thlu_top = thlu[kpen - 1] + (thl0[kpen] + ssthl0[kpen] * (-ppen) / 2.0 - thlu[kpen - 1]) * fer[kpen] * (-ppen);
                     qtu_top = qtu[kpen - 1] + (qt0[kpen] + ssqt0[kpen] * (-ppen) / 2.0 - qtu[kpen - 1]) * fer[kpen] * (-ppen);
                 } else {
-                    const double ef = exp(-fer[kpen] * (-ppen));
+                    const double ef = uw_exp(-fer[kpen] * (-ppen));
                     thlu_top = (thl0[kpen] + ssthl0[kpen] / fer[kpen] - ssthl0[kpen] * (-ppen) / 2.0) -
                                (thl0[kpen] + ssthl0[kpen] * (-ppen) / 2.0 - thlu[kpen - 1] + ssthl0[kpen] / fer[kpen]) * ef;
                     qtu_top = (qt0[kpen] + ssqt0[kpen] / fer[kpen] - ssqt0[kpen] * (-ppen) / 2.0) -
                               (qt0[kpen] + ssqt0[kpen] * (-ppen) / 2.0 - qtu[kpen - 1] + ssqt0[kpen] / fer[kpen]) * ef;
                 }
-                exntop = pow((ps0[kpen - 1] + ppen) / p00, rovcp);
+                exntop = uw_pow((ps0[kpen - 1] + ppen) / p00, rovcp);
                 if (conden(ps0[kpen - 1] + ppen, exntop, thlu_top, qtu_top, thj, qvj, qlj, qij, tbl)) {
                     xflags |= UW_X_CONDEN;
                     id_exit = true;

@@ -18,6 +18,7 @@
 
 #include "uwshcu.h"
 #include "uwshcu_common.cuh"
+#include "uw_math.h"
 
 #define UW_DECL(KP, NC)                                                                              \
     extern "C" cudaError_t uw_fp64_set_constants_k##KP##n##NC(const UwConst* h, const double* tbl); \
@@ -28,6 +29,13 @@ UW_DECL(64, 5)
 UW_DECL(32, 32)
 UW_DECL(64, 32)
 #undef UW_DECL
+#define UW_DECL_MIXED(KP, NC)                                                                              \
+    extern "C" cudaError_t uw_mixed_set_constants_k##KP##n##NC(const UwConst* h, const double* tbl);       \
+    extern "C" cudaError_t uw_mixed_launch_k##KP##n##NC(const UwArgs* a, int mode, int* wl, int* wl_count, \
+                                                        int nthreads, int block, cudaStream_t stream);
+UW_DECL_MIXED(32, 5)
+UW_DECL_MIXED(64, 5)
+#undef UW_DECL_MIXED
 
 namespace {
 
@@ -40,12 +48,19 @@ cudaError_t set_constants_all(const UwConst* k, const double* tbl)
     if ((e = uw_fp64_set_constants_k32n5(k, tbl)) != cudaSuccess) return e;
     if ((e = uw_fp64_set_constants_k64n5(k, tbl)) != cudaSuccess) return e;
     if ((e = uw_fp64_set_constants_k32n32(k, tbl)) != cudaSuccess) return e;
-    return uw_fp64_set_constants_k64n32(k, tbl);
+    if ((e = uw_fp64_set_constants_k64n32(k, tbl)) != cudaSuccess) return e;
+    if ((e = uw_mixed_set_constants_k32n5(k, tbl)) != cudaSuccess) return e;
+    return uw_mixed_set_constants_k64n5(k, tbl);
 }
 
-cudaError_t launch_mode(const UwArgs* a, int mode, int* wl, int* wl_count, int nthreads, int block,
+cudaError_t launch_mode(const UwArgs* a, int prec, int mode, int* wl, int* wl_count, int nthreads, int block,
                         cudaStream_t st)
 {
+    if (prec == UWSHCU_PREC_MIXED) {
+        if (a->mkx + 1 <= 32 && a->ncnst <= 5) return uw_mixed_launch_k32n5(a, mode, wl, wl_count, nthreads, block, st);
+        if (a->mkx + 1 <= 64 && a->ncnst <= 5) return uw_mixed_launch_k64n5(a, mode, wl, wl_count, nthreads, block, st);
+        return cudaErrorInvalidValue;
+    }
     if (a->mkx + 1 <= 32 && a->ncnst <= 5) return uw_fp64_launch_k32n5(a, mode, wl, wl_count, nthreads, block, st);
     if (a->mkx + 1 <= 64 && a->ncnst <= 5) return uw_fp64_launch_k64n5(a, mode, wl, wl_count, nthreads, block, st);
     if (a->mkx + 1 <= 32 && a->ncnst <= UW_NCMAX) return uw_fp64_launch_k32n32(a, mode, wl, wl_count, nthreads, block, st);
@@ -254,7 +269,7 @@ int enqueue(DeviceState& d, const UwArgs& A, cudaStream_t st)
     State& s = S();
     cudaError_t e;
     if (s.schedule == UWSHCU_SCHED_SINGLE_PASS) {
-        if ((e = launch_mode(&A, kModeAll, nullptr, nullptr, A.iend, s.block, st)) != cudaSuccess) return cuda_fail(e);
+        if ((e = launch_mode(&A, s.precision, kModeAll, nullptr, nullptr, A.iend, s.block, st)) != cudaSuccess) return cuda_fail(e);
         return UWSHCU_OK;
     }
     int rc = grow_worklist(d, (size_t)A.iend);
@@ -270,15 +285,16 @@ int enqueue(DeviceState& d, const UwArgs& A, cudaStream_t st)
     }
     if ((e = cudaMemsetAsync(count, 0, sizeof(int), st)) != cudaSuccess) return cuda_fail(e);
     if (ev && (e = cudaEventRecord(ev[0], st)) != cudaSuccess) return cuda_fail(e);
-    if ((e = launch_mode(&A, kModeTrigger, list, count, A.iend, s.block, st)) != cudaSuccess) return cuda_fail(e);
+    if ((e = launch_mode(&A, s.precision, kModeTrigger, list, count, A.iend, s.block, st)) != cudaSuccess) return cuda_fail(e);
     if (ev && (e = cudaEventRecord(ev[1], st)) != cudaSuccess) return cuda_fail(e);
-    if ((e = launch_mode(&A, kModeList, list, count, A.iend, s.block, st)) != cudaSuccess) return cuda_fail(e);
+    if ((e = launch_mode(&A, s.precision, kModeList, list, count, A.iend, s.block, st)) != cudaSuccess) return cuda_fail(e);
     if (ev && (e = cudaEventRecord(ev[2], st)) != cudaSuccess) return cuda_fail(e);
     return UWSHCU_OK;
 }
 
 bool bad_dims(int mix, int mkx, int iend, int ncnst)
 {
+    if (S().precision == UWSHCU_PREC_MIXED && ncnst > 5) return true;
     return mix < 1 || mkx < 3 || mkx > UWSHCU_MAX_LEVELS || iend < 0 || iend > mix || ncnst < 3 ||
            ncnst > UWSHCU_MAX_TRACERS || ncnst != S().k.ncnst;
 }
@@ -414,6 +430,21 @@ int host_call(int inv, int mix, int mkx, int iend, int ncnst, double dt, const d
     return status_from_bits(hbits);
 }
 
+__global__ void eval_math_kernel(int fn, const double* __restrict__ x, const double* __restrict__ y,
+                                 double* __restrict__ out, int n)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double v;
+    switch (fn) {
+    case 0: v = uw_exp(x[i]); break;
+    case 1: v = uw_log(x[i]); break;
+    case 2: v = uw_pow(x[i], y[i]); break;
+    default: v = uw_erfc(x[i]); break;
+    }
+    out[i] = v;
+}
+
 }  // namespace
 
 // ================================================================================== C ABI ======
@@ -506,7 +537,7 @@ int uwshcu_set_precision(int mode)
 {
     State& s = S();
     std::lock_guard<std::mutex> lock(s.mu);
-    if (mode != UWSHCU_PREC_FP64) return UWSHCU_ERR_BAD_ARGS;
+    if (mode != UWSHCU_PREC_FP64 && mode != UWSHCU_PREC_MIXED) return UWSHCU_ERR_BAD_ARGS;
     s.precision = mode;
     return UWSHCU_OK;
 }
@@ -729,6 +760,19 @@ int uwshcu_compute_device(int mix, int mkx, int iend, int ncnst, double dt, int 
     A.cnt = cnt; A.cnb = cnb; A.dpdry0 = dpdry0; A.wu = wu; A.diag_int = diag_int; A.diag_real = diag_real;
     A.err = d->d_err;
     return enqueue(*d, A, (cudaStream_t)stream);
+}
+
+int uwshcu_eval_math(int fn, const double* x, const double* y, double* out, int n, void* stream)
+{
+    if (fn < 0 || fn > 3 || n < 0 || (n > 0 && (!x || !out || (fn == 2 && !y)))) return UWSHCU_ERR_BAD_ARGS;
+    if (n == 0) return UWSHCU_OK;
+    eval_math_kernel<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(fn, x, fn == 2 ? y : x, out, n);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        std::lock_guard<std::mutex> lock(S().mu);
+        return cuda_fail(e);
+    }
+    return UWSHCU_OK;
 }
 
 int uwshcu_device_status(void* stream)

@@ -35,7 +35,7 @@ EXPORTS = ("uwshcu_init", "uwshcu_set_rpen", "uwshcu_init_default", "uwshcu_set_
            "uwshcu_set_block", "uwshcu_set_schedule", "uwshcu_set_profiling",
            "uwshcu_profile_read", "uwshcu_get_estbl", "uwshcu_finalize", "uwshcu_last_cuda_error",
            "compute_uwshcu_", "compute_uwshcu_inv_", "bxcompute_uwshcu_inv_",
-           "uwshcu_compute_device", "uwshcu_device_status")
+           "uwshcu_compute_device", "uwshcu_device_status", "uwshcu_eval_math")
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
@@ -73,6 +73,14 @@ def init(xlv, cp, xlf, zvir, r, g, ep2, tmin, tmax, ttrice, icephs, epsqs, rgasv
 
 def set_rpen(rpen):
     return lib().uwshcu_set_rpen(ctypes.c_double(rpen))
+
+
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+
+def set_precision(mode):
+    return lib().uwshcu_set_precision(ctypes.c_int(mode))
 
 
 SCHED_SINGLE_PASS = 0
@@ -222,3 +230,19 @@ class DeviceCase:
             o["diag_int"] = self.diag_int.cpu().numpy()
             o["diag_real"] = self.diag_real.cpu().numpy()
         return o
+
+
+def eval_math_device(fn, x, y=None):
+    """Evaluate the library's exp/log/pow/erfc (fn 0..3) on the GPU for numpy inputs."""
+    import torch
+    xd = torch.from_numpy(np.ascontiguousarray(x, dtype=np.float64)).cuda()
+    yd = torch.from_numpy(np.ascontiguousarray(y if y is not None else x, dtype=np.float64)).cuda()
+    od = torch.empty_like(xd)
+    st = torch.cuda.current_stream()
+    rc = lib().uwshcu_eval_math(ctypes.c_int(fn), ctypes.c_void_p(xd.data_ptr()),
+                                ctypes.c_void_p(yd.data_ptr()), ctypes.c_void_p(od.data_ptr()),
+                                ctypes.c_int(xd.numel()), ctypes.c_void_p(st.cuda_stream))
+    if rc != 0:
+        raise RuntimeError("uwshcu_eval_math: %d" % rc)
+    st.synchronize()
+    return od.cpu().numpy()

@@ -34,6 +34,8 @@ extern "C" {
 
 /* Precision modes of the device path (uwshcu_set_precision). */
 #define UWSHCU_PREC_FP64 0               /* FP64 throughout, Fortran evaluation order, no FMA      */
+#define UWSHCU_PREC_MIXED 1              /* FP32 bulk, FP64 conden/roots/qsinvert/implicit CIN/
+                                            positive_moisture, Kahan vertical sums (ncnst <= 5)    */
 
 /* ---- set-up -------------------------------------------------------------------------------- */
 
@@ -55,7 +57,7 @@ int uwshcu_set_rpen(double rpen);
  * qmin = {1e-12, 0, 0, 0, 0}. */
 int uwshcu_init_default(void);
 
-/* Precision of the device path: UWSHCU_PREC_FP64. */
+/* Precision of the device path: UWSHCU_PREC_FP64 (default) or UWSHCU_PREC_MIXED. */
 int uwshcu_set_precision(int mode);
 
 /* Kernel schedules (uwshcu_set_schedule). */
@@ -179,6 +181,11 @@ int uwshcu_compute_device(int mix, int mkx, int iend, int ncnst, double dt, int 
 /* Wait for `stream` and return the status collected by the device calls enqueued on it since the
  * previous uwshcu_device_status call. */
 int uwshcu_device_status(void *stream);
+
+/* Evaluate the library's exp (fn 0), log (1), pow (2, with y) or erfc (3) on n device values, on
+ * the GPU, with the routines the kernels use.  They give the same bits as the host build of the
+ * same routines, which is what makes the FP64 path reproducible on the CPU. */
+int uwshcu_eval_math(int fn, const double *x, const double *y, double *out, int n, void *stream);
 
 #ifdef __cplusplus
 }

@@ -12,7 +12,9 @@ import subprocess
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_build", "libuwshcu_oracle.so")
+LIB_PATHS = {"glibc": os.path.join(HERE, "_build", "libuwshcu_oracle.so"),
+             "portable": os.path.join(HERE, "_build", "libuwshcu_oracle_pm.so")}
+LIB_PATH = LIB_PATHS["glibc"]
 
 OUT_IFACE = ("umf", "slflx", "qtflx", "flxprc1", "flxsnow1", "wu")
 OUT_LAYER = ("qvten", "qlten", "qiten", "sten", "uten", "vten", "qrten", "qsten", "evapc",
@@ -21,6 +23,7 @@ OUT_COL = ("precip", "snow", "cbmf", "rliq", "cnt", "cnb", "cush")
 NDI, NDR = 8, 8
 
 _lib = None
+_libs = {}
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
 
@@ -29,12 +32,24 @@ def build():
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
+def set_variant(variant):
+    """Select the oracle build: 'glibc' (transcendentals from glibc; pinned bit for bit to the
+    reference's drop-in) or 'portable' (the host/device-identical routines of uw_math.h that the
+    CUDA path uses).  Each build keeps its own constants; the selected one is initialised with the
+    default constants on first use."""
+    global _lib, LIB_PATH
+    LIB_PATH = LIB_PATHS[variant]
+    _lib = _libs.get(variant)
+    return lib()
+
+
 def lib():
     global _lib
     if _lib is None:
         if not os.path.exists(LIB_PATH):
             build()
         _lib = ctypes.CDLL(LIB_PATH)
+        _libs[[k for k, v in LIB_PATHS.items() if v == LIB_PATH][0] if LIB_PATH in LIB_PATHS.values() else LIB_PATH] = _lib
         _lib.uwo_init_default.restype = ctypes.c_int
         _lib.uwo_compute_uwshcu.restype = ctypes.c_int
         _lib.uwo_compute_uwshcu_inv.restype = ctypes.c_int
@@ -134,3 +149,12 @@ def consts():
     c = np.zeros(22)
     lib().uwo_get_consts(_p(c))
     return c
+
+
+def uwmath(fn, x, y=None):
+    """Host evaluation of uw_math.h: fn 0 exp, 1 log, 2 pow, 3 erfc."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.ascontiguousarray(y if y is not None else np.zeros_like(x), dtype=np.float64)
+    out = np.zeros_like(x)
+    lib().uwo_uwmath(ctypes.c_int(fn), _p(x), _p(y), _p(out), ctypes.c_int(x.size))
+    return out

@@ -24,6 +24,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include "uwshcu_oracle.h"
+#include "uw_math.h"
 #ifdef _OPENMP
 #include <omp.h>
 #define UWO_MAXTHREADS() omp_get_max_threads()
@@ -128,6 +129,21 @@ static void gestbl(double tmn, double tmx, double trice, int ip, double epsil, d
     S.pcf[5] = 0.0;
 }
 
+/* The column physics below calls EXP/LOG/POW/ERFC: glibc by default; with UWO_PORTABLE_MATH the
+ * host/device-identical routines of uw_math.h (hpc-and-climate-model_b200/csrc), which is how the
+ * CUDA path evaluates them.  The saturation table above always uses glibc, as the library does. */
+#ifdef UWO_PORTABLE_MATH
+#define EXP(x) uw_exp(x)
+#define LOG(x) uw_log(x)
+#define POW(x, y) uw_pow(x, y)
+#define ERFC(x) uw_erfc(x)
+#else
+#define EXP(x) exp(x)
+#define LOG(x) log(x)
+#define POW(x, y) pow(x, y)
+#define ERFC(x) erfc(x)
+#endif
+
 /* estblf (wv_saturation.F90:64-80) */
 static double estblf(double td)
 {
@@ -183,7 +199,7 @@ done:
 /* ---------------------------------------------------------------------------- uwshcu helpers */
 
 /* exnf (uwshcu.F90:50-54) */
-static double exnf(double p) { return pow(p / S.p00, S.rovcp); }
+static double exnf(double p) { return POW(p / S.p00, S.rovcp); }
 
 /* conden (uwshcu.F90:4718-4785) */
 static void conden(double p, double thl, double qt, double *th, double *qv, double *ql, double *qi,
@@ -270,15 +286,15 @@ static double qsinvert(double qt, double thl, double psfc)
     int i;
     psmin = 100.0 * 100.0;
     dpsmax = 1.0;
-    Ti = thl * pow(psfc / S.p00, S.rovcp);
+    Ti = thl * POW(psfc / S.p00, S.rovcp);
     qsat1(Ti, psfc, &es, &qs, &gam);
     rhi = qt / qs;
     if (rhi <= 0.01) return psmin;
-    TLCL = 55.0 + 1.0 / (1.0 / (Ti - 55.0) - log(rhi) / 2840.0);
+    TLCL = 55.0 + 1.0 / (1.0 / (Ti - 55.0) - LOG(rhi) / 2840.0);
     PiLCL = TLCL / thl;
-    ps = S.p00 * pow(PiLCL, 1.0 / S.rovcp);
+    ps = S.p00 * POW(PiLCL, 1.0 / S.rovcp);
     for (i = 1; i <= 10; i++) {
-        Pis = pow(ps / S.p00, S.rovcp);
+        Pis = POW(ps / S.p00, S.rovcp);
         Ts = thl * Pis;
         qsat1(Ts, ps, &es, &qs, &gam);
         err = qt - qs;
@@ -303,7 +319,7 @@ static double compute_alpha(double del_CIN, double ke)
     double x0 = 0.0, x1;
     int it;
     for (it = 1; it <= 10; it++) {
-        x1 = x0 - (exp(-x0 * ke * del_CIN) - x0) / (-ke * del_CIN * exp(-x0 * ke * del_CIN) - 1.0);
+        x1 = x0 - (EXP(-x0 * ke * del_CIN) - x0) / (-ke * del_CIN * EXP(-x0 * ke * del_CIN) - 1.0);
         x0 = x1;
     }
     return x0;
@@ -316,8 +332,8 @@ static double compute_mumin2(double mulcl, double rmaxfrac, double mulow)
     int it;
     x0 = mulow;
     for (it = 1; it <= 10; it++) {
-        ex = exp(-(x0 * x0));
-        ef = erfc(x0);
+        ex = EXP(-(x0 * x0));
+        ef = ERFC(x0);
         exf = ex / ef;
         t1 = ex / 2.0 / rmaxfrac;
         t2 = mulcl * 2.5066 / 2.0;
@@ -343,9 +359,9 @@ static double compute_ppen(double wtwb, double D, double bogbot, double bogtop, 
         if (s00 >= 0.0) x0 = dpen;
         else x0 = 0.0;
         for (it = 1; it <= 5; it++) {
-            f = exp(-2.0 * D * x0) * (wtwb - (bogbot - SB / (2.0 * D)) / (D * rho0j)) +
+            f = EXP(-2.0 * D * x0) * (wtwb - (bogbot - SB / (2.0 * D)) / (D * rho0j)) +
                 (SB * x0 + bogbot - SB / (2.0 * D)) / (D * rho0j);
-            fs = -2.0 * D * exp(-2.0 * D * x0) * (wtwb - (bogbot - SB / (2.0 * D)) / (D * rho0j)) +
+            fs = -2.0 * D * EXP(-2.0 * D * x0) * (wtwb - (bogbot - SB / (2.0 * D)) / (D * rho0j)) +
                  (SB) / (D * rho0j);
             if (fs >= 0.0) fs = MX(fs, 1.e-10);
             else fs = MN(fs, -1.e-10);
@@ -477,7 +493,7 @@ static int findsp_point(double q, double t, double p, double *tsp_o, double *qsp
     int doit, l, lflg, iter;
     omeps = 1.0 - S.epsqs;
     trinv = 1.0 / S.ttrice;
-    a1 = 7.5 * log(10.0);
+    a1 = 7.5 * LOG(10.0);
     rair = 287.04;
     c3 = rair * a1 / S.cpws;
     dttol = 1.e-4;
@@ -725,8 +741,8 @@ static int uw_column(const uwo_io *A, int i)
     cush = A->cush[i - 1];
 
     /* 1. environmental variables (:1255-1259) */
-    for (k = 1; k <= mkx; k++) exn0[k] = pow(p0[k] / p00, rovcp);
-    for (k = 0; k <= mkx; k++) exns0[k] = pow(ps0[k] / p00, rovcp);
+    for (k = 1; k <= mkx; k++) exn0[k] = POW(p0[k] / p00, rovcp);
+    for (k = 0; k <= mkx; k++) exns0[k] = POW(ps0[k] / p00, rovcp);
     for (k = 1; k <= mkx; k++) {
         qt0[k] = (qv0[k] + ql0[k] + qi0[k]);
         thl0[k] = (t0[k] - xlv * ql0[k] / cp - xls * qi0[k] / cp) / exn0[k];
@@ -1196,14 +1212,14 @@ static int uw_column(const uwo_io *A, int i)
             goto l333;
         }
         rho0inv = ps0[kinv - 1] / (r * thv0top[kinv - 1] * exns0[kinv - 1]);
-        cbmf = (rho0inv * sigmaw / 2.5066) * exp(-(mu * mu));
+        cbmf = (rho0inv * sigmaw / 2.5066) * EXP(-(mu * mu));
         cbmflimit = 0.9 * dp0[kinv - 1] / g / dt;
         mumin0 = 0.0;
-        if (cbmf > cbmflimit) mumin0 = sqrt(-log(2.5066 * cbmflimit / rho0inv / sigmaw));
+        if (cbmf > cbmflimit) mumin0 = sqrt(-LOG(2.5066 * cbmflimit / rho0inv / sigmaw));
         mu = MX(MX(mu, mumin0), mumin1);
         mulcl = sqrt(2.0 * cinlcl * rbuoy) / 1.4142 / sigmaw;
         {
-            double ta = exp(-(mu * mu)) / 2.5066, te = erfc(mu);
+            double ta = EXP(-(mu * mu)) / 2.5066, te = ERFC(mu);
             mulclstar = sqrt(MX(0.0, 2.0 * (ta * ta) * (1.0 / (te * te) - 0.25 / (rmaxfrac * rmaxfrac))));
         }
         if (mulcl > 1.e-8 && mulcl > mulclstar) {
@@ -1214,8 +1230,8 @@ static int uw_column(const uwo_io *A, int i)
         }
         if (mu == mumin0) lflags |= L_CBMF;
         if (mu == mumin1) lflags |= L_UFRC;
-        cbmf = (rho0inv * sigmaw / 2.5066) * exp(-(mu * mu));
-        winv = sigmaw * (2.0 / 2.5066) * exp(-(mu * mu)) / erfc(mu);
+        cbmf = (rho0inv * sigmaw / 2.5066) * EXP(-(mu * mu));
+        winv = sigmaw * (2.0 / 2.5066) * EXP(-(mu * mu)) / ERFC(mu);
         ufrcinv = cbmf / winv / rho0inv;
         (void)ufrcinv;
         wtw = winv * winv - 2.0 * cinlcl * rbuoy;
@@ -1377,10 +1393,10 @@ static int uw_column(const uwo_io *A, int i)
                     ee2 = xc * xc;
                     ud2 = 1.0 - 2.0 * xc + xc * xc;
                     rei[k] = (0.5 * rkm / z0[k] / g / rho0j);
-                    if (xc > 0.5) rei[k] = MN(rei[k], 0.9 * log(dp0[k] / g / dt / umf[km1] + 1.0) / dpe / (2.0 * xc - 1.0));
+                    if (xc > 0.5) rei[k] = MN(rei[k], 0.9 * LOG(dp0[k] / g / dt / umf[km1] + 1.0) / dpe / (2.0 * xc - 1.0));
                     fer[k] = rei[k] * ee2;
                     fdr[k] = rei[k] * ud2;
-                    umf[k] = umf[km1] * exp(dpe * (fer[k] - fdr[k]));
+                    umf[k] = umf[km1] * EXP(dpe * (fer[k] - fdr[k]));
                     emf[k] = 0.0;
                     if (fer[k] * dpe < 1.e-4) {
                         thlu[k] = thlu[km1] + (thle + ssthl0[k] * dpe / 2.0 - thlu[km1]) * fer[k] * dpe;
@@ -1391,16 +1407,16 @@ static int uw_column(const uwo_io *A, int i)
                             tru[m][k] = tru[m][km1] + (tre[m] + sstr0[m][k] * dpe / 2.0 - tru[m][km1]) * fer[k] * dpe;
                     } else {
                         thlu[k] = (thle + ssthl0[k] / fer[k] - ssthl0[k] * dpe / 2.0) -
-                                  (thle + ssthl0[k] * dpe / 2.0 - thlu[km1] + ssthl0[k] / fer[k]) * exp(-fer[k] * dpe);
+                                  (thle + ssthl0[k] * dpe / 2.0 - thlu[km1] + ssthl0[k] / fer[k]) * EXP(-fer[k] * dpe);
                         qtu[k] = (qte + ssqt0[k] / fer[k] - ssqt0[k] * dpe / 2.0) -
-                                 (qte + ssqt0[k] * dpe / 2.0 - qtu[km1] + ssqt0[k] / fer[k]) * exp(-fer[k] * dpe);
+                                 (qte + ssqt0[k] * dpe / 2.0 - qtu[km1] + ssqt0[k] / fer[k]) * EXP(-fer[k] * dpe);
                         uu[k] = (ue + (1.0 - PGFc) * ssu0[k] / fer[k] - ssu0[k] * dpe / 2.0) -
-                                (ue + ssu0[k] * dpe / 2.0 - uu[km1] + (1.0 - PGFc) * ssu0[k] / fer[k]) * exp(-fer[k] * dpe);
+                                (ue + ssu0[k] * dpe / 2.0 - uu[km1] + (1.0 - PGFc) * ssu0[k] / fer[k]) * EXP(-fer[k] * dpe);
                         vu[k] = (ve + (1.0 - PGFc) * ssv0[k] / fer[k] - ssv0[k] * dpe / 2.0) -
-                                (ve + ssv0[k] * dpe / 2.0 - vu[km1] + (1.0 - PGFc) * ssv0[k] / fer[k]) * exp(-fer[k] * dpe);
+                                (ve + ssv0[k] * dpe / 2.0 - vu[km1] + (1.0 - PGFc) * ssv0[k] / fer[k]) * EXP(-fer[k] * dpe);
                         for (m = 1; m <= ncnst; m++)
                             tru[m][k] = (tre[m] + sstr0[m][k] / fer[k] - sstr0[m][k] * dpe / 2.0) -
-                                        (tre[m] + sstr0[m][k] * dpe / 2.0 - tru[m][km1] + sstr0[m][k] / fer[k]) * exp(-fer[k] * dpe);
+                                        (tre[m] + sstr0[m][k] * dpe / 2.0 - tru[m][km1] + sstr0[m][k] / fer[k]) * EXP(-fer[k] * dpe);
                     }
                     conden(ps0[k], thlu[k], qtu[k], &thj, &qvj, &qlj, &qij, &qse, &id_check);
                     if (id_check == 1) {
@@ -1430,7 +1446,7 @@ static int uw_column(const uwo_io *A, int i)
                     bogtop = rbuoy * (thvu[k] / thv0top[k] - 1.0);
                     delbog = bogtop - bogbot;
                     drage = fer[k] * (1.0 + rdrag);
-                    expfac = exp(-2.0 * drage * dpe);
+                    expfac = EXP(-2.0 * drage * dpe);
                     wtwb = wtw;
                     if (drage * dpe > 1.e-3)
                         wtw = wtw * expfac + (delbog + (1.0 - expfac) * (bogbot + delbog / (-2.0 * drage * dpe))) / (rho0j * drage);
@@ -1463,7 +1479,7 @@ static int uw_column(const uwo_io *A, int i)
                     lflags |= L_UFRC;
                     ufrc[k] = rmaxfrac;
                     umf[k] = rmaxfrac * rhos0j * wu[k];
-                    fdr[k] = fer[k] - log(umf[k] / umf[km1]) / dpe;
+                    fdr[k] = fer[k] - LOG(umf[k] / umf[km1]) / dpe;
                 }
                 pe = p0[k + 1];
                 dpe = dp0[k + 1];
@@ -1505,9 +1521,9 @@ static int uw_column(const uwo_io *A, int i)
                 qtu_top = qtu[kpen - 1] + (qt0[kpen] + ssqt0[kpen] * (-ppen) / 2.0 - qtu[kpen - 1]) * fer[kpen] * (-ppen);
             } else {
                 thlu_top = (thl0[kpen] + ssthl0[kpen] / fer[kpen] - ssthl0[kpen] * (-ppen) / 2.0) -
-                           (thl0[kpen] + ssthl0[kpen] * (-ppen) / 2.0 - thlu[kpen - 1] + ssthl0[kpen] / fer[kpen]) * exp(-fer[kpen] * (-ppen));
+                           (thl0[kpen] + ssthl0[kpen] * (-ppen) / 2.0 - thlu[kpen - 1] + ssthl0[kpen] / fer[kpen]) * EXP(-fer[kpen] * (-ppen));
                 qtu_top = (qt0[kpen] + ssqt0[kpen] / fer[kpen] - ssqt0[kpen] * (-ppen) / 2.0) -
-                          (qt0[kpen] + ssqt0[kpen] * (-ppen) / 2.0 - qtu[kpen - 1] + ssqt0[kpen] / fer[kpen]) * exp(-fer[kpen] * (-ppen));
+                          (qt0[kpen] + ssqt0[kpen] * (-ppen) / 2.0 - qtu[kpen - 1] + ssqt0[kpen] / fer[kpen]) * EXP(-fer[kpen] * (-ppen));
             }
             conden(ps0[kpen - 1] + ppen, thlu_top, qtu_top, &thj, &qvj, &qlj, &qij, &qse, &id_check);
             if (id_check == 1) {
@@ -1515,7 +1531,7 @@ static int uw_column(const uwo_io *A, int i)
                 id_exit = 1;
                 goto l333;
             }
-            exntop = pow((ps0[kpen - 1] + ppen) / p00, rovcp);
+            exntop = POW((ps0[kpen - 1] + ppen) / p00, rovcp);
             if ((qlj + qij) > criqc) {
                 dwten[kpen] = ((qlj + qij) - criqc) * qlj / (qlj + qij);
                 diten[kpen] = ((qlj + qij) - criqc) * qij / (qlj + qij);
@@ -2449,4 +2465,18 @@ void uwo_positive_moisture_single(double xlv, double xls, int mkx, double dt, do
     /* 0-based arrays from the caller; shift to the 1-based internal form */
     positive_moisture_single(xlv, xls, mkx, dt, qvmin, qlmin, qimin, dp - 1, qv - 1, ql - 1, qi - 1,
                              s - 1, qvten - 1, qlten - 1, qiten - 1, sten - 1);
+}
+
+/* Evaluate the uw_math.h routines on the host (fn: 0 exp, 1 log, 2 pow, 3 erfc). */
+void uwo_uwmath(int fn, const double *x, const double *y, double *out, int n)
+{
+    int i;
+    for (i = 0; i < n; i++) {
+        switch (fn) {
+        case 0: out[i] = uw_exp(x[i]); break;
+        case 1: out[i] = uw_log(x[i]); break;
+        case 2: out[i] = uw_pow(x[i], y[i]); break;
+        default: out[i] = uw_erfc(x[i]); break;
+        }
+    }
 }

@@ -110,6 +110,8 @@ void   uwo_positive_moisture_single(double xlv, double xls, int mkx, double dt, 
                                     double qlmin, double qimin, const double *dp, double *qv,
                                     double *ql, double *qi, double *s, double *qvten,
                                     double *qlten, double *qiten, double *sten);
+/* The host-side evaluation of the portable math routines (uw_math.h): fn 0 exp, 1 log, 2 pow, 3 erfc. */
+void   uwo_uwmath(int fn, const double *x, const double *y, double *out, int n);
 /* findsp (uwshcu.F90:5164-5454) over columns 1..ncol of (mix, pver) arrays; returns the status. */
 int    uwo_findsp(int mix, int ncol, int pver, const double *q, const double *t, const double *p,
                   double *tsp, double *qsp);

@@ -16,9 +16,39 @@ def pytest_configure(config):
 
 @pytest.fixture(scope="session")
 def oracle():
+    """The oracle build pinned to the reference (glibc transcendentals)."""
     import oracle as o
+    o.set_variant("glibc")
     o.init_default()
     return o
+
+
+class _Portable:
+    """The oracle build with the host/device-identical math routines the CUDA path uses; every
+    call selects that build and switches back to the glibc build afterwards."""
+
+    def __init__(self, mod):
+        self.m = mod
+
+    def __getattr__(self, name):
+        f = getattr(self.m, name)
+        if not callable(f):
+            return f
+
+        def call(*a, **k):
+            self.m.set_variant("portable")
+            try:
+                return f(*a, **k)
+            finally:
+                self.m.set_variant("glibc")
+        return call
+
+
+@pytest.fixture(scope="session")
+def oracle_pm(oracle):
+    p = _Portable(oracle)
+    p.init_default()
+    return p
 
 
 @pytest.fixture(scope="session")
