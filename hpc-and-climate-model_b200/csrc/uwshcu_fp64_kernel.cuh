@@ -459,6 +459,10 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
     unsigned int errbits = 0;
     int xflags = 0, lflags = 0;
     bool id_exit = false;
+    // stop: the column leaves the scheme (the Fortran's `go to 333`).  Exits leave every loop through
+    // the loop's own exit (break, then `if (stop) break;` after each inner loop) so that lanes that
+    // leave a loop at different iterations reconverge right after it.
+    bool stop = false;
     int kinv = 0, klcl = 0, klfc = 0, krel = 0, kbup = 0, kpen = 0;
     int kinv_s = 0, klcl_s = 0, klfc_s = 0, krel_s = 0, kbup_s = 0, kpen_s = 0;
     double cin = 0, cinlcl = 0, plcl = 0, plfc = 0, prel = 0, exlcl = 1.0, exprel = 1.0, tkeavg = 0,
@@ -542,7 +546,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
         if (conden(ps0[k - 1], exns0[k - 1], thl0bot, qt0bot, thj, qvj, qlj, qij, tbl)) {
             xflags |= UW_X_CONDEN;
             id_exit = true;
-            goto l333;
+            stop = true;
+            break;
         }
         thv0bot[k] = thj * (1.0 + zvir * qvj - qlj - qij);
         thvl0bot[k] = thl0bot * (1.0 + zvir * qt0bot);
@@ -551,7 +556,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
         if (conden(ps0[k], exns0[k], thl0top, qt0top, thj, qvj, qlj, qij, tbl)) {
             xflags |= UW_X_CONDEN;
             id_exit = true;
-            goto l333;
+            stop = true;
+            break;
         }
         thv0top[k] = thj * (1.0 + zvir * qvj - qlj - qij);
         thvl0top[k] = thl0top * (1.0 + zvir * qt0top);
@@ -560,6 +566,7 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
         thvl0bot_o[k] = thvl0bot[k];
         thvl0top_o[k] = thvl0top[k];
     }
+    if (!stop) {
     // per-column initialisation (:1333-1408)
     for (int k = 0; k <= mkx; k++) {
         umf[k] = 0.0; emf[k] = 0.0; slflx[k] = 0.0; qtflx[k] = 0.0; uflx[k] = 0.0; vflx[k] = 0.0;
@@ -582,9 +589,10 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
     }
     cnt = (double)mkx;
     cnb = 0.0;
+    }
 
     // ---- implicit-CIN loop (uwshcu.F90:1421-4331) --------------------------------------------
-    for (int iter = 1; iter <= 2; iter++) {
+    for (int iter = 1; iter <= 2 && !stop; iter++) {
         double tscaleh = cush;
         cush = -1.0;
 
@@ -599,7 +607,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
         if (kinv <= 1) {
             xflags |= UW_X_KINV1;
             id_exit = true;
-            goto l333;
+            stop = true;
+            break;
         }
         // tkeavg, thvlmin (:1484-1499)
         {
@@ -637,7 +646,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
         if (plcl < 30000.0) {
             xflags |= UW_X_KLCLMKX;
             id_exit = true;
-            goto l333;
+            stop = true;
+            break;
         }
         exlcl = exnf(plcl);
         {
@@ -646,7 +656,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
             if (conden(plcl, exlcl, thl0lcl, qt0lcl, thj, qvj, qlj, qij, tbl)) {
                 xflags |= UW_X_CONDEN;
                 id_exit = true;
-                goto l333;
+                stop = true;
+            break;
             }
             thv0lcl = thj * (1.0 + zvir * qvj - qlj - qij);
         }
@@ -674,7 +685,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                         if (conden(ps0[k], exns0[k], thlsrc, qtsrc, thj, qvj, qlj, qij, tbl)) {
                             xflags |= UW_X_CONDEN;
                             id_exit = true;
-                            goto l333;
+                            stop = true;
+            break;
                         }
                         thvutop = thj * (1.0 + zvir * qvj - qlj - qij);
                         getbuoy(plcl, exlcl, thv0lcl, ps0[k], exns0[k], thv0top[k], thvubot, thvutop, plfc, cin);
@@ -687,7 +699,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                         if (conden(ps0[k], exns0[k], thlsrc, qtsrc, thj, qvj, qlj, qij, tbl)) {
                             xflags |= UW_X_CONDEN;
                             id_exit = true;
-                            goto l333;
+                            stop = true;
+            break;
                         }
                         thvutop = thj * (1.0 + zvir * qvj - qlj - qij);
                         getbuoy(ps0[k - 1], exns0[k - 1], thv0bot[k], ps0[k], exns0[k], thv0top[k], thvubot, thvutop, plfc, cin);
@@ -703,13 +716,15 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                     if (conden(ps0[k - 1], exns0[k - 1], thlsrc, qtsrc, thj, qvj, qlj, qij, tbl)) {
                         xflags |= UW_X_CONDEN;
                         id_exit = true;
-                        goto l333;
+                        stop = true;
+            break;
                     }
                     thvubot = thj * (1.0 + zvir * qvj - qlj - qij);
                     if (conden(ps0[k], exns0[k], thlsrc, qtsrc, thj, qvj, qlj, qij, tbl)) {
                         xflags |= UW_X_CONDEN;
                         id_exit = true;
-                        goto l333;
+                        stop = true;
+            break;
                     }
                     thvutop = thj * (1.0 + zvir * qvj - qlj - qij);
                     getbuoy(ps0[k - 1], exns0[k - 1], thv0bot[k], ps0[k], exns0[k], thv0top[k], thvubot, thvutop, plfc, cin);
@@ -720,6 +735,7 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                 }
             }
         }
+        if (stop) break;
         // (label 35, :1676-1685)
         if (cin < 0.0) lflags |= UW_L_CIN;
         cin = MX(0.0, cin);
@@ -727,7 +743,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
             klfc = mkx;
             xflags |= UW_X_KLFCMKX;
             id_exit = true;
-            goto l333;
+            stop = true;
+            break;
         }
         if (iter == 1) {
             cin_i = cin;
@@ -802,7 +819,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                 }
                 kinv = kinv_s; klcl = klcl_s; klfc = klfc_s; krel = krel_s; kbup = kbup_s; kpen = kpen_s;
                 id_exit = false;
-                goto l333;
+                stop = true;
+            break;
             }
         }
 
@@ -824,7 +842,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
             double mu = wcrit / sigmaw / 1.4142;
             if (mu >= 3.0) {
                 id_exit = true;
-                goto l333;
+                stop = true;
+            break;
             }
             double rho0inv = ps0[kinv - 1] / (r * thv0top[kinv - 1] * exns0[kinv - 1]);
             cbmf = (rho0inv * sigmaw / 2.5066) * uw_exp(-(mu * mu));
@@ -849,14 +868,16 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
             if (wtw <= 0.0) {
                 xflags |= UW_X_WTW;
                 id_exit = true;
-                goto l333;
+                stop = true;
+            break;
             }
             wlcl = sqrt(wtw);
             ufrclcl = cbmf / wlcl / rho0inv;
             if (ufrclcl <= 0.0001) {
                 xflags |= UW_X_UFRC;
                 id_exit = true;
-                goto l333;
+                stop = true;
+            break;
             }
             ufrc[krel - 1] = ufrclcl;
             for (int k = kinv - 1; k <= krel - 1; k++) {
@@ -867,7 +888,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
         if (MODE == UW_MODE_TRIGGER) {
             // the column convects past the closure: hand it to the worklist pass
             cand = true;
-            goto l_done;
+            stop = true;
+            break;
         }
         // updraft at the release level (:2205-2236)
         emf[krel - 1] = 0.0;
@@ -878,7 +900,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
         if (conden(prel, exprel, thlsrc, qtsrc, thj, qvj, qlj, qij, tbl)) {
             xflags |= UW_X_CONDEN;
             id_exit = true;
-            goto l333;
+            stop = true;
+            break;
         }
         thvu[krel - 1] = thj * (1.0 + zvir * qvj - qlj - qij);
         {
@@ -928,7 +951,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                         if (conden(pe, exne, thle, qte, thj, qvj, qlj, qij, tbl)) {
                             xflags |= UW_X_CONDEN;
                             id_exit = true;
-                            goto l333;
+                            stop = true;
+            break;
                         }
                         double thv0j = thj * (1.0 + zvir * qvj - qlj - qij);
                         rho0j = pe / (r * thv0j * exne);
@@ -936,7 +960,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                         if (conden(pe, exne, thlue, qtue, thj, qvj, qlj, qij, tbl)) {
                             xflags |= UW_X_CONDEN;
                             id_exit = true;
-                            goto l333;
+                            stop = true;
+            break;
                         }
                         if ((qlj + qij) > criqc) {
                             double exql = ((qlj + qij) - criqc) * qlj / (qlj + qij);
@@ -947,7 +972,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                         if (conden(pe, exne, thlue, qtue, thj, qvj, qlj, qij, tbl)) {
                             xflags |= UW_X_CONDEN;
                             id_exit = true;
-                            goto l333;
+                            stop = true;
+            break;
                         }
                         double thvj = thj * (1.0 + zvir * qvj - qlj - qij);
                         double excessu = qtue - qsat_qs(thlue * exne, pe, tbl);
@@ -962,7 +988,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                             if (conden(pe, exne, thlxsat, qtxsat, thj, qvj, qlj, qij, tbl)) {
                                 xflags |= UW_X_CONDEN;
                                 id_exit = true;
-                                goto l333;
+                                stop = true;
+            break;
                             }
                             double thvxsat = thj * (1.0 + zvir * qvj - qlj - qij);
                             double x_cu = 0.0, x_en = 0.0;
@@ -1029,7 +1056,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                         if (conden(ps0[k], exns0[k], thlu[k], qtu[k], thj, qvj, qlj, qij, tbl)) {
                             xflags |= UW_X_CONDEN;
                             id_exit = true;
-                            goto l333;
+                            stop = true;
+            break;
                         }
                         if ((qlj + qij) > criqc) {
                             double exql = ((qlj + qij) - criqc) * qlj / (qlj + qij);
@@ -1045,7 +1073,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                         if (conden(ps0[k], exns0[k], thlu[k], qtu[k], thj, qvj, qlj, qij, tbl)) {
                             xflags |= UW_X_CONDEN;
                             id_exit = true;
-                            goto l333;
+                            stop = true;
+            break;
                         }
                         thvu[k] = thj * (1.0 + zvir * qvj - qlj - qij);
                         bogbot = rbuoy * (thvu[km1] / thvebot - 1.0);
@@ -1066,6 +1095,7 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                             break;   // go to 111
                         }
                     }
+                    if (stop) break;
                     // (label 111, :2726-2793)
                     if (umf[k] == 0.0) wtw = -1.0;
                     if (bogtop > 0.0 && wtw > 0.0) kbup = k;
@@ -1077,7 +1107,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                     if (wu[k] > 100.0) {
                         xflags |= UW_X_WU;
                         id_exit = true;
-                        goto l333;
+                        stop = true;
+            break;
                     }
                     {
                         double rhos0j = ps0[k] / (r * 0.5 * (thv0bot[k + 1] + thv0top[k]) * exns0[k]);
@@ -1099,6 +1130,7 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                     ve = GL(v0, k + 1);
                     for (int m = 0; m < ncnst; m++) tre[m] = GT(m + 1, k + 1);
                 }
+                if (stop) break;
                 // (label 45) penetration depth (:2884-2907)
                 if (drage == 0.0) {
                     double aquad = (bogtop - bogbot) / (ps0[kpen] - ps0[kpen - 1]);
@@ -1137,7 +1169,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                 if (conden(ps0[kpen - 1] + ppen, exntop, thlu_top, qtu_top, thj, qvj, qlj, qij, tbl)) {
                     xflags |= UW_X_CONDEN;
                     id_exit = true;
-                    goto l333;
+                    stop = true;
+            break;
                 }
                 if ((qlj + qij) > criqc) {
                     dwten[kpen] = ((qlj + qij) - criqc) * qlj / (qlj + qij);
@@ -1155,12 +1188,14 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                 scaleh = cush;
             }
         }
+        if (stop) break;
         // forcedCu filter (:2964-2992)
         if (kbup == krel) {
             lflags |= UW_L_SHCU;
             xflags |= UW_X_CUFILTER;
             id_exit = true;
-            goto l333;
+            stop = true;
+            break;
         }
         lflags &= ~UW_L_SHCU;
         for (int k = kpen; k <= mkx; k++) {
@@ -1319,7 +1354,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                 double qt_prog = MX(qt0[k] + qtten_sub * dt, 1.e-12);
                 if (conden(p0[k], exn0[k], thl_prog, qt_prog, thj, qvj, qlj, qij, tbl)) {
                     id_exit = true;
-                    goto l333;
+                    stop = true;
+            break;
                 }
                 qlten_sink[k] = MX(qlten_sub, -ql0[k] / dt);
                 qiten_sink[k] = MX(qiten_sub, -qi0[k] / dt);
@@ -1328,6 +1364,7 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
             }
 #undef UEMF
         }
+        if (stop) break;
         // momentum tendency (:3488-3501)
         for (int k = 1; k <= kpen; k++) {
             uten[k] = (uflx[k - 1] - uflx[k]) * g / dp0[k];
@@ -1381,14 +1418,16 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                     if (conden(prel, exprel, thlu[krel - 1], qtu[krel - 1], thj, qvj, qlj, qij, tbl)) {
                         xflags |= UW_X_CONDEN;
                         id_exit = true;
-                        goto l333;
+                        stop = true;
+            break;
                     }
                     qlubelow = qlj;
                     qiubelow = qij;
                     if (conden(ps0[k], exns0[k], thlu[k], qtu[k], thj, qvj, qlj, qij, tbl)) {
                         xflags |= UW_X_CONDEN;
                         id_exit = true;
-                        goto l333;
+                        stop = true;
+            break;
                     }
                     qlu_mid = 0.5 * (qlubelow + qlj) * (prel - ps0[k]) / (ps0[k - 1] - ps0[k]);
                     qiu_mid = 0.5 * (qiubelow + qij) * (prel - ps0[k]) / (ps0[k - 1] - ps0[k]);
@@ -1396,7 +1435,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                     if (conden(ps0[k - 1] + ppen, exntop, thlu_top, qtu_top, thj, qvj, qlj, qij, tbl)) {
                         xflags |= UW_X_CONDEN;
                         id_exit = true;
-                        goto l333;
+                        stop = true;
+            break;
                     }
                     qlu_mid = 0.5 * (qlubelow + qlj) * (-ppen) / (ps0[k - 1] - ps0[k]);
                     qiu_mid = 0.5 * (qiubelow + qij) * (-ppen) / (ps0[k - 1] - ps0[k]);
@@ -1404,7 +1444,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                     if (conden(ps0[k], exns0[k], thlu[k], qtu[k], thj, qvj, qlj, qij, tbl)) {
                         xflags |= UW_X_CONDEN;
                         id_exit = true;
-                        goto l333;
+                        stop = true;
+            break;
                     }
                     qlu_mid = 0.5 * (qlubelow + qlj);
                     qiu_mid = 0.5 * (qiubelow + qij);
@@ -1439,7 +1480,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                     double ql_emf_kbup, qi_emf_kbup, thjj, qvjj;
                     if (conden(p0[k], exn0[k], thlu_emf[k], qtu_emf[k], thjj, qvjj, ql_emf_kbup, qi_emf_kbup, tbl)) {
                         id_exit = true;
-                        goto l333;
+                        stop = true;
+            break;
                     }
                     double nl_emf_kbup = (ql_emf_kbup > 0.0) ? tru_emf[ixnumliq - 1][k] : 0.0;
                     double ni_emf_kbup = (qi_emf_kbup > 0.0) ? tru_emf[ixnumice - 1][k] : 0.0;
@@ -1458,6 +1500,7 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                 rliq = rliq + qc[k] * dp0[k] / g / 1000.0;
             }
         }
+        if (stop) break;
         // evaporation and melting of precipitation (:3808-3934)
         {
             double evpint_rain = 0.0, evpint_snow = 0.0;
@@ -1592,7 +1635,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
         if (conden(prel, exprel, thlu[krel - 1], qtu[krel - 1], thj, qvj, qlj, qij, tbl)) {
             xflags |= UW_X_CONDEN;
             id_exit = true;
-            goto l333;
+            stop = true;
+            break;
         }
         {
             double qcubelow = qlj + qij, qlubelow = qlj, qiubelow = qij;
@@ -1603,7 +1647,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                 if (idc) {
                     xflags |= UW_X_CONDEN;
                     id_exit = true;
-                    goto l333;
+                    stop = true;
+            break;
                 }
                 qcu[k] = 0.5 * (qcubelow + qlj + qij);
                 qlu[k] = 0.5 * (qlubelow + qlj);
@@ -1624,6 +1669,7 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                 qiubelow = qij;
             }
         }
+        if (stop) break;
         cnt = (double)kpen;
         cnb = (double)(krel - 1);
 
@@ -1675,7 +1721,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                 if (conden(ps0[k - 1], exns0[k - 1], thl0bot, qt0bot, thj, qvj, qlj, qij, tbl)) {
                     xflags |= UW_X_CONDEN;
                     id_exit = true;
-                    goto l333;
+                    stop = true;
+            break;
                 }
                 thv0bot[k] = thj * (1.0 + zvir * qvj - qlj - qij);
                 thvl0bot[k] = thl0bot * (1.0 + zvir * qt0bot);
@@ -1684,15 +1731,18 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                 if (conden(ps0[k], exns0[k], thl0top, qt0top, thj, qvj, qlj, qij, tbl)) {
                     xflags |= UW_X_CONDEN;
                     id_exit = true;
-                    goto l333;
+                    stop = true;
+            break;
                 }
                 thv0top[k] = thj * (1.0 + zvir * qvj - qlj - qij);
                 thvl0top[k] = thl0top * (1.0 + zvir * qt0top);
             }
+            if (stop) break;
         }
     }
 
     // ---- final outputs (uwshcu.F90:4337-4370) --------------------------------------------------
+    if (!stop) {
     for (int k = 0; k <= mkx; k++) {
         OI(umf, k) = umf[k];
         OI(wu, k) = wu[k];
@@ -1726,8 +1776,10 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
         A.diag_real[UW_DR_PPEN * (size_t)mix + i] = ps0[kpen - 1] + ppen;
         A.diag_real[UW_DR_TKEAVG * (size_t)mix + i] = tkeavg;
     }
+    }
 
-l333:
+    // (label 333, :4448-4549)
+    if (!cand) {
     if (id_exit) {
         xflags |= UW_X_UWCU;
         for (int k = 0; k <= mkx; k++) {
@@ -1769,7 +1821,7 @@ l333:
         A.diag_int[UW_DI_KBUP * (size_t)mix + i] = kbup;
         A.diag_int[UW_DI_KPEN * (size_t)mix + i] = kpen;
     }
-l_done:
+    }
     if (errbits) atomicOr(A.err, errbits);
     }  // active
     if (MODE == UW_MODE_TRIGGER) {

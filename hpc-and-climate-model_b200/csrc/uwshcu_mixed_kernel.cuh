@@ -474,6 +474,10 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
     unsigned int errbits = 0;
     int xflags = 0, lflags = 0;
     bool id_exit = false;
+    // stop: the column leaves the scheme (the Fortran's `go to 333`).  Exits leave every loop through
+    // the loop's own exit (break, then `if (stop) break;` after each inner loop) so that lanes that
+    // leave a loop at different iterations reconverge right after it.
+    bool stop = false;
     int kinv = 0, klcl = 0, klfc = 0, krel = 0, kbup = 0, kpen = 0;
     int kinv_s = 0, klcl_s = 0, klfc_s = 0, krel_s = 0, kbup_s = 0, kpen_s = 0;
     double cin = 0, cinlcl = 0;
@@ -561,7 +565,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
         if (conden(ps0[k - 1], exns0[k - 1], thl0bot, qt0bot, thj, qvj, qlj, qij, tbld, tblf)) {
             xflags |= UW_X_CONDEN;
             id_exit = true;
-            goto l333;
+            stop = true;
+            break;
         }
         thv0bot[k] = thj * (1.0f + zvir * qvj - qlj - qij);
         thvl0bot[k] = thl0bot * (1.0f + zvir * qt0bot);
@@ -570,7 +575,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
         if (conden(ps0[k], exns0[k], thl0top, qt0top, thj, qvj, qlj, qij, tbld, tblf)) {
             xflags |= UW_X_CONDEN;
             id_exit = true;
-            goto l333;
+            stop = true;
+            break;
         }
         thv0top[k] = thj * (1.0f + zvir * qvj - qlj - qij);
         thvl0top[k] = thl0top * (1.0f + zvir * qt0top);
@@ -579,6 +585,7 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
         thvl0bot_o[k] = thvl0bot[k];
         thvl0top_o[k] = thvl0top[k];
     }
+    if (!stop) {
     // per-column initialisation (:1333-1408)
     for (int k = 0; k <= mkx; k++) {
         umf[k] = 0.0f; emf[k] = 0.0f; slflx[k] = 0.0f; qtflx[k] = 0.0f; uflx[k] = 0.0f; vflx[k] = 0.0f;
@@ -601,9 +608,10 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
     }
     cnt = (R)mkx;
     cnb = 0.0f;
+    }
 
     // ---- implicit-CIN loop (uwshcu.F90:1421-4331) --------------------------------------------
-    for (int iter = 1; iter <= 2; iter++) {
+    for (int iter = 1; iter <= 2 && !stop; iter++) {
         R tscaleh = cush;
         cush = -1.0f;
 
@@ -618,7 +626,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
         if (kinv <= 1) {
             xflags |= UW_X_KINV1;
             id_exit = true;
-            goto l333;
+            stop = true;
+            break;
         }
         // tkeavg, thvlmin (:1484-1499)
         {
@@ -655,7 +664,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
         if (plcl < 30000.0f) {
             xflags |= UW_X_KLCLMKX;
             id_exit = true;
-            goto l333;
+            stop = true;
+            break;
         }
         exlcl = exnf(plcl);
         {
@@ -664,7 +674,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
             if (conden(plcl, exlcl, thl0lcl, qt0lcl, thj, qvj, qlj, qij, tbld, tblf)) {
                 xflags |= UW_X_CONDEN;
                 id_exit = true;
-                goto l333;
+                stop = true;
+            break;
             }
             thv0lcl = thj * (1.0f + zvir * qvj - qlj - qij);
         }
@@ -692,7 +703,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                         if (conden(ps0[k], exns0[k], thlsrc, qtsrc, thj, qvj, qlj, qij, tbld, tblf)) {
                             xflags |= UW_X_CONDEN;
                             id_exit = true;
-                            goto l333;
+                            stop = true;
+            break;
                         }
                         thvutop = thj * (1.0f + zvir * qvj - qlj - qij);
                         getbuoy(plcl, exlcl, thv0lcl, ps0[k], exns0[k], thv0top[k], thvubot, thvutop, plfc, cin);
@@ -705,7 +717,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                         if (conden(ps0[k], exns0[k], thlsrc, qtsrc, thj, qvj, qlj, qij, tbld, tblf)) {
                             xflags |= UW_X_CONDEN;
                             id_exit = true;
-                            goto l333;
+                            stop = true;
+            break;
                         }
                         thvutop = thj * (1.0f + zvir * qvj - qlj - qij);
                         getbuoy(ps0[k - 1], exns0[k - 1], thv0bot[k], ps0[k], exns0[k], thv0top[k], thvubot, thvutop, plfc, cin);
@@ -721,13 +734,15 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                     if (conden(ps0[k - 1], exns0[k - 1], thlsrc, qtsrc, thj, qvj, qlj, qij, tbld, tblf)) {
                         xflags |= UW_X_CONDEN;
                         id_exit = true;
-                        goto l333;
+                        stop = true;
+            break;
                     }
                     thvubot = thj * (1.0f + zvir * qvj - qlj - qij);
                     if (conden(ps0[k], exns0[k], thlsrc, qtsrc, thj, qvj, qlj, qij, tbld, tblf)) {
                         xflags |= UW_X_CONDEN;
                         id_exit = true;
-                        goto l333;
+                        stop = true;
+            break;
                     }
                     thvutop = thj * (1.0f + zvir * qvj - qlj - qij);
                     getbuoy(ps0[k - 1], exns0[k - 1], thv0bot[k], ps0[k], exns0[k], thv0top[k], thvubot, thvutop, plfc, cin);
@@ -738,6 +753,7 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                 }
             }
         }
+        if (stop) break;
         // (label 35, :1676-1685)
         if (cin < 0.0f) lflags |= UW_L_CIN;
         cin = MX(0.0f, cin);
@@ -745,7 +761,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
             klfc = mkx;
             xflags |= UW_X_KLFCMKX;
             id_exit = true;
-            goto l333;
+            stop = true;
+            break;
         }
         if (iter == 1) {
             cin_i = cin;
@@ -820,7 +837,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                 }
                 kinv = kinv_s; klcl = klcl_s; klfc = klfc_s; krel = krel_s; kbup = kbup_s; kpen = kpen_s;
                 id_exit = false;
-                goto l333;
+                stop = true;
+            break;
             }
         }
 
@@ -842,7 +860,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
             R mu = wcrit / sigmaw / 1.4142f;
             if (mu >= 3.0f) {
                 id_exit = true;
-                goto l333;
+                stop = true;
+            break;
             }
             R rho0inv = ps0[kinv - 1] / (r * thv0top[kinv - 1] * exns0[kinv - 1]);
             cbmf = (rho0inv * sigmaw / 2.5066f) * expf(-(mu * mu));
@@ -867,14 +886,16 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
             if (wtw <= 0.0f) {
                 xflags |= UW_X_WTW;
                 id_exit = true;
-                goto l333;
+                stop = true;
+            break;
             }
             wlcl = sqrtf(wtw);
             ufrclcl = cbmf / wlcl / rho0inv;
             if (ufrclcl <= 0.0001f) {
                 xflags |= UW_X_UFRC;
                 id_exit = true;
-                goto l333;
+                stop = true;
+            break;
             }
             ufrc[krel - 1] = ufrclcl;
             for (int k = kinv - 1; k <= krel - 1; k++) {
@@ -885,7 +906,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
         if (MODE == UW_MODE_TRIGGER) {
             // the column convects past the closure: hand it to the worklist pass
             cand = true;
-            goto l_done;
+            stop = true;
+            break;
         }
         // updraft at the release level (:2205-2236)
         emf[krel - 1] = 0.0f;
@@ -896,7 +918,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
         if (conden(prel, exprel, thlsrc, qtsrc, thj, qvj, qlj, qij, tbld, tblf)) {
             xflags |= UW_X_CONDEN;
             id_exit = true;
-            goto l333;
+            stop = true;
+            break;
         }
         thvu[krel - 1] = thj * (1.0f + zvir * qvj - qlj - qij);
         {
@@ -946,7 +969,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                         if (conden(pe, exne, thle, qte, thj, qvj, qlj, qij, tbld, tblf)) {
                             xflags |= UW_X_CONDEN;
                             id_exit = true;
-                            goto l333;
+                            stop = true;
+            break;
                         }
                         R thv0j = thj * (1.0f + zvir * qvj - qlj - qij);
                         rho0j = pe / (r * thv0j * exne);
@@ -954,7 +978,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                         if (conden(pe, exne, thlue, qtue, thj, qvj, qlj, qij, tbld, tblf)) {
                             xflags |= UW_X_CONDEN;
                             id_exit = true;
-                            goto l333;
+                            stop = true;
+            break;
                         }
                         if ((qlj + qij) > criqc) {
                             R exql = ((qlj + qij) - criqc) * qlj / (qlj + qij);
@@ -965,7 +990,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                         if (conden(pe, exne, thlue, qtue, thj, qvj, qlj, qij, tbld, tblf)) {
                             xflags |= UW_X_CONDEN;
                             id_exit = true;
-                            goto l333;
+                            stop = true;
+            break;
                         }
                         R thvj = thj * (1.0f + zvir * qvj - qlj - qij);
                         R excessu = qtue - qsat_qs(thlue * exne, pe, tbld, tblf);
@@ -980,7 +1006,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                             if (conden(pe, exne, thlxsat, qtxsat, thj, qvj, qlj, qij, tbld, tblf)) {
                                 xflags |= UW_X_CONDEN;
                                 id_exit = true;
-                                goto l333;
+                                stop = true;
+            break;
                             }
                             R thvxsat = thj * (1.0f + zvir * qvj - qlj - qij);
                             R x_cu = 0.0f, x_en = 0.0f;
@@ -1047,7 +1074,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                         if (conden(ps0[k], exns0[k], thlu[k], qtu[k], thj, qvj, qlj, qij, tbld, tblf)) {
                             xflags |= UW_X_CONDEN;
                             id_exit = true;
-                            goto l333;
+                            stop = true;
+            break;
                         }
                         if ((qlj + qij) > criqc) {
                             R exql = ((qlj + qij) - criqc) * qlj / (qlj + qij);
@@ -1063,7 +1091,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                         if (conden(ps0[k], exns0[k], thlu[k], qtu[k], thj, qvj, qlj, qij, tbld, tblf)) {
                             xflags |= UW_X_CONDEN;
                             id_exit = true;
-                            goto l333;
+                            stop = true;
+            break;
                         }
                         thvu[k] = thj * (1.0f + zvir * qvj - qlj - qij);
                         bogbot = rbuoy * (thvu[km1] / thvebot - 1.0f);
@@ -1084,6 +1113,7 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                             break;   // go to 111
                         }
                     }
+                    if (stop) break;
                     // (label 111, :2726-2793)
                     if (umf[k] == 0.0f) wtw = -1.0f;
                     if (bogtop > 0.0f && wtw > 0.0f) kbup = k;
@@ -1095,7 +1125,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                     if (wu[k] > 100.0f) {
                         xflags |= UW_X_WU;
                         id_exit = true;
-                        goto l333;
+                        stop = true;
+            break;
                     }
                     {
                         R rhos0j = ps0[k] / (r * 0.5f * (thv0bot[k + 1] + thv0top[k]) * exns0[k]);
@@ -1117,6 +1148,7 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                     ve = GL(v0, k + 1);
                     for (int m = 0; m < ncnst; m++) tre[m] = GT(m + 1, k + 1);
                 }
+                if (stop) break;
                 // (label 45) penetration depth (:2884-2907)
                 if (drage == 0.0f) {
                     R aquad = (bogtop - bogbot) / (ps0[kpen] - ps0[kpen - 1]);
@@ -1155,7 +1187,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                 if (conden(ps0[kpen - 1] + ppen, exntop, thlu_top, qtu_top, thj, qvj, qlj, qij, tbld, tblf)) {
                     xflags |= UW_X_CONDEN;
                     id_exit = true;
-                    goto l333;
+                    stop = true;
+            break;
                 }
                 if ((qlj + qij) > criqc) {
                     dwten[kpen] = ((qlj + qij) - criqc) * qlj / (qlj + qij);
@@ -1173,12 +1206,14 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                 scaleh = cush;
             }
         }
+        if (stop) break;
         // forcedCu filter (:2964-2992)
         if (kbup == krel) {
             lflags |= UW_L_SHCU;
             xflags |= UW_X_CUFILTER;
             id_exit = true;
-            goto l333;
+            stop = true;
+            break;
         }
         lflags &= ~UW_L_SHCU;
         for (int k = kpen; k <= mkx; k++) {
@@ -1337,7 +1372,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                 R qt_prog = MX(qt0[k] + qtten_sub * dt, 1.e-12f);
                 if (conden(p0[k], exn0[k], thl_prog, qt_prog, thj, qvj, qlj, qij, tbld, tblf)) {
                     id_exit = true;
-                    goto l333;
+                    stop = true;
+            break;
                 }
                 qlten_sink[k] = MX(qlten_sub, -ql0[k] / dt);
                 qiten_sink[k] = MX(qiten_sub, -qi0[k] / dt);
@@ -1346,6 +1382,7 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
             }
 #undef UEMF
         }
+        if (stop) break;
         // momentum tendency (:3488-3501)
         for (int k = 1; k <= kpen; k++) {
             uten[k] = (uflx[k - 1] - uflx[k]) * g / dp0[k];
@@ -1399,14 +1436,16 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                     if (conden(prel, exprel, thlu[krel - 1], qtu[krel - 1], thj, qvj, qlj, qij, tbld, tblf)) {
                         xflags |= UW_X_CONDEN;
                         id_exit = true;
-                        goto l333;
+                        stop = true;
+            break;
                     }
                     qlubelow = qlj;
                     qiubelow = qij;
                     if (conden(ps0[k], exns0[k], thlu[k], qtu[k], thj, qvj, qlj, qij, tbld, tblf)) {
                         xflags |= UW_X_CONDEN;
                         id_exit = true;
-                        goto l333;
+                        stop = true;
+            break;
                     }
                     qlu_mid = 0.5f * (qlubelow + qlj) * (prel - ps0[k]) / (ps0[k - 1] - ps0[k]);
                     qiu_mid = 0.5f * (qiubelow + qij) * (prel - ps0[k]) / (ps0[k - 1] - ps0[k]);
@@ -1414,7 +1453,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                     if (conden(ps0[k - 1] + ppen, exntop, thlu_top, qtu_top, thj, qvj, qlj, qij, tbld, tblf)) {
                         xflags |= UW_X_CONDEN;
                         id_exit = true;
-                        goto l333;
+                        stop = true;
+            break;
                     }
                     qlu_mid = 0.5f * (qlubelow + qlj) * (-ppen) / (ps0[k - 1] - ps0[k]);
                     qiu_mid = 0.5f * (qiubelow + qij) * (-ppen) / (ps0[k - 1] - ps0[k]);
@@ -1422,7 +1462,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                     if (conden(ps0[k], exns0[k], thlu[k], qtu[k], thj, qvj, qlj, qij, tbld, tblf)) {
                         xflags |= UW_X_CONDEN;
                         id_exit = true;
-                        goto l333;
+                        stop = true;
+            break;
                     }
                     qlu_mid = 0.5f * (qlubelow + qlj);
                     qiu_mid = 0.5f * (qiubelow + qij);
@@ -1457,7 +1498,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                     R ql_emf_kbup, qi_emf_kbup, thjj, qvjj;
                     if (conden(p0[k], exn0[k], thlu_emf[k], qtu_emf[k], thjj, qvjj, ql_emf_kbup, qi_emf_kbup, tbld, tblf)) {
                         id_exit = true;
-                        goto l333;
+                        stop = true;
+            break;
                     }
                     R nl_emf_kbup = (ql_emf_kbup > 0.0f) ? tru_emf[ixnumliq - 1][k] : 0.0f;
                     R ni_emf_kbup = (qi_emf_kbup > 0.0f) ? tru_emf[ixnumice - 1][k] : 0.0f;
@@ -1476,6 +1518,7 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                 rliq.add(qc[k] * dp0[k] / g / 1000.0f);
             }
         }
+        if (stop) break;
         // evaporation and melting of precipitation (:3808-3934)
         {
             Kahan evpint_rain, evpint_snow;
@@ -1614,7 +1657,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
         if (conden(prel, exprel, thlu[krel - 1], qtu[krel - 1], thj, qvj, qlj, qij, tbld, tblf)) {
             xflags |= UW_X_CONDEN;
             id_exit = true;
-            goto l333;
+            stop = true;
+            break;
         }
         {
             R qcubelow = qlj + qij, qlubelow = qlj, qiubelow = qij;
@@ -1625,7 +1669,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                 if (idc) {
                     xflags |= UW_X_CONDEN;
                     id_exit = true;
-                    goto l333;
+                    stop = true;
+            break;
                 }
                 qcu[k] = 0.5f * (qcubelow + qlj + qij);
                 qlu[k] = 0.5f * (qlubelow + qlj);
@@ -1646,6 +1691,7 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                 qiubelow = qij;
             }
         }
+        if (stop) break;
         cnt = (R)kpen;
         cnb = (R)(krel - 1);
 
@@ -1697,7 +1743,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                 if (conden(ps0[k - 1], exns0[k - 1], thl0bot, qt0bot, thj, qvj, qlj, qij, tbld, tblf)) {
                     xflags |= UW_X_CONDEN;
                     id_exit = true;
-                    goto l333;
+                    stop = true;
+            break;
                 }
                 thv0bot[k] = thj * (1.0f + zvir * qvj - qlj - qij);
                 thvl0bot[k] = thl0bot * (1.0f + zvir * qt0bot);
@@ -1706,15 +1753,18 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                 if (conden(ps0[k], exns0[k], thl0top, qt0top, thj, qvj, qlj, qij, tbld, tblf)) {
                     xflags |= UW_X_CONDEN;
                     id_exit = true;
-                    goto l333;
+                    stop = true;
+            break;
                 }
                 thv0top[k] = thj * (1.0f + zvir * qvj - qlj - qij);
                 thvl0top[k] = thl0top * (1.0f + zvir * qt0top);
             }
+            if (stop) break;
         }
     }
 
     // ---- final outputs (uwshcu.F90:4337-4370) --------------------------------------------------
+    if (!stop) {
     for (int k = 0; k <= mkx; k++) {
         OI(umf, k) = umf[k];
         OI(wu, k) = wu[k];
@@ -1748,8 +1798,10 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
         A.diag_real[UW_DR_PPEN * (size_t)mix + i] = ps0[kpen - 1] + ppen;
         A.diag_real[UW_DR_TKEAVG * (size_t)mix + i] = tkeavg;
     }
+    }
 
-l333:
+    // (label 333, :4448-4549)
+    if (!cand) {
     if (id_exit) {
         xflags |= UW_X_UWCU;
         for (int k = 0; k <= mkx; k++) {
@@ -1791,7 +1843,7 @@ l333:
         A.diag_int[UW_DI_KBUP * (size_t)mix + i] = kbup;
         A.diag_int[UW_DI_KPEN * (size_t)mix + i] = kpen;
     }
-l_done:
+    }
     if (errbits) atomicOr(A.err, errbits);
     }  // active
     if (MODE == UW_MODE_TRIGGER) {
