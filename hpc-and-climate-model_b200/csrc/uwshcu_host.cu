@@ -791,3 +791,113 @@ int uwshcu_device_status(void* stream)
 }
 
 }  // extern "C"
+
+// ---- uwshcu_compute_device_noalloc: the two-phase schedule with a fixed, library-owned worklist
+//
+// For callers that cannot allocate device memory at the point where they call the scheme: a host
+// model whose memory manager claims the device's memory at start-up and hands out only its own
+// pool (a cudaMalloc of ours would fail or fragment that pool), and codes that must not call
+// cudaMalloc/cudaFree inside a time step because those calls can synchronize the device.  The
+// worklist of convecting columns (count, endrun bits, column ids), which uwshcu_compute_device
+// grows with cudaMalloc, lives here in one file-scope device array sized for
+// UWSHCU_NOALLOC_MAX_COLUMNS columns (4 MiB + 256 B).  Every GPU that loads the library holds the
+// array until the process exits.  In host code g_noalloc_scratch is only a host-side stand-in for
+// the symbol; its device address comes from cudaGetSymbolAddress, once per device, with that
+// device current.
+constexpr int kNoallocHeader = 64;   // ints before the column ids: [0] count, [1] endrun bits
+static __device__ __align__(256) int g_noalloc_scratch[kNoallocHeader + UWSHCU_NOALLOC_MAX_COLUMNS];
+
+namespace {
+
+struct NoallocDevice {
+    int* scratch = nullptr;          // device address of g_noalloc_scratch on this device
+};
+NoallocDevice g_noalloc_dev[kMaxDev];
+
+// Set-up of the current device without allocating: the scratch's device address, and the
+// constants (cudaMemcpyToSymbol into the kernels' __constant__ banks) when they are missing or
+// older than the last uwshcu_init / uwshcu_set_rpen.
+int noalloc_device(int** scratch)
+{
+    State& s = S();
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev <= 0) {
+        std::snprintf(s.lasterr, sizeof(s.lasterr), "%s", e != cudaSuccess ? cudaGetErrorString(e) : "no device");
+        return UWSHCU_ERR_NO_DEVICE;
+    }
+    int dev = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return cuda_fail(e);
+    if (dev < 0 || dev >= kMaxDev) return UWSHCU_ERR_NO_DEVICE;
+    NoallocDevice& nd = g_noalloc_dev[dev];
+    if (!nd.scratch) {
+        void* ptr = nullptr;
+        if ((e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch)) != cudaSuccess) return cuda_fail(e);
+        nd.scratch = static_cast<int*>(ptr);
+    }
+    DeviceState& d = s.dev[dev];
+    if (d.uploaded_gen != s.gen) {
+        if ((e = set_constants_all(&s.k, s.tbl)) != cudaSuccess) return cuda_fail(e);
+        d.uploaded_gen = s.gen;
+    }
+    *scratch = nd.scratch;
+    return UWSHCU_OK;
+}
+
+}  // namespace
+
+extern "C" int uwshcu_compute_device_noalloc(
+    int mix, int mkx, int iend, int ncnst, double dt, int inv, const double* ps0, const double* zs0,
+    const double* p0, const double* z0, const double* dp0, const double* u0, const double* v0,
+    const double* qv0, const double* ql0, const double* qi0, const double* t0, const double* s0,
+    const double* tr0, const double* tke, const double* pblh, double* cush, double* umf, double* slflx,
+    double* qtflx, double* flxprc1, double* flxsnow1, double* qvten, double* qlten, double* qiten,
+    double* sten, double* uten, double* vten, double* trten, double* qrten, double* qsten,
+    double* precip, double* snow, double* evapc, double* cufrc, double* qcu, double* qlu, double* qiu,
+    double* cbmf, double* qc, double* rliq, double* cnt, double* cnb, const double* dpdry0, double* wu,
+    int* diag_int, double* diag_real, unsigned int* status_bits, void* stream)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    if (!s.init) return UWSHCU_ERR_NOT_INITIALIZED;
+    if (bad_dims(mix, mkx, iend, ncnst) || (inv != 0 && inv != 1)) return UWSHCU_ERR_BAD_ARGS;
+    if (iend > UWSHCU_NOALLOC_MAX_COLUMNS) {
+        std::snprintf(s.lasterr, sizeof(s.lasterr),
+                      "uwshcu_compute_device_noalloc: iend = %d exceeds its fixed worklist of %d columns "
+                      "(UWSHCU_NOALLOC_MAX_COLUMNS); split the call or use uwshcu_compute_device",
+                      iend, UWSHCU_NOALLOC_MAX_COLUMNS);
+        return UWSHCU_ERR_TOO_LARGE;
+    }
+    const void* need[] = {ps0, zs0, p0, z0, dp0, u0, v0, qv0, ql0, qi0, t0, s0, tr0, tke, pblh, cush,
+                          umf, slflx, qtflx, flxprc1, flxsnow1, qvten, qlten, qiten, sten, uten, vten,
+                          trten, qrten, qsten, precip, snow, evapc, cufrc, qcu, qlu, qiu, cbmf, qc, rliq,
+                          cnt, cnb, dpdry0, wu};
+    for (const void* p : need)
+        if (!p) return UWSHCU_ERR_BAD_ARGS;
+    int* scratch = nullptr;
+    int rc = noalloc_device(&scratch);
+    if (rc != UWSHCU_OK) return rc;
+    UwArgs A{};
+    A.mix = mix; A.mkx = mkx; A.iend = iend; A.ncnst = ncnst; A.inv = inv; A.dt = dt;
+    A.ps0 = ps0; A.zs0 = zs0; A.p0 = p0; A.z0 = z0; A.dp0 = dp0; A.u0 = u0; A.v0 = v0; A.qv0 = qv0;
+    A.ql0 = ql0; A.qi0 = qi0; A.t0 = t0; A.s0 = s0; A.tr0 = tr0; A.tke = tke; A.pblh = pblh; A.cush = cush;
+    A.umf = umf; A.slflx = slflx; A.qtflx = qtflx; A.flxprc1 = flxprc1; A.flxsnow1 = flxsnow1;
+    A.qvten = qvten; A.qlten = qlten; A.qiten = qiten; A.sten = sten; A.uten = uten; A.vten = vten;
+    A.trten = trten; A.qrten = qrten; A.qsten = qsten; A.precip = precip; A.snow = snow; A.evapc = evapc;
+    A.cufrc = cufrc; A.qcu = qcu; A.qlu = qlu; A.qiu = qiu; A.cbmf = cbmf; A.qc = qc; A.rliq = rliq;
+    A.cnt = cnt; A.cnb = cnb; A.dpdry0 = dpdry0; A.wu = wu; A.diag_int = diag_int; A.diag_real = diag_real;
+    int* count = scratch;
+    int* list = scratch + kNoallocHeader;
+    A.err = status_bits ? status_bits : reinterpret_cast<unsigned int*>(scratch + 1);
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e;
+    // the array keeps the previous call's contents: the count and the endrun bits start at zero
+    if ((e = cudaMemsetAsync(scratch, 0, 2 * sizeof(int), st)) != cudaSuccess) return cuda_fail(e);
+    if (status_bits && (e = cudaMemsetAsync(status_bits, 0, sizeof(unsigned int), st)) != cudaSuccess)
+        return cuda_fail(e);
+    if ((e = launch_mode(&A, s.precision, kModeTrigger, list, count, iend, s.block, st)) != cudaSuccess)
+        return cuda_fail(e);
+    if ((e = launch_mode(&A, s.precision, kModeList, list, count, iend, s.block, st)) != cudaSuccess)
+        return cuda_fail(e);
+    return UWSHCU_OK;
+}

@@ -30,12 +30,15 @@ ERR_NOT_INITIALIZED = -2
 ERR_CUDA = -3
 ERR_NO_DEVICE = -4
 ERR_ALLOC = -5
+ERR_TOO_LARGE = -6
+NOALLOC_MAX_COLUMNS = 1048576
 
 EXPORTS = ("uwshcu_init", "uwshcu_set_rpen", "uwshcu_init_default", "uwshcu_set_precision",
            "uwshcu_set_block", "uwshcu_set_schedule", "uwshcu_set_profiling",
            "uwshcu_profile_read", "uwshcu_get_estbl", "uwshcu_finalize", "uwshcu_last_cuda_error",
            "compute_uwshcu_", "compute_uwshcu_inv_", "bxcompute_uwshcu_inv_",
-           "uwshcu_compute_device", "uwshcu_device_status", "uwshcu_eval_math")
+           "uwshcu_compute_device", "uwshcu_device_status", "uwshcu_eval_math",
+           "uwshcu_compute_device_noalloc")
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
@@ -217,6 +220,29 @@ class DeviceCase:
             P(o["cnt"]), P(o["cnb"]), P(i["dpdry0"]), P(o["wu"]),
             P(self.diag_int) if self.diag_int is not None else None,
             P(self.diag_real) if self.diag_real is not None else None,
+            ctypes.c_void_p(st.cuda_stream))
+
+    def launch_noalloc(self, inv=0, stream=None, status_bits=None):
+        """Enqueue one call of uwshcu_compute_device_noalloc on `stream`; status_bits is None or a
+        one-element torch.int32 device tensor that receives the call's endrun bits."""
+        torch = self.torch
+        st = stream if stream is not None else torch.cuda.current_stream()
+        P = lambda t: ctypes.c_void_p(t.data_ptr())
+        i, o = self.inp, self.out
+        return lib().uwshcu_compute_device_noalloc(
+            ctypes.c_int(self.n), ctypes.c_int(self.mkx), ctypes.c_int(self.n),
+            ctypes.c_int(self.ncnst), ctypes.c_double(self.dt), ctypes.c_int(inv),
+            P(i["ps0"]), P(i["zs0"]), P(i["p0"]), P(i["z0"]), P(i["dp0"]), P(i["u0"]), P(i["v0"]),
+            P(i["qv0"]), P(i["ql0"]), P(i["qi0"]), P(i["t0"]), P(i["s0"]), P(i["tr0"]),
+            P(i["tke"]), P(i["pblh"]), P(o["cush"]), P(o["umf"]), P(o["slflx"]), P(o["qtflx"]),
+            P(o["flxprc1"]), P(o["flxsnow1"]), P(o["qvten"]), P(o["qlten"]), P(o["qiten"]),
+            P(o["sten"]), P(o["uten"]), P(o["vten"]), P(o["trten"]), P(o["qrten"]),
+            P(o["qsten"]), P(o["precip"]), P(o["snow"]), P(o["evapc"]), P(o["cufrc"]),
+            P(o["qcu"]), P(o["qlu"]), P(o["qiu"]), P(o["cbmf"]), P(o["qc"]), P(o["rliq"]),
+            P(o["cnt"]), P(o["cnb"]), P(i["dpdry0"]), P(o["wu"]),
+            P(self.diag_int) if self.diag_int is not None else None,
+            P(self.diag_real) if self.diag_real is not None else None,
+            P(status_bits) if status_bits is not None else None,
             ctypes.c_void_p(st.cuda_stream))
 
     def status(self, stream=None):

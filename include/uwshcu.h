@@ -28,6 +28,7 @@ extern "C" {
 #define UWSHCU_ERR_CUDA (-3)             /* CUDA runtime error (uwshcu_last_cuda_error names it)   */
 #define UWSHCU_ERR_NO_DEVICE (-4)        /* no CUDA device visible                                 */
 #define UWSHCU_ERR_ALLOC (-5)            /* device or pinned host allocation failed                */
+#define UWSHCU_ERR_TOO_LARGE (-6)        /* size beyond a fixed limit (UWSHCU_NOALLOC_MAX_COLUMNS) */
 
 #define UWSHCU_MAX_LEVELS 63             /* mkx limit of the compiled kernels                      */
 #define UWSHCU_MAX_TRACERS 32            /* ncnst limit of the compiled kernels                    */
@@ -181,6 +182,53 @@ int uwshcu_compute_device(int mix, int mkx, int iend, int ncnst, double dt, int 
 /* Wait for `stream` and return the status collected by the device calls enqueued on it since the
  * previous uwshcu_device_status call. */
 int uwshcu_device_status(void *stream);
+
+/* Column limit of uwshcu_compute_device_noalloc: its worklist is one fixed device array of
+ * 64 + UWSHCU_NOALLOC_MAX_COLUMNS ints (4 MiB + 256 B) that every GPU which loads the library holds
+ * until the process exits. */
+#define UWSHCU_NOALLOC_MAX_COLUMNS 1048576
+
+/* No counterpart in the reference.  uwshcu_compute_device with the two-phase schedule (trigger
+ * pass, then the convecting columns' pass) that allocates nothing: for callers that cannot
+ * allocate device memory when they call the scheme -- a host model whose memory manager claims
+ * the GPU's memory at start-up and hands out only its own pool, where a cudaMalloc of this library
+ * would fail or fragment that pool, and time-step code that must not call cudaMalloc/cudaFree
+ * because they can synchronize the whole device.  The caller passes the inputs and outputs as for
+ * uwshcu_compute_device (device pointers, enqueued on `stream`, same precision and block settings);
+ * the worklist of convecting columns lives in a file-scope device array of the library instead of
+ * a cudaMalloc'd buffer, and the call makes no cudaMalloc, cudaFree or other allocating call.
+ *   - iend > UWSHCU_NOALLOC_MAX_COLUMNS is rejected with UWSHCU_ERR_TOO_LARGE
+ *     (uwshcu_last_cuda_error names the limit); split larger calls.
+ *   - The first call on each device does the set-up: it looks up the array's device address
+ *     (cudaGetSymbolAddress) with that device current and, unless another entry point already
+ *     did, copies the constants to the device (cudaMemcpyToSymbol); the first call after each
+ *     uwshcu_init / uwshcu_set_rpen copies them again.  Make that first call before any stream
+ *     capture.
+ *   - Every call on a device shares the one array, which keeps the last call's contents; each
+ *     call clears the parts that must start at zero on its stream.  Calls whose GPU work overlaps
+ *     (two streams, two host threads, or a call running beside another) race on the array and
+ *     give wrong results: order them on one stream or with events.
+ *   - status_bits: NULL, or a device pointer to one unsigned int that the call zeroes on `stream`
+ *     and into which the kernels OR the endrun conditions of this call (1 mu inconsistency,
+ *     2 findsp non-convergence, 4 findsp enthalpy).  uwshcu_device_status does not see them.
+ *   - Launching the kernels can make the CUDA driver enlarge the context's local-memory
+ *     reservation for their stack frames the first time; make one call during set-up if that
+ *     matters. */
+int uwshcu_compute_device_noalloc(int mix, int mkx, int iend, int ncnst, double dt, int inv,
+                                  const double *ps0, const double *zs0, const double *p0,
+                                  const double *z0, const double *dp0, const double *u0,
+                                  const double *v0, const double *qv0, const double *ql0,
+                                  const double *qi0, const double *t0, const double *s0,
+                                  const double *tr0, const double *tke, const double *pblh,
+                                  double *cush, double *umf, double *slflx, double *qtflx,
+                                  double *flxprc1, double *flxsnow1, double *qvten, double *qlten,
+                                  double *qiten, double *sten, double *uten, double *vten,
+                                  double *trten, double *qrten, double *qsten, double *precip,
+                                  double *snow, double *evapc, double *cufrc, double *qcu,
+                                  double *qlu, double *qiu, double *cbmf, double *qc, double *rliq,
+                                  double *cnt, double *cnb, const double *dpdry0, double *wu,
+                                  int *diag_int, double *diag_real, unsigned int *status_bits,
+                                  void *stream);
 
 /* Evaluate the library's exp (fn 0), log (1), pow (2, with y) or erfc (3) on n device values, on
  * the GPU, with the routines the kernels use.  They give the same bits as the host build of the
