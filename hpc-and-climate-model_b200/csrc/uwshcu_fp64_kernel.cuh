@@ -94,8 +94,10 @@ __device__ __forceinline__ double qsat_qs(double t, double p, const double* __re
 
 __device__ __forceinline__ double exnf(double p) { return uw_pow(p / c.p00, c.rovcp); }
 
-// conden (uwshcu.F90:4718-4785) with ex = exnf(p) supplied by the caller.
-__device__ __forceinline__ int conden(double p, double ex, double thl, double qt, double& th, double& qv,
+// conden (uwshcu.F90:4718-4785) with ex = exnf(p) supplied by the caller.  Not inlined: the kernel
+// calls it from ~30 sites, and one shared copy keeps the kernel inside the instruction cache
+// (inlined, the stall on instruction fetch doubled the run time).
+__device__ __noinline__ int conden(double p, double ex, double thl, double qt, double& th, double& qv,
                                       double& ql, double& qi, const double* __restrict__ tbl)
 {
     double tc = thl * ex;
@@ -103,27 +105,29 @@ __device__ __forceinline__ int conden(double p, double ex, double thl, double qt
     double leff = (1.0 - nu) * c.xlv + nu * c.xls;
     double temps = tc;
     double rvls = qsat_qs(temps, p, tbl);
+    int id_check = 0;
     if (rvls >= qt) {
         qv = qt;
         ql = 0.0;
         qi = 0.0;
         th = tc / ex;
-        return 0;
-    }
-    double qs = rvls;
+    } else {
+        double qs = rvls;
 #pragma unroll 1
-    for (int it = 0; it < 10; it++) {
-        temps = temps + ((tc - temps) * c.cp / leff + qt - rvls) /
-                            (c.cp / leff + c.ep2 * leff * rvls / c.r / temps / temps);
-        qs = qsat_qs(temps, p, tbl);
-        rvls = qs;
+        for (int it = 0; it < 10; it++) {
+            temps = temps + ((tc - temps) * c.cp / leff + qt - rvls) /
+                                (c.cp / leff + c.ep2 * leff * rvls / c.r / temps / temps);
+            qs = qsat_qs(temps, p, tbl);
+            rvls = qs;
+        }
+        double qc = MX(qt - qs, 0.0);
+        qv = qt - qc;
+        ql = qc * (1.0 - nu);
+        qi = nu * qc;
+        th = temps / ex;
+        id_check = (fabs((temps - (leff / c.cp) * qc) - tc) >= 1.0) ? 1 : 0;
     }
-    double qc = MX(qt - qs, 0.0);
-    qv = qt - qc;
-    ql = qc * (1.0 - nu);
-    qi = nu * qc;
-    th = temps / ex;
-    return (fabs((temps - (leff / c.cp) * qc) - tc) >= 1.0) ? 1 : 0;
+    return id_check;
 }
 
 // roots (uwshcu.F90:4787-4829); r1/r2 keep the caller's values on the failure branches.
@@ -168,40 +172,49 @@ __device__ __forceinline__ void slope(int mkx, const double* field, const double
 }
 
 // qsinvert (uwshcu.F90:4863-4929) with exsfc = exnf(psfc).
-__device__ double qsinvert(double qt, double thl, double psfc, double exsfc, const double* __restrict__ tbl)
+__device__ __noinline__ double qsinvert(double qt, double thl, double psfc, double exsfc, const double* __restrict__ tbl)
 {
     const double psmin = 100.0 * 100.0, dpsmax = 1.0;
     double es, qs, gam;
     double Ti = thl * exsfc;
     qsat3(Ti, psfc, es, qs, gam, tbl);
     double rhi = qt / qs;
-    if (rhi <= 0.01) return psmin;
-    double TLCL = 55.0 + 1.0 / (1.0 / (Ti - 55.0) - uw_log(rhi) / 2840.0);
-    double PiLCL = TLCL / thl;
-    double ps = c.p00 * uw_pow(PiLCL, 1.0 / c.rovcp);
+    // single exit, fixed trip count: every lane of a warp leaves together
+    double result = psmin;
+    if (!(rhi <= 0.01)) {
+        double TLCL = 55.0 + 1.0 / (1.0 / (Ti - 55.0) - uw_log(rhi) / 2840.0);
+        double PiLCL = TLCL / thl;
+        double ps = c.p00 * uw_pow(PiLCL, 1.0 / c.rovcp);
+        bool done = false;
 #pragma unroll 1
-    for (int i = 1; i <= 10; i++) {
-        double Pis = uw_pow(ps / c.p00, c.rovcp);
-        double Ts = thl * Pis;
-        qsat3(Ts, ps, es, qs, gam, tbl);
-        double err = qt - qs;
-        double nu = MX(MN((268.0 - Ts) / 20.0, 1.0), 0.0);
-        double leff = (1.0 - nu) * c.xlv + nu * c.xls;
-        double dlnqsdT = gam * (c.cp / leff) / qs;
-        double dTdPis = thl;
-        double dPisdps = c.rovcp * Pis / ps;
-        double dlnqsdps = -1.0 / (ps - (1.0 - c.ep2) * es);
-        double derrdps = -qs * (dlnqsdT * dTdPis * dPisdps + dlnqsdps);
-        double dps = -err / derrdps;
-        ps = ps + dps;
-        if (ps < 0.0) return psmin;
-        if (fabs(dps) <= dpsmax) return ps;
+        for (int i = 1; i <= 10; i++) {
+            if (done) continue;
+            double Pis = uw_pow(ps / c.p00, c.rovcp);
+            double Ts = thl * Pis;
+            qsat3(Ts, ps, es, qs, gam, tbl);
+            double err = qt - qs;
+            double nu = MX(MN((268.0 - Ts) / 20.0, 1.0), 0.0);
+            double leff = (1.0 - nu) * c.xlv + nu * c.xls;
+            double dlnqsdT = gam * (c.cp / leff) / qs;
+            double dTdPis = thl;
+            double dPisdps = c.rovcp * Pis / ps;
+            double dlnqsdps = -1.0 / (ps - (1.0 - c.ep2) * es);
+            double derrdps = -qs * (dlnqsdT * dTdPis * dPisdps + dlnqsdps);
+            double dps = -err / derrdps;
+            ps = ps + dps;
+            if (ps < 0.0) {
+                done = true;
+            } else if (fabs(dps) <= dpsmax) {
+                result = ps;
+                done = true;
+            }
+        }
     }
-    return psmin;
+    return result;
 }
 
 // compute_alpha (uwshcu.F90:4931-4950)
-__device__ double compute_alpha(double del_CIN, double ke)
+__device__ __noinline__ double compute_alpha(double del_CIN, double ke)
 {
     double x0 = 0.0;
 #pragma unroll 1
@@ -213,7 +226,7 @@ __device__ double compute_alpha(double del_CIN, double ke)
 }
 
 // compute_mumin2 (uwshcu.F90:4952-4979)
-__device__ double compute_mumin2(double mulcl, double rmaxfrac, double mulow)
+__device__ __noinline__ double compute_mumin2(double mulcl, double rmaxfrac, double mulow)
 {
     double x0 = mulow;
 #pragma unroll 1
@@ -232,7 +245,7 @@ __device__ double compute_mumin2(double mulcl, double rmaxfrac, double mulow)
 }
 
 // compute_ppen (uwshcu.F90:4981-5028); the 1.e-8 at :4998 is a default-real literal.
-__device__ double compute_ppen(double wtwb, double D, double bogbot, double bogtop, double rho0j, double dpen)
+__device__ __noinline__ double compute_ppen(double wtwb, double D, double bogbot, double bogtop, double rho0j, double dpen)
 {
     double x0;
     double SB = (bogtop - bogbot) / dpen;
@@ -416,6 +429,9 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
         i = tid;
     }
     bool cand = false;
+    // lanes of this warp that run a column; UW_SYNC() joins them where every one of them arrives
+    const unsigned live = __ballot_sync(0xffffffffu, active);
+#define UW_SYNC() __syncwarp(live)
     if (active) {
 
     const int mix = A.mix, mkx = A.mkx, ncnst = A.ncnst;
@@ -459,9 +475,7 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
     unsigned int errbits = 0;
     int xflags = 0, lflags = 0;
     bool id_exit = false;
-    // stop: the column leaves the scheme (the Fortran's `go to 333`).  Exits leave every loop through
-    // the loop's own exit (break, then `if (stop) break;` after each inner loop) so that lanes that
-    // leave a loop at different iterations reconverge right after it.
+    // stop: the column leaves the scheme (the Fortran's `go to 333`); every later section skips.
     bool stop = false;
     int kinv = 0, klcl = 0, klfc = 0, krel = 0, kbup = 0, kpen = 0;
     int kinv_s = 0, klcl_s = 0, klfc_s = 0, krel_s = 0, kbup_s = 0, kpen_s = 0;
@@ -591,17 +605,31 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
     cnb = 0.0;
     }
 
+    UW_SYNC();
+
     // ---- implicit-CIN loop (uwshcu.F90:1421-4331) --------------------------------------------
-    for (int iter = 1; iter <= 2 && !stop; iter++) {
-        double tscaleh = cush;
+    // Lockstep skeleton.  Every lane of the warp runs the same iterations of this loop and of every
+    // level loop inside it: a column's own level range and its exits are per-lane predicates.  Each
+    // section is `if (!stop) do { ... } while (0);`, so an exit (`stop = true; break;`) skips the
+    // rest of the section and every later one, and the lanes meet again at UW_SYNC() between
+    // sections.  (Lanes that leave a loop at different iterations otherwise run apart for the rest
+    // of the column: the worklist kernel ran with 1.9 of 32 lanes active.)  Loops marked `uniform`
+    // have the same trip count on every live lane; UW_SYNC() appears only directly inside them.
+    for (int iter = 1; iter <= (MODE == UW_MODE_TRIGGER ? 1 : 2); iter++) {   // uniform
+        double tscaleh = 0.0;
+        if (!stop) do {
+        tscaleh = cush;
         cush = -1.0;
 
-        // kinv (:1455-1468)
+        // kinv (:1455-1468): the first interface from the top whose layer brackets pblh + 5
         kinv = 1;
-        for (int k = mkx - 1; k >= 1; k--) {
-            if ((pblh + 5.0 - zs0[k]) * (pblh + 5.0 - zs0[k + 1]) < 0.0) {
-                kinv = k + 1;
-                break;
+        {
+            bool found = false;
+            for (int k = mkx - 1; k >= 1; k--) {
+                if (!found && (pblh + 5.0 - zs0[k]) * (pblh + 5.0 - zs0[k + 1]) < 0.0) {
+                    kinv = k + 1;
+                    found = true;
+                }
             }
         }
         if (kinv <= 1) {
@@ -615,7 +643,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
             double dpsum = 0.0;
             tkeavg = 0.0;
             thvlmin = 1000.0;
-            for (int k = 0; k <= kinv - 1; k++) {
+            for (int k = 0; k <= mkx; k++) {
+                if (k > kinv - 1) continue;
                 double dpi;
                 if (k == 0) dpi = ps0[0] - p0[1];
                 else if (k == (kinv - 1)) dpi = p0[kinv - 1] - ps0[kinv - 1];
@@ -633,13 +662,19 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
         usrc = GL(u0, kinv - 1) + ssu0[kinv - 1] * (ps0[kinv - 1] - p0[kinv - 1]);
         vsrc = GL(v0, kinv - 1) + ssv0[kinv - 1] * (ps0[kinv - 1] - p0[kinv - 1]);
         for (int m = 1; m <= ncnst; m++) trsrc[m - 1] = GT(m, 1);
+        } while (0);
+        UW_SYNC();
         // LCL (:1533-1549)
+        if (!stop) do {
         plcl = qsinvert(qtsrc, thlsrc, ps0[0], exns0[0], tbl);
         klcl = mkx;
-        for (int k = 0; k <= mkx; k++) {
-            if (ps0[k] < plcl) {
-                klcl = k;
-                break;
+        {
+            bool found = false;
+            for (int k = 0; k <= mkx; k++) {
+                if (!found && ps0[k] < plcl) {
+                    klcl = k;
+                    found = true;
+                }
             }
         }
         klcl = MX(1, klcl);
@@ -661,20 +696,42 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
             }
             thv0lcl = thj * (1.0 + zvir * qvj - qlj - qij);
         }
-        // CIN (:1592-1685)
-        cin = 0.0;
-        cinlcl = 0.0;
-        plfc = 0.0;
-        klfc = mkx;
+        } while (0);
+        UW_SYNC();
+        // CIN (:1592-1685).  One loop over k = kinv .. mkx-1 serves both cases of the Fortran (LCL at
+        // or above kinv, LCL below kinv), with one conden call at ps0(k) per level for every lane.
+        // When the LCL is below kinv the Fortran also calls conden at ps0(k-1) with the same source
+        // air; above the first level that repeats the previous level's call bit for bit, so only
+        // the first level makes it here.
+        if (!stop) {
+            cin = 0.0;
+            cinlcl = 0.0;
+            plfc = 0.0;
+            klfc = mkx;
+        }
         {
-            double thvubot, thvutop = 0.0;
-            if (klcl >= kinv) {
-                for (int k = kinv; k <= mkx - 1; k++) {
-                    if (k < klcl) {
+            const bool lcl_above = (klcl >= kinv);
+            double thvubot = 0.0, thvutop = 0.0;
+            bool ldone = stop;
+            for (int k = 2; k <= mkx - 1; k++) {   // uniform (kinv >= 2)
+                if (!ldone && k >= kinv) do {
+                    if (lcl_above && k < klcl) {
                         thvubot = thvlsrc;
                         thvutop = thvlsrc;
                         cin = cin + single_cin(ps0[k - 1], exns0[k - 1], thv0bot[k], ps0[k], exns0[k], thv0top[k], thvubot, thvutop);
-                    } else if (k == klcl) {
+                        break;
+                    }
+                    if (!lcl_above && k == kinv) {
+                        if (conden(ps0[k - 1], exns0[k - 1], thlsrc, qtsrc, thj, qvj, qlj, qij, tbl)) {
+                            xflags |= UW_X_CONDEN;
+                            id_exit = true;
+                            stop = true;
+                            break;
+                        }
+                        thvutop = thj * (1.0 + zvir * qvj - qlj - qij);
+                    }
+                    const bool atlcl = lcl_above && k == klcl;
+                    if (atlcl) {
                         thvubot = thvlsrc;
                         thvutop = thvlsrc;
                         cin = cin + single_cin(ps0[k - 1], exns0[k - 1], thv0bot[k], plcl, exlcl, thv0lcl, thvubot, thvutop);
@@ -682,60 +739,28 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                         cinlcl = MX(cin, 0.0);
                         cin = cinlcl;
                         thvubot = thvlsrc;
-                        if (conden(ps0[k], exns0[k], thlsrc, qtsrc, thj, qvj, qlj, qij, tbl)) {
-                            xflags |= UW_X_CONDEN;
-                            id_exit = true;
-                            stop = true;
-            break;
-                        }
-                        thvutop = thj * (1.0 + zvir * qvj - qlj - qij);
-                        getbuoy(plcl, exlcl, thv0lcl, ps0[k], exns0[k], thv0top[k], thvubot, thvutop, plfc, cin);
-                        if (plfc > 0.0) {
-                            klfc = k;
-                            break;
-                        }
                     } else {
                         thvubot = thvutop;
-                        if (conden(ps0[k], exns0[k], thlsrc, qtsrc, thj, qvj, qlj, qij, tbl)) {
-                            xflags |= UW_X_CONDEN;
-                            id_exit = true;
-                            stop = true;
-            break;
-                        }
-                        thvutop = thj * (1.0 + zvir * qvj - qlj - qij);
-                        getbuoy(ps0[k - 1], exns0[k - 1], thv0bot[k], ps0[k], exns0[k], thv0top[k], thvubot, thvutop, plfc, cin);
-                        if (plfc > 0.0) {
-                            klfc = k;
-                            break;
-                        }
                     }
-                }
-            } else {
-                cinlcl = 0.0;
-                for (int k = kinv; k <= mkx - 1; k++) {
-                    if (conden(ps0[k - 1], exns0[k - 1], thlsrc, qtsrc, thj, qvj, qlj, qij, tbl)) {
-                        xflags |= UW_X_CONDEN;
-                        id_exit = true;
-                        stop = true;
-            break;
-                    }
-                    thvubot = thj * (1.0 + zvir * qvj - qlj - qij);
                     if (conden(ps0[k], exns0[k], thlsrc, qtsrc, thj, qvj, qlj, qij, tbl)) {
                         xflags |= UW_X_CONDEN;
                         id_exit = true;
                         stop = true;
-            break;
-                    }
-                    thvutop = thj * (1.0 + zvir * qvj - qlj - qij);
-                    getbuoy(ps0[k - 1], exns0[k - 1], thv0bot[k], ps0[k], exns0[k], thv0top[k], thvubot, thvutop, plfc, cin);
-                    if (plfc > 0.0) {
-                        klfc = k;
                         break;
                     }
-                }
+                    thvutop = thj * (1.0 + zvir * qvj - qlj - qij);
+                    getbuoy(atlcl ? plcl : ps0[k - 1], atlcl ? exlcl : exns0[k - 1], atlcl ? thv0lcl : thv0bot[k],
+                            ps0[k], exns0[k], thv0top[k], thvubot, thvutop, plfc, cin);
+                    if (plfc > 0.0) {
+                        klfc = k;
+                        ldone = true;
+                    }
+                } while (0);
+                if (stop) ldone = true;
             }
         }
-        if (stop) break;
+        UW_SYNC();
+        if (!stop) do {
         // (label 35, :1676-1685)
         if (cin < 0.0) lflags |= UW_L_CIN;
         cin = MX(0.0, cin);
@@ -824,7 +849,10 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
             }
         }
 
+        } while (0);
+        UW_SYNC();
         // ---- release level and closure (:2035-2184) ------------------------------------------
+        if (!stop) do {
         if (klcl < kinv) {
             krel = kinv;
             prel = ps0[krel - 1];
@@ -880,18 +908,24 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
             break;
             }
             ufrc[krel - 1] = ufrclcl;
-            for (int k = kinv - 1; k <= krel - 1; k++) {
+            for (int k = 0; k <= mkx; k++) {
+                if (k < kinv - 1 || k > krel - 1) continue;
                 umf[k] = cbmf;
                 wu[k] = winv;
             }
         }
+        } while (0);
         if (MODE == UW_MODE_TRIGGER) {
             // the column convects past the closure: hand it to the worklist pass
-            cand = true;
-            stop = true;
-            break;
+            if (!stop) {
+                cand = true;
+                stop = true;
+            }
         }
+        UW_SYNC();
+        if (MODE != UW_MODE_TRIGGER) {   // uniform
         // updraft at the release level (:2205-2236)
+        if (!stop) do {
         emf[krel - 1] = 0.0;
         umf[krel - 1] = cbmf;
         wu[krel - 1] = wlcl;
@@ -910,7 +944,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                 uplus = PGFc * ssu0[kinv] * (prel - ps0[kinv - 1]);
                 vplus = PGFc * ssv0[kinv] * (prel - ps0[kinv - 1]);
             } else {
-                for (int k = kinv; k <= MX(krel - 1, kinv); k++) {
+                for (int k = 0; k <= mkx; k++) {
+                    if (k < kinv || k > MX(krel - 1, kinv)) continue;
                     uplus = uplus + PGFc * ssu0[k] * (ps0[k] - ps0[k - 1]);
                     vplus = vplus + PGFc * ssv0[k] * (ps0[k] - ps0[k - 1]);
                 }
@@ -921,32 +956,44 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
             vu[krel - 1] = vsrc + vplus;
         }
         for (int m = 0; m < ncnst; m++) tru[m][krel - 1] = trsrc[m];
+        } while (0);
+        UW_SYNC();
 
         {
             double scaleh = tscaleh;
             if (tscaleh < 0.0) scaleh = 1000.0;
             // ---- buoyancy-sorting updraft, iter_scaleh loop (:2306-2952) ----------------------
-            for (int iter_scaleh = 1; iter_scaleh <= 3; iter_scaleh++) {
-                kbup = krel;
-                kpen = krel;
-                wtw = wlcl * wlcl;
-                double pe = 0.5 * (prel + ps0[krel]);
-                double dpe = prel - ps0[krel];
-                double exne = exnf(pe);
-                double thvebot = thv0rel;
-                double thle = thl0[krel] + ssthl0[krel] * (pe - p0[krel]);
-                double qte = qt0[krel] + ssqt0[krel] * (pe - p0[krel]);
-                double ue = GL(u0, krel) + ssu0[krel] * (pe - p0[krel]);
-                double ve = GL(v0, krel) + ssv0[krel] * (pe - p0[krel]);
-                for (int m = 0; m < ncnst; m++) tre[m] = GT(m + 1, krel) + sstr0[m][krel] * (pe - p0[krel]);
+            for (int iter_scaleh = 1; iter_scaleh <= 3; iter_scaleh++) {   // uniform
+                double pe = 0.0, dpe = 0.0, exne = 1.0, thvebot = 0.0, thle = 0.0, qte = 0.0, ue = 0.0, ve = 0.0;
+                if (!stop) {
+                    kbup = krel;
+                    kpen = krel;
+                    wtw = wlcl * wlcl;
+                    pe = 0.5 * (prel + ps0[krel]);
+                    dpe = prel - ps0[krel];
+                    exne = exnf(pe);
+                    thvebot = thv0rel;
+                    thle = thl0[krel] + ssthl0[krel] * (pe - p0[krel]);
+                    qte = qt0[krel] + ssqt0[krel] * (pe - p0[krel]);
+                    ue = GL(u0, krel) + ssu0[krel] * (pe - p0[krel]);
+                    ve = GL(v0, krel) + ssv0[krel] * (pe - p0[krel]);
+                    for (int m = 0; m < ncnst; m++) tre[m] = GT(m + 1, krel) + sstr0[m][krel] * (pe - p0[krel]);
+                }
 
-                for (int k = krel; k <= mkx - 1; k++) {
+                // levels k = krel .. mkx-1, taken by every lane as k = krel + j
+                bool ldone = stop;
+                for (int j = 0; j <= mkx - 2; j++) {   // uniform
+                    const int k = krel + j;
+                    if (k > mkx - 1) ldone = true;
+                    if (!ldone) do {
                     const int km1 = k - 1;
                     double thlue = thlu[km1];
                     double qtue = qtu[km1];
                     double wue = wu[km1];
                     wtwb = wtw;
+                    bool xdone = false;
                     for (int iter_xc = 1; iter_xc <= 2; iter_xc++) {
+                        if (!xdone && !stop) do {
                         wtw = wu[km1] * wu[km1];
                         if (conden(pe, exne, thle, qte, thj, qvj, qlj, qij, tbl)) {
                             xflags |= UW_X_CONDEN;
@@ -1092,8 +1139,9 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                             qtue = 0.5 * (qtu[km1] + qtu[k]);
                             wue = 0.5 * sqrt(MX(wtwb + wtw, 0.0));
                         } else {
-                            break;   // go to 111
+                            xdone = true;   // go to 111
                         }
+                        } while (0);
                     }
                     if (stop) break;
                     // (label 111, :2726-2793)
@@ -1101,6 +1149,7 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                     if (bogtop > 0.0 && wtw > 0.0) kbup = k;
                     if (wtw <= 0.0) {
                         kpen = k;
+                        ldone = true;
                         break;   // go to 45
                     }
                     wu[k] = sqrt(wtw);
@@ -1129,9 +1178,13 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                     ue = GL(u0, k + 1);
                     ve = GL(v0, k + 1);
                     for (int m = 0; m < ncnst; m++) tre[m] = GT(m + 1, k + 1);
+                    } while (0);
+                    if (stop) ldone = true;
+                    UW_SYNC();
                 }
-                if (stop) break;
+                UW_SYNC();
                 // (label 45) penetration depth (:2884-2907)
+                if (!stop) do {
                 if (drage == 0.0) {
                     double aquad = (bogtop - bogbot) / (ps0[kpen] - ps0[kpen - 1]);
                     double bquad = 2.0 * bogbot;
@@ -1186,10 +1239,12 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                     cush = zs0[kpen - 1] - ppen / rhos0j / g;
                 }
                 scaleh = cush;
+                } while (0);
+                UW_SYNC();
             }
         }
-        if (stop) break;
         // forcedCu filter (:2964-2992)
+        if (!stop) do {
         if (kbup == krel) {
             lflags |= UW_L_SHCU;
             xflags |= UW_X_CUFILTER;
@@ -1198,12 +1253,14 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
             break;
         }
         lflags &= ~UW_L_SHCU;
-        for (int k = kpen; k <= mkx; k++) {
+        for (int k = 0; k <= mkx; k++) {
+            if (k < kpen) continue;
             umf[k] = 0.0;
             emf[k] = 0.0;
             ufrc[k] = 0.0;
         }
-        for (int k = kpen + 1; k <= mkx; k++) {
+        for (int k = 0; k <= mkx; k++) {
+            if (k < kpen + 1) continue;
             dwten[k] = 0.0;
             diten[k] = 0.0;
             fer[k] = 0.0;
@@ -1217,7 +1274,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
             vu_emf[k] = vu[k];
             for (int m = 0; m < ncnst; m++) tru_emf[m][k] = tru[m][k];
         }
-        for (int k = kpen - 1; k >= kbup; k--) {
+        for (int k = mkx; k >= 0; k--) {
+            if (k > kpen - 1 || k < kbup) continue;
             double rhos0j = ps0[k] / (r * 0.5 * (thv0bot[k + 1] + thv0top[k]) * exns0[k]);
             if (k == kpen - 1) {
                 if ((umf[k] * ppen * rei[kpen] * rpen) < -0.1 * rhos0j) lflags |= UW_L_EMF;
@@ -1254,38 +1312,39 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
             double xtop = qt0[kinv + 1] + ssqt0[kinv + 1] * (ps0[kinv] - p0[kinv + 1]);
             double xbot = qt0[kinv - 1] + ssqt0[kinv - 1] * (ps0[kinv - 1] - p0[kinv - 1]);
             fluxbelowinv(cbmf, ps0, kinv, dt, xsrc, xmean, xtop, xbot, xflx);
-            for (int k = 0; k <= kinv - 1; k++) qtflx[k] = xflx[k];
+            for (int k = 0; k <= mkx; k++) if (k <= kinv - 1) qtflx[k] = xflx[k];
             xsrc = thlsrc;
             xmean = thl0[kinv];
             xtop = thl0[kinv + 1] + ssthl0[kinv + 1] * (ps0[kinv] - p0[kinv + 1]);
             xbot = thl0[kinv - 1] + ssthl0[kinv - 1] * (ps0[kinv - 1] - p0[kinv - 1]);
             fluxbelowinv(cbmf, ps0, kinv, dt, xsrc, xmean, xtop, xbot, xflx);
-            for (int k = 0; k <= kinv - 1; k++) slflx[k] = cp * exns0[k] * xflx[k];
+            for (int k = 0; k <= mkx; k++) if (k <= kinv - 1) slflx[k] = cp * exns0[k] * xflx[k];
             xsrc = usrc;
             xmean = GL(u0, kinv);
             xtop = GL(u0, kinv + 1) + ssu0[kinv + 1] * (ps0[kinv] - p0[kinv + 1]);
             xbot = GL(u0, kinv - 1) + ssu0[kinv - 1] * (ps0[kinv - 1] - p0[kinv - 1]);
             fluxbelowinv(cbmf, ps0, kinv, dt, xsrc, xmean, xtop, xbot, xflx);
-            for (int k = 0; k <= kinv - 1; k++) uflx[k] = xflx[k];
+            for (int k = 0; k <= mkx; k++) if (k <= kinv - 1) uflx[k] = xflx[k];
             xsrc = vsrc;
             xmean = GL(v0, kinv);
             xtop = GL(v0, kinv + 1) + ssv0[kinv + 1] * (ps0[kinv] - p0[kinv + 1]);
             xbot = GL(v0, kinv - 1) + ssv0[kinv - 1] * (ps0[kinv - 1] - p0[kinv - 1]);
             fluxbelowinv(cbmf, ps0, kinv, dt, xsrc, xmean, xtop, xbot, xflx);
-            for (int k = 0; k <= kinv - 1; k++) vflx[k] = xflx[k];
+            for (int k = 0; k <= mkx; k++) if (k <= kinv - 1) vflx[k] = xflx[k];
             for (int m = 0; m < ncnst; m++) {
                 xsrc = trsrc[m];
                 xmean = GT(m + 1, kinv);
                 xtop = GT(m + 1, kinv + 1) + sstr0[m][kinv + 1] * (ps0[kinv] - p0[kinv + 1]);
                 xbot = GT(m + 1, kinv - 1) + sstr0[m][kinv - 1] * (ps0[kinv - 1] - p0[kinv - 1]);
                 fluxbelowinv(cbmf, ps0, kinv, dt, xsrc, xmean, xtop, xbot, xflx);
-                for (int k = 0; k <= kinv - 1; k++) trflx[m][k] = xflx[k];
+                for (int k = 0; k <= mkx; k++) if (k <= kinv - 1) trflx[m][k] = xflx[k];
             }
         }
         // 2. non-buoyancy-sorting fluxes (:3300-3313)
         {
             double uplus = 0.0, vplus = 0.0;
-            for (int k = kinv; k <= krel - 1; k++) {
+            for (int k = 0; k <= mkx; k++) {
+                if (k < kinv || k > krel - 1) continue;
                 const int kp1 = k + 1;
                 qtflx[k] = cbmf * (qtsrc - (qt0[kp1] + ssqt0[kp1] * (ps0[k] - p0[kp1])));
                 slflx[k] = cbmf * (thlsrc - (thl0[kp1] + ssthl0[kp1] * (ps0[k] - p0[kp1]))) * cp * exns0[k];
@@ -1298,7 +1357,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
             }
         }
         // 3. buoyancy-sorting fluxes (:3322-3331)
-        for (int k = krel; k <= kbup - 1; k++) {
+        for (int k = 0; k <= mkx; k++) {
+            if (k < krel || k > kbup - 1) continue;
             const int kp1 = k + 1;
             slflx[k] = cp * exns0[k] * umf[k] * (thlu[k] - (thl0[kp1] + ssthl0[kp1] * (ps0[k] - p0[kp1])));
             qtflx[k] = umf[k] * (qtu[k] - (qt0[kp1] + ssqt0[kp1] * (ps0[k] - p0[kp1])));
@@ -1308,7 +1368,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                 trflx[m][k] = umf[k] * (tru[m][k] - (GT(m + 1, kp1) + sstr0[m][kp1] * (ps0[k] - p0[kp1])));
         }
         // 4. penetrative-entrainment fluxes (:3392-3401)
-        for (int k = kbup; k <= kpen - 1; k++) {
+        for (int k = 0; k <= mkx; k++) {
+            if (k < kbup || k > kpen - 1) continue;
             slflx[k] = cp * exns0[k] * emf[k] * (thlu_emf[k] - (thl0[k] + ssthl0[k] * (ps0[k] - p0[k])));
             qtflx[k] = emf[k] * (qtu_emf[k] - (qt0[k] + ssqt0[k] * (ps0[k] - p0[k])));
             uflx[k] = emf[k] * (uu_emf[k] - (GL(u0, k) + ssu0[k] * (ps0[k] - p0[k])));
@@ -1316,13 +1377,18 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
             for (int m = 0; m < ncnst; m++)
                 trflx[m][k] = emf[k] * (tru_emf[m][k] - (GT(m + 1, k) + sstr0[m][k] * (ps0[k] - p0[k])));
         }
+        } while (0);
+        UW_SYNC();
         // condensate tendency by compensating subsidence (:3416-3476)
         {
             // uemf(k), evaluated on demand with the same expressions as :3416-3422
 #define UEMF(kk)                                                                                          \
     ((kk) <= kinv - 2 ? cbmf * (ps0[0] - ps0[(kk)]) / (ps0[0] - ps0[kinv - 1])                             \
                       : ((kk) <= krel - 1 ? cbmf : ((kk) <= kbup - 1 ? umf[(kk)] : ((kk) <= kpen - 1 ? emf[(kk)] : 0.0))))
-            for (int k = 1; k <= kpen; k++) {
+            bool ldone = stop;
+            for (int k = 1; k <= mkx; k++) {   // uniform
+                if (k > kpen) ldone = true;
+                if (!ldone) do {
                 double comsub = 0.5 * (UEMF(k) + UEMF(k - 1));
                 double thlten_sub, qtten_sub, qlten_sub, qiten_sub, nlten_sub, niten_sub;
                 if (comsub >= 0.0) {
@@ -1361,12 +1427,16 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                 qiten_sink[k] = MX(qiten_sub, -qi0[k] / dt);
                 nlten_sink[k] = MX(nlten_sub, -GT(ixnumliq, k) / dt);
                 niten_sink[k] = MX(niten_sub, -GT(ixnumice, k) / dt);
+                } while (0);
+                if (stop) ldone = true;
             }
 #undef UEMF
         }
-        if (stop) break;
+        UW_SYNC();
+        if (!stop) do {
         // momentum tendency (:3488-3501)
-        for (int k = 1; k <= kpen; k++) {
+        for (int k = 1; k <= mkx; k++) {
+            if (k > kpen) continue;
             uten[k] = (uflx[k - 1] - uflx[k]) * g / dp0[k];
             vten[k] = (vflx[k - 1] - vflx[k]) * g / dp0[k];
             uf[k] = GL(u0, k) + uten[k] * dt;
@@ -1376,9 +1446,14 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
         rliq = 0.0;
         rainflx = 0.0;
         snowflx = 0.0;
+        } while (0);
+        UW_SYNC();
         {
             double qlubelow = 0.0, qiubelow = 0.0;
-            for (int k = 1; k <= kpen; k++) {
+            bool ldone = stop;
+            for (int k = 1; k <= mkx; k++) {   // uniform
+                if (k > kpen) ldone = true;
+                if (!ldone) do {
                 const int km1 = k - 1;
                 dwten[k] = dwten[k] * 0.5 * (umf[k - 1] + umf[k]) * g / dp0[k];
                 diten[k] = diten[k] * 0.5 * (umf[k - 1] + umf[k]) * g / dp0[k];
@@ -1414,41 +1489,36 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                     qiu_mid = 0.0;
                     qlj = 0.0;
                     qij = 0.0;
-                } else if (k == krel) {
-                    if (conden(prel, exprel, thlu[krel - 1], qtu[krel - 1], thj, qvj, qlj, qij, tbl)) {
-                        xflags |= UW_X_CONDEN;
-                        id_exit = true;
-                        stop = true;
-            break;
-                    }
-                    qlubelow = qlj;
-                    qiubelow = qij;
-                    if (conden(ps0[k], exns0[k], thlu[k], qtu[k], thj, qvj, qlj, qij, tbl)) {
-                        xflags |= UW_X_CONDEN;
-                        id_exit = true;
-                        stop = true;
-            break;
-                    }
-                    qlu_mid = 0.5 * (qlubelow + qlj) * (prel - ps0[k]) / (ps0[k - 1] - ps0[k]);
-                    qiu_mid = 0.5 * (qiubelow + qij) * (prel - ps0[k]) / (ps0[k - 1] - ps0[k]);
-                } else if (k == kpen) {
-                    if (conden(ps0[k - 1] + ppen, exntop, thlu_top, qtu_top, thj, qvj, qlj, qij, tbl)) {
-                        xflags |= UW_X_CONDEN;
-                        id_exit = true;
-                        stop = true;
-            break;
-                    }
-                    qlu_mid = 0.5 * (qlubelow + qlj) * (-ppen) / (ps0[k - 1] - ps0[k]);
-                    qiu_mid = 0.5 * (qiubelow + qij) * (-ppen) / (ps0[k - 1] - ps0[k]);
                 } else {
-                    if (conden(ps0[k], exns0[k], thlu[k], qtu[k], thj, qvj, qlj, qij, tbl)) {
+                    // one conden call site for the release level, the cloud top and the levels between
+                    const bool atrel = (k == krel), attop = (k != krel && k == kpen);
+                    if (atrel) {
+                        if (conden(prel, exprel, thlu[krel - 1], qtu[krel - 1], thj, qvj, qlj, qij, tbl)) {
+                            xflags |= UW_X_CONDEN;
+                            id_exit = true;
+                            stop = true;
+                            break;
+                        }
+                        qlubelow = qlj;
+                        qiubelow = qij;
+                    }
+                    if (conden(attop ? ps0[k - 1] + ppen : ps0[k], attop ? exntop : exns0[k], attop ? thlu_top : thlu[k],
+                               attop ? qtu_top : qtu[k], thj, qvj, qlj, qij, tbl)) {
                         xflags |= UW_X_CONDEN;
                         id_exit = true;
                         stop = true;
-            break;
+                        break;
                     }
-                    qlu_mid = 0.5 * (qlubelow + qlj);
-                    qiu_mid = 0.5 * (qiubelow + qij);
+                    if (atrel) {
+                        qlu_mid = 0.5 * (qlubelow + qlj) * (prel - ps0[k]) / (ps0[k - 1] - ps0[k]);
+                        qiu_mid = 0.5 * (qiubelow + qij) * (prel - ps0[k]) / (ps0[k - 1] - ps0[k]);
+                    } else if (attop) {
+                        qlu_mid = 0.5 * (qlubelow + qlj) * (-ppen) / (ps0[k - 1] - ps0[k]);
+                        qiu_mid = 0.5 * (qiubelow + qij) * (-ppen) / (ps0[k - 1] - ps0[k]);
+                    } else {
+                        qlu_mid = 0.5 * (qlubelow + qlj);
+                        qiu_mid = 0.5 * (qiubelow + qij);
+                    }
                 }
                 qlubelow = qlj;
                 qiubelow = qij;
@@ -1498,10 +1568,13 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                 sten[k] = slten[k] + xlv * qlten[k] + xls * qiten[k];
                 qc[k] = qc_l[k] + qc_i[k];
                 rliq = rliq + qc[k] * dp0[k] / g / 1000.0;
+                } while (0);
+                if (stop) ldone = true;
             }
         }
-        if (stop) break;
+        UW_SYNC();
         // evaporation and melting of precipitation (:3808-3934)
+        if (!stop) do {
         {
             double evpint_rain = 0.0, evpint_snow = 0.0;
             for (int k = 0; k <= mkx; k++) {
@@ -1552,7 +1625,8 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
             snow = flxsnow[0] / 1000.0;
         }
         // remove detrained condensate (:3966-3981)
-        for (int k = 1; k <= kpen; k++) {
+        for (int k = 1; k <= mkx; k++) {
+            if (k > kpen) continue;
             qtten[k] = qtten[k] - qc[k];
             qlten[k] = qlten[k] - qc_l[k];
             qiten[k] = qiten[k] - qc_i[k];
@@ -1638,17 +1712,23 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
             stop = true;
             break;
         }
+        } while (0);
+        UW_SYNC();
         {
             double qcubelow = qlj + qij, qlubelow = qlj, qiubelow = qij;
-            for (int k = krel; k <= kpen; k++) {
-                int idc;
-                if (k == kpen) idc = conden(ps0[k - 1] + ppen, exntop, thlu_top, qtu_top, thj, qvj, qlj, qij, tbl);
-                else idc = conden(ps0[k], exns0[k], thlu[k], qtu[k], thj, qvj, qlj, qij, tbl);
+            bool ldone = stop;
+            for (int j = 0; j <= mkx; j++) {   // uniform
+                const int k = krel + j;
+                if (k > kpen) ldone = true;
+                if (!ldone) do {
+                const bool attop = (k == kpen);
+                const int idc = conden(attop ? ps0[k - 1] + ppen : ps0[k], attop ? exntop : exns0[k],
+                                       attop ? thlu_top : thlu[k], attop ? qtu_top : qtu[k], thj, qvj, qlj, qij, tbl);
                 if (idc) {
                     xflags |= UW_X_CONDEN;
                     id_exit = true;
                     stop = true;
-            break;
+                    break;
                 }
                 qcu[k] = 0.5 * (qcubelow + qlj + qij);
                 qlu[k] = 0.5 * (qlubelow + qlj);
@@ -1667,9 +1747,12 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                 qcubelow = qlj + qij;
                 qlubelow = qlj;
                 qiubelow = qij;
+                } while (0);
+                if (stop) ldone = true;
             }
         }
-        if (stop) break;
+        UW_SYNC();
+        if (!stop) do {
         cnt = (double)kpen;
         cnb = (double)(krel - 1);
 
@@ -1715,14 +1798,20 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
             }
             slope<KP>(mkx, thl0, p0, ssthl0);
             slope<KP>(mkx, qt0, p0, ssqt0);
-            for (int k = 1; k <= mkx; k++) {
+        }
+        } while (0);
+        UW_SYNC();
+        if (iter == 1) {   // uniform
+            bool ldone = stop;
+            for (int k = 1; k <= mkx; k++) {   // uniform
+                if (!ldone) do {
                 double thl0bot = thl0[k] + ssthl0[k] * (ps0[k - 1] - p0[k]);
                 double qt0bot = qt0[k] + ssqt0[k] * (ps0[k - 1] - p0[k]);
                 if (conden(ps0[k - 1], exns0[k - 1], thl0bot, qt0bot, thj, qvj, qlj, qij, tbl)) {
                     xflags |= UW_X_CONDEN;
                     id_exit = true;
                     stop = true;
-            break;
+                    break;
                 }
                 thv0bot[k] = thj * (1.0 + zvir * qvj - qlj - qij);
                 thvl0bot[k] = thl0bot * (1.0 + zvir * qt0bot);
@@ -1732,13 +1821,16 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
                     xflags |= UW_X_CONDEN;
                     id_exit = true;
                     stop = true;
-            break;
+                    break;
                 }
                 thv0top[k] = thj * (1.0 + zvir * qvj - qlj - qij);
                 thvl0top[k] = thl0top * (1.0 + zvir * qt0top);
+                } while (0);
+                if (stop) ldone = true;
             }
-            if (stop) break;
         }
+        UW_SYNC();
+        }   // MODE != UW_MODE_TRIGGER
     }
 
     // ---- final outputs (uwshcu.F90:4337-4370) --------------------------------------------------
@@ -1836,6 +1928,7 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
             if (cand) wl[base + __popc(mask & ((1u << lane) - 1u))] = i;
         }
     }
+#undef UW_SYNC
 #undef RI
 #undef RL
 #undef CNT
