@@ -94,3 +94,17 @@ struct UwArgs {
     double *diag_real;   // optional (UW_NDR, mix)
     unsigned int *err;   // device error word
 };
+
+// ---- batched launches --------------------------------------------------------------------------
+// Members of one batch that share a level/tracer class run in one trigger launch and one persistent
+// worklist launch.  Passed by value as a __grid_constant__ kernel parameter.
+#define UW_MAXM 8
+struct UwBatch {
+    int nm;                          // members in this launch (<= UW_MAXM)
+    int chunk;                       // worklist entries per task = 32 * chunk
+    int block_start[UW_MAXM + 1];    // trigger launch: first block of each member
+    int *count;                      // per-member worklist counts (device, nm ints)
+    int *task_head;                  // device task counter of the persistent worklist launch
+    int *wl[UW_MAXM];                // per-member worklists (device)
+    UwArgs m[UW_MAXM];
+};

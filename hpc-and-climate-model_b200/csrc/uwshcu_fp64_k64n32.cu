@@ -21,3 +21,30 @@ extern "C" cudaError_t uw_fp64_launch_k64n32(const UwArgs* a, int mode, int* wl,
     else uwshcu_fp64_kernel<64, 32, UW_MODE_LIST><<<grid, block, 0, stream>>>(*a, wl, wl_count);
     return cudaGetLastError();
 }
+
+// Batched trigger (phase 0) and persistent worklist (phase 1) launches; minb selects the
+// worklist instantiation (register cap = 65536 / (128 * minb)).  Returns cudaErrorInvalidValue
+// for a minb that is not compiled here.
+extern "C" cudaError_t uw_fp64_batch_k64n32(const UwBatch* b, int phase, int grid, int block, int minb,
+                                          cudaStream_t stream)
+{
+    if (grid <= 0) return cudaSuccess;
+    if (phase == 0) {
+        uwshcu_batch_trigger<64, 32><<<grid, block, 0, stream>>>(*b);
+        return cudaGetLastError();
+    }
+    if (minb == 4) {
+        uwshcu_batch_list<64, 32, 4><<<grid, block, 0, stream>>>(*b);
+        return cudaGetLastError();
+    }
+    return cudaErrorInvalidValue;
+}
+
+// Resident blocks per SM of the worklist instantiation minb at this block size (0 if absent).
+extern "C" cudaError_t uw_fp64_batch_occupancy_k64n32(int minb, int block, int* blocks_per_sm)
+{
+    *blocks_per_sm = 0;
+    if (minb == 4)
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, uwshcu_batch_list<64, 32, 4>, block, 0);
+    return cudaSuccess;
+}

@@ -21,3 +21,42 @@ extern "C" cudaError_t uw_fp64_launch_k64n5(const UwArgs* a, int mode, int* wl, 
     else uwshcu_fp64_kernel<64, 5, UW_MODE_LIST><<<grid, block, 0, stream>>>(*a, wl, wl_count);
     return cudaGetLastError();
 }
+
+// Batched trigger (phase 0) and persistent worklist (phase 1) launches; minb selects the
+// worklist instantiation (register cap = 65536 / (128 * minb)).  Returns cudaErrorInvalidValue
+// for a minb that is not compiled here.
+extern "C" cudaError_t uw_fp64_batch_k64n5(const UwBatch* b, int phase, int grid, int block, int minb,
+                                          cudaStream_t stream)
+{
+    if (grid <= 0) return cudaSuccess;
+    if (phase == 0) {
+        uwshcu_batch_trigger<64, 5><<<grid, block, 0, stream>>>(*b);
+        return cudaGetLastError();
+    }
+    if (minb == 3) {
+        uwshcu_batch_list<64, 5, 3><<<grid, block, 0, stream>>>(*b);
+        return cudaGetLastError();
+    }
+    if (minb == 4) {
+        uwshcu_batch_list<64, 5, 4><<<grid, block, 0, stream>>>(*b);
+        return cudaGetLastError();
+    }
+    if (minb == 6) {
+        uwshcu_batch_list<64, 5, 6><<<grid, block, 0, stream>>>(*b);
+        return cudaGetLastError();
+    }
+    return cudaErrorInvalidValue;
+}
+
+// Resident blocks per SM of the worklist instantiation minb at this block size (0 if absent).
+extern "C" cudaError_t uw_fp64_batch_occupancy_k64n5(int minb, int block, int* blocks_per_sm)
+{
+    *blocks_per_sm = 0;
+    if (minb == 3)
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, uwshcu_batch_list<64, 5, 3>, block, 0);
+    if (minb == 4)
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, uwshcu_batch_list<64, 5, 4>, block, 0);
+    if (minb == 6)
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, uwshcu_batch_list<64, 5, 6>, block, 0);
+    return cudaSuccess;
+}

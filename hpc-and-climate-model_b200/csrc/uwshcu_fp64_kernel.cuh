@@ -411,23 +411,13 @@ __device__ double findsp_point(double q, double t, double p, unsigned int& errbi
 #define UW_MODE_TRIGGER 1
 #define UW_MODE_LIST 2
 
+// One column per lane: column i of A when `active`.  All 32 lanes of the warp must call it together
+// (it starts with a warp ballot).  `tbl` is the saturation table in shared memory.  In
+// UW_MODE_TRIGGER, convecting columns are appended to wl / *wl_count.
 template <int KP, int NC, int MODE>
-__global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restrict__ wl, int* __restrict__ wl_count)
+__device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restrict__ tbl, const int i,
+                                          const bool active, int* __restrict__ wl, int* __restrict__ wl_count)
 {
-    __shared__ double tbl[UW_TBL];
-    for (int t = threadIdx.x; t < UW_TBL; t += blockDim.x) tbl[t] = c_estbl[t];
-    __syncthreads();
-
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    int i;
-    bool active;
-    if (MODE == UW_MODE_LIST) {
-        active = tid < *wl_count;
-        i = active ? wl[tid] : 0;
-    } else {
-        active = tid < A.iend;
-        i = tid;
-    }
     bool cand = false;
     // lanes of this warp that run a column; UW_SYNC() joins them where every one of them arrives
     const unsigned live = __ballot_sync(0xffffffffu, active);
@@ -1940,3 +1930,85 @@ __global__ void __launch_bounds__(128) uwshcu_fp64_kernel(UwArgs A, int* __restr
 #undef OT
 }
 
+// ---- kernels ---------------------------------------------------------------------------------------
+
+// The worklist pass is capped at 128 registers (4 blocks of 128 per SM instead of 3 at its natural
+// 168): the extra resident warps hide more FP64 and local-memory latency than the added spills
+// cost (-10 % time on the benchmark workload).
+template <int KP, int NC, int MODE>
+__global__ void __launch_bounds__(128, MODE == UW_MODE_LIST ? 4 : (MODE == UW_MODE_TRIGGER ? 5 : 3))
+uwshcu_fp64_kernel(const __grid_constant__ UwArgs A, int* __restrict__ wl, int* __restrict__ wl_count)
+{
+    __shared__ double tbl[UW_TBL];
+    for (int t = threadIdx.x; t < UW_TBL; t += blockDim.x) tbl[t] = c_estbl[t];
+    __syncthreads();
+
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    int i;
+    bool active;
+    if (MODE == UW_MODE_LIST) {
+        active = tid < *wl_count;
+        i = active ? wl[tid] : 0;
+    } else {
+        active = tid < A.iend;
+        i = tid;
+    }
+    uw_column<KP, NC, MODE>(A, tbl, i, active, wl, wl_count);
+}
+
+// Batched trigger pass: every column of every member of B (members of one level/tracer class).
+// Blocks [block_start[m], block_start[m+1]) cover member m; its convecting columns go to
+// wl[m] / count[m].
+template <int KP, int NC>
+__global__ void __launch_bounds__(128, 5) uwshcu_batch_trigger(const __grid_constant__ UwBatch B)
+{
+    __shared__ double tbl[UW_TBL];
+    for (int t = threadIdx.x; t < UW_TBL; t += blockDim.x) tbl[t] = c_estbl[t];
+    __syncthreads();
+
+    int m = 0;
+    while (m + 1 < B.nm && (int)blockIdx.x >= B.block_start[m + 1]) m++;
+    const int tid = ((int)blockIdx.x - B.block_start[m]) * blockDim.x + threadIdx.x;
+    const bool active = tid < B.m[m].iend;
+    uw_column<KP, NC, UW_MODE_TRIGGER>(B.m[m], tbl, tid, active, B.wl[m], B.count + m);
+}
+
+// Batched worklist pass, persistent: each warp takes the next task (32 * B.chunk consecutive queue
+// entries of one member) from the device counter *B.task_head until the queues are drained, so a
+// warp never mixes members (their level counts differ).  Task t of member m covers entries
+// [t * 32 * chunk, (t + 1) * 32 * chunk) of wl[m].
+template <int KP, int NC, int MINB>
+__global__ void __launch_bounds__(128, MINB) uwshcu_batch_list(const __grid_constant__ UwBatch B)
+{
+    __shared__ double tbl[UW_TBL];
+    for (int t = threadIdx.x; t < UW_TBL; t += blockDim.x) tbl[t] = c_estbl[t];
+    __syncthreads();
+
+    const int lane = threadIdx.x & 31;
+    const int per_task = 32 * B.chunk;
+    for (;;) {
+        int task = 0;
+        if (lane == 0) task = atomicAdd(B.task_head, 1);
+        task = __shfl_sync(0xffffffffu, task, 0);
+        int m = -1, first = 0;
+        for (int j = 0; j < B.nm; j++) {
+            const int nt = (B.count[j] + per_task - 1) / per_task;
+            if (m < 0) {
+                if (task < nt) {
+                    m = j;
+                    first = task * per_task;
+                } else {
+                    task -= nt;
+                }
+            }
+        }
+        if (m < 0) break;   // same task on every lane: the whole warp leaves
+        const int n = B.count[m];
+        for (int c = 0; c < B.chunk; c++) {
+            const int idx = first + c * 32 + lane;
+            const bool active = idx < n;
+            const int i = active ? B.wl[m][idx] : 0;
+            uw_column<KP, NC, UW_MODE_LIST>(B.m[m], tbl, i, active, nullptr, nullptr);
+        }
+    }
+}

@@ -901,3 +901,354 @@ extern "C" int uwshcu_compute_device_noalloc(
         return cuda_fail(e);
     return UWSHCU_OK;
 }
+
+// ---- batched uneven launches: plans ----------------------------------------------------------------
+#define UW_DECL_BATCH(KP, NC)                                                                         \
+    extern "C" cudaError_t uw_fp64_batch_k##KP##n##NC(const UwBatch* b, int phase, int grid, int block, \
+                                                      int minb, cudaStream_t stream);                 \
+    extern "C" cudaError_t uw_fp64_batch_occupancy_k##KP##n##NC(int minb, int block, int* blocks_per_sm);
+UW_DECL_BATCH(32, 5)
+UW_DECL_BATCH(64, 5)
+UW_DECL_BATCH(32, 32)
+UW_DECL_BATCH(64, 32)
+#undef UW_DECL_BATCH
+
+namespace {
+
+// Level/tracer classes of the compiled instantiations: bit 0 = 64-level bound, bit 1 = 32 tracers.
+constexpr int kClasses = 4;
+cudaError_t batch_launch(int cls, const UwBatch* b, int phase, int grid, int block, int minb, cudaStream_t st)
+{
+    switch (cls) {
+    case 0: return uw_fp64_batch_k32n5(b, phase, grid, block, minb, st);
+    case 1: return uw_fp64_batch_k64n5(b, phase, grid, block, minb, st);
+    case 2: return uw_fp64_batch_k32n32(b, phase, grid, block, minb, st);
+    default: return uw_fp64_batch_k64n32(b, phase, grid, block, minb, st);
+    }
+}
+cudaError_t batch_occupancy(int cls, int minb, int block, int* per_sm)
+{
+    switch (cls) {
+    case 0: return uw_fp64_batch_occupancy_k32n5(minb, block, per_sm);
+    case 1: return uw_fp64_batch_occupancy_k64n5(minb, block, per_sm);
+    case 2: return uw_fp64_batch_occupancy_k32n32(minb, block, per_sm);
+    default: return uw_fp64_batch_occupancy_k64n32(minb, block, per_sm);
+    }
+}
+// register caps compiled per class (the 32-tracer classes carry only the 128-register one)
+bool batch_has_minb(int cls, int minb) { return cls < 2 ? (minb == 3 || minb == 4 || minb == 6) : minb == 4; }
+
+struct BatchPlan {
+    int dev = 0;
+    int nm = 0;
+    uwshcu_member mem[UWSHCU_MAX_MEMBERS];
+    int ncls = 0;
+    int cls_id[kClasses];          // class of each used slot
+    UwBatch b[kClasses];           // per used class
+    int trig_grid[kClasses];
+    int* d_scratch = nullptr;      // [0, 64): counts of all members, [64, 64 + kClasses): task heads,
+                                   // then the worklists
+    unsigned int* d_err = nullptr;
+    double* d_cush_save = nullptr; // autotune only
+    int block = 128, minb = 4, chunk = 1;
+    int nsm = 1;
+    cudaGraphExec_t exec = nullptr;
+};
+
+int plan_enqueue(BatchPlan& P, cudaStream_t st)
+{
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(P.d_scratch, 0, (64 + kClasses) * sizeof(int), st)) != cudaSuccess) return cuda_fail(e);
+    for (int c = 0; c < P.ncls; c++) {
+        P.b[c].chunk = P.chunk;
+        if ((e = batch_launch(P.cls_id[c], &P.b[c], 0, P.trig_grid[c], P.block, 0, st)) != cudaSuccess) return cuda_fail(e);
+    }
+    for (int c = 0; c < P.ncls; c++) {
+        int per_sm = 0;
+        if ((e = batch_occupancy(P.cls_id[c], P.minb, P.block, &per_sm)) != cudaSuccess) return cuda_fail(e);
+        if (per_sm <= 0) return UWSHCU_ERR_BAD_ARGS;
+        if ((e = batch_launch(P.cls_id[c], &P.b[c], 1, P.nsm * per_sm, P.block, P.minb, st)) != cudaSuccess)
+            return cuda_fail(e);
+    }
+    return UWSHCU_OK;
+}
+
+void plan_free(BatchPlan* P)
+{
+    if (P->exec) cudaGraphExecDestroy(P->exec);
+    if (P->d_scratch) cudaFree(P->d_scratch);
+    if (P->d_err) cudaFree(P->d_err);
+    if (P->d_cush_save) cudaFree(P->d_cush_save);
+    delete P;
+}
+
+}  // namespace
+
+extern "C" int uwshcu_batch_create(int nmembers, const uwshcu_member* members, void** plan)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    if (!plan) return UWSHCU_ERR_BAD_ARGS;
+    *plan = nullptr;
+    if (!s.init) return UWSHCU_ERR_NOT_INITIALIZED;
+    if (nmembers < 1 || nmembers > UWSHCU_MAX_MEMBERS || !members) return UWSHCU_ERR_BAD_ARGS;
+    if (s.precision != UWSHCU_PREC_FP64) return UWSHCU_ERR_BAD_ARGS;   // the batch path is FP64
+    const int ncnst = s.k.ncnst;
+    size_t total = 0;
+    for (int j = 0; j < nmembers; j++) {
+        const uwshcu_member& m = members[j];
+        if (bad_dims(m.mix, m.mkx, m.iend, ncnst) || (m.inv != 0 && m.inv != 1)) return UWSHCU_ERR_BAD_ARGS;
+        const void* need[] = {m.ps0, m.zs0, m.p0, m.z0, m.dp0, m.u0, m.v0, m.qv0, m.ql0, m.qi0, m.t0, m.s0, m.tr0,
+                              m.tke, m.pblh, m.cush, m.umf, m.slflx, m.qtflx, m.flxprc1, m.flxsnow1, m.qvten,
+                              m.qlten, m.qiten, m.sten, m.uten, m.vten, m.trten, m.qrten, m.qsten, m.precip,
+                              m.snow, m.evapc, m.cufrc, m.qcu, m.qlu, m.qiu, m.cbmf, m.qc, m.rliq, m.cnt,
+                              m.cnb, m.dpdry0, m.wu};
+        for (const void* p : need)
+            if (!p) return UWSHCU_ERR_BAD_ARGS;
+        total += (size_t)m.iend;
+    }
+    DeviceState* d = nullptr;
+    int rc = ensure_device(&d);
+    if (rc != UWSHCU_OK) return rc;
+    BatchPlan* P = new BatchPlan();
+    P->nm = nmembers;
+    cudaError_t e;
+    if ((e = cudaGetDevice(&P->dev)) != cudaSuccess || (e = cudaDeviceGetAttribute(&P->nsm, cudaDevAttrMultiProcessorCount, P->dev)) != cudaSuccess) {
+        plan_free(P);
+        return cuda_fail(e);
+    }
+    if ((e = cudaMalloc(&P->d_scratch, (64 + kClasses + total) * sizeof(int))) != cudaSuccess ||
+        (e = cudaMalloc(&P->d_err, sizeof(unsigned int))) != cudaSuccess ||
+        (e = cudaMemset(P->d_err, 0, sizeof(unsigned int))) != cudaSuccess) {
+        plan_free(P);
+        return cuda_fail(e);
+    }
+    int cls_slot[kClasses] = {-1, -1, -1, -1};
+    size_t wl_off = 64 + kClasses;
+    for (int j = 0; j < nmembers; j++) {
+        const uwshcu_member& m = members[j];
+        P->mem[j] = m;
+        const int cls = (m.mkx + 1 <= 32 ? 0 : 1) + (ncnst <= 5 ? 0 : 2);
+        if (cls_slot[cls] < 0) {
+            cls_slot[cls] = P->ncls;
+            P->cls_id[P->ncls] = cls;
+            UwBatch& b = P->b[P->ncls];
+            b = UwBatch{};
+            b.task_head = P->d_scratch + 64 + P->ncls;
+            P->trig_grid[P->ncls] = 0;
+            P->ncls++;
+        }
+        const int c = cls_slot[cls];
+        UwBatch& b = P->b[c];
+        const int slot = b.nm++;
+        UwArgs& A = b.m[slot];
+        A = UwArgs{};
+        A.mix = m.mix; A.mkx = m.mkx; A.iend = m.iend; A.ncnst = ncnst; A.inv = m.inv; A.dt = m.dt;
+        A.ps0 = m.ps0; A.zs0 = m.zs0; A.p0 = m.p0; A.z0 = m.z0; A.dp0 = m.dp0; A.u0 = m.u0; A.v0 = m.v0;
+        A.qv0 = m.qv0; A.ql0 = m.ql0; A.qi0 = m.qi0; A.t0 = m.t0; A.s0 = m.s0; A.tr0 = m.tr0; A.tke = m.tke;
+        A.pblh = m.pblh; A.cush = m.cush; A.umf = m.umf; A.slflx = m.slflx; A.qtflx = m.qtflx;
+        A.flxprc1 = m.flxprc1; A.flxsnow1 = m.flxsnow1; A.qvten = m.qvten; A.qlten = m.qlten; A.qiten = m.qiten;
+        A.sten = m.sten; A.uten = m.uten; A.vten = m.vten; A.trten = m.trten; A.qrten = m.qrten;
+        A.qsten = m.qsten; A.precip = m.precip; A.snow = m.snow; A.evapc = m.evapc; A.cufrc = m.cufrc;
+        A.qcu = m.qcu; A.qlu = m.qlu; A.qiu = m.qiu; A.cbmf = m.cbmf; A.qc = m.qc; A.rliq = m.rliq;
+        A.cnt = m.cnt; A.cnb = m.cnb; A.dpdry0 = m.dpdry0; A.wu = m.wu; A.diag_int = m.diag_int;
+        A.diag_real = m.diag_real; A.err = P->d_err;
+        b.wl[slot] = P->d_scratch + wl_off;
+        wl_off += (size_t)m.iend;
+    }
+    // per-class member counts sit in consecutive ints of the header; block ranges of the trigger
+    int next_count = 0;
+    for (int c = 0; c < P->ncls; c++) {
+        UwBatch& b = P->b[c];
+        b.count = P->d_scratch + next_count;
+        next_count += b.nm;
+        b.block_start[0] = 0;
+        for (int j = 0; j < b.nm; j++)
+            b.block_start[j + 1] = b.block_start[j] + (b.m[j].iend + P->block - 1) / P->block;
+        P->trig_grid[c] = b.block_start[b.nm];
+    }
+    *plan = P;
+    return UWSHCU_OK;
+}
+
+namespace {
+// block ranges depend on the block size
+void plan_set_block(BatchPlan& P, int block)
+{
+    P.block = block;
+    for (int c = 0; c < P.ncls; c++) {
+        UwBatch& b = P.b[c];
+        b.block_start[0] = 0;
+        for (int j = 0; j < b.nm; j++) b.block_start[j + 1] = b.block_start[j] + (b.m[j].iend + block - 1) / block;
+        P.trig_grid[c] = b.block_start[b.nm];
+    }
+}
+}  // namespace
+
+extern "C" int uwshcu_batch_run(void* plan, void* stream)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    if (!plan) return UWSHCU_ERR_BAD_ARGS;
+    BatchPlan& P = *static_cast<BatchPlan*>(plan);
+    DeviceState* d = nullptr;
+    int rc = ensure_device(&d);   // constants current on this device
+    if (rc != UWSHCU_OK) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (P.exec) {
+        cudaError_t e = cudaGraphLaunch(P.exec, st);
+        return e == cudaSuccess ? UWSHCU_OK : cuda_fail(e);
+    }
+    return plan_enqueue(P, st);
+}
+
+extern "C" int uwshcu_batch_capture(void* plan, void* stream)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    if (!plan || !stream) return UWSHCU_ERR_BAD_ARGS;   // capture needs a non-default stream
+    BatchPlan& P = *static_cast<BatchPlan*>(plan);
+    DeviceState* d = nullptr;
+    int rc = ensure_device(&d);
+    if (rc != UWSHCU_OK) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (P.exec) {
+        cudaGraphExecDestroy(P.exec);
+        P.exec = nullptr;
+    }
+    cudaError_t e;
+    if ((e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return cuda_fail(e);
+    rc = plan_enqueue(P, st);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(st, &g);
+    if (rc != UWSHCU_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return cuda_fail(e);
+    e = cudaGraphInstantiate(&P.exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        P.exec = nullptr;
+        return cuda_fail(e);
+    }
+    return UWSHCU_OK;
+}
+
+extern "C" int uwshcu_batch_autotune(void* plan, void* stream, int* block_out, int* minb_out, int* chunk_out)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    if (!plan) return UWSHCU_ERR_BAD_ARGS;
+    BatchPlan& P = *static_cast<BatchPlan*>(plan);
+    DeviceState* d = nullptr;
+    int rc = ensure_device(&d);
+    if (rc != UWSHCU_OK) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e;
+    if (P.exec) {
+        cudaGraphExecDestroy(P.exec);
+        P.exec = nullptr;
+    }
+    // keep cush (in/out) so that every trial sees the same inputs
+    size_t ncush = 0;
+    for (int j = 0; j < P.nm; j++) ncush += (size_t)P.mem[j].iend;
+    if (!P.d_cush_save && (e = cudaMalloc(&P.d_cush_save, ncush * sizeof(double))) != cudaSuccess) return cuda_fail(e);
+    auto save_restore = [&](bool save) -> cudaError_t {
+        size_t off = 0;
+        for (int j = 0; j < P.nm; j++) {
+            const size_t nb = (size_t)P.mem[j].iend * sizeof(double);
+            cudaError_t ee = save ? cudaMemcpyAsync(P.d_cush_save + off, P.mem[j].cush, nb, cudaMemcpyDeviceToDevice, st)
+                                  : cudaMemcpyAsync(P.mem[j].cush, P.d_cush_save + off, nb, cudaMemcpyDeviceToDevice, st);
+            if (ee != cudaSuccess) return ee;
+            off += (size_t)P.mem[j].iend;
+        }
+        return cudaSuccess;
+    };
+    if ((e = save_restore(true)) != cudaSuccess) return cuda_fail(e);
+    cudaEvent_t e0, e1;
+    if ((e = cudaEventCreate(&e0)) != cudaSuccess) return cuda_fail(e);
+    if ((e = cudaEventCreate(&e1)) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return cuda_fail(e);
+    }
+    const int blocks[] = {128, 64};
+    const int minbs[] = {3, 4, 6};
+    const int chunks[] = {1, 2};
+    float best = 1e30f;
+    int bb = P.block, bm = P.minb, bc = P.chunk;
+    rc = UWSHCU_OK;
+    bool warm = false;
+    for (int block : blocks) {
+        for (int minb : minbs) {
+            bool ok = true;
+            for (int c = 0; c < P.ncls; c++) ok = ok && batch_has_minb(P.cls_id[c], minb);
+            if (!ok) continue;
+            for (int chunk : chunks) {
+                plan_set_block(P, block);
+                P.minb = minb;
+                P.chunk = chunk;
+                float tmin = 1e30f;
+                for (int rep = 0; rep < (warm ? 2 : 3); rep++) {
+                    if ((e = save_restore(false)) != cudaSuccess) { rc = cuda_fail(e); break; }
+                    if ((e = cudaEventRecord(e0, st)) != cudaSuccess) { rc = cuda_fail(e); break; }
+                    if ((rc = plan_enqueue(P, st)) != UWSHCU_OK) break;
+                    if ((e = cudaEventRecord(e1, st)) != cudaSuccess || (e = cudaEventSynchronize(e1)) != cudaSuccess) {
+                        rc = cuda_fail(e);
+                        break;
+                    }
+                    float ms = 0.f;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    if (warm || rep > 0) tmin = std::min(tmin, ms);
+                }
+                warm = true;
+                if (rc != UWSHCU_OK) break;
+                if (tmin < best) {
+                    best = tmin;
+                    bb = block;
+                    bm = minb;
+                    bc = chunk;
+                }
+            }
+            if (rc != UWSHCU_OK) break;
+        }
+        if (rc != UWSHCU_OK) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    plan_set_block(P, bb);
+    P.minb = bm;
+    P.chunk = bc;
+    cudaError_t er = save_restore(false);
+    if (rc == UWSHCU_OK && er != cudaSuccess) rc = cuda_fail(er);
+    if (rc == UWSHCU_OK && (er = cudaStreamSynchronize(st)) != cudaSuccess) rc = cuda_fail(er);
+    // runs of the tuner report no endrun status
+    cudaMemset(P.d_err, 0, sizeof(unsigned int));
+    if (block_out) *block_out = bb;
+    if (minb_out) *minb_out = bm;
+    if (chunk_out) *chunk_out = bc;
+    return rc;
+}
+
+extern "C" int uwshcu_batch_status(void* plan, void* stream)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    if (!plan) return UWSHCU_ERR_BAD_ARGS;
+    BatchPlan& P = *static_cast<BatchPlan*>(plan);
+    cudaError_t e;
+    unsigned int bits = 0;
+    if ((e = cudaStreamSynchronize((cudaStream_t)stream)) != cudaSuccess) return cuda_fail(e);
+    if ((e = cudaMemcpy(&bits, P.d_err, sizeof(bits), cudaMemcpyDeviceToHost)) != cudaSuccess) return cuda_fail(e);
+    if ((e = cudaMemset(P.d_err, 0, sizeof(unsigned int))) != cudaSuccess) return cuda_fail(e);
+    return status_from_bits(bits);
+}
+
+extern "C" int uwshcu_batch_destroy(void* plan)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    if (!plan) return UWSHCU_ERR_BAD_ARGS;
+    plan_free(static_cast<BatchPlan*>(plan));
+    return UWSHCU_OK;
+}

@@ -38,7 +38,9 @@ EXPORTS = ("uwshcu_init", "uwshcu_set_rpen", "uwshcu_init_default", "uwshcu_set_
            "uwshcu_profile_read", "uwshcu_get_estbl", "uwshcu_finalize", "uwshcu_last_cuda_error",
            "compute_uwshcu_", "compute_uwshcu_inv_", "bxcompute_uwshcu_inv_",
            "uwshcu_compute_device", "uwshcu_device_status", "uwshcu_eval_math",
-           "uwshcu_compute_device_noalloc")
+           "uwshcu_compute_device_noalloc", "uwshcu_batch_create", "uwshcu_batch_run",
+           "uwshcu_batch_capture", "uwshcu_batch_autotune", "uwshcu_batch_status",
+           "uwshcu_batch_destroy")
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
@@ -272,3 +274,75 @@ def eval_math_device(fn, x, y=None):
         raise RuntimeError("uwshcu_eval_math: %d" % rc)
     st.synchronize()
     return od.cpu().numpy()
+
+
+# ---- batched uneven launches -----------------------------------------------------------------------
+MAX_MEMBERS = 8
+_MEMBER_PTRS = ("ps0 zs0 p0 z0 dp0 u0 v0 qv0 ql0 qi0 t0 s0 tr0 tke pblh cush umf slflx qtflx flxprc1 "
+                "flxsnow1 qvten qlten qiten sten uten vten trten qrten qsten precip snow evapc cufrc qcu "
+                "qlu qiu cbmf qc rliq cnt cnb dpdry0 wu diag_int diag_real").split()
+
+
+class Member(ctypes.Structure):
+    """uwshcu_member of include/uwshcu.h."""
+    _fields_ = ([("mix", ctypes.c_int), ("mkx", ctypes.c_int), ("iend", ctypes.c_int), ("inv", ctypes.c_int),
+                 ("dt", ctypes.c_double)] + [(n, ctypes.c_void_p) for n in _MEMBER_PTRS])
+
+
+def member_of(case, inv=0):
+    """The uwshcu_member of a DeviceCase."""
+    m = Member()
+    m.mix = m.iend = case.n
+    m.mkx = case.mkx
+    m.inv = inv
+    m.dt = case.dt
+    for name in _MEMBER_PTRS:
+        if name in ("diag_int", "diag_real"):
+            t = getattr(case, name)
+        elif name in case.out:
+            t = case.out[name]
+        else:
+            t = case.inp[name]
+        setattr(m, name, t.data_ptr() if t is not None else None)
+    return m
+
+
+class BatchPlan:
+    """uwshcu_batch_* over a list of DeviceCase objects (one member each)."""
+
+    def __init__(self, cases, inv=0):
+        self.cases = list(cases)
+        arr = (Member * len(self.cases))(*[member_of(c, inv) for c in self.cases])
+        self._members = arr
+        self.handle = ctypes.c_void_p()
+        rc = lib().uwshcu_batch_create(ctypes.c_int(len(self.cases)), arr, ctypes.byref(self.handle))
+        if rc != 0:
+            raise RuntimeError("uwshcu_batch_create: %d %s" % (rc, last_cuda_error()))
+
+    @staticmethod
+    def _st(stream):
+        import torch
+        st = stream if stream is not None else torch.cuda.current_stream()
+        return ctypes.c_void_p(st.cuda_stream)
+
+    def run(self, stream=None):
+        return lib().uwshcu_batch_run(self.handle, self._st(stream))
+
+    def capture(self, stream):
+        return lib().uwshcu_batch_capture(self.handle, self._st(stream))
+
+    def autotune(self, stream=None):
+        b, m, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        rc = lib().uwshcu_batch_autotune(self.handle, self._st(stream), ctypes.byref(b), ctypes.byref(m),
+                                         ctypes.byref(c))
+        if rc != 0:
+            raise RuntimeError("uwshcu_batch_autotune: %d %s" % (rc, last_cuda_error()))
+        return b.value, m.value, c.value
+
+    def status(self, stream=None):
+        return lib().uwshcu_batch_status(self.handle, self._st(stream))
+
+    def close(self):
+        if self.handle:
+            lib().uwshcu_batch_destroy(self.handle)
+            self.handle = ctypes.c_void_p()

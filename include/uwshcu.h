@@ -183,6 +183,54 @@ int uwshcu_compute_device(int mix, int mkx, int iend, int ncnst, double dt, int 
  * previous uwshcu_device_status call. */
 int uwshcu_device_status(void *stream);
 
+/* ---- batched uneven launches ----------------------------------------------------------------- */
+
+/* One ensemble member / grid of a batch: the arguments of uwshcu_compute_device for one set of
+ * device-resident arrays (ncnst is the one given to uwshcu_init).  Members may differ in mkx, mix,
+ * iend and level order. */
+typedef struct uwshcu_member {
+    int mix, mkx, iend, inv;
+    double dt;
+    const double *ps0, *zs0, *p0, *z0, *dp0, *u0, *v0, *qv0, *ql0, *qi0, *t0, *s0, *tr0, *tke, *pblh;
+    double *cush, *umf, *slflx, *qtflx, *flxprc1, *flxsnow1, *qvten, *qlten, *qiten, *sten, *uten,
+        *vten, *trten, *qrten, *qsten, *precip, *snow, *evapc, *cufrc, *qcu, *qlu, *qiu, *cbmf, *qc,
+        *rliq, *cnt, *cnb;
+    const double *dpdry0;
+    double *wu;
+    int *diag_int;      /* optional, as in uwshcu_compute_device */
+    double *diag_real;  /* optional */
+} uwshcu_member;
+
+#define UWSHCU_MAX_MEMBERS 8
+
+/* No counterpart in the reference (CAM calls compute_uwshcu once per chunk; the reference's
+ * load-balanced ports, mpiuwshcu.cpp / bxcompute_uwshcu_inv.cpp, launch one grid per call).
+ * A batch plan for up to UWSHCU_MAX_MEMBERS members on the current device: the library allocates
+ * the plan's worklists and counters here, once.  A run makes one trigger launch and one persistent
+ * worklist launch per level class (mkx + 1 <= 32 or <= 64): the worklist kernel pulls warps of
+ * one member's convecting columns from a device counter until every member's queue is drained.
+ * Results are the same bits as uwshcu_compute_device on each member. */
+int uwshcu_batch_create(int nmembers, const uwshcu_member *members, void **plan);
+
+/* Enqueue one run of the plan on `stream` (the captured CUDA graph when there is one). */
+int uwshcu_batch_run(void *plan, void *stream);
+
+/* Capture one run into a CUDA graph held by the plan; later uwshcu_batch_run calls replay it.
+ * The capture itself launches nothing. */
+int uwshcu_batch_capture(void *plan, void *stream);
+
+/* Time the compiled launch shapes of the worklist pass (block of 64 or 128 threads, register cap
+ * 168/128/80 = 3/4/6 blocks of 128 per SM, 32 or 64 columns per warp task) on this plan's data
+ * and keep the fastest in the plan (it drops a captured graph).  Runs the scheme several times:
+ * the outputs are overwritten and cush is restored to its value on entry.  Reports the choice. */
+int uwshcu_batch_autotune(void *plan, void *stream, int *block, int *regcap_blocks, int *chunk);
+
+/* Wait for `stream` and return the endrun status collected by the plan's runs since the last call. */
+int uwshcu_batch_status(void *plan, void *stream);
+
+/* Release the plan (its graph, worklists and counters). */
+int uwshcu_batch_destroy(void *plan);
+
 /* Column limit of uwshcu_compute_device_noalloc: its worklist is one fixed device array of
  * 64 + UWSHCU_NOALLOC_MAX_COLUMNS ints (4 MiB + 256 B) that every GPU which loads the library holds
  * until the process exits. */

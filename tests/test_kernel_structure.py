@@ -1,8 +1,9 @@
 """Static check of the column kernel's warp-level control skeleton (no GPU needed).
 
-The FP64 kernel joins the live lanes of a warp with __syncwarp(live) (the UW_SYNC() macro).  That is
-only well defined if every live lane executes the same sequence of UW_SYNC() calls, so each call
-must sit directly inside blocks that all live lanes enter equally often: the kernel body, the
+The FP64 column code (uw_column, which every kernel runs) joins the live lanes of a warp with
+__syncwarp(live) (the UW_SYNC() macro).  That is only well defined if every live lane executes the
+same sequence of UW_SYNC() calls, so each call
+must sit directly inside blocks that all live lanes enter equally often: the function body, the
 `if (active)` block, plain `{ }` blocks, and loops marked `// uniform` (same trip count on every
 lane).  Such a loop must also have no `break` or `continue` of its own, which would let some lanes
 leave it or skip its UW_SYNC().  This test parses the kernel's braces and checks both rules."""
@@ -26,7 +27,7 @@ def _scan():
     in_kernel = False
     for ln, (line, rline) in enumerate(zip(code, raw), 1):
         body = line.split("//")[0]
-        if "uwshcu_fp64_kernel(UwArgs A" in body:
+        if "void uw_column(" in body:
             in_kernel = True
         if not in_kernel:
             continue
@@ -63,7 +64,7 @@ def _scan():
 
 def _allowed(entry):
     ln, head, kind, uniform = entry
-    if "uwshcu_fp64_kernel(UwArgs A" in head or head.startswith("__global__"):
+    if "uw_column(" in head:
         return True
     if head == "if (active)":
         return True
