@@ -82,6 +82,10 @@ struct DeviceState {
     static constexpr int kSlots = 256;
     cudaEvent_t ev[kSlots][3] = {};
     int nrec = 0;                // calls recorded since the last read (capped at kSlots)
+    // host-array calls: column chunks pipelined over kPipe streams (copy in, compute, copy out)
+    static constexpr int kPipe = 4;
+    cudaStream_t pipe[kPipe] = {};
+    std::vector<cudaEvent_t> done;   // one per chunk, grown on demand
 };
 
 struct State {
@@ -94,6 +98,8 @@ struct State {
     int schedule = UWSHCU_SCHED_TWO_PHASE;
     int block = 128;
     bool profiling = false;
+    int chunk_columns = 32768;   // host-array calls: columns per pipeline chunk (0: one chunk)
+    int pipe_streams = 4;        // host-array calls: streams the chunks alternate over
     DeviceState dev[kMaxDev];
     char lasterr[256] = "";
 };
@@ -329,105 +335,143 @@ int host_call(int inv, int mix, int mkx, int iend, int ncnst, double dt, const d
 
     const size_t n = (size_t)iend, ld = (size_t)mix, KI = (size_t)mkx + 1, KL = (size_t)mkx;
     const size_t KT = KL * (size_t)ncnst;
-    // packed input block: 3 interface fields, 11 layer fields, tracers, pblh, cush
-    const size_t nin = (3 * KI + 11 * KL + KT + 2) * n;
-    // packed output block: 6 interface fields, 14 layer fields, tracers, 7 column fields
-    const size_t nout = (6 * KI + 14 * KL + KT + 7) * n;
-    if ((rc = grow(*d, nin + nout, nin + nout)) != UWSHCU_OK) return rc;
-
-    double* hin = d->h_buf;
-    double* hout = d->h_buf + nin;
-    double* din = d->d_buf;
-    double* dout = d->d_buf + nin;
-    // input planes
-    std::vector<Plane> in;
-    size_t off = 0;
-    auto add_in = [&](const double* a, size_t rows) -> const double* {
-        in.push_back(Plane{a, hin + off, rows, ld, n, n});
-        const double* dp = din + off;
-        off += rows * n;
-        return dp;
-    };
-    UwArgs A{};
-    A.mix = (int)n;
-    A.mkx = mkx;
-    A.iend = iend;
-    A.ncnst = ncnst;
-    A.inv = inv;
-    A.dt = dt;
-    A.ps0 = add_in(ps0, KI);
-    A.zs0 = add_in(zs0, KI);
-    A.tke = add_in(tke, KI);
-    A.p0 = add_in(p0, KL);
-    A.z0 = add_in(z0, KL);
-    A.dp0 = add_in(dp0, KL);
-    A.u0 = add_in(u0, KL);
-    A.v0 = add_in(v0, KL);
-    A.qv0 = add_in(qv0, KL);
-    A.ql0 = add_in(ql0, KL);
-    A.qi0 = add_in(qi0, KL);
-    A.t0 = add_in(t0, KL);
-    A.s0 = add_in(s0, KL);
-    A.dpdry0 = add_in(dpdry0, KL);
-    A.tr0 = add_in(tr0, KT);   // (mix, mkx, ncnst) rows of mix: mkx*ncnst rows
-    A.pblh = add_in(pblh, 1);
-    double* d_cush = const_cast<double*>(add_in(cush, 1));
-    A.cush = d_cush;
-    copy_planes(in);
-
-    std::vector<Plane> out;
-    size_t oo = 0;
-    auto add_out = [&](double* a, size_t rows) -> double* {
-        out.push_back(Plane{hout + oo, a, rows, n, ld, n});
-        double* dp = dout + oo;
-        oo += rows * n;
-        return dp;
-    };
-    A.umf = add_out(umf, KI);
-    A.slflx = add_out(slflx, KI);
-    A.qtflx = add_out(qtflx, KI);
-    A.flxprc1 = add_out(flxprc1, KI);
-    A.flxsnow1 = add_out(flxsnow1, KI);
-    A.wu = add_out(wu, KI);
-    A.qvten = add_out(qvten, KL);
-    A.qlten = add_out(qlten, KL);
-    A.qiten = add_out(qiten, KL);
-    A.sten = add_out(sten, KL);
-    A.uten = add_out(uten, KL);
-    A.vten = add_out(vten, KL);
-    A.qrten = add_out(qrten, KL);
-    A.qsten = add_out(qsten, KL);
-    A.evapc = add_out(evapc, KL);
-    A.cufrc = add_out(cufrc, KL);
-    A.qcu = add_out(qcu, KL);
-    A.qlu = add_out(qlu, KL);
-    A.qiu = add_out(qiu, KL);
-    A.qc = add_out(qc, KL);
-    A.trten = add_out(trten, KT);
-    A.precip = add_out(precip, 1);
-    A.snow = add_out(snow, 1);
-    A.cbmf = add_out(cbmf, 1);
-    A.rliq = add_out(rliq, 1);
-    A.cnt = add_out(cnt, 1);
-    A.cnb = add_out(cnb, 1);
-    // cush is in/out: the kernel reads and rewrites it in place in the input block
-    out.push_back(Plane{hin + (A.cush - din), cush, 1, n, ld, n});
-    A.err = d->d_err;
-    A.diag_int = nullptr;
-    A.diag_real = nullptr;
-
+    // Column chunks, each a compact (nc-column) copy of its inputs and outputs in the arena and the
+    // pinned staging area.  Chunk c runs on pipe[c % kPipe]: copy in, trigger + worklist pass, copy
+    // out.  The host packs chunk c+1 while the GPU works on chunk c and unpacks chunk c while the
+    // GPU works on the later ones.  Each chunk has its own worklist and endrun word.
+    const size_t per_in = 3 * KI + 11 * KL + KT + 2;     // doubles per column, input block
+    const size_t per_out = 6 * KI + 14 * KL + KT + 7;    // doubles per column, output block
+    const size_t csz = s.chunk_columns > 0 ? (size_t)s.chunk_columns : n;
+    const size_t nch = (n + csz - 1) / csz;
+    const size_t nin = per_in * n, nout = per_out * n;
+    if ((rc = grow(*d, nin + nout, nin + nout + 2 * nch)) != UWSHCU_OK) return rc;
+    if ((rc = grow_worklist(*d, n + 2 * nch)) != UWSHCU_OK) return rc;
     cudaError_t e;
-    cudaStream_t st = d->stream;
-    unsigned int hbits = 0;
-    if ((e = cudaMemsetAsync(d->d_err, 0, sizeof(unsigned int), st)) != cudaSuccess) return cuda_fail(e);
-    if ((e = cudaMemcpyAsync(din, hin, nin * sizeof(double), cudaMemcpyHostToDevice, st)) != cudaSuccess) return cuda_fail(e);
-    if ((rc = enqueue(*d, A, st)) != UWSHCU_OK) return rc;
-    if ((e = cudaMemcpyAsync(hout, dout, nout * sizeof(double), cudaMemcpyDeviceToHost, st)) != cudaSuccess) return cuda_fail(e);
-    if ((e = cudaMemcpyAsync(hin + (A.cush - din), A.cush, n * sizeof(double), cudaMemcpyDeviceToHost, st)) != cudaSuccess) return cuda_fail(e);
-    if ((e = cudaMemcpyAsync(&hbits, d->d_err, sizeof(unsigned int), cudaMemcpyDeviceToHost, st)) != cudaSuccess) return cuda_fail(e);
-    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e);
-    copy_planes(out);
-    return status_from_bits(hbits);
+    for (int j = 0; j < DeviceState::kPipe; j++)
+        if (!d->pipe[j] && (e = cudaStreamCreateWithFlags(&d->pipe[j], cudaStreamNonBlocking)) != cudaSuccess)
+            return cuda_fail(e);
+    while (d->done.size() < nch) {
+        cudaEvent_t ev;
+        if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return cuda_fail(e);
+        d->done.push_back(ev);
+    }
+    unsigned int* hbits = reinterpret_cast<unsigned int*>(d->h_buf + nin + nout);   // nch words
+
+    std::vector<std::vector<Plane>> outs(nch);
+    size_t base_in = 0, base_out = 0;
+    for (size_t c = 0; c < nch; c++) {
+        const size_t c0 = c * csz, nc = std::min(csz, n - c0);
+        double* hin = d->h_buf + base_in;
+        double* hout = d->h_buf + nin + base_out;
+        double* din = d->d_buf + base_in;
+        double* dout = d->d_buf + nin + base_out;
+        base_in += per_in * nc;
+        base_out += per_out * nc;
+        std::vector<Plane> in;
+        size_t off = 0;
+        auto add_in = [&](const double* a, size_t rows) -> const double* {
+            in.push_back(Plane{a + c0, hin + off, rows, ld, nc, nc});
+            const double* dp = din + off;
+            off += rows * nc;
+            return dp;
+        };
+        UwArgs A{};
+        A.mix = (int)nc;
+        A.mkx = mkx;
+        A.iend = (int)nc;
+        A.ncnst = ncnst;
+        A.inv = inv;
+        A.dt = dt;
+        A.ps0 = add_in(ps0, KI);
+        A.zs0 = add_in(zs0, KI);
+        A.tke = add_in(tke, KI);
+        A.p0 = add_in(p0, KL);
+        A.z0 = add_in(z0, KL);
+        A.dp0 = add_in(dp0, KL);
+        A.u0 = add_in(u0, KL);
+        A.v0 = add_in(v0, KL);
+        A.qv0 = add_in(qv0, KL);
+        A.ql0 = add_in(ql0, KL);
+        A.qi0 = add_in(qi0, KL);
+        A.t0 = add_in(t0, KL);
+        A.s0 = add_in(s0, KL);
+        A.dpdry0 = add_in(dpdry0, KL);
+        A.tr0 = add_in(tr0, KT);   // (mix, mkx, ncnst): mkx*ncnst rows of mix
+        A.pblh = add_in(pblh, 1);
+        A.cush = const_cast<double*>(add_in(cush, 1));
+        copy_planes(in);
+
+        std::vector<Plane>& out = outs[c];
+        size_t oo = 0;
+        auto add_out = [&](double* a, size_t rows) -> double* {
+            out.push_back(Plane{hout + oo, a + c0, rows, nc, ld, nc});
+            double* dp = dout + oo;
+            oo += rows * nc;
+            return dp;
+        };
+        A.umf = add_out(umf, KI);
+        A.slflx = add_out(slflx, KI);
+        A.qtflx = add_out(qtflx, KI);
+        A.flxprc1 = add_out(flxprc1, KI);
+        A.flxsnow1 = add_out(flxsnow1, KI);
+        A.wu = add_out(wu, KI);
+        A.qvten = add_out(qvten, KL);
+        A.qlten = add_out(qlten, KL);
+        A.qiten = add_out(qiten, KL);
+        A.sten = add_out(sten, KL);
+        A.uten = add_out(uten, KL);
+        A.vten = add_out(vten, KL);
+        A.qrten = add_out(qrten, KL);
+        A.qsten = add_out(qsten, KL);
+        A.evapc = add_out(evapc, KL);
+        A.cufrc = add_out(cufrc, KL);
+        A.qcu = add_out(qcu, KL);
+        A.qlu = add_out(qlu, KL);
+        A.qiu = add_out(qiu, KL);
+        A.qc = add_out(qc, KL);
+        A.trten = add_out(trten, KT);
+        A.precip = add_out(precip, 1);
+        A.snow = add_out(snow, 1);
+        A.cbmf = add_out(cbmf, 1);
+        A.rliq = add_out(rliq, 1);
+        A.cnt = add_out(cnt, 1);
+        A.cnb = add_out(cnb, 1);
+        // cush is in/out: the kernel rewrites it in place in the input block
+        out.push_back(Plane{hin + (A.cush - din), cush + c0, 1, nc, ld, nc});
+        // this chunk's worklist region: [0] count, [1] endrun bits, [2 ..] column ids
+        int* wreg = d->d_wl + (c0 + 2 * c);
+        A.err = reinterpret_cast<unsigned int*>(wreg + 1);
+        A.diag_int = nullptr;
+        A.diag_real = nullptr;
+
+        cudaStream_t st = d->pipe[c % (size_t)s.pipe_streams];
+        if ((e = cudaMemsetAsync(wreg, 0, 2 * sizeof(int), st)) != cudaSuccess) return cuda_fail(e);
+        if ((e = cudaMemcpyAsync(din, hin, per_in * nc * sizeof(double), cudaMemcpyHostToDevice, st)) != cudaSuccess)
+            return cuda_fail(e);
+        if (s.schedule == UWSHCU_SCHED_SINGLE_PASS) {
+            if ((e = launch_mode(&A, s.precision, kModeAll, nullptr, nullptr, A.iend, s.block, st)) != cudaSuccess)
+                return cuda_fail(e);
+        } else {
+            if ((e = launch_mode(&A, s.precision, kModeTrigger, wreg + 2, wreg, A.iend, s.block, st)) != cudaSuccess)
+                return cuda_fail(e);
+            if ((e = launch_mode(&A, s.precision, kModeList, wreg + 2, wreg, A.iend, s.block, st)) != cudaSuccess)
+                return cuda_fail(e);
+        }
+        if ((e = cudaMemcpyAsync(hout, dout, per_out * nc * sizeof(double), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+            return cuda_fail(e);
+        if ((e = cudaMemcpyAsync(hin + (A.cush - din), A.cush, nc * sizeof(double), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+            return cuda_fail(e);
+        if ((e = cudaMemcpyAsync(hbits + c, wreg + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+            return cuda_fail(e);
+        if ((e = cudaEventRecord(d->done[c], st)) != cudaSuccess) return cuda_fail(e);
+    }
+    unsigned int bits = 0;
+    for (size_t c = 0; c < nch; c++) {
+        if ((e = cudaEventSynchronize(d->done[c])) != cudaSuccess) return cuda_fail(e);
+        copy_planes(outs[c]);
+        bits |= hbits[c];
+    }
+    return status_from_bits(bits);
 }
 
 __global__ void eval_math_kernel(int fn, const double* __restrict__ x, const double* __restrict__ y,
@@ -590,6 +634,16 @@ int uwshcu_profile_read(int* calls, double* trigger_ms, double* list_ms, int* li
     return UWSHCU_OK;
 }
 
+int uwshcu_set_pipeline(int chunk_columns, int streams)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    if (chunk_columns < 0 || streams < 1 || streams > DeviceState::kPipe) return UWSHCU_ERR_BAD_ARGS;
+    s.chunk_columns = chunk_columns;
+    s.pipe_streams = streams;
+    return UWSHCU_OK;
+}
+
 int uwshcu_set_block(int threads)
 {
     State& s = S();
@@ -618,7 +672,7 @@ int uwshcu_finalize(void)
     bool have = cudaGetDevice(&cur) == cudaSuccess;
     for (int dv = 0; dv < kMaxDev; dv++) {
         DeviceState& d = s.dev[dv];
-        if (!d.d_err && !d.d_buf && !d.h_buf && !d.stream) continue;
+        if (!d.d_err && !d.d_buf && !d.h_buf && !d.stream && !d.pipe[0]) continue;
         cudaSetDevice(dv);
         if (d.d_buf) cudaFree(d.d_buf);
         if (d.h_buf) cudaFreeHost(d.h_buf);
@@ -628,6 +682,9 @@ int uwshcu_finalize(void)
             for (int j = 0; j < 3; j++)
                 if (d.ev[n][j]) cudaEventDestroy(d.ev[n][j]);
         if (d.stream) cudaStreamDestroy(d.stream);
+        for (int j = 0; j < DeviceState::kPipe; j++)
+            if (d.pipe[j]) cudaStreamDestroy(d.pipe[j]);
+        for (cudaEvent_t ev : d.done) cudaEventDestroy(ev);
         d = DeviceState{};
     }
     if (have) cudaSetDevice(cur);

@@ -40,7 +40,7 @@ EXPORTS = ("uwshcu_init", "uwshcu_set_rpen", "uwshcu_init_default", "uwshcu_set_
            "uwshcu_compute_device", "uwshcu_device_status", "uwshcu_eval_math",
            "uwshcu_compute_device_noalloc", "uwshcu_batch_create", "uwshcu_batch_run",
            "uwshcu_batch_capture", "uwshcu_batch_autotune", "uwshcu_batch_status",
-           "uwshcu_batch_destroy")
+           "uwshcu_batch_destroy", "uwshcu_set_pipeline")
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
@@ -107,6 +107,10 @@ def profile_read():
     if rc != 0:
         raise RuntimeError("uwshcu_profile_read: %d" % rc)
     return n.value, a.value, b.value, c.value
+
+
+def set_pipeline(chunk_columns, streams):
+    return lib().uwshcu_set_pipeline(ctypes.c_int(chunk_columns), ctypes.c_int(streams))
 
 
 def set_block(threads):

@@ -134,3 +134,23 @@ def test_math_routines_are_bit_identical_on_host_and_device(uw, oracle, cuda):
         dev = uw.eval_math_device(fn, x, y)
         host = oracle.uwmath(fn, x, y)
         assert np.array_equal(dev.view(np.int64), host.view(np.int64)), fn
+
+
+@pytest.mark.gpu
+def test_pipelined_host_entries_match_one_chunk(uw, cuda):
+    """Host-array calls split into column chunks over several streams give the same bits as one
+    chunk, for both level orders and with mix > iend."""
+    s = soundings.make_soundings(5000, 30, seed=61)
+    try:
+        for entry in ("compute_uwshcu_", "compute_uwshcu_inv_"):
+            si = s if entry == "compute_uwshcu_" else soundings.to_inv(s)
+            assert uw.set_pipeline(0, 1) == 0
+            rc0, o0 = uw.compute_host(si, entry=entry, iend=4700)
+            for chunk, streams in ((1024, 3), (777, 2), (4096, 4)):
+                assert uw.set_pipeline(chunk, streams) == 0
+                rc, o = uw.compute_host(si, entry=entry, iend=4700)
+                assert rc == rc0
+                bad = [k for k in o0 if not np.array_equal(o[k], o0[k])]
+                assert not bad, (entry, chunk, streams, bad)
+    finally:
+        assert uw.set_pipeline(32768, 4) == 0
