@@ -40,6 +40,16 @@ RH_PBL = (0.675, 0.93)
 METRIC = "columns/s (compute_uwshcu, FP64, 259,200 x 30 levels)"
 
 
+# From the ncu capture of the worklist kernel on the 65,536-column case of this workload (29,956
+# worklist columns; summary in profiles/uwshcu_fp64_kernel_bench65k.txt): DRAM bytes read + written
+# per worklist column, and FP64 operations executed per worklist column (2 x DFMA + DADD + DMUL
+# thread instructions, Newton steps of the IEEE divisions included).  Both scale with the columns
+# a launch processes.
+NCU_DRAM_BYTES_PER_LIST_COLUMN = 10.494e9 / 29_956
+NCU_FP64_OPS_PER_LIST_COLUMN = 776.1 * 17.77e-3 * 1.858e9 / 29_956
+FP64_DFMA_PER_CYCLE = 9472    # ncu sm__sass_thread_inst_executed_op_dfma_pred_on.sum.peak_sustained
+
+
 def bytes_per_column(mkx=PVER, ncnst=NCNST):
     """Algorithmic bytes of one column: inputs read + outputs written (FP64)."""
     n_in = 3 * (mkx + 1) + 10 * mkx + ncnst * mkx + 2
@@ -246,7 +256,7 @@ def run_batched(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--ncol", type=int, default=NCOL)
@@ -348,8 +358,16 @@ def main():
                "status": int(rc)}
 
     peak, peak_kind = peaks()
-    # algorithmic bytes of the dominant launch: the columns it processes x bytes per column
     ncols_dom = phases["worklist_columns"] if phases else n
+    fp64 = None
+    if phases and clk is not None and clk.summary().get("sm_mhz"):
+        hz = clk.summary()["sm_mhz"] * 1e6
+        ach = NCU_FP64_OPS_PER_LIST_COLUMN * ncols_dom / (kernel_ms * 1e-3) / 1e12
+        pk = 2 * FP64_DFMA_PER_CYCLE * hz / 1e12
+        fp64 = {"achieved": ach, "peak": pk, "unit": "TFLOP/s", "frac": ach / pk,
+                "what": "executed FP64 ops (ncu count per worklist column) / live kernel time; peak = "
+                        "2 x 9472 DFMA/cycle x median SM clock"}
+    # algorithmic bytes of the dominant launch: the columns it processes x bytes per column
     alg = ncols_dom * (nbytes_in + nbytes_out)
     achieved = alg / (kernel_ms * 1e-3) / 1e9
     line = {
@@ -358,15 +376,20 @@ def main():
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded soundings, PCG64 seed 1+rank)",
         "config": {"workload": "compute_uwshcu 259,200 columns (720x360) x 30 levels, 5 tracers, "
-                               "dt=1800 s, ~40%% convecting", "ncol_per_gpu": n, "pver": PVER,
+                               "dt=1800 s, ~40% convecting", "ncol_per_gpu": n, "pver": PVER,
                    "ncnst": NCNST, "trigger_fraction": trig, "l2": "inputs (1.2 GB) larger than L2",
                    "parallelism": "column shards, %d rank(s), no collective" % world},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                     "frac": achieved / peak,
+                     "traffic": (NCU_DRAM_BYTES_PER_LIST_COLUMN * ncols_dom) if phases else None,
+                     "peak_kind": peak_kind,
                      "kernel": "uwshcu_fp64_kernel<32,5,%s>" % ("UW_MODE_LIST" if phases else "UW_MODE_ALL"),
                      "kernel_ms": kernel_ms, "columns_per_launch": ncols_dom,
-                     "note": "FP64 column physics is compute-bound; algorithmic bytes = "
-                             "%d B/column" % (nbytes_in + nbytes_out)},
+                     "fp64": fp64,
+                     "note": "branchy FP64 column physics: neither HBM nor the FP64 pipe is the bound "
+                             "(issue latency is); algorithmic bytes = %d B/column; traffic = ncu DRAM "
+                             "bytes per worklist column x columns (the per-thread stack of level "
+                             "profiles spills out of L1/L2)" % (nbytes_in + nbytes_out)},
         "schedule": args.schedule,
         "phases": phases,
         "gpu_launches": args.steps * (2 if two_phase else 1),
