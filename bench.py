@@ -264,6 +264,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--schedule", default="two-phase", choices=["two-phase", "single-pass"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fast", "mixed"],
+                    help="fp64: bit-exact (default); fast: FP64 with the early-stopping conden; "
+                         "mixed: FP32 bulk with FP64 islands")
     ap.add_argument("--config", default="fp64", choices=["fp64", "batched"],
                     help="fp64: the 259,200-column workload (default); batched: 4 uneven members")
     args = ap.parse_args()
@@ -285,6 +288,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         pg = dist
     assert uw.init_default() == 0
+    prec = {"fp64": uw.PREC_FP64, "fast": uw.PREC_FAST, "mixed": uw.PREC_MIXED}[args.precision]
+    assert uw.set_precision(prec) == 0, "precision %s not available" % args.precision
     two_phase = args.schedule == "two-phase"
     assert uw.set_schedule(uw.SCHED_TWO_PHASE if two_phase else uw.SCHED_SINGLE_PASS) == 0
     n = args.ncol
@@ -357,10 +362,25 @@ def main():
                "d2h_bytes_per_step": int(n * nbytes_out), "ms_per_step": sec * 1e3,
                "status": int(rc)}
 
+    err = None
+    if prec != uw.PREC_FP64:
+        import errstats
+        out_r = case.outputs_numpy()
+        assert uw.set_precision(uw.PREC_FP64) == 0
+        case.reset_cush()
+        assert case.launch(stream=stream) == 0
+        stream.synchronize()
+        rep = errstats.report(out_r, case.outputs_numpy(), s["dp0"])
+        assert uw.set_precision(prec) == 0
+        err = {"vs": "FP64 path (bit-identical to the FP64 oracle), same inputs",
+               "column_rel_rms": {k: v["rel_rms"] for k, v in rep["column"].items()},
+               "flips": rep["flips"],
+               "field_rel_rms_max": max(v["rel_rms"] for v in rep["fields"].values())}
+
     peak, peak_kind = peaks()
     ncols_dom = phases["worklist_columns"] if phases else n
     fp64 = None
-    if phases and clk is not None and clk.summary().get("sm_mhz"):
+    if phases and prec == uw.PREC_FP64 and clk is not None and clk.summary().get("sm_mhz"):
         hz = clk.summary()["sm_mhz"] * 1e6
         ach = NCU_FP64_OPS_PER_LIST_COLUMN * ncols_dom / (kernel_ms * 1e-3) / 1e12
         pk = 2 * FP64_DFMA_PER_CYCLE * hz / 1e12
@@ -371,9 +391,11 @@ def main():
     alg = ncols_dom * (nbytes_in + nbytes_out)
     achieved = alg / (kernel_ms * 1e-3) / 1e9
     line = {
-        "metric": METRIC, "value": value, "unit": "columns/s", "n_gpus": world,
+        "metric": METRIC if prec == uw.PREC_FP64 else METRIC.replace("FP64", args.precision),
+        "value": value, "unit": "columns/s", "n_gpus": world,
         "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64" if prec == uw.PREC_MIXED else "f64",
         "data": "synthetic (seeded soundings, PCG64 seed 1+rank)",
         "config": {"workload": "compute_uwshcu 259,200 columns (720x360) x 30 levels, 5 tracers, "
                                "dt=1800 s, ~40% convecting", "ncol_per_gpu": n, "pver": PVER,
@@ -381,9 +403,11 @@ def main():
                    "parallelism": "column shards, %d rank(s), no collective" % world},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak,
-                     "traffic": (NCU_DRAM_BYTES_PER_LIST_COLUMN * ncols_dom) if phases else None,
+                     "traffic": (NCU_DRAM_BYTES_PER_LIST_COLUMN * ncols_dom)
+                                if (phases and prec == uw.PREC_FP64) else None,
                      "peak_kind": peak_kind,
-                     "kernel": "uwshcu_fp64_kernel<32,5,%s>" % ("UW_MODE_LIST" if phases else "UW_MODE_ALL"),
+                     "kernel": "uwshcu_%s_kernel<32,5,%s>" % ({"fp64": "fp64", "fast": "fast", "mixed": "mixed"}[args.precision],
+                                                              "UW_MODE_LIST" if phases else "UW_MODE_ALL"),
                      "kernel_ms": kernel_ms, "columns_per_launch": ncols_dom,
                      "fp64": fp64,
                      "note": "branchy FP64 column physics: neither HBM nor the FP64 pipe is the bound "
@@ -391,12 +415,15 @@ def main():
                              "bytes per worklist column x columns (the per-thread stack of level "
                              "profiles spills out of L1/L2)" % (nbytes_in + nbytes_out)},
         "schedule": args.schedule,
+        "precision": args.precision,
         "phases": phases,
         "gpu_launches": args.steps * (2 if two_phase else 1),
         "status": st,
     }
     if e2e is not None:
         line["e2e"] = e2e
+    if err is not None:
+        line["error_vs_fp64"] = err
     if clk is not None:
         line["clocks"] = clk.summary()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

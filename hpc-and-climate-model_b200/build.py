@@ -26,6 +26,11 @@ UNITS = {
     "uwshcu_fp64_k64n5.cu": ["-fmad=false"],
     "uwshcu_fp64_k32n32.cu": ["-fmad=false"],
     "uwshcu_fp64_k64n32.cu": ["-fmad=false"],
+    # the fast-FP64 mode is not bit-exact by design: FMA contraction allowed
+    "uwshcu_fast_k32n5.cu": [],
+    "uwshcu_fast_k64n5.cu": [],
+    "uwshcu_fast_k32n32.cu": [],
+    "uwshcu_fast_k64n32.cu": [],
     "uwshcu_mixed_k32n5.cu": [],
     "uwshcu_mixed_k64n5.cu": [],
     "uwshcu_host.cu": [],

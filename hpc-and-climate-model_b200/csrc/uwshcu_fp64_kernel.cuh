@@ -130,6 +130,50 @@ __device__ __noinline__ int conden(double p, double ex, double thl, double qt, d
     return id_check;
 }
 
+// conden for the fast-FP64 precision mode: the same saturation adjustment with one reciprocal of the
+// temperature per Newton step (2 divisions instead of 5) and a stop once every lane of the warp has
+// taken a step smaller than 1e-10 T.  The Fortran always takes 10 steps; the steps shrink about
+// 100x per iteration and fall below 1e-10 T after 5-7, so the result differs from conden by about
+// 1e-12 relative.  The warp-wide vote (__all_sync over the lanes active at the call) keeps the
+// lanes of a warp together.
+__device__ __noinline__ int conden_fast(double p, double ex, double thl, double qt, double& th, double& qv,
+                                        double& ql, double& qi, const double* __restrict__ tbl)
+{
+    double tc = thl * ex;
+    double nu = MX(MN((268.0 - tc) / 20.0, 1.0), 0.0);
+    double leff = (1.0 - nu) * c.xlv + nu * c.xls;
+    double temps = tc;
+    double rvls = qsat_qs(temps, p, tbl);
+    int id_check = 0;
+    if (rvls >= qt) {
+        qv = qt;
+        ql = 0.0;
+        qi = 0.0;
+        th = tc / ex;
+    } else {
+        const double cpl = c.cp / leff;
+        const double a2 = c.ep2 * leff / c.r;
+        double qs = rvls;
+#pragma unroll 1
+        for (int it = 0; it < 10; it++) {
+            const double rt = 1.0 / temps;
+            const double dT = ((tc - temps) * cpl + qt - rvls) / (cpl + a2 * rvls * rt * rt);
+            temps = temps + dT;
+            qs = qsat_qs(temps, p, tbl);
+            rvls = qs;
+            const bool conv = fabs(dT) < 1.e-10 * temps;
+            if (__all_sync(__activemask(), conv)) break;
+        }
+        double qc = MX(qt - qs, 0.0);
+        qv = qt - qc;
+        ql = qc * (1.0 - nu);
+        qi = nu * qc;
+        th = temps / ex;
+        id_check = (fabs((temps - (leff / c.cp) * qc) - tc) >= 1.0) ? 1 : 0;
+    }
+    return id_check;
+}
+
 // roots (uwshcu.F90:4787-4829); r1/r2 keep the caller's values on the failure branches.
 __device__ __forceinline__ int roots(double a, double b, double cc, double& r1, double& r2)
 {
@@ -414,10 +458,12 @@ __device__ double findsp_point(double q, double t, double p, unsigned int& errbi
 // One column per lane: column i of A when `active`.  All 32 lanes of the warp must call it together
 // (it starts with a warp ballot).  `tbl` is the saturation table in shared memory.  In
 // UW_MODE_TRIGGER, convecting columns are appended to wl / *wl_count.
-template <int KP, int NC, int MODE>
+// FAST = 1: the fast-FP64 precision mode (conden_fast in place of conden), not bit-exact.
+template <int KP, int NC, int MODE, int FAST>
 __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restrict__ tbl, const int i,
                                           const bool active, int* __restrict__ wl, int* __restrict__ wl_count)
 {
+#define CONDEN(...) (FAST ? conden_fast(__VA_ARGS__) : conden(__VA_ARGS__))
     bool cand = false;
     // lanes of this warp that run a column; UW_SYNC() joins them where every one of them arrives
     const unsigned live = __ballot_sync(0xffffffffu, active);
@@ -547,7 +593,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
     for (int k = 1; k <= mkx; k++) {
         double thl0bot = thl0[k] + ssthl0[k] * (ps0[k - 1] - p0[k]);
         double qt0bot = qt0[k] + ssqt0[k] * (ps0[k - 1] - p0[k]);
-        if (conden(ps0[k - 1], exns0[k - 1], thl0bot, qt0bot, thj, qvj, qlj, qij, tbl)) {
+        if (CONDEN(ps0[k - 1], exns0[k - 1], thl0bot, qt0bot, thj, qvj, qlj, qij, tbl)) {
             xflags |= UW_X_CONDEN;
             id_exit = true;
             stop = true;
@@ -557,7 +603,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
         thvl0bot[k] = thl0bot * (1.0 + zvir * qt0bot);
         double thl0top = thl0[k] + ssthl0[k] * (ps0[k] - p0[k]);
         double qt0top = qt0[k] + ssqt0[k] * (ps0[k] - p0[k]);
-        if (conden(ps0[k], exns0[k], thl0top, qt0top, thj, qvj, qlj, qij, tbl)) {
+        if (CONDEN(ps0[k], exns0[k], thl0top, qt0top, thj, qvj, qlj, qij, tbl)) {
             xflags |= UW_X_CONDEN;
             id_exit = true;
             stop = true;
@@ -678,7 +724,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
         {
             double thl0lcl = thl0[klcl] + ssthl0[klcl] * (plcl - p0[klcl]);
             double qt0lcl = qt0[klcl] + ssqt0[klcl] * (plcl - p0[klcl]);
-            if (conden(plcl, exlcl, thl0lcl, qt0lcl, thj, qvj, qlj, qij, tbl)) {
+            if (CONDEN(plcl, exlcl, thl0lcl, qt0lcl, thj, qvj, qlj, qij, tbl)) {
                 xflags |= UW_X_CONDEN;
                 id_exit = true;
                 stop = true;
@@ -712,7 +758,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                         break;
                     }
                     if (!lcl_above && k == kinv) {
-                        if (conden(ps0[k - 1], exns0[k - 1], thlsrc, qtsrc, thj, qvj, qlj, qij, tbl)) {
+                        if (CONDEN(ps0[k - 1], exns0[k - 1], thlsrc, qtsrc, thj, qvj, qlj, qij, tbl)) {
                             xflags |= UW_X_CONDEN;
                             id_exit = true;
                             stop = true;
@@ -732,7 +778,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                     } else {
                         thvubot = thvutop;
                     }
-                    if (conden(ps0[k], exns0[k], thlsrc, qtsrc, thj, qvj, qlj, qij, tbl)) {
+                    if (CONDEN(ps0[k], exns0[k], thlsrc, qtsrc, thj, qvj, qlj, qij, tbl)) {
                         xflags |= UW_X_CONDEN;
                         id_exit = true;
                         stop = true;
@@ -921,7 +967,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
         wu[krel - 1] = wlcl;
         thlu[krel - 1] = thlsrc;
         qtu[krel - 1] = qtsrc;
-        if (conden(prel, exprel, thlsrc, qtsrc, thj, qvj, qlj, qij, tbl)) {
+        if (CONDEN(prel, exprel, thlsrc, qtsrc, thj, qvj, qlj, qij, tbl)) {
             xflags |= UW_X_CONDEN;
             id_exit = true;
             stop = true;
@@ -982,35 +1028,42 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                     double wue = wu[km1];
                     wtwb = wtw;
                     bool xdone = false;
+                    // environment at the layer midpoint: the same in both iter_xc passes, so the
+                    // second pass reuses the first one's conden and qsat results (same bits)
+                    double thv0j = 0.0, excess0 = 0.0;
                     for (int iter_xc = 1; iter_xc <= 2; iter_xc++) {
                         if (!xdone && !stop) do {
                         wtw = wu[km1] * wu[km1];
-                        if (conden(pe, exne, thle, qte, thj, qvj, qlj, qij, tbl)) {
-                            xflags |= UW_X_CONDEN;
-                            id_exit = true;
-                            stop = true;
-            break;
+                        if (iter_xc == 1) {
+                            if (CONDEN(pe, exne, thle, qte, thj, qvj, qlj, qij, tbl)) {
+                                xflags |= UW_X_CONDEN;
+                                id_exit = true;
+                                stop = true;
+                                break;
+                            }
+                            thv0j = thj * (1.0 + zvir * qvj - qlj - qij);
+                            excess0 = qte - qsat_qs(thle * exne, pe, tbl);
                         }
-                        double thv0j = thj * (1.0 + zvir * qvj - qlj - qij);
                         rho0j = pe / (r * thv0j * exne);
-                        double excess0 = qte - qsat_qs(thle * exne, pe, tbl);
-                        if (conden(pe, exne, thlue, qtue, thj, qvj, qlj, qij, tbl)) {
+                        if (CONDEN(pe, exne, thlue, qtue, thj, qvj, qlj, qij, tbl)) {
                             xflags |= UW_X_CONDEN;
                             id_exit = true;
                             stop = true;
             break;
                         }
+                        // condensate above criqc leaves the updraft; without it the Fortran's
+                        // second conden call repeats the first one's arguments and results
                         if ((qlj + qij) > criqc) {
                             double exql = ((qlj + qij) - criqc) * qlj / (qlj + qij);
                             double exqi = ((qlj + qij) - criqc) * qij / (qlj + qij);
                             qtue = qtue - exql - exqi;
                             thlue = thlue + (xlv / cp / exne) * exql + (xls / cp / exne) * exqi;
-                        }
-                        if (conden(pe, exne, thlue, qtue, thj, qvj, qlj, qij, tbl)) {
-                            xflags |= UW_X_CONDEN;
-                            id_exit = true;
-                            stop = true;
-            break;
+                            if (CONDEN(pe, exne, thlue, qtue, thj, qvj, qlj, qij, tbl)) {
+                                xflags |= UW_X_CONDEN;
+                                id_exit = true;
+                                stop = true;
+                                break;
+                            }
                         }
                         double thvj = thj * (1.0 + zvir * qvj - qlj - qij);
                         double excessu = qtue - qsat_qs(thlue * exne, pe, tbl);
@@ -1022,7 +1075,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                             double xsat = excessu / (excessu - excess0);
                             double thlxsat = thlue + xsat * (thle - thlue);
                             double qtxsat = qtue + xsat * (qte - qtue);
-                            if (conden(pe, exne, thlxsat, qtxsat, thj, qvj, qlj, qij, tbl)) {
+                            if (CONDEN(pe, exne, thlxsat, qtxsat, thj, qvj, qlj, qij, tbl)) {
                                 xflags |= UW_X_CONDEN;
                                 id_exit = true;
                                 stop = true;
@@ -1090,7 +1143,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                                 tru[m][k] = (tre[m] + sstr0[m][k] / fer[k] - sstr0[m][k] * dpe / 2.0) -
                                             (tre[m] + sstr0[m][k] * dpe / 2.0 - tru[m][km1] + sstr0[m][k] / fer[k]) * ef;
                         }
-                        if (conden(ps0[k], exns0[k], thlu[k], qtu[k], thj, qvj, qlj, qij, tbl)) {
+                        if (CONDEN(ps0[k], exns0[k], thlu[k], qtu[k], thj, qvj, qlj, qij, tbl)) {
                             xflags |= UW_X_CONDEN;
                             id_exit = true;
                             stop = true;
@@ -1103,15 +1156,16 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                             thlu[k] = thlu[k] + (xlv / cp / exns0[k]) * exql + (xls / cp / exns0[k]) * exqi;
                             dwten[k] = exql;
                             diten[k] = exqi;
+                            if (CONDEN(ps0[k], exns0[k], thlu[k], qtu[k], thj, qvj, qlj, qij, tbl)) {
+                                xflags |= UW_X_CONDEN;
+                                id_exit = true;
+                                stop = true;
+                                break;
+                            }
                         } else {
+                            // nothing removed: the Fortran's second conden call repeats the first
                             dwten[k] = 0.0;
                             diten[k] = 0.0;
-                        }
-                        if (conden(ps0[k], exns0[k], thlu[k], qtu[k], thj, qvj, qlj, qij, tbl)) {
-                            xflags |= UW_X_CONDEN;
-                            id_exit = true;
-                            stop = true;
-            break;
                         }
                         thvu[k] = thj * (1.0 + zvir * qvj - qlj - qij);
                         bogbot = rbuoy * (thvu[km1] / thvebot - 1.0);
@@ -1209,7 +1263,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                               (qt0[kpen] + ssqt0[kpen] * (-ppen) / 2.0 - qtu[kpen - 1] + ssqt0[kpen] / fer[kpen]) * ef;
                 }
                 exntop = uw_pow((ps0[kpen - 1] + ppen) / p00, rovcp);
-                if (conden(ps0[kpen - 1] + ppen, exntop, thlu_top, qtu_top, thj, qvj, qlj, qij, tbl)) {
+                if (CONDEN(ps0[kpen - 1] + ppen, exntop, thlu_top, qtu_top, thj, qvj, qlj, qij, tbl)) {
                     xflags |= UW_X_CONDEN;
                     id_exit = true;
                     stop = true;
@@ -1408,7 +1462,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                 }
                 double thl_prog = thl0[k] + thlten_sub * dt;
                 double qt_prog = MX(qt0[k] + qtten_sub * dt, 1.e-12);
-                if (conden(p0[k], exn0[k], thl_prog, qt_prog, thj, qvj, qlj, qij, tbl)) {
+                if (CONDEN(p0[k], exn0[k], thl_prog, qt_prog, thj, qvj, qlj, qij, tbl)) {
                     id_exit = true;
                     stop = true;
             break;
@@ -1483,7 +1537,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                     // one conden call site for the release level, the cloud top and the levels between
                     const bool atrel = (k == krel), attop = (k != krel && k == kpen);
                     if (atrel) {
-                        if (conden(prel, exprel, thlu[krel - 1], qtu[krel - 1], thj, qvj, qlj, qij, tbl)) {
+                        if (CONDEN(prel, exprel, thlu[krel - 1], qtu[krel - 1], thj, qvj, qlj, qij, tbl)) {
                             xflags |= UW_X_CONDEN;
                             id_exit = true;
                             stop = true;
@@ -1492,7 +1546,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                         qlubelow = qlj;
                         qiubelow = qij;
                     }
-                    if (conden(attop ? ps0[k - 1] + ppen : ps0[k], attop ? exntop : exns0[k], attop ? thlu_top : thlu[k],
+                    if (CONDEN(attop ? ps0[k - 1] + ppen : ps0[k], attop ? exntop : exns0[k], attop ? thlu_top : thlu[k],
                                attop ? qtu_top : qtu[k], thj, qvj, qlj, qij, tbl)) {
                         xflags |= UW_X_CONDEN;
                         id_exit = true;
@@ -1538,7 +1592,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                     nc_lm = nc_lm - g * umf[k] * trl / (ps0[k - 1] - ps0[k]);
                     nc_im = nc_im - g * umf[k] * tri / (ps0[k - 1] - ps0[k]);
                     double ql_emf_kbup, qi_emf_kbup, thjj, qvjj;
-                    if (conden(p0[k], exn0[k], thlu_emf[k], qtu_emf[k], thjj, qvjj, ql_emf_kbup, qi_emf_kbup, tbl)) {
+                    if (CONDEN(p0[k], exn0[k], thlu_emf[k], qtu_emf[k], thjj, qvjj, ql_emf_kbup, qi_emf_kbup, tbl)) {
                         id_exit = true;
                         stop = true;
             break;
@@ -1696,7 +1750,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
             }
         }
         // in-cloud diagnostics (:4092-4158)
-        if (conden(prel, exprel, thlu[krel - 1], qtu[krel - 1], thj, qvj, qlj, qij, tbl)) {
+        if (CONDEN(prel, exprel, thlu[krel - 1], qtu[krel - 1], thj, qvj, qlj, qij, tbl)) {
             xflags |= UW_X_CONDEN;
             id_exit = true;
             stop = true;
@@ -1712,7 +1766,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                 if (k > kpen) ldone = true;
                 if (!ldone) do {
                 const bool attop = (k == kpen);
-                const int idc = conden(attop ? ps0[k - 1] + ppen : ps0[k], attop ? exntop : exns0[k],
+                const int idc = CONDEN(attop ? ps0[k - 1] + ppen : ps0[k], attop ? exntop : exns0[k],
                                        attop ? thlu_top : thlu[k], attop ? qtu_top : qtu[k], thj, qvj, qlj, qij, tbl);
                 if (idc) {
                     xflags |= UW_X_CONDEN;
@@ -1797,7 +1851,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                 if (!ldone) do {
                 double thl0bot = thl0[k] + ssthl0[k] * (ps0[k - 1] - p0[k]);
                 double qt0bot = qt0[k] + ssqt0[k] * (ps0[k - 1] - p0[k]);
-                if (conden(ps0[k - 1], exns0[k - 1], thl0bot, qt0bot, thj, qvj, qlj, qij, tbl)) {
+                if (CONDEN(ps0[k - 1], exns0[k - 1], thl0bot, qt0bot, thj, qvj, qlj, qij, tbl)) {
                     xflags |= UW_X_CONDEN;
                     id_exit = true;
                     stop = true;
@@ -1807,7 +1861,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                 thvl0bot[k] = thl0bot * (1.0 + zvir * qt0bot);
                 double thl0top = thl0[k] + ssthl0[k] * (ps0[k] - p0[k]);
                 double qt0top = qt0[k] + ssqt0[k] * (ps0[k] - p0[k]);
-                if (conden(ps0[k], exns0[k], thl0top, qt0top, thj, qvj, qlj, qij, tbl)) {
+                if (CONDEN(ps0[k], exns0[k], thl0top, qt0top, thj, qvj, qlj, qij, tbl)) {
                     xflags |= UW_X_CONDEN;
                     id_exit = true;
                     stop = true;
@@ -1919,6 +1973,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
         }
     }
 #undef UW_SYNC
+#undef CONDEN
 #undef RI
 #undef RL
 #undef CNT
@@ -1953,7 +2008,29 @@ uwshcu_fp64_kernel(const __grid_constant__ UwArgs A, int* __restrict__ wl, int* 
         active = tid < A.iend;
         i = tid;
     }
-    uw_column<KP, NC, MODE>(A, tbl, i, active, wl, wl_count);
+    uw_column<KP, NC, MODE, 0>(A, tbl, i, active, wl, wl_count);
+}
+
+// The fast-FP64 precision mode: same launch shapes as uwshcu_fp64_kernel.
+template <int KP, int NC, int MODE>
+__global__ void __launch_bounds__(128, MODE == UW_MODE_LIST ? 4 : (MODE == UW_MODE_TRIGGER ? 5 : 3))
+uwshcu_fast_kernel(const __grid_constant__ UwArgs A, int* __restrict__ wl, int* __restrict__ wl_count)
+{
+    __shared__ double tbl[UW_TBL];
+    for (int t = threadIdx.x; t < UW_TBL; t += blockDim.x) tbl[t] = c_estbl[t];
+    __syncthreads();
+
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    int i;
+    bool active;
+    if (MODE == UW_MODE_LIST) {
+        active = tid < *wl_count;
+        i = active ? wl[tid] : 0;
+    } else {
+        active = tid < A.iend;
+        i = tid;
+    }
+    uw_column<KP, NC, MODE, 1>(A, tbl, i, active, wl, wl_count);
 }
 
 // Batched trigger pass: every column of every member of B (members of one level/tracer class).
@@ -1970,7 +2047,7 @@ __global__ void __launch_bounds__(128, 5) uwshcu_batch_trigger(const __grid_cons
     while (m + 1 < B.nm && (int)blockIdx.x >= B.block_start[m + 1]) m++;
     const int tid = ((int)blockIdx.x - B.block_start[m]) * blockDim.x + threadIdx.x;
     const bool active = tid < B.m[m].iend;
-    uw_column<KP, NC, UW_MODE_TRIGGER>(B.m[m], tbl, tid, active, B.wl[m], B.count + m);
+    uw_column<KP, NC, UW_MODE_TRIGGER, 0>(B.m[m], tbl, tid, active, B.wl[m], B.count + m);
 }
 
 // Batched worklist pass, persistent: each warp takes the next task (32 * B.chunk consecutive queue
@@ -2008,7 +2085,7 @@ __global__ void __launch_bounds__(128, MINB) uwshcu_batch_list(const __grid_cons
             const int idx = first + c * 32 + lane;
             const bool active = idx < n;
             const int i = active ? B.wl[m][idx] : 0;
-            uw_column<KP, NC, UW_MODE_LIST>(B.m[m], tbl, i, active, nullptr, nullptr);
+            uw_column<KP, NC, UW_MODE_LIST, 0>(B.m[m], tbl, i, active, nullptr, nullptr);
         }
     }
 }

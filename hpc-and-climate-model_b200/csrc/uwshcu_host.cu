@@ -29,6 +29,15 @@ UW_DECL(64, 5)
 UW_DECL(32, 32)
 UW_DECL(64, 32)
 #undef UW_DECL
+#define UW_DECL_FAST(KP, NC)                                                                              \
+    extern "C" cudaError_t uw_fast_set_constants_k##KP##n##NC(const UwConst* h, const double* tbl);       \
+    extern "C" cudaError_t uw_fast_launch_k##KP##n##NC(const UwArgs* a, int mode, int* wl, int* wl_count, \
+                                                       int nthreads, int block, cudaStream_t stream);
+UW_DECL_FAST(32, 5)
+UW_DECL_FAST(64, 5)
+UW_DECL_FAST(32, 32)
+UW_DECL_FAST(64, 32)
+#undef UW_DECL_FAST
 #define UW_DECL_MIXED(KP, NC)                                                                              \
     extern "C" cudaError_t uw_mixed_set_constants_k##KP##n##NC(const UwConst* h, const double* tbl);       \
     extern "C" cudaError_t uw_mixed_launch_k##KP##n##NC(const UwArgs* a, int mode, int* wl, int* wl_count, \
@@ -49,6 +58,10 @@ cudaError_t set_constants_all(const UwConst* k, const double* tbl)
     if ((e = uw_fp64_set_constants_k64n5(k, tbl)) != cudaSuccess) return e;
     if ((e = uw_fp64_set_constants_k32n32(k, tbl)) != cudaSuccess) return e;
     if ((e = uw_fp64_set_constants_k64n32(k, tbl)) != cudaSuccess) return e;
+    if ((e = uw_fast_set_constants_k32n5(k, tbl)) != cudaSuccess) return e;
+    if ((e = uw_fast_set_constants_k64n5(k, tbl)) != cudaSuccess) return e;
+    if ((e = uw_fast_set_constants_k32n32(k, tbl)) != cudaSuccess) return e;
+    if ((e = uw_fast_set_constants_k64n32(k, tbl)) != cudaSuccess) return e;
     if ((e = uw_mixed_set_constants_k32n5(k, tbl)) != cudaSuccess) return e;
     return uw_mixed_set_constants_k64n5(k, tbl);
 }
@@ -59,6 +72,13 @@ cudaError_t launch_mode(const UwArgs* a, int prec, int mode, int* wl, int* wl_co
     if (prec == UWSHCU_PREC_MIXED) {
         if (a->mkx + 1 <= 32 && a->ncnst <= 5) return uw_mixed_launch_k32n5(a, mode, wl, wl_count, nthreads, block, st);
         if (a->mkx + 1 <= 64 && a->ncnst <= 5) return uw_mixed_launch_k64n5(a, mode, wl, wl_count, nthreads, block, st);
+        return cudaErrorInvalidValue;
+    }
+    if (prec == UWSHCU_PREC_FAST) {
+        if (a->mkx + 1 <= 32 && a->ncnst <= 5) return uw_fast_launch_k32n5(a, mode, wl, wl_count, nthreads, block, st);
+        if (a->mkx + 1 <= 64 && a->ncnst <= 5) return uw_fast_launch_k64n5(a, mode, wl, wl_count, nthreads, block, st);
+        if (a->mkx + 1 <= 32 && a->ncnst <= UW_NCMAX) return uw_fast_launch_k32n32(a, mode, wl, wl_count, nthreads, block, st);
+        if (a->mkx + 1 <= 64 && a->ncnst <= UW_NCMAX) return uw_fast_launch_k64n32(a, mode, wl, wl_count, nthreads, block, st);
         return cudaErrorInvalidValue;
     }
     if (a->mkx + 1 <= 32 && a->ncnst <= 5) return uw_fp64_launch_k32n5(a, mode, wl, wl_count, nthreads, block, st);
@@ -581,7 +601,7 @@ int uwshcu_set_precision(int mode)
 {
     State& s = S();
     std::lock_guard<std::mutex> lock(s.mu);
-    if (mode != UWSHCU_PREC_FP64 && mode != UWSHCU_PREC_MIXED) return UWSHCU_ERR_BAD_ARGS;
+    if (mode != UWSHCU_PREC_FP64 && mode != UWSHCU_PREC_MIXED && mode != UWSHCU_PREC_FAST) return UWSHCU_ERR_BAD_ARGS;
     s.precision = mode;
     return UWSHCU_OK;
 }

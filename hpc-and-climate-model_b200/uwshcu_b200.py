@@ -82,6 +82,7 @@ def set_rpen(rpen):
 
 PREC_FP64 = 0
 PREC_MIXED = 1
+PREC_FAST = 2
 
 
 def set_precision(mode):

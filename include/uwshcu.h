@@ -37,6 +37,10 @@ extern "C" {
 #define UWSHCU_PREC_FP64 0               /* FP64 throughout, Fortran evaluation order, no FMA      */
 #define UWSHCU_PREC_MIXED 1              /* FP32 bulk, FP64 conden/roots/qsinvert/implicit CIN/
                                             positive_moisture, Kahan vertical sums (ncnst <= 5)    */
+#define UWSHCU_PREC_FAST 2               /* FP64 throughout with a Newton conden that stops once the
+                                            warp's steps are below 1e-10 T and divides twice per
+                                            step instead of five times; FMA contraction allowed.
+                                            Not bit-exact: ~1e-12 relative per conden call     */
 
 /* ---- set-up -------------------------------------------------------------------------------- */
 
@@ -58,7 +62,7 @@ int uwshcu_set_rpen(double rpen);
  * qmin = {1e-12, 0, 0, 0, 0}. */
 int uwshcu_init_default(void);
 
-/* Precision of the device path: UWSHCU_PREC_FP64 (default) or UWSHCU_PREC_MIXED. */
+/* Precision of the device path: UWSHCU_PREC_FP64 (default), UWSHCU_PREC_MIXED or UWSHCU_PREC_FAST. */
 int uwshcu_set_precision(int mode);
 
 /* Kernel schedules (uwshcu_set_schedule). */

@@ -1,0 +1,35 @@
+"""Reduced-precision device paths against the FP64 path on the same inputs (the FP64 path is bit for
+bit the oracle).  The bar of the precision targets: at most 1e-4 relative RMS error in column
+heating, moistening and precipitation, and the decisions (trigger, cloud base, cloud top) of at
+least 99.9 % of the columns unchanged."""
+import numpy as np
+import pytest
+
+import errstats
+import soundings
+
+
+def _run(uw, s, prec):
+    assert uw.set_precision(prec) == 0
+    try:
+        case = uw.DeviceCase(s)
+        assert case.launch() == 0, uw.last_cuda_error()
+        st = case.status()
+        return st, case.outputs_numpy()
+    finally:
+        uw.set_precision(uw.PREC_FP64)
+
+
+@pytest.mark.gpu
+def test_fast_fp64_mode_within_precision_bar(uw, cuda):
+    assert uw.init_default() == 0
+    s = soundings.make_soundings(16384, 30, seed=71, rh_pbl=(0.675, 0.93))
+    st64, ref = _run(uw, s, uw.PREC_FP64)
+    stf, out = _run(uw, s, uw.PREC_FAST)
+    assert st64 == 0 and stf == 0
+    rep = errstats.report(out, ref, s["dp0"])
+    for k, v in rep["column"].items():
+        assert v["rel_rms"] <= 1e-4, (k, v)
+    flips = rep["flips"]
+    n = rep["columns"]
+    assert flips["trigger"] + flips["cloud_base"] + flips["cloud_top"] <= 1e-3 * n, flips
