@@ -12,7 +12,7 @@
 //
 // The FP64 islands use algebraically equal but cheaper forms than the Fortran (one division per
 // Newton step instead of six, FMA contraction allowed) and stop the conden iteration once the
-// temperature change is below 1e-9 K; this kernel is checked against the FP64 oracle with error
+// temperature change is below 1e-9 K on every lane of the warp; this kernel is checked against the FP64 oracle with error
 // statistics, not bit for bit.
 #pragma once
 #include <cuda_runtime.h>
@@ -101,7 +101,7 @@ __device__ __forceinline__ void qsat3_d(double t, double p, double& es, double& 
 __device__ __forceinline__ float exnf(float p) { return powf(p / (float)c.p00, (float)c.rovcp); }
 
 // conden (uwshcu.F90:4718-4785): FP64 saturation adjustment from FP32 (p, exner, thl, qt).
-__device__ __forceinline__ int conden(R p, R ex, R thl, R qt, R& th, R& qv, R& ql, R& qi,
+__device__ __noinline__ int conden(R p, R ex, R thl, R qt, R& th, R& qv, R& ql, R& qi,
                                       const double* __restrict__ tbld, const float* __restrict__ tblf)
 {
     (void)tblf;
@@ -130,7 +130,7 @@ __device__ __forceinline__ int conden(R p, R ex, R thl, R qt, R& th, R& qv, R& q
         es = estblf_d(temps, tbld);
         rvls = MN(1.0, c.epsqs * es / (pd - c.omeps * es));
         if (rvls < 0.0) rvls = 1.0;
-        if (fabs(dT) < 1.e-9) break;
+        if (__all_sync(__activemask(), fabs(dT) < 1.e-9)) break;
     }
     const double qc = MX(qtd - rvls, 0.0);
     qv = (R)(qtd - qc);
@@ -409,28 +409,19 @@ __device__ R findsp_point(R q, R t, R p, unsigned int& errbits, const double* __
 // The worklist path recomputes the phase-1 part of a convecting column instead of storing it: the
 // heavy buoyancy-sorting work then runs in warps made only of convecting columns.
 
-template <int KP, int NC, int MODE>
-__global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __restrict__ wl, int* __restrict__ wl_count)
+// One column per lane: column i of A when `active`.  All 32 lanes of the warp must call it together
+// (it starts with a warp ballot).  `tbl` is the saturation table in shared memory.  In
+// UW_MODE_TRIGGER, convecting columns are appended to wl / *wl_count.
+// FAST = 1: the fast-FP64 precision mode (conden_fast in place of conden), not bit-exact.
+template <int KP, int NC, int MODE, int FAST>
+__device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restrict__ tbld, const float* __restrict__ tblf, const int i,
+                                          const bool active, int* __restrict__ wl, int* __restrict__ wl_count)
 {
-    __shared__ double tbld[UW_TBL];
-    __shared__ float tblf[UW_TBL];
-    for (int t = threadIdx.x; t < UW_TBL; t += blockDim.x) {
-        tbld[t] = c_estbl[t];
-        tblf[t] = (float)c_estbl[t];
-    }
-    __syncthreads();
-
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    int i;
-    bool active;
-    if (MODE == UW_MODE_LIST) {
-        active = tid < *wl_count;
-        i = active ? wl[tid] : 0;
-    } else {
-        active = tid < A.iend;
-        i = tid;
-    }
+#define CONDEN(...) conden(__VA_ARGS__)
     bool cand = false;
+    // lanes of this warp that run a column; UW_SYNC() joins them where every one of them arrives
+    const unsigned live = __ballot_sync(0xffffffffu, active);
+#define UW_SYNC() __syncwarp(live)
     if (active) {
 
     const int mix = A.mix, mkx = A.mkx, ncnst = A.ncnst;
@@ -474,9 +465,7 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
     unsigned int errbits = 0;
     int xflags = 0, lflags = 0;
     bool id_exit = false;
-    // stop: the column leaves the scheme (the Fortran's `go to 333`).  Exits leave every loop through
-    // the loop's own exit (break, then `if (stop) break;` after each inner loop) so that lanes that
-    // leave a loop at different iterations reconverge right after it.
+    // stop: the column leaves the scheme (the Fortran's `go to 333`); every later section skips.
     bool stop = false;
     int kinv = 0, klcl = 0, klfc = 0, krel = 0, kbup = 0, kpen = 0;
     int kinv_s = 0, klcl_s = 0, klfc_s = 0, krel_s = 0, kbup_s = 0, kpen_s = 0;
@@ -562,7 +551,7 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
     for (int k = 1; k <= mkx; k++) {
         R thl0bot = thl0[k] + ssthl0[k] * (ps0[k - 1] - p0[k]);
         R qt0bot = qt0[k] + ssqt0[k] * (ps0[k - 1] - p0[k]);
-        if (conden(ps0[k - 1], exns0[k - 1], thl0bot, qt0bot, thj, qvj, qlj, qij, tbld, tblf)) {
+        if (CONDEN(ps0[k - 1], exns0[k - 1], thl0bot, qt0bot, thj, qvj, qlj, qij, tbld, tblf)) {
             xflags |= UW_X_CONDEN;
             id_exit = true;
             stop = true;
@@ -572,7 +561,7 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
         thvl0bot[k] = thl0bot * (1.0f + zvir * qt0bot);
         R thl0top = thl0[k] + ssthl0[k] * (ps0[k] - p0[k]);
         R qt0top = qt0[k] + ssqt0[k] * (ps0[k] - p0[k]);
-        if (conden(ps0[k], exns0[k], thl0top, qt0top, thj, qvj, qlj, qij, tbld, tblf)) {
+        if (CONDEN(ps0[k], exns0[k], thl0top, qt0top, thj, qvj, qlj, qij, tbld, tblf)) {
             xflags |= UW_X_CONDEN;
             id_exit = true;
             stop = true;
@@ -610,17 +599,31 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
     cnb = 0.0f;
     }
 
+    UW_SYNC();
+
     // ---- implicit-CIN loop (uwshcu.F90:1421-4331) --------------------------------------------
-    for (int iter = 1; iter <= 2 && !stop; iter++) {
-        R tscaleh = cush;
+    // Lockstep skeleton.  Every lane of the warp runs the same iterations of this loop and of every
+    // level loop inside it: a column's own level range and its exits are per-lane predicates.  Each
+    // section is `if (!stop) do { ... } while (0);`, so an exit (`stop = true; break;`) skips the
+    // rest of the section and every later one, and the lanes meet again at UW_SYNC() between
+    // sections.  (Lanes that leave a loop at different iterations otherwise run apart for the rest
+    // of the column: the worklist kernel ran with 1.9f of 32 lanes active.)  Loops marked `uniform`
+    // have the same trip count on every live lane; UW_SYNC() appears only directly inside them.
+    for (int iter = 1; iter <= (MODE == UW_MODE_TRIGGER ? 1 : 2); iter++) {   // uniform
+        R tscaleh = 0.0f;
+        if (!stop) do {
+        tscaleh = cush;
         cush = -1.0f;
 
-        // kinv (:1455-1468)
+        // kinv (:1455-1468): the first interface from the top whose layer brackets pblh + 5
         kinv = 1;
-        for (int k = mkx - 1; k >= 1; k--) {
-            if ((pblh + 5.0f - zs0[k]) * (pblh + 5.0f - zs0[k + 1]) < 0.0f) {
-                kinv = k + 1;
-                break;
+        {
+            bool found = false;
+            for (int k = mkx - 1; k >= 1; k--) {
+                if (!found && (pblh + 5.0f - zs0[k]) * (pblh + 5.0f - zs0[k + 1]) < 0.0f) {
+                    kinv = k + 1;
+                    found = true;
+                }
             }
         }
         if (kinv <= 1) {
@@ -633,7 +636,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
         {
             Kahan dpsum, tksum;
             thvlmin = 1000.0f;
-            for (int k = 0; k <= kinv - 1; k++) {
+            for (int k = 0; k <= mkx; k++) {
+                if (k > kinv - 1) continue;
                 R dpi;
                 if (k == 0) dpi = ps0[0] - p0[1];
                 else if (k == (kinv - 1)) dpi = p0[kinv - 1] - ps0[kinv - 1];
@@ -651,13 +655,19 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
         usrc = GL(u0, kinv - 1) + ssu0[kinv - 1] * (ps0[kinv - 1] - p0[kinv - 1]);
         vsrc = GL(v0, kinv - 1) + ssv0[kinv - 1] * (ps0[kinv - 1] - p0[kinv - 1]);
         for (int m = 1; m <= ncnst; m++) trsrc[m - 1] = GT(m, 1);
+        } while (0);
+        UW_SYNC();
         // LCL (:1533-1549)
+        if (!stop) do {
         plcl = qsinvert(qtsrc, thlsrc, ps0[0], exns0[0], tbld, tblf);
         klcl = mkx;
-        for (int k = 0; k <= mkx; k++) {
-            if (ps0[k] < plcl) {
-                klcl = k;
-                break;
+        {
+            bool found = false;
+            for (int k = 0; k <= mkx; k++) {
+                if (!found && ps0[k] < plcl) {
+                    klcl = k;
+                    found = true;
+                }
             }
         }
         klcl = MX(1, klcl);
@@ -671,7 +681,7 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
         {
             R thl0lcl = thl0[klcl] + ssthl0[klcl] * (plcl - p0[klcl]);
             R qt0lcl = qt0[klcl] + ssqt0[klcl] * (plcl - p0[klcl]);
-            if (conden(plcl, exlcl, thl0lcl, qt0lcl, thj, qvj, qlj, qij, tbld, tblf)) {
+            if (CONDEN(plcl, exlcl, thl0lcl, qt0lcl, thj, qvj, qlj, qij, tbld, tblf)) {
                 xflags |= UW_X_CONDEN;
                 id_exit = true;
                 stop = true;
@@ -679,20 +689,42 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
             }
             thv0lcl = thj * (1.0f + zvir * qvj - qlj - qij);
         }
-        // CIN (:1592-1685)
-        cin = 0.0f;
-        cinlcl = 0.0f;
-        plfc = 0.0f;
-        klfc = mkx;
+        } while (0);
+        UW_SYNC();
+        // CIN (:1592-1685).  One loop over k = kinv .. mkx-1 serves both cases of the Fortran (LCL at
+        // or above kinv, LCL below kinv), with one conden call at ps0(k) per level for every lane.
+        // When the LCL is below kinv the Fortran also calls conden at ps0(k-1) with the same source
+        // air; above the first level that repeats the previous level's call bit for bit, so only
+        // the first level makes it here.
+        if (!stop) {
+            cin = 0.0f;
+            cinlcl = 0.0f;
+            plfc = 0.0f;
+            klfc = mkx;
+        }
         {
-            R thvubot, thvutop = 0.0f;
-            if (klcl >= kinv) {
-                for (int k = kinv; k <= mkx - 1; k++) {
-                    if (k < klcl) {
+            const bool lcl_above = (klcl >= kinv);
+            R thvubot = 0.0f, thvutop = 0.0f;
+            bool ldone = stop;
+            for (int k = 2; k <= mkx - 1; k++) {   // uniform (kinv >= 2)
+                if (!ldone && k >= kinv) do {
+                    if (lcl_above && k < klcl) {
                         thvubot = thvlsrc;
                         thvutop = thvlsrc;
                         cin = cin + single_cin(ps0[k - 1], exns0[k - 1], thv0bot[k], ps0[k], exns0[k], thv0top[k], thvubot, thvutop);
-                    } else if (k == klcl) {
+                        break;
+                    }
+                    if (!lcl_above && k == kinv) {
+                        if (CONDEN(ps0[k - 1], exns0[k - 1], thlsrc, qtsrc, thj, qvj, qlj, qij, tbld, tblf)) {
+                            xflags |= UW_X_CONDEN;
+                            id_exit = true;
+                            stop = true;
+                            break;
+                        }
+                        thvutop = thj * (1.0f + zvir * qvj - qlj - qij);
+                    }
+                    const bool atlcl = lcl_above && k == klcl;
+                    if (atlcl) {
                         thvubot = thvlsrc;
                         thvutop = thvlsrc;
                         cin = cin + single_cin(ps0[k - 1], exns0[k - 1], thv0bot[k], plcl, exlcl, thv0lcl, thvubot, thvutop);
@@ -700,60 +732,28 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                         cinlcl = MX(cin, 0.0f);
                         cin = cinlcl;
                         thvubot = thvlsrc;
-                        if (conden(ps0[k], exns0[k], thlsrc, qtsrc, thj, qvj, qlj, qij, tbld, tblf)) {
-                            xflags |= UW_X_CONDEN;
-                            id_exit = true;
-                            stop = true;
-            break;
-                        }
-                        thvutop = thj * (1.0f + zvir * qvj - qlj - qij);
-                        getbuoy(plcl, exlcl, thv0lcl, ps0[k], exns0[k], thv0top[k], thvubot, thvutop, plfc, cin);
-                        if (plfc > 0.0f) {
-                            klfc = k;
-                            break;
-                        }
                     } else {
                         thvubot = thvutop;
-                        if (conden(ps0[k], exns0[k], thlsrc, qtsrc, thj, qvj, qlj, qij, tbld, tblf)) {
-                            xflags |= UW_X_CONDEN;
-                            id_exit = true;
-                            stop = true;
-            break;
-                        }
-                        thvutop = thj * (1.0f + zvir * qvj - qlj - qij);
-                        getbuoy(ps0[k - 1], exns0[k - 1], thv0bot[k], ps0[k], exns0[k], thv0top[k], thvubot, thvutop, plfc, cin);
-                        if (plfc > 0.0f) {
-                            klfc = k;
-                            break;
-                        }
                     }
-                }
-            } else {
-                cinlcl = 0.0f;
-                for (int k = kinv; k <= mkx - 1; k++) {
-                    if (conden(ps0[k - 1], exns0[k - 1], thlsrc, qtsrc, thj, qvj, qlj, qij, tbld, tblf)) {
+                    if (CONDEN(ps0[k], exns0[k], thlsrc, qtsrc, thj, qvj, qlj, qij, tbld, tblf)) {
                         xflags |= UW_X_CONDEN;
                         id_exit = true;
                         stop = true;
-            break;
-                    }
-                    thvubot = thj * (1.0f + zvir * qvj - qlj - qij);
-                    if (conden(ps0[k], exns0[k], thlsrc, qtsrc, thj, qvj, qlj, qij, tbld, tblf)) {
-                        xflags |= UW_X_CONDEN;
-                        id_exit = true;
-                        stop = true;
-            break;
-                    }
-                    thvutop = thj * (1.0f + zvir * qvj - qlj - qij);
-                    getbuoy(ps0[k - 1], exns0[k - 1], thv0bot[k], ps0[k], exns0[k], thv0top[k], thvubot, thvutop, plfc, cin);
-                    if (plfc > 0.0f) {
-                        klfc = k;
                         break;
                     }
-                }
+                    thvutop = thj * (1.0f + zvir * qvj - qlj - qij);
+                    getbuoy(atlcl ? plcl : ps0[k - 1], atlcl ? exlcl : exns0[k - 1], atlcl ? thv0lcl : thv0bot[k],
+                            ps0[k], exns0[k], thv0top[k], thvubot, thvutop, plfc, cin);
+                    if (plfc > 0.0f) {
+                        klfc = k;
+                        ldone = true;
+                    }
+                } while (0);
+                if (stop) ldone = true;
             }
         }
-        if (stop) break;
+        UW_SYNC();
+        if (!stop) do {
         // (label 35, :1676-1685)
         if (cin < 0.0f) lflags |= UW_L_CIN;
         cin = MX(0.0f, cin);
@@ -842,7 +842,10 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
             }
         }
 
+        } while (0);
+        UW_SYNC();
         // ---- release level and closure (:2035-2184) ------------------------------------------
+        if (!stop) do {
         if (klcl < kinv) {
             krel = kinv;
             prel = ps0[krel - 1];
@@ -898,24 +901,30 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
             break;
             }
             ufrc[krel - 1] = ufrclcl;
-            for (int k = kinv - 1; k <= krel - 1; k++) {
+            for (int k = 0; k <= mkx; k++) {
+                if (k < kinv - 1 || k > krel - 1) continue;
                 umf[k] = cbmf;
                 wu[k] = winv;
             }
         }
+        } while (0);
         if (MODE == UW_MODE_TRIGGER) {
             // the column convects past the closure: hand it to the worklist pass
-            cand = true;
-            stop = true;
-            break;
+            if (!stop) {
+                cand = true;
+                stop = true;
+            }
         }
+        UW_SYNC();
+        if (MODE != UW_MODE_TRIGGER) {   // uniform
         // updraft at the release level (:2205-2236)
+        if (!stop) do {
         emf[krel - 1] = 0.0f;
         umf[krel - 1] = cbmf;
         wu[krel - 1] = wlcl;
         thlu[krel - 1] = thlsrc;
         qtu[krel - 1] = qtsrc;
-        if (conden(prel, exprel, thlsrc, qtsrc, thj, qvj, qlj, qij, tbld, tblf)) {
+        if (CONDEN(prel, exprel, thlsrc, qtsrc, thj, qvj, qlj, qij, tbld, tblf)) {
             xflags |= UW_X_CONDEN;
             id_exit = true;
             stop = true;
@@ -928,7 +937,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                 uplus = PGFc * ssu0[kinv] * (prel - ps0[kinv - 1]);
                 vplus = PGFc * ssv0[kinv] * (prel - ps0[kinv - 1]);
             } else {
-                for (int k = kinv; k <= MX(krel - 1, kinv); k++) {
+                for (int k = 0; k <= mkx; k++) {
+                    if (k < kinv || k > MX(krel - 1, kinv)) continue;
                     uplus = uplus + PGFc * ssu0[k] * (ps0[k] - ps0[k - 1]);
                     vplus = vplus + PGFc * ssv0[k] * (ps0[k] - ps0[k - 1]);
                 }
@@ -939,59 +949,78 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
             vu[krel - 1] = vsrc + vplus;
         }
         for (int m = 0; m < ncnst; m++) tru[m][krel - 1] = trsrc[m];
+        } while (0);
+        UW_SYNC();
 
         {
             R scaleh = tscaleh;
             if (tscaleh < 0.0f) scaleh = 1000.0f;
             // ---- buoyancy-sorting updraft, iter_scaleh loop (:2306-2952) ----------------------
-            for (int iter_scaleh = 1; iter_scaleh <= 3; iter_scaleh++) {
-                kbup = krel;
-                kpen = krel;
-                wtw = wlcl * wlcl;
-                R pe = 0.5f * (prel + ps0[krel]);
-                R dpe = prel - ps0[krel];
-                R exne = exnf(pe);
-                R thvebot = thv0rel;
-                R thle = thl0[krel] + ssthl0[krel] * (pe - p0[krel]);
-                R qte = qt0[krel] + ssqt0[krel] * (pe - p0[krel]);
-                R ue = GL(u0, krel) + ssu0[krel] * (pe - p0[krel]);
-                R ve = GL(v0, krel) + ssv0[krel] * (pe - p0[krel]);
-                for (int m = 0; m < ncnst; m++) tre[m] = GT(m + 1, krel) + sstr0[m][krel] * (pe - p0[krel]);
+            for (int iter_scaleh = 1; iter_scaleh <= 3; iter_scaleh++) {   // uniform
+                R pe = 0.0f, dpe = 0.0f, exne = 1.0f, thvebot = 0.0f, thle = 0.0f, qte = 0.0f, ue = 0.0f, ve = 0.0f;
+                if (!stop) {
+                    kbup = krel;
+                    kpen = krel;
+                    wtw = wlcl * wlcl;
+                    pe = 0.5f * (prel + ps0[krel]);
+                    dpe = prel - ps0[krel];
+                    exne = exnf(pe);
+                    thvebot = thv0rel;
+                    thle = thl0[krel] + ssthl0[krel] * (pe - p0[krel]);
+                    qte = qt0[krel] + ssqt0[krel] * (pe - p0[krel]);
+                    ue = GL(u0, krel) + ssu0[krel] * (pe - p0[krel]);
+                    ve = GL(v0, krel) + ssv0[krel] * (pe - p0[krel]);
+                    for (int m = 0; m < ncnst; m++) tre[m] = GT(m + 1, krel) + sstr0[m][krel] * (pe - p0[krel]);
+                }
 
-                for (int k = krel; k <= mkx - 1; k++) {
+                // levels k = krel .. mkx-1, taken by every lane as k = krel + j
+                bool ldone = stop;
+                for (int j = 0; j <= mkx - 2; j++) {   // uniform
+                    const int k = krel + j;
+                    if (k > mkx - 1) ldone = true;
+                    if (!ldone) do {
                     const int km1 = k - 1;
                     R thlue = thlu[km1];
                     R qtue = qtu[km1];
                     R wue = wu[km1];
                     wtwb = wtw;
+                    bool xdone = false;
+                    // environment at the layer midpoint: the same in both iter_xc passes, so the
+                    // second pass reuses the first one's conden and qsat results (same bits)
+                    R thv0j = 0.0f, excess0 = 0.0f;
                     for (int iter_xc = 1; iter_xc <= 2; iter_xc++) {
+                        if (!xdone && !stop) do {
                         wtw = wu[km1] * wu[km1];
-                        if (conden(pe, exne, thle, qte, thj, qvj, qlj, qij, tbld, tblf)) {
-                            xflags |= UW_X_CONDEN;
-                            id_exit = true;
-                            stop = true;
-            break;
+                        if (iter_xc == 1) {
+                            if (CONDEN(pe, exne, thle, qte, thj, qvj, qlj, qij, tbld, tblf)) {
+                                xflags |= UW_X_CONDEN;
+                                id_exit = true;
+                                stop = true;
+                                break;
+                            }
+                            thv0j = thj * (1.0f + zvir * qvj - qlj - qij);
+                            excess0 = qte - qsat_qs(thle * exne, pe, tbld, tblf);
                         }
-                        R thv0j = thj * (1.0f + zvir * qvj - qlj - qij);
                         rho0j = pe / (r * thv0j * exne);
-                        R excess0 = qte - qsat_qs(thle * exne, pe, tbld, tblf);
-                        if (conden(pe, exne, thlue, qtue, thj, qvj, qlj, qij, tbld, tblf)) {
+                        if (CONDEN(pe, exne, thlue, qtue, thj, qvj, qlj, qij, tbld, tblf)) {
                             xflags |= UW_X_CONDEN;
                             id_exit = true;
                             stop = true;
             break;
                         }
+                        // condensate above criqc leaves the updraft; without it the Fortran's
+                        // second conden call repeats the first one's arguments and results
                         if ((qlj + qij) > criqc) {
                             R exql = ((qlj + qij) - criqc) * qlj / (qlj + qij);
                             R exqi = ((qlj + qij) - criqc) * qij / (qlj + qij);
                             qtue = qtue - exql - exqi;
                             thlue = thlue + (xlv / cp / exne) * exql + (xls / cp / exne) * exqi;
-                        }
-                        if (conden(pe, exne, thlue, qtue, thj, qvj, qlj, qij, tbld, tblf)) {
-                            xflags |= UW_X_CONDEN;
-                            id_exit = true;
-                            stop = true;
-            break;
+                            if (CONDEN(pe, exne, thlue, qtue, thj, qvj, qlj, qij, tbld, tblf)) {
+                                xflags |= UW_X_CONDEN;
+                                id_exit = true;
+                                stop = true;
+                                break;
+                            }
                         }
                         R thvj = thj * (1.0f + zvir * qvj - qlj - qij);
                         R excessu = qtue - qsat_qs(thlue * exne, pe, tbld, tblf);
@@ -1003,7 +1032,7 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                             R xsat = excessu / (excessu - excess0);
                             R thlxsat = thlue + xsat * (thle - thlue);
                             R qtxsat = qtue + xsat * (qte - qtue);
-                            if (conden(pe, exne, thlxsat, qtxsat, thj, qvj, qlj, qij, tbld, tblf)) {
+                            if (CONDEN(pe, exne, thlxsat, qtxsat, thj, qvj, qlj, qij, tbld, tblf)) {
                                 xflags |= UW_X_CONDEN;
                                 id_exit = true;
                                 stop = true;
@@ -1071,7 +1100,7 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                                 tru[m][k] = (tre[m] + sstr0[m][k] / fer[k] - sstr0[m][k] * dpe / 2.0f) -
                                             (tre[m] + sstr0[m][k] * dpe / 2.0f - tru[m][km1] + sstr0[m][k] / fer[k]) * ef;
                         }
-                        if (conden(ps0[k], exns0[k], thlu[k], qtu[k], thj, qvj, qlj, qij, tbld, tblf)) {
+                        if (CONDEN(ps0[k], exns0[k], thlu[k], qtu[k], thj, qvj, qlj, qij, tbld, tblf)) {
                             xflags |= UW_X_CONDEN;
                             id_exit = true;
                             stop = true;
@@ -1084,15 +1113,16 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                             thlu[k] = thlu[k] + (xlv / cp / exns0[k]) * exql + (xls / cp / exns0[k]) * exqi;
                             dwten[k] = exql;
                             diten[k] = exqi;
+                            if (CONDEN(ps0[k], exns0[k], thlu[k], qtu[k], thj, qvj, qlj, qij, tbld, tblf)) {
+                                xflags |= UW_X_CONDEN;
+                                id_exit = true;
+                                stop = true;
+                                break;
+                            }
                         } else {
+                            // nothing removed: the Fortran's second conden call repeats the first
                             dwten[k] = 0.0f;
                             diten[k] = 0.0f;
-                        }
-                        if (conden(ps0[k], exns0[k], thlu[k], qtu[k], thj, qvj, qlj, qij, tbld, tblf)) {
-                            xflags |= UW_X_CONDEN;
-                            id_exit = true;
-                            stop = true;
-            break;
                         }
                         thvu[k] = thj * (1.0f + zvir * qvj - qlj - qij);
                         bogbot = rbuoy * (thvu[km1] / thvebot - 1.0f);
@@ -1110,8 +1140,9 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                             qtue = 0.5f * (qtu[km1] + qtu[k]);
                             wue = 0.5f * sqrtf(MX(wtwb + wtw, 0.0f));
                         } else {
-                            break;   // go to 111
+                            xdone = true;   // go to 111
                         }
+                        } while (0);
                     }
                     if (stop) break;
                     // (label 111, :2726-2793)
@@ -1119,6 +1150,7 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                     if (bogtop > 0.0f && wtw > 0.0f) kbup = k;
                     if (wtw <= 0.0f) {
                         kpen = k;
+                        ldone = true;
                         break;   // go to 45
                     }
                     wu[k] = sqrtf(wtw);
@@ -1147,9 +1179,13 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                     ue = GL(u0, k + 1);
                     ve = GL(v0, k + 1);
                     for (int m = 0; m < ncnst; m++) tre[m] = GT(m + 1, k + 1);
+                    } while (0);
+                    if (stop) ldone = true;
+                    UW_SYNC();
                 }
-                if (stop) break;
+                UW_SYNC();
                 // (label 45) penetration depth (:2884-2907)
+                if (!stop) do {
                 if (drage == 0.0f) {
                     R aquad = (bogtop - bogbot) / (ps0[kpen] - ps0[kpen - 1]);
                     R bquad = 2.0f * bogbot;
@@ -1184,7 +1220,7 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                               (qt0[kpen] + ssqt0[kpen] * (-ppen) / 2.0f - qtu[kpen - 1] + ssqt0[kpen] / fer[kpen]) * ef;
                 }
                 exntop = powf((ps0[kpen - 1] + ppen) / p00, rovcp);
-                if (conden(ps0[kpen - 1] + ppen, exntop, thlu_top, qtu_top, thj, qvj, qlj, qij, tbld, tblf)) {
+                if (CONDEN(ps0[kpen - 1] + ppen, exntop, thlu_top, qtu_top, thj, qvj, qlj, qij, tbld, tblf)) {
                     xflags |= UW_X_CONDEN;
                     id_exit = true;
                     stop = true;
@@ -1204,10 +1240,12 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                     cush = zs0[kpen - 1] - ppen / rhos0j / g;
                 }
                 scaleh = cush;
+                } while (0);
+                UW_SYNC();
             }
         }
-        if (stop) break;
         // forcedCu filter (:2964-2992)
+        if (!stop) do {
         if (kbup == krel) {
             lflags |= UW_L_SHCU;
             xflags |= UW_X_CUFILTER;
@@ -1216,12 +1254,14 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
             break;
         }
         lflags &= ~UW_L_SHCU;
-        for (int k = kpen; k <= mkx; k++) {
+        for (int k = 0; k <= mkx; k++) {
+            if (k < kpen) continue;
             umf[k] = 0.0f;
             emf[k] = 0.0f;
             ufrc[k] = 0.0f;
         }
-        for (int k = kpen + 1; k <= mkx; k++) {
+        for (int k = 0; k <= mkx; k++) {
+            if (k < kpen + 1) continue;
             dwten[k] = 0.0f;
             diten[k] = 0.0f;
             fer[k] = 0.0f;
@@ -1235,7 +1275,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
             vu_emf[k] = vu[k];
             for (int m = 0; m < ncnst; m++) tru_emf[m][k] = tru[m][k];
         }
-        for (int k = kpen - 1; k >= kbup; k--) {
+        for (int k = mkx; k >= 0; k--) {
+            if (k > kpen - 1 || k < kbup) continue;
             R rhos0j = ps0[k] / (r * 0.5f * (thv0bot[k + 1] + thv0top[k]) * exns0[k]);
             if (k == kpen - 1) {
                 if ((umf[k] * ppen * rei[kpen] * rpen) < -0.1f * rhos0j) lflags |= UW_L_EMF;
@@ -1272,38 +1313,39 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
             R xtop = qt0[kinv + 1] + ssqt0[kinv + 1] * (ps0[kinv] - p0[kinv + 1]);
             R xbot = qt0[kinv - 1] + ssqt0[kinv - 1] * (ps0[kinv - 1] - p0[kinv - 1]);
             fluxbelowinv(cbmf, ps0, kinv, dt, xsrc, xmean, xtop, xbot, xflx);
-            for (int k = 0; k <= kinv - 1; k++) qtflx[k] = xflx[k];
+            for (int k = 0; k <= mkx; k++) if (k <= kinv - 1) qtflx[k] = xflx[k];
             xsrc = thlsrc;
             xmean = thl0[kinv];
             xtop = thl0[kinv + 1] + ssthl0[kinv + 1] * (ps0[kinv] - p0[kinv + 1]);
             xbot = thl0[kinv - 1] + ssthl0[kinv - 1] * (ps0[kinv - 1] - p0[kinv - 1]);
             fluxbelowinv(cbmf, ps0, kinv, dt, xsrc, xmean, xtop, xbot, xflx);
-            for (int k = 0; k <= kinv - 1; k++) slflx[k] = cp * exns0[k] * xflx[k];
+            for (int k = 0; k <= mkx; k++) if (k <= kinv - 1) slflx[k] = cp * exns0[k] * xflx[k];
             xsrc = usrc;
             xmean = GL(u0, kinv);
             xtop = GL(u0, kinv + 1) + ssu0[kinv + 1] * (ps0[kinv] - p0[kinv + 1]);
             xbot = GL(u0, kinv - 1) + ssu0[kinv - 1] * (ps0[kinv - 1] - p0[kinv - 1]);
             fluxbelowinv(cbmf, ps0, kinv, dt, xsrc, xmean, xtop, xbot, xflx);
-            for (int k = 0; k <= kinv - 1; k++) uflx[k] = xflx[k];
+            for (int k = 0; k <= mkx; k++) if (k <= kinv - 1) uflx[k] = xflx[k];
             xsrc = vsrc;
             xmean = GL(v0, kinv);
             xtop = GL(v0, kinv + 1) + ssv0[kinv + 1] * (ps0[kinv] - p0[kinv + 1]);
             xbot = GL(v0, kinv - 1) + ssv0[kinv - 1] * (ps0[kinv - 1] - p0[kinv - 1]);
             fluxbelowinv(cbmf, ps0, kinv, dt, xsrc, xmean, xtop, xbot, xflx);
-            for (int k = 0; k <= kinv - 1; k++) vflx[k] = xflx[k];
+            for (int k = 0; k <= mkx; k++) if (k <= kinv - 1) vflx[k] = xflx[k];
             for (int m = 0; m < ncnst; m++) {
                 xsrc = trsrc[m];
                 xmean = GT(m + 1, kinv);
                 xtop = GT(m + 1, kinv + 1) + sstr0[m][kinv + 1] * (ps0[kinv] - p0[kinv + 1]);
                 xbot = GT(m + 1, kinv - 1) + sstr0[m][kinv - 1] * (ps0[kinv - 1] - p0[kinv - 1]);
                 fluxbelowinv(cbmf, ps0, kinv, dt, xsrc, xmean, xtop, xbot, xflx);
-                for (int k = 0; k <= kinv - 1; k++) trflx[m][k] = xflx[k];
+                for (int k = 0; k <= mkx; k++) if (k <= kinv - 1) trflx[m][k] = xflx[k];
             }
         }
         // 2.f non-buoyancy-sorting fluxes (:3300-3313)
         {
             R uplus = 0.0f, vplus = 0.0f;
-            for (int k = kinv; k <= krel - 1; k++) {
+            for (int k = 0; k <= mkx; k++) {
+                if (k < kinv || k > krel - 1) continue;
                 const int kp1 = k + 1;
                 qtflx[k] = cbmf * (qtsrc - (qt0[kp1] + ssqt0[kp1] * (ps0[k] - p0[kp1])));
                 slflx[k] = cbmf * (thlsrc - (thl0[kp1] + ssthl0[kp1] * (ps0[k] - p0[kp1]))) * cp * exns0[k];
@@ -1316,7 +1358,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
             }
         }
         // 3.f buoyancy-sorting fluxes (:3322-3331)
-        for (int k = krel; k <= kbup - 1; k++) {
+        for (int k = 0; k <= mkx; k++) {
+            if (k < krel || k > kbup - 1) continue;
             const int kp1 = k + 1;
             slflx[k] = cp * exns0[k] * umf[k] * (thlu[k] - (thl0[kp1] + ssthl0[kp1] * (ps0[k] - p0[kp1])));
             qtflx[k] = umf[k] * (qtu[k] - (qt0[kp1] + ssqt0[kp1] * (ps0[k] - p0[kp1])));
@@ -1326,7 +1369,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                 trflx[m][k] = umf[k] * (tru[m][k] - (GT(m + 1, kp1) + sstr0[m][kp1] * (ps0[k] - p0[kp1])));
         }
         // 4.f penetrative-entrainment fluxes (:3392-3401)
-        for (int k = kbup; k <= kpen - 1; k++) {
+        for (int k = 0; k <= mkx; k++) {
+            if (k < kbup || k > kpen - 1) continue;
             slflx[k] = cp * exns0[k] * emf[k] * (thlu_emf[k] - (thl0[k] + ssthl0[k] * (ps0[k] - p0[k])));
             qtflx[k] = emf[k] * (qtu_emf[k] - (qt0[k] + ssqt0[k] * (ps0[k] - p0[k])));
             uflx[k] = emf[k] * (uu_emf[k] - (GL(u0, k) + ssu0[k] * (ps0[k] - p0[k])));
@@ -1334,13 +1378,18 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
             for (int m = 0; m < ncnst; m++)
                 trflx[m][k] = emf[k] * (tru_emf[m][k] - (GT(m + 1, k) + sstr0[m][k] * (ps0[k] - p0[k])));
         }
+        } while (0);
+        UW_SYNC();
         // condensate tendency by compensating subsidence (:3416-3476)
         {
             // uemf(k), evaluated on demand with the same expressions as :3416-3422
 #define UEMF(kk)                                                                                          \
     ((kk) <= kinv - 2 ? cbmf * (ps0[0] - ps0[(kk)]) / (ps0[0] - ps0[kinv - 1])                             \
                       : ((kk) <= krel - 1 ? cbmf : ((kk) <= kbup - 1 ? umf[(kk)] : ((kk) <= kpen - 1 ? emf[(kk)] : 0.0f))))
-            for (int k = 1; k <= kpen; k++) {
+            bool ldone = stop;
+            for (int k = 1; k <= mkx; k++) {   // uniform
+                if (k > kpen) ldone = true;
+                if (!ldone) do {
                 R comsub = 0.5f * (UEMF(k) + UEMF(k - 1));
                 R thlten_sub, qtten_sub, qlten_sub, qiten_sub, nlten_sub, niten_sub;
                 if (comsub >= 0.0f) {
@@ -1370,7 +1419,7 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                 }
                 R thl_prog = thl0[k] + thlten_sub * dt;
                 R qt_prog = MX(qt0[k] + qtten_sub * dt, 1.e-12f);
-                if (conden(p0[k], exn0[k], thl_prog, qt_prog, thj, qvj, qlj, qij, tbld, tblf)) {
+                if (CONDEN(p0[k], exn0[k], thl_prog, qt_prog, thj, qvj, qlj, qij, tbld, tblf)) {
                     id_exit = true;
                     stop = true;
             break;
@@ -1379,12 +1428,16 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                 qiten_sink[k] = MX(qiten_sub, -qi0[k] / dt);
                 nlten_sink[k] = MX(nlten_sub, -GT(ixnumliq, k) / dt);
                 niten_sink[k] = MX(niten_sub, -GT(ixnumice, k) / dt);
+                } while (0);
+                if (stop) ldone = true;
             }
 #undef UEMF
         }
-        if (stop) break;
+        UW_SYNC();
+        if (!stop) do {
         // momentum tendency (:3488-3501)
-        for (int k = 1; k <= kpen; k++) {
+        for (int k = 1; k <= mkx; k++) {
+            if (k > kpen) continue;
             uten[k] = (uflx[k - 1] - uflx[k]) * g / dp0[k];
             vten[k] = (vflx[k - 1] - vflx[k]) * g / dp0[k];
             uf[k] = GL(u0, k) + uten[k] * dt;
@@ -1394,9 +1447,14 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
         rliq.reset();
         rainflx.reset();
         snowflx.reset();
+        } while (0);
+        UW_SYNC();
         {
             R qlubelow = 0.0f, qiubelow = 0.0f;
-            for (int k = 1; k <= kpen; k++) {
+            bool ldone = stop;
+            for (int k = 1; k <= mkx; k++) {   // uniform
+                if (k > kpen) ldone = true;
+                if (!ldone) do {
                 const int km1 = k - 1;
                 dwten[k] = dwten[k] * 0.5f * (umf[k - 1] + umf[k]) * g / dp0[k];
                 diten[k] = diten[k] * 0.5f * (umf[k - 1] + umf[k]) * g / dp0[k];
@@ -1432,41 +1490,36 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                     qiu_mid = 0.0f;
                     qlj = 0.0f;
                     qij = 0.0f;
-                } else if (k == krel) {
-                    if (conden(prel, exprel, thlu[krel - 1], qtu[krel - 1], thj, qvj, qlj, qij, tbld, tblf)) {
-                        xflags |= UW_X_CONDEN;
-                        id_exit = true;
-                        stop = true;
-            break;
-                    }
-                    qlubelow = qlj;
-                    qiubelow = qij;
-                    if (conden(ps0[k], exns0[k], thlu[k], qtu[k], thj, qvj, qlj, qij, tbld, tblf)) {
-                        xflags |= UW_X_CONDEN;
-                        id_exit = true;
-                        stop = true;
-            break;
-                    }
-                    qlu_mid = 0.5f * (qlubelow + qlj) * (prel - ps0[k]) / (ps0[k - 1] - ps0[k]);
-                    qiu_mid = 0.5f * (qiubelow + qij) * (prel - ps0[k]) / (ps0[k - 1] - ps0[k]);
-                } else if (k == kpen) {
-                    if (conden(ps0[k - 1] + ppen, exntop, thlu_top, qtu_top, thj, qvj, qlj, qij, tbld, tblf)) {
-                        xflags |= UW_X_CONDEN;
-                        id_exit = true;
-                        stop = true;
-            break;
-                    }
-                    qlu_mid = 0.5f * (qlubelow + qlj) * (-ppen) / (ps0[k - 1] - ps0[k]);
-                    qiu_mid = 0.5f * (qiubelow + qij) * (-ppen) / (ps0[k - 1] - ps0[k]);
                 } else {
-                    if (conden(ps0[k], exns0[k], thlu[k], qtu[k], thj, qvj, qlj, qij, tbld, tblf)) {
+                    // one conden call site for the release level, the cloud top and the levels between
+                    const bool atrel = (k == krel), attop = (k != krel && k == kpen);
+                    if (atrel) {
+                        if (CONDEN(prel, exprel, thlu[krel - 1], qtu[krel - 1], thj, qvj, qlj, qij, tbld, tblf)) {
+                            xflags |= UW_X_CONDEN;
+                            id_exit = true;
+                            stop = true;
+                            break;
+                        }
+                        qlubelow = qlj;
+                        qiubelow = qij;
+                    }
+                    if (CONDEN(attop ? ps0[k - 1] + ppen : ps0[k], attop ? exntop : exns0[k], attop ? thlu_top : thlu[k],
+                               attop ? qtu_top : qtu[k], thj, qvj, qlj, qij, tbld, tblf)) {
                         xflags |= UW_X_CONDEN;
                         id_exit = true;
                         stop = true;
-            break;
+                        break;
                     }
-                    qlu_mid = 0.5f * (qlubelow + qlj);
-                    qiu_mid = 0.5f * (qiubelow + qij);
+                    if (atrel) {
+                        qlu_mid = 0.5f * (qlubelow + qlj) * (prel - ps0[k]) / (ps0[k - 1] - ps0[k]);
+                        qiu_mid = 0.5f * (qiubelow + qij) * (prel - ps0[k]) / (ps0[k - 1] - ps0[k]);
+                    } else if (attop) {
+                        qlu_mid = 0.5f * (qlubelow + qlj) * (-ppen) / (ps0[k - 1] - ps0[k]);
+                        qiu_mid = 0.5f * (qiubelow + qij) * (-ppen) / (ps0[k - 1] - ps0[k]);
+                    } else {
+                        qlu_mid = 0.5f * (qlubelow + qlj);
+                        qiu_mid = 0.5f * (qiubelow + qij);
+                    }
                 }
                 qlubelow = qlj;
                 qiubelow = qij;
@@ -1496,7 +1549,7 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                     nc_lm = nc_lm - g * umf[k] * trl / (ps0[k - 1] - ps0[k]);
                     nc_im = nc_im - g * umf[k] * tri / (ps0[k - 1] - ps0[k]);
                     R ql_emf_kbup, qi_emf_kbup, thjj, qvjj;
-                    if (conden(p0[k], exn0[k], thlu_emf[k], qtu_emf[k], thjj, qvjj, ql_emf_kbup, qi_emf_kbup, tbld, tblf)) {
+                    if (CONDEN(p0[k], exn0[k], thlu_emf[k], qtu_emf[k], thjj, qvjj, ql_emf_kbup, qi_emf_kbup, tbld, tblf)) {
                         id_exit = true;
                         stop = true;
             break;
@@ -1516,10 +1569,13 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                 sten[k] = slten[k] + xlv * qlten[k] + xls * qiten[k];
                 qc[k] = qc_l[k] + qc_i[k];
                 rliq.add(qc[k] * dp0[k] / g / 1000.0f);
+                } while (0);
+                if (stop) ldone = true;
             }
         }
-        if (stop) break;
+        UW_SYNC();
         // evaporation and melting of precipitation (:3808-3934)
+        if (!stop) do {
         {
             Kahan evpint_rain, evpint_snow;
             for (int k = 0; k <= mkx; k++) {
@@ -1570,7 +1626,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
             snow = flxsnow[0] / 1000.0f;
         }
         // remove detrained condensate (:3966-3981)
-        for (int k = 1; k <= kpen; k++) {
+        for (int k = 1; k <= mkx; k++) {
+            if (k > kpen) continue;
             qtten[k] = qtten[k] - qc[k];
             qlten[k] = qlten[k] - qc_l[k];
             qiten[k] = qiten[k] - qc_i[k];
@@ -1654,23 +1711,29 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
             }
         }
         // in-cloud diagnostics (:4092-4158)
-        if (conden(prel, exprel, thlu[krel - 1], qtu[krel - 1], thj, qvj, qlj, qij, tbld, tblf)) {
+        if (CONDEN(prel, exprel, thlu[krel - 1], qtu[krel - 1], thj, qvj, qlj, qij, tbld, tblf)) {
             xflags |= UW_X_CONDEN;
             id_exit = true;
             stop = true;
             break;
         }
+        } while (0);
+        UW_SYNC();
         {
             R qcubelow = qlj + qij, qlubelow = qlj, qiubelow = qij;
-            for (int k = krel; k <= kpen; k++) {
-                int idc;
-                if (k == kpen) idc = conden(ps0[k - 1] + ppen, exntop, thlu_top, qtu_top, thj, qvj, qlj, qij, tbld, tblf);
-                else idc = conden(ps0[k], exns0[k], thlu[k], qtu[k], thj, qvj, qlj, qij, tbld, tblf);
+            bool ldone = stop;
+            for (int j = 0; j <= mkx; j++) {   // uniform
+                const int k = krel + j;
+                if (k > kpen) ldone = true;
+                if (!ldone) do {
+                const bool attop = (k == kpen);
+                const int idc = CONDEN(attop ? ps0[k - 1] + ppen : ps0[k], attop ? exntop : exns0[k],
+                                       attop ? thlu_top : thlu[k], attop ? qtu_top : qtu[k], thj, qvj, qlj, qij, tbld, tblf);
                 if (idc) {
                     xflags |= UW_X_CONDEN;
                     id_exit = true;
                     stop = true;
-            break;
+                    break;
                 }
                 qcu[k] = 0.5f * (qcubelow + qlj + qij);
                 qlu[k] = 0.5f * (qlubelow + qlj);
@@ -1689,9 +1752,12 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
                 qcubelow = qlj + qij;
                 qlubelow = qlj;
                 qiubelow = qij;
+                } while (0);
+                if (stop) ldone = true;
             }
         }
-        if (stop) break;
+        UW_SYNC();
+        if (!stop) do {
         cnt = (R)kpen;
         cnb = (R)(krel - 1);
 
@@ -1737,30 +1803,39 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
             }
             slope<KP>(mkx, thl0, p0, ssthl0);
             slope<KP>(mkx, qt0, p0, ssqt0);
-            for (int k = 1; k <= mkx; k++) {
+        }
+        } while (0);
+        UW_SYNC();
+        if (iter == 1) {   // uniform
+            bool ldone = stop;
+            for (int k = 1; k <= mkx; k++) {   // uniform
+                if (!ldone) do {
                 R thl0bot = thl0[k] + ssthl0[k] * (ps0[k - 1] - p0[k]);
                 R qt0bot = qt0[k] + ssqt0[k] * (ps0[k - 1] - p0[k]);
-                if (conden(ps0[k - 1], exns0[k - 1], thl0bot, qt0bot, thj, qvj, qlj, qij, tbld, tblf)) {
+                if (CONDEN(ps0[k - 1], exns0[k - 1], thl0bot, qt0bot, thj, qvj, qlj, qij, tbld, tblf)) {
                     xflags |= UW_X_CONDEN;
                     id_exit = true;
                     stop = true;
-            break;
+                    break;
                 }
                 thv0bot[k] = thj * (1.0f + zvir * qvj - qlj - qij);
                 thvl0bot[k] = thl0bot * (1.0f + zvir * qt0bot);
                 R thl0top = thl0[k] + ssthl0[k] * (ps0[k] - p0[k]);
                 R qt0top = qt0[k] + ssqt0[k] * (ps0[k] - p0[k]);
-                if (conden(ps0[k], exns0[k], thl0top, qt0top, thj, qvj, qlj, qij, tbld, tblf)) {
+                if (CONDEN(ps0[k], exns0[k], thl0top, qt0top, thj, qvj, qlj, qij, tbld, tblf)) {
                     xflags |= UW_X_CONDEN;
                     id_exit = true;
                     stop = true;
-            break;
+                    break;
                 }
                 thv0top[k] = thj * (1.0f + zvir * qvj - qlj - qij);
                 thvl0top[k] = thl0top * (1.0f + zvir * qt0top);
+                } while (0);
+                if (stop) ldone = true;
             }
-            if (stop) break;
         }
+        UW_SYNC();
+        }   // MODE != UW_MODE_TRIGGER
     }
 
     // ---- final outputs (uwshcu.F90:4337-4370) --------------------------------------------------
@@ -1858,6 +1933,8 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
             if (cand) wl[base + __popc(mask & ((1u << lane) - 1u))] = i;
         }
     }
+#undef UW_SYNC
+#undef CONDEN
 #undef RI
 #undef RL
 #undef CNT
@@ -1869,3 +1946,32 @@ __global__ void __launch_bounds__(128) uwshcu_mixed_kernel(UwArgs A, int* __rest
 #undef OT
 }
 
+// ---- kernels ---------------------------------------------------------------------------------------
+
+// The worklist pass is capped at 128 registers (4 blocks of 128 per SM instead of 3 at its natural
+// 168): the extra resident warps hide more FP64 and local-memory latency than the added spills
+// cost (-10 % time on the benchmark workload).
+template <int KP, int NC, int MODE>
+__global__ void __launch_bounds__(128, MODE == UW_MODE_LIST ? 4 : (MODE == UW_MODE_TRIGGER ? 5 : 3))
+uwshcu_mixed_kernel(const __grid_constant__ UwArgs A, int* __restrict__ wl, int* __restrict__ wl_count)
+{
+    __shared__ double tbld[UW_TBL];
+    __shared__ float tblf[UW_TBL];
+    for (int t = threadIdx.x; t < UW_TBL; t += blockDim.x) {
+        tbld[t] = c_estbl[t];
+        tblf[t] = (float)c_estbl[t];
+    }
+    __syncthreads();
+
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    int i;
+    bool active;
+    if (MODE == UW_MODE_LIST) {
+        active = tid < *wl_count;
+        i = active ? wl[tid] : 0;
+    } else {
+        active = tid < A.iend;
+        i = tid;
+    }
+    uw_column<KP, NC, MODE, 0>(A, tbld, tblf, i, active, wl, wl_count);
+}
