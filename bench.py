@@ -362,6 +362,10 @@ def main():
                "d2h_bytes_per_step": int(n * nbytes_out), "ms_per_step": sec * 1e3,
                "status": int(rc)}
 
+    # column energy and water budgets of the last step (CAM's check_energy_chng thresholds)
+    te_r, tw_r = case.budgets(stream=stream)
+    budget = {"te_rer_max": float(np.max(np.abs(te_r))), "tw_rer_max": float(np.max(np.abs(tw_r))),
+              "columns_over_cam_thresholds": int(np.sum((np.abs(te_r) > 1e-14) | (np.abs(tw_r) > 1e-10)))}
     err = None
     if prec != uw.PREC_FP64:
         import errstats
@@ -424,6 +428,7 @@ def main():
         line["e2e"] = e2e
     if err is not None:
         line["error_vs_fp64"] = err
+    line["budgets"] = budget
     if clk is not None:
         line["clocks"] = clk.summary()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

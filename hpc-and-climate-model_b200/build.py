@@ -33,6 +33,7 @@ UNITS = {
     "uwshcu_fast_k64n32.cu": [],
     "uwshcu_mixed_k32n5.cu": [],
     "uwshcu_mixed_k64n5.cu": [],
+    "uwshcu_budget.cu": ["-fmad=false"],
     "uwshcu_host.cu": [],
 }
 

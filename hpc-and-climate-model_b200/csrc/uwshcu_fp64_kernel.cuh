@@ -474,8 +474,8 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
     const double dt = A.dt;
     const double xlv = c.xlv, xls = c.xls, cp = c.cp, zvir = c.zvir, r = c.r, g = c.g, p00 = c.p00,
                  rovcp = c.rovcp, rpen = c.rpen;
-    const double rle = 0.1, rkm = 14.0, rkfre = 1.0, rmaxfrac = 0.10, mumin1 = 0.906, rbuoy = 1.0,
-                 rdrag = 1.0, epsvarw = 5.e-4, PGFc = 0.7, criqc = 0.7e-3, frc_rasn = 1.0, kevp = 2.e-6;
+    const double rle = c.rle, rkm = c.rkm, rkfre = 1.0, rmaxfrac = 0.10, mumin1 = 0.906, rbuoy = 1.0,
+                 rdrag = 1.0, epsvarw = 5.e-4, PGFc = 0.7, criqc = c.criqc, frc_rasn = 1.0, kevp = 2.e-6;
     const int ixnumliq = c.ixnumliq, ixnumice = c.ixnumice;
 
     // Row of level k in the caller's arrays: bottom-up (compute_uwshcu) or CAM's top-down order

@@ -38,6 +38,14 @@ UW_DECL_FAST(64, 5)
 UW_DECL_FAST(32, 32)
 UW_DECL_FAST(64, 32)
 #undef UW_DECL_FAST
+extern "C" cudaError_t uw_budget_launch(int mix, int mkx, int iend, int inv, double dt, double latvap,
+                                        double latice, double g, const double* s0, const double* qv0,
+                                        const double* ql0, const double* qi0, const double* u0,
+                                        const double* v0, const double* dp0, const double* sten,
+                                        const double* qvten, const double* qlten, const double* qiten,
+                                        const double* uten, const double* vten, const double* precip,
+                                        const double* snow, const double* rliq, double* te_rer,
+                                        double* tw_rer, cudaStream_t stream);
 #define UW_DECL_MIXED(KP, NC)                                                                              \
     extern "C" cudaError_t uw_mixed_set_constants_k##KP##n##NC(const UwConst* h, const double* tbl);       \
     extern "C" cudaError_t uw_mixed_launch_k##KP##n##NC(const UwArgs* a, int mode, int* wl, int* wl_count, \
@@ -540,6 +548,9 @@ int uwshcu_init(double xlv, double cp, double xlf, double zvir, double r, double
     k.p00 = 1.e5;
     k.rovcp = k.r / k.cp;
     k.rpen = rpen;
+    k.rle = s.init ? s.k.rle : 0.1;       // uwshcu.F90:1036
+    k.rkm = s.init ? s.k.rkm : 14.0;      // uwshcu.F90:1038
+    k.criqc = s.init ? s.k.criqc : 0.7e-3; // uwshcu.F90:1065
     // gestbl (wv_saturation.F90:129-138, 181-185); esinti passes latvap, latice, rh2o, cpair
     k.tmin = tmin;
     k.tmax = tmax;
@@ -573,6 +584,20 @@ int uwshcu_init(double xlv, double cp, double xlf, double zvir, double r, double
     return UWSHCU_OK;
 }
 
+int uwshcu_set_params(double rpen, double rle, double rkm, double criqc)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    if (!s.init) return UWSHCU_ERR_NOT_INITIALIZED;
+    if (!(rpen > 0.0) || !(rle > 0.0) || !(rkm > 0.0) || !(criqc >= 0.0)) return UWSHCU_ERR_BAD_ARGS;
+    s.k.rpen = rpen;
+    s.k.rle = rle;
+    s.k.rkm = rkm;
+    s.k.criqc = criqc;
+    s.gen++;
+    return UWSHCU_OK;
+}
+
 int uwshcu_set_rpen(double rpen)
 {
     State& s = S();
@@ -594,7 +619,7 @@ int uwshcu_init_default(void)
     int rc = uwshcu_init(2.501e6, 1.00464e3, 3.337e5, zv, rdair, 9.80616, mwwv / mwdair, 173.16, 375.16,
                          20.0, 1, mwwv / mwdair, rwv, 273.15, 5, qmin, wet, 4, 5);
     if (rc != UWSHCU_OK) return rc;
-    return uwshcu_set_rpen(10.0);
+    return uwshcu_set_params(10.0, 0.1, 14.0, 0.7e-3);
 }
 
 int uwshcu_set_precision(int mode)
@@ -837,6 +862,27 @@ int uwshcu_compute_device(int mix, int mkx, int iend, int ncnst, double dt, int 
     A.cnt = cnt; A.cnb = cnb; A.dpdry0 = dpdry0; A.wu = wu; A.diag_int = diag_int; A.diag_real = diag_real;
     A.err = d->d_err;
     return enqueue(*d, A, (cudaStream_t)stream);
+}
+
+int uwshcu_budget_device(int mix, int mkx, int iend, int inv, double dt, const double* s0,
+                         const double* qv0, const double* ql0, const double* qi0, const double* u0,
+                         const double* v0, const double* dp0, const double* sten, const double* qvten,
+                         const double* qlten, const double* qiten, const double* uten,
+                         const double* vten, const double* precip, const double* snow,
+                         const double* rliq, double* te_rer, double* tw_rer, void* stream)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    if (!s.init) return UWSHCU_ERR_NOT_INITIALIZED;
+    if (mix < 1 || mkx < 1 || iend < 0 || iend > mix || (inv != 0 && inv != 1)) return UWSHCU_ERR_BAD_ARGS;
+    const void* need[] = {s0, qv0, ql0, qi0, u0, v0, dp0, sten, qvten, qlten, qiten, uten, vten, precip,
+                          snow, rliq, te_rer, tw_rer};
+    for (const void* p : need)
+        if (!p) return UWSHCU_ERR_BAD_ARGS;
+    cudaError_t e = uw_budget_launch(mix, mkx, iend, inv, dt, s.k.xlv, s.k.xlf, s.k.g, s0, qv0, ql0, qi0, u0, v0,
+                                     dp0, sten, qvten, qlten, qiten, uten, vten, precip, snow, rliq, te_rer,
+                                     tw_rer, (cudaStream_t)stream);
+    return e == cudaSuccess ? UWSHCU_OK : cuda_fail(e);
 }
 
 int uwshcu_eval_math(int fn, const double* x, const double* y, double* out, int n, void* stream)

@@ -428,8 +428,8 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
     const R dt = A.dt;
     const R xlv = c.xlv, xls = c.xls, cp = c.cp, zvir = c.zvir, r = c.r, g = c.g, p00 = c.p00,
                  rovcp = c.rovcp, rpen = c.rpen;
-    const R rle = 0.1f, rkm = 14.0f, rkfre = 1.0f, rmaxfrac = 0.10f, mumin1 = 0.906f, rbuoy = 1.0f,
-                 rdrag = 1.0f, epsvarw = 5.e-4f, PGFc = 0.7f, criqc = 0.7e-3f, frc_rasn = 1.0f, kevp = 2.e-6f;
+    const R rle = c.rle, rkm = c.rkm, rkfre = 1.0f, rmaxfrac = 0.10f, mumin1 = 0.906f, rbuoy = 1.0f,
+                 rdrag = 1.0f, epsvarw = 5.e-4f, PGFc = 0.7f, criqc = c.criqc, frc_rasn = 1.0f, kevp = 2.e-6f;
     const int ixnumliq = c.ixnumliq, ixnumice = c.ixnumice;
 
     // Row of level k in the caller's arrays: bottom-up (compute_uwshcu) or CAM's top-down order

@@ -40,7 +40,8 @@ EXPORTS = ("uwshcu_init", "uwshcu_set_rpen", "uwshcu_init_default", "uwshcu_set_
            "uwshcu_compute_device", "uwshcu_device_status", "uwshcu_eval_math",
            "uwshcu_compute_device_noalloc", "uwshcu_batch_create", "uwshcu_batch_run",
            "uwshcu_batch_capture", "uwshcu_batch_autotune", "uwshcu_batch_status",
-           "uwshcu_batch_destroy", "uwshcu_set_pipeline")
+           "uwshcu_batch_destroy", "uwshcu_set_pipeline", "uwshcu_set_params",
+           "uwshcu_budget_device")
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
@@ -83,6 +84,11 @@ def set_rpen(rpen):
 PREC_FP64 = 0
 PREC_MIXED = 1
 PREC_FAST = 2
+
+
+def set_params(rpen, rle, rkm, criqc):
+    d = ctypes.c_double
+    return lib().uwshcu_set_params(d(rpen), d(rle), d(rkm), d(criqc))
 
 
 def set_precision(mode):
@@ -256,6 +262,26 @@ class DeviceCase:
         torch = self.torch
         st = stream if stream is not None else torch.cuda.current_stream()
         return lib().uwshcu_device_status(ctypes.c_void_p(st.cuda_stream))
+
+    def budgets(self, inv=0, stream=None):
+        """CAM's energy and water budget relative errors of the last call (uwshcu_budget_device),
+        as two numpy arrays."""
+        torch = self.torch
+        st = stream if stream is not None else torch.cuda.current_stream()
+        P = lambda t: ctypes.c_void_p(t.data_ptr())
+        i, o = self.inp, self.out
+        te = torch.empty(self.n, dtype=torch.float64, device=o["sten"].device)
+        tw = torch.empty_like(te)
+        rc = lib().uwshcu_budget_device(
+            ctypes.c_int(self.n), ctypes.c_int(self.mkx), ctypes.c_int(self.n), ctypes.c_int(inv),
+            ctypes.c_double(self.dt), P(i["s0"]), P(i["qv0"]), P(i["ql0"]), P(i["qi0"]), P(i["u0"]),
+            P(i["v0"]), P(i["dp0"]), P(o["sten"]), P(o["qvten"]), P(o["qlten"]), P(o["qiten"]),
+            P(o["uten"]), P(o["vten"]), P(o["precip"]), P(o["snow"]), P(o["rliq"]), P(te), P(tw),
+            ctypes.c_void_p(st.cuda_stream))
+        if rc != 0:
+            raise RuntimeError("uwshcu_budget_device: %d %s" % (rc, last_cuda_error()))
+        st.synchronize()
+        return te.cpu().numpy(), tw.cpu().numpy()
 
     def outputs_numpy(self):
         o = {k: v.cpu().numpy() for k, v in self.out.items()}

@@ -60,8 +60,15 @@ int uwshcu_init(double xlv, double cp, double xlf, double zvir, double r, double
 /* Replaces uwshcu_readnl (uwshcu.F90:58-98): the penetrative-entrainment efficiency rpen. */
 int uwshcu_set_rpen(double rpen);
 
-/* uwshcu_init + uwshcu_set_rpen with the CESM shr_const values CAM passes (convect_shallow.F90:280,
- * physpkg.F90:638), rpen = 10, five tracers (Q, CLDLIQ, CLDICE, NUMLIQ, NUMICE) with
+/* Tuning parameters: rpen (as uwshcu_set_rpen) and the compute_uwshcu parameters rle (critical
+ * stopping distance for lateral entrainment), rkm (air involved in buoyancy sorting) and criqc
+ * (maximum updraft condensate), Fortran parameters at uwshcu.F90:1036, 1038, 1065 with the values
+ * 0.1, 14 and 0.7e-3 that uwshcu_init_default sets.  Must follow uwshcu_init; non-positive values
+ * (negative criqc) are rejected. */
+int uwshcu_set_params(double rpen, double rle, double rkm, double criqc);
+
+/* uwshcu_init + uwshcu_set_params with the CESM shr_const values CAM passes (convect_shallow.F90:280,
+ * physpkg.F90:638), rpen = 10, rle = 0.1, rkm = 14, criqc = 0.7e-3, five tracers (Q, CLDLIQ, CLDICE, NUMLIQ, NUMICE) with
  * qmin = {1e-12, 0, 0, 0, 0}. */
 int uwshcu_init_default(void);
 
@@ -291,6 +298,20 @@ int uwshcu_compute_device_noalloc(int mix, int mkx, int iend, int ncnst, double 
                                   double *cnt, double *cnb, const double *dpdry0, double *wu,
                                   int *diag_int, double *diag_real, unsigned int *status_bits,
                                   void *stream);
+
+/* Column energy and water budgets of a call, on device arrays: check_energy_chng
+ * (check_energy.F90:321-395) as CAM applies it after the shallow scheme (tphysbc.F90:446-447),
+ * for the state before the call (s0, qv0, ql0, qi0, u0, v0, dp0: the call's inputs) and the
+ * state advanced by dt with the call's tendencies.  Writes CAM's relative errors te_rer and
+ * tw_rer (iend values; CAM flags |te_rer| > 1e-14 and |tw_rer| > 1e-10).  Level order as the call
+ * (inv).  Enqueued on `stream`. */
+int uwshcu_budget_device(int mix, int mkx, int iend, int inv, double dt, const double *s0,
+                         const double *qv0, const double *ql0, const double *qi0, const double *u0,
+                         const double *v0, const double *dp0, const double *sten,
+                         const double *qvten, const double *qlten, const double *qiten,
+                         const double *uten, const double *vten, const double *precip,
+                         const double *snow, const double *rliq, double *te_rer, double *tw_rer,
+                         void *stream);
 
 /* Evaluate the library's exp (fn 0), log (1), pow (2, with y) or erfc (3) on n device values, on
  * the GPU, with the routines the kernels use.  They give the same bits as the host build of the

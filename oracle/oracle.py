@@ -76,6 +76,11 @@ def init(xlv, cp, xlf, zvir, r, g, ep2, rpen, tmn, tmx, trice, icephs, epsqs, rg
         raise RuntimeError("uwo_init failed: %d" % rc)
 
 
+def set_params(rpen, rle, rkm, criqc):
+    f = ctypes.c_double
+    return lib().uwo_set_params(f(rpen), f(rle), f(rkm), f(criqc))
+
+
 def init_default():
     rc = lib().uwo_init_default()
     if rc != 0:

@@ -39,6 +39,8 @@
 typedef struct {
     /* uwshcu module constants (uwshcu.F90:25-37) */
     double xlv, xlf, xls, cp, zvir, r, g, ep2, p00, rovcp, rpen;
+    /* compute_uwshcu parameters rle, rkm, criqc (uwshcu.F90:1036, 1038, 1065), settable for tuning */
+    double rle, rkm, criqc;
     /* wv_saturation module data (wv_saturation.F90:43-59) */
     double estbl[250];
     double tmin, tmax, ttrice, pcf[6], epsqs, rgasv, hlatf, hlatv, cpws, tmelt;
@@ -608,8 +610,8 @@ static int uw_column(const uwo_io *A, int i)
     const double xlv = S.xlv, xls = S.xls, cp = S.cp, zvir = S.zvir, r = S.r, g = S.g, p00 = S.p00,
                  rovcp = S.rovcp, rpen = S.rpen;
     const int niter_xc = 2, iter_cin = 2;
-    const double rle = 0.1, rkm = 14.0, rkfre = 1.0, rmaxfrac = 0.10, mumin1 = 0.906, rbuoy = 1.0,
-                 rdrag = 1.0, epsvarw = 5.e-4, PGFc = 0.7, criqc = 0.7e-3, frc_rasn = 1.0, kevp = 2.e-6;
+    const double rle = S.rle, rkm = S.rkm, rkfre = 1.0, rmaxfrac = 0.10, mumin1 = 0.906, rbuoy = 1.0,
+                 rdrag = 1.0, epsvarw = 5.e-4, PGFc = 0.7, criqc = S.criqc, frc_rasn = 1.0, kevp = 2.e-6;
     const int ixnumliq = S.ixnumliq, ixnumice = S.ixnumice;
     int status_ret = 0;
 
@@ -2216,6 +2218,10 @@ int uwo_init(double xlv, double cp, double xlf, double zvir, double r, double g,
     S.p00 = 1.e5;
     S.rovcp = S.r / S.cp;
     S.rpen = rpen;
+    /* the Fortran parameter values (uwshcu.F90:1036, 1038, 1065) */
+    S.rle = 0.1;
+    S.rkm = 14.0;
+    S.criqc = 0.7e-3;
     /* esinti -> gestbl (esinti.F90:44-51) */
     gestbl(tmn, tmx, trice, icephs, epsqs, xlv, xlf, rgasv, cp, tmelt);
     S.ncnst = ncnst;
@@ -2225,6 +2231,16 @@ int uwo_init(double xlv, double cp, double xlf, double zvir, double r, double g,
     }
     S.ixnumliq = ixnumliq;
     S.ixnumice = ixnumice;
+    return 0;
+}
+
+int uwo_set_params(double rpen, double rle, double rkm, double criqc)
+{
+    if (!(rpen > 0.0) || !(rle > 0.0) || !(rkm > 0.0) || !(criqc >= 0.0)) return -1;
+    S.rpen = rpen;
+    S.rle = rle;
+    S.rkm = rkm;
+    S.criqc = criqc;
     return 0;
 }
 

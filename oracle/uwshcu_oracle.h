@@ -47,6 +47,11 @@ int uwo_init(double xlv, double cp, double xlf, double zvir, double r, double g,
  * qmin = {1e-12, 0, 0, 0, 0}, all wet, ixnumliq = 4, ixnumice = 5). */
 int uwo_init_default(void);
 
+/* Tuning parameters: rpen (namelist, uwshcu.F90:58-98) and the compute_uwshcu parameters rle, rkm,
+ * criqc (uwshcu.F90:1036, 1038, 1065; uwo_init sets the Fortran values 0.1, 14, 0.7e-3).
+ * Returns -1 for non-positive values (criqc may be 0). */
+int uwo_set_params(double rpen, double rle, double rkm, double criqc);
+
 /* Copy of the 250-entry saturation-vapour-pressure table built by uwo_init. */
 void uwo_get_estbl(double *out250);
 /* Constants in the order: xlv xlf xls cp zvir r g ep2 p00 rovcp rpen tmin tmax ttrice epsqs rgasv

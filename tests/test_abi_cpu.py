@@ -70,3 +70,22 @@ def test_compute_without_device_reports_no_device(uw):
     s = soundings.make_soundings(4, 30, seed=2)
     rc, _ = uw.compute_host(s)
     assert rc == uw.ERR_NO_DEVICE
+
+
+def test_tuning_parameters(uw, oracle):
+    """set_params validation (C ABI and oracle), and the oracle's result depends on the values."""
+    import soundings as snd
+    assert uw.init_default() == 0
+    assert uw.set_params(-1.0, 0.1, 14.0, 0.7e-3) == uw.ERR_BAD_ARGS
+    assert uw.set_params(10.0, 0.0, 14.0, 0.7e-3) == uw.ERR_BAD_ARGS
+    assert uw.set_params(10.0, 0.1, 14.0, -1e-3) == uw.ERR_BAD_ARGS
+    assert uw.set_params(10.0, 0.1, 14.0, 0.7e-3) == 0
+    s = snd.make_soundings(256, 30, seed=5)
+    try:
+        a = oracle.compute(s, diag=False)
+        assert oracle.set_params(10.0, 0.1, 18.0, 0.7e-3) == 0
+        b = oracle.compute(s, diag=False)
+        assert not np.array_equal(a["sten"], b["sten"])
+        assert oracle.set_params(-1.0, 0.1, 14.0, 0.7e-3) == -1
+    finally:
+        oracle.init_default()

@@ -154,3 +154,19 @@ def test_pipelined_host_entries_match_one_chunk(uw, cuda):
                 assert not bad, (entry, chunk, streams, bad)
     finally:
         assert uw.set_pipeline(32768, 4) == 0
+
+
+@pytest.mark.gpu
+def test_tuning_parameters_match_oracle(uw, oracle_pm, cuda):
+    """uwshcu_set_params (rpen, rle, rkm, criqc) against the oracle with the same values."""
+    s = soundings.make_soundings(2048, 30, seed=81)
+    try:
+        assert uw.set_params(12.0, 0.12, 15.0, 0.6e-3) == 0
+        assert oracle_pm.set_params(12.0, 0.12, 15.0, 0.6e-3) == 0
+        ref = oracle_pm.compute(s, diag=False)
+        rc, out = uw.compute_host(s)
+        assert rc == ref["status"]
+        _check(out, ref, 2048)
+    finally:
+        assert uw.init_default() == 0
+        oracle_pm.init_default()
