@@ -48,6 +48,20 @@ METRIC = "columns/s (compute_uwshcu, FP64, 259,200 x 30 levels)"
 NCU_DRAM_BYTES_PER_LIST_COLUMN = 10.494e9 / 29_956
 NCU_FP64_OPS_PER_LIST_COLUMN = 776.1 * 17.77e-3 * 1.858e9 / 29_956
 FP64_DFMA_PER_CYCLE = 9472    # ncu sm__sass_thread_inst_executed_op_dfma_pred_on.sum.peak_sustained
+# Algorithmic FP64 operations per convecting / other column of each workload, counted by the
+# oracle's operation-counting build (written by oracle/opcount.py; a data file, read as text).
+FLOPS_JSON = os.path.join(REPO, "profiles", "flops_per_column.json")
+
+
+def algorithmic_ops(workload, ncol, convecting_fraction):
+    """FP64 operations of one step over ncol columns of `workload`, or None."""
+    try:
+        with open(FLOPS_JSON) as f:
+            w = json.load(f)["workloads"][workload]
+    except (OSError, KeyError, ValueError):
+        return None
+    return ncol * (convecting_fraction * w["ops_per_convecting_column"] +
+                   (1.0 - convecting_fraction) * w["ops_per_other_column"])
 
 
 def bytes_per_column(mkx=PVER, ncnst=NCNST):
@@ -234,6 +248,15 @@ def run_batched(args):
     ms = ev0.elapsed_time(ev1) / args.steps
     ncol = sum(m[0] for m in BATCH_MEMBERS)
     nclass = len({(m[1] + 1) <= 32 for m in BATCH_MEMBERS})
+    names = ("batched_member_30L_5pct", "batched_member_35L_25pct", "batched_member_51L_45pct",
+             "batched_member_30L_60pct")
+    ops = [algorithmic_ops(nm, m[0], t) for nm, m, t in zip(names, BATCH_MEMBERS, trig)]
+    fp64_alg = None
+    if all(o is not None for o in ops) and clk is not None and clk.summary().get("sm_mhz"):
+        pk = 2 * FP64_DFMA_PER_CYCLE * clk.summary()["sm_mhz"] * 1e6 / 1e12
+        ach = sum(ops) / (ms * 1e-3) / 1e12
+        fp64_alg = {"ops_per_step": sum(ops), "achieved": ach, "peak": pk, "unit": "TFLOP/s",
+                    "frac": ach / pk, "t_roof_ms": sum(ops) / (pk * 1e12) * 1e3}
     line = {
         "metric": "columns/s (batched uneven compute_uwshcu, FP64, 4 members x 262,144 columns)",
         "value": ncol / (ms * 1e-3), "unit": "columns/s", "n_gpus": 1, "steps": args.steps,
@@ -246,6 +269,7 @@ def run_batched(args):
                              "launch; autotuned block %d, register cap %d blocks/SM, %d column(s) "
                              "per lane per task" % tuned},
         "gpu_launches": args.steps * 2 * nclass, "status": st,
+        "roofline": {"fp64_algorithmic": fp64_alg},
     }
     if clk is not None:
         line["clocks"] = clk.summary()
@@ -384,6 +408,16 @@ def main():
     peak, peak_kind = peaks()
     ncols_dom = phases["worklist_columns"] if phases else n
     fp64 = None
+    fp64_alg = None
+    ops = algorithmic_ops("fp64_259200x30", world * n, trig) if PVER == 30 else None
+    if ops and clk is not None and clk.summary().get("sm_mhz"):
+        pk = 2 * FP64_DFMA_PER_CYCLE * clk.summary()["sm_mhz"] * 1e6 / 1e12
+        ach = ops / (ms * 1e-3) / 1e12
+        fp64_alg = {"ops_per_step": ops, "achieved": ach, "peak": pk, "unit": "TFLOP/s",
+                    "frac": ach / pk, "t_roof_ms": ops / (pk * 1e12) * 1e3,
+                    "what": "algorithmic FP64 operations of the whole step (oracle operation count "
+                            "per convecting / other column x columns) / step time, against 2 x 9472 "
+                            "DFMA/cycle x median SM clock"}
     if phases and prec == uw.PREC_FP64 and clk is not None and clk.summary().get("sm_mhz"):
         hz = clk.summary()["sm_mhz"] * 1e6
         ach = NCU_FP64_OPS_PER_LIST_COLUMN * ncols_dom / (kernel_ms * 1e-3) / 1e12
@@ -413,7 +447,7 @@ def main():
                      "kernel": "uwshcu_%s_kernel<32,5,%s>" % ({"fp64": "fp64", "fast": "fast", "mixed": "mixed"}[args.precision],
                                                               "UW_MODE_LIST" if phases else "UW_MODE_ALL"),
                      "kernel_ms": kernel_ms, "columns_per_launch": ncols_dom,
-                     "fp64": fp64,
+                     "fp64": fp64, "fp64_algorithmic": fp64_alg,
                      "note": "branchy FP64 column physics: neither HBM nor the FP64 pipe is the bound "
                              "(issue latency is); algorithmic bytes = %d B/column; traffic = ncu DRAM "
                              "bytes per worklist column x columns (the per-thread stack of level "

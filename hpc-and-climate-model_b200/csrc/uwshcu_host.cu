@@ -110,8 +110,10 @@ struct DeviceState {
     static constexpr int kSlots = 256;
     cudaEvent_t ev[kSlots][3] = {};
     int nrec = 0;                // calls recorded since the last read (capped at kSlots)
-    // host-array calls: column chunks pipelined over kPipe streams (copy in, compute, copy out)
-    static constexpr int kPipe = 4;
+    // host-array calls: column chunks pipelined over kPipe streams (copy in, compute, copy out);
+    // stream j has the j-th highest priority, so earlier chunks finish first and their copies out
+    // overlap the later chunks' computation
+    static constexpr int kPipe = 8;
     cudaStream_t pipe[kPipe] = {};
     std::vector<cudaEvent_t> done;   // one per chunk, grown on demand
 };
@@ -375,9 +377,15 @@ int host_call(int inv, int mix, int mkx, int iend, int ncnst, double dt, const d
     if ((rc = grow(*d, nin + nout, nin + nout + 2 * nch)) != UWSHCU_OK) return rc;
     if ((rc = grow_worklist(*d, n + 2 * nch)) != UWSHCU_OK) return rc;
     cudaError_t e;
-    for (int j = 0; j < DeviceState::kPipe; j++)
-        if (!d->pipe[j] && (e = cudaStreamCreateWithFlags(&d->pipe[j], cudaStreamNonBlocking)) != cudaSuccess)
-            return cuda_fail(e);
+    if (!d->pipe[0]) {
+        int least = 0, greatest = 0;
+        if ((e = cudaDeviceGetStreamPriorityRange(&least, &greatest)) != cudaSuccess) return cuda_fail(e);
+        for (int j = 0; j < DeviceState::kPipe; j++) {
+            const int prio = greatest + (least - greatest) * j / (DeviceState::kPipe - 1);
+            if ((e = cudaStreamCreateWithPriority(&d->pipe[j], cudaStreamNonBlocking, prio)) != cudaSuccess)
+                return cuda_fail(e);
+        }
+    }
     while (d->done.size() < nch) {
         cudaEvent_t ev;
         if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return cuda_fail(e);

@@ -92,10 +92,10 @@ int uwshcu_set_profiling(int on);
 int uwshcu_profile_read(int *calls, double *trigger_ms, double *list_ms, int *list_columns);
 
 /* Host-array entries (compute_uwshcu_, compute_uwshcu_inv_, bxcompute_uwshcu_inv_): split a call
- * into chunks of chunk_columns columns (0: one chunk) pipelined over `streams` CUDA streams (1..4),
- * so that copies in and out and the host-side packing overlap the computation.  Results do not
- * depend on it.  Default: 32768 columns, 4 streams (measured best of 0/32k/64k/128k x 1-4
- * streams on the 259,200-column workload: 88 ms per call against 159 ms for one chunk). */
+ * into chunks of chunk_columns columns (0: one chunk) pipelined over `streams` CUDA streams (1..8)
+ * of decreasing priority, so that copies in and out and the host-side packing overlap the
+ * computation.  Results do not depend on it.  Default: 32768 columns, 4 streams (259,200 columns:
+ * 87 ms per call against 157 ms as one chunk; more concurrent chunks compute slower). */
 int uwshcu_set_pipeline(int chunk_columns, int streams);
 
 /* Threads per block of the column kernel (0 = built-in default). */

@@ -13,7 +13,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATHS = {"glibc": os.path.join(HERE, "_build", "libuwshcu_oracle.so"),
-             "portable": os.path.join(HERE, "_build", "libuwshcu_oracle_pm.so")}
+             "portable": os.path.join(HERE, "_build", "libuwshcu_oracle_pm.so"),
+             # operation-counting build (opcount.hpp): same results as "glibc", plus uwo_opcount
+             "ops": os.path.join(HERE, "_build", "libuwshcu_oracle_ops.so")}
 LIB_PATH = LIB_PATHS["glibc"]
 
 OUT_IFACE = ("umf", "slflx", "qtflx", "flxprc1", "flxsnow1", "wu")

@@ -45,3 +45,29 @@ def test_uw_math_accuracy(oracle):
     x = rng.uniform(-2, 6, 20000)
     ref = np.array([math.erfc(v) for v in x])
     assert np.max(np.abs(oracle.uwmath(3, x) - ref) / ref) < 2e-15
+
+
+def test_operation_counting_build_is_the_oracle():
+    """The operation-counting oracle build (oracle/opcount.hpp) computes the glibc build's bits and
+    counts a convecting column at 1e5-1e6 FP64 operations (divisions included)."""
+    import ctypes
+    import oracle as o
+    import soundings
+    s = soundings.make_soundings(256, 30, seed=7)
+    try:
+        o.set_variant("glibc")
+        o.init_default()
+        a = o.compute(s, diag=True)
+        o.set_variant("ops")
+        o.init_default()
+        L = o.lib()
+        buf = (ctypes.c_ulonglong * 5)()
+        L.uwo_opcount(buf, 1)
+        b = o.compute(s, diag=True, nthreads=1)
+        L.uwo_opcount(buf, 1)
+    finally:
+        o.set_variant("glibc")
+    assert all(np.array_equal(a[k], b[k]) for k in a if isinstance(a[k], np.ndarray))
+    nconv = int(np.sum(a["cush"] != -1.0))
+    total = sum(int(x) for x in buf)
+    assert nconv > 0 and 1e5 * nconv < total < 1e6 * 256
