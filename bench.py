@@ -277,6 +277,54 @@ def run_batched(args):
     plan.close()
 
 
+def run_tangent(args):
+    """Cost of the tangent-linear model against the forward pass: 65,536 columns x 30 levels, one
+    direction in t0, qv0, tke and pblh and all four tuning parameters."""
+    import torch
+    import soundings
+    import uwshcu_b200 as uw
+
+    torch.cuda.set_device(0)
+    assert uw.init_default() == 0
+    n = 65_536
+    s = soundings.make_soundings(n, PVER, seed=301, rh_pbl=RH_PBL)
+    case = uw.DeviceCase(s)
+    rng = np.random.default_rng(7)
+    dirs = {k: torch.from_numpy(np.ascontiguousarray(s[k] * rng.uniform(-1e-3, 1e-3, s[k].shape))).cuda()
+            for k in ("t0", "qv0", "tke", "pblh")}
+    dparams = (1e-2, 1e-4, 1.4e-2, 7e-7)
+    stream = torch.cuda.Stream()
+
+    def timed(fn):
+        with torch.cuda.stream(stream):
+            for _ in range(max(args.warmup, 3)):
+                case.reset_cush()
+                fn()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                case.reset_cush()
+                fn()
+            e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    fwd = timed(lambda: case.launch(stream=stream))
+    assert uw.set_schedule(uw.SCHED_SINGLE_PASS) == 0
+    fwd1 = timed(lambda: case.launch(stream=stream))
+    assert uw.set_schedule(uw.SCHED_TWO_PHASE) == 0
+    tl = timed(lambda: uw.tangent_launch(case, dirs, dparams, stream=stream))
+    line = {"metric": "tangent-linear cost / forward cost (compute_uwshcu, 65,536 x 30, FP64)",
+            "value": tl / fwd, "unit": "ratio", "higher_is_better": False, "n_gpus": 1,
+            "steps": args.steps, "warmup": max(args.warmup, 3), "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "65,536 columns x 30 levels, one direction in t0/qv0/tke/pblh and "
+                                   "rpen/rle/rkm/criqc"},
+            "forward_ms": fwd, "forward_single_pass_ms": fwd1, "tangent_ms": tl,
+            "tangent_vs_single_pass": tl / fwd1,
+            "memory": "tangent: 54 KB stack per thread (forward 27 KB), 26 extra output arrays"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -291,13 +339,15 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fast", "mixed"],
                     help="fp64: bit-exact (default); fast: FP64 with the early-stopping conden; "
                          "mixed: FP32 bulk with FP64 islands")
-    ap.add_argument("--config", default="fp64", choices=["fp64", "batched"],
+    ap.add_argument("--config", default="fp64", choices=["fp64", "batched", "tangent"],
                     help="fp64: the 259,200-column workload (default); batched: 4 uneven members")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
     if args.config == "batched":
         return run_batched(args)
+    if args.config == "tangent":
+        return run_tangent(args)
 
     import torch
     import soundings

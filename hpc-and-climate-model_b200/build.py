@@ -34,6 +34,9 @@ UNITS = {
     "uwshcu_mixed_k32n5.cu": [],
     "uwshcu_mixed_k64n5.cu": [],
     "uwshcu_budget.cu": ["-fmad=false"],
+    # tangent-linear kernels: no FMA contraction, so their values are the FP64 path's bits
+    "uwshcu_tl_k32n5.cu": ["-fmad=false"],
+    "uwshcu_tl_k64n5.cu": ["-fmad=false"],
     "uwshcu_host.cu": [],
 }
 

@@ -46,6 +46,12 @@ extern "C" cudaError_t uw_budget_launch(int mix, int mkx, int iend, int inv, dou
                                         const double* uten, const double* vten, const double* precip,
                                         const double* snow, const double* rliq, double* te_rer,
                                         double* tw_rer, cudaStream_t stream);
+extern "C" cudaError_t uw_tl_set_constants_k32n5(const UwConst* h, const double* tbl);
+extern "C" cudaError_t uw_tl_set_constants_k64n5(const UwConst* h, const double* tbl);
+extern "C" cudaError_t uw_tl_launch_k32n5(const UwArgs* a, const uwshcu_tangent* t, int mode, int* wl,
+                                           int* wl_count, int nthreads, int block, cudaStream_t stream);
+extern "C" cudaError_t uw_tl_launch_k64n5(const UwArgs* a, const uwshcu_tangent* t, int mode, int* wl,
+                                           int* wl_count, int nthreads, int block, cudaStream_t stream);
 #define UW_DECL_MIXED(KP, NC)                                                                              \
     extern "C" cudaError_t uw_mixed_set_constants_k##KP##n##NC(const UwConst* h, const double* tbl);       \
     extern "C" cudaError_t uw_mixed_launch_k##KP##n##NC(const UwArgs* a, int mode, int* wl, int* wl_count, \
@@ -70,6 +76,8 @@ cudaError_t set_constants_all(const UwConst* k, const double* tbl)
     if ((e = uw_fast_set_constants_k64n5(k, tbl)) != cudaSuccess) return e;
     if ((e = uw_fast_set_constants_k32n32(k, tbl)) != cudaSuccess) return e;
     if ((e = uw_fast_set_constants_k64n32(k, tbl)) != cudaSuccess) return e;
+    if ((e = uw_tl_set_constants_k32n5(k, tbl)) != cudaSuccess) return e;
+    if ((e = uw_tl_set_constants_k64n5(k, tbl)) != cudaSuccess) return e;
     if ((e = uw_mixed_set_constants_k32n5(k, tbl)) != cudaSuccess) return e;
     return uw_mixed_set_constants_k64n5(k, tbl);
 }
@@ -891,6 +899,50 @@ int uwshcu_budget_device(int mix, int mkx, int iend, int inv, double dt, const d
                                      dp0, sten, qvten, qlten, qiten, uten, vten, precip, snow, rliq, te_rer,
                                      tw_rer, (cudaStream_t)stream);
     return e == cudaSuccess ? UWSHCU_OK : cuda_fail(e);
+}
+
+int uwshcu_tangent_device(const uwshcu_member* m, const uwshcu_tangent* t, void* stream)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    if (!s.init) return UWSHCU_ERR_NOT_INITIALIZED;
+    if (!m || !t) return UWSHCU_ERR_BAD_ARGS;
+    const int ncnst = s.k.ncnst;
+    if (s.precision != UWSHCU_PREC_FP64 || ncnst > 5 || m->mkx + 1 > 64) return UWSHCU_ERR_BAD_ARGS;
+    if (bad_dims(m->mix, m->mkx, m->iend, ncnst) || (m->inv != 0 && m->inv != 1)) return UWSHCU_ERR_BAD_ARGS;
+    const void* need[] = {m->ps0, m->zs0, m->p0, m->z0, m->dp0, m->u0, m->v0, m->qv0, m->ql0, m->qi0, m->t0,
+                          m->s0, m->tr0, m->tke, m->pblh, m->cush, m->umf, m->slflx, m->qtflx, m->flxprc1,
+                          m->flxsnow1, m->qvten, m->qlten, m->qiten, m->sten, m->uten, m->vten, m->trten,
+                          m->qrten, m->qsten, m->precip, m->snow, m->evapc, m->cufrc, m->qcu, m->qlu, m->qiu,
+                          m->cbmf, m->qc, m->rliq, m->cnt, m->cnb, m->dpdry0, m->wu,
+                          t->cush, t->umf, t->slflx, t->qtflx, t->flxprc1, t->flxsnow1, t->qvten, t->qlten,
+                          t->qiten, t->sten, t->uten, t->vten, t->trten, t->qrten, t->qsten, t->precip,
+                          t->snow, t->evapc, t->cufrc, t->qcu, t->qlu, t->qiu, t->cbmf, t->qc, t->rliq, t->wu};
+    for (const void* p : need)
+        if (!p) return UWSHCU_ERR_BAD_ARGS;
+    DeviceState* d = nullptr;
+    int rc = ensure_device(&d);
+    if (rc != UWSHCU_OK) return rc;
+    UwArgs A{};
+    A.mix = m->mix; A.mkx = m->mkx; A.iend = m->iend; A.ncnst = ncnst; A.inv = m->inv; A.dt = m->dt;
+    A.ps0 = m->ps0; A.zs0 = m->zs0; A.p0 = m->p0; A.z0 = m->z0; A.dp0 = m->dp0; A.u0 = m->u0; A.v0 = m->v0;
+    A.qv0 = m->qv0; A.ql0 = m->ql0; A.qi0 = m->qi0; A.t0 = m->t0; A.s0 = m->s0; A.tr0 = m->tr0; A.tke = m->tke;
+    A.pblh = m->pblh; A.cush = m->cush; A.umf = m->umf; A.slflx = m->slflx; A.qtflx = m->qtflx;
+    A.flxprc1 = m->flxprc1; A.flxsnow1 = m->flxsnow1; A.qvten = m->qvten; A.qlten = m->qlten;
+    A.qiten = m->qiten; A.sten = m->sten; A.uten = m->uten; A.vten = m->vten; A.trten = m->trten;
+    A.qrten = m->qrten; A.qsten = m->qsten; A.precip = m->precip; A.snow = m->snow; A.evapc = m->evapc;
+    A.cufrc = m->cufrc; A.qcu = m->qcu; A.qlu = m->qlu; A.qiu = m->qiu; A.cbmf = m->cbmf; A.qc = m->qc;
+    A.rliq = m->rliq; A.cnt = m->cnt; A.cnb = m->cnb; A.dpdry0 = m->dpdry0; A.wu = m->wu;
+    A.diag_int = m->diag_int; A.diag_real = m->diag_real; A.err = d->d_err;
+    // the forward path's two-phase schedule: trigger pass, then the convecting columns
+    auto launch = (m->mkx + 1 <= 32) ? uw_tl_launch_k32n5 : uw_tl_launch_k64n5;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e;
+    if ((rc = grow_worklist(*d, (size_t)m->iend)) != UWSHCU_OK) return rc;
+    if ((e = cudaMemsetAsync(d->d_wl, 0, sizeof(int), st)) != cudaSuccess) return cuda_fail(e);
+    if ((e = launch(&A, t, kModeTrigger, d->d_wl + 1, d->d_wl, m->iend, 128, st)) != cudaSuccess) return cuda_fail(e);
+    if ((e = launch(&A, t, kModeList, d->d_wl + 1, d->d_wl, m->iend, 128, st)) != cudaSuccess) return cuda_fail(e);
+    return UWSHCU_OK;
 }
 
 int uwshcu_eval_math(int fn, const double* x, const double* y, double* out, int n, void* stream)

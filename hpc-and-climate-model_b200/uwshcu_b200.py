@@ -41,7 +41,7 @@ EXPORTS = ("uwshcu_init", "uwshcu_set_rpen", "uwshcu_init_default", "uwshcu_set_
            "uwshcu_compute_device_noalloc", "uwshcu_batch_create", "uwshcu_batch_run",
            "uwshcu_batch_capture", "uwshcu_batch_autotune", "uwshcu_batch_status",
            "uwshcu_batch_destroy", "uwshcu_set_pipeline", "uwshcu_set_params",
-           "uwshcu_budget_device")
+           "uwshcu_budget_device", "uwshcu_tangent_device")
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
@@ -377,3 +377,37 @@ class BatchPlan:
         if self.handle:
             lib().uwshcu_batch_destroy(self.handle)
             self.handle = ctypes.c_void_p()
+
+
+# ---- tangent-linear model ----------------------------------------------------------------------------
+_TANGENT_OUT = ("cush umf slflx qtflx flxprc1 flxsnow1 qvten qlten qiten sten uten vten trten qrten qsten "
+                "precip snow evapc cufrc qcu qlu qiu cbmf qc rliq wu").split()
+
+
+class Tangent(ctypes.Structure):
+    """uwshcu_tangent of include/uwshcu.h."""
+    _fields_ = ([(n, ctypes.c_void_p) for n in ("dt0", "dqv0", "dtke", "dpblh")] +
+                [(n, ctypes.c_double) for n in ("drpen", "drle", "drkm", "dcriqc")] +
+                [(n, ctypes.c_void_p) for n in _TANGENT_OUT])
+
+
+def tangent_launch(case, dirs=None, dparams=(0.0, 0.0, 0.0, 0.0), inv=0, stream=None):
+    """One uwshcu_tangent_device call on a DeviceCase: `dirs` maps t0/qv0/tke/pblh to device tensors
+    (the direction), dparams = (drpen, drle, drkm, dcriqc).  Returns the tangent outputs (torch
+    tensors shaped like case.out); the case's own outputs get the FP64 values."""
+    import torch
+    st = stream if stream is not None else torch.cuda.current_stream()
+    dirs = dirs or {}
+    tout = {k: torch.zeros_like(case.out[k]) for k in _TANGENT_OUT}
+    t = Tangent()
+    for k in ("t0", "qv0", "tke", "pblh"):
+        d = dirs.get(k)
+        setattr(t, "d" + k, d.data_ptr() if d is not None else None)
+    t.drpen, t.drle, t.drkm, t.dcriqc = [float(x) for x in dparams]
+    for k in _TANGENT_OUT:
+        setattr(t, k, tout[k].data_ptr())
+    m = member_of(case, inv)
+    rc = lib().uwshcu_tangent_device(ctypes.byref(m), ctypes.byref(t), ctypes.c_void_p(st.cuda_stream))
+    if rc != 0:
+        raise RuntimeError("uwshcu_tangent_device: %d %s" % (rc, last_cuda_error()))
+    return tout

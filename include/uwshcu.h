@@ -252,6 +252,26 @@ int uwshcu_batch_status(void *plan, void *stream);
 /* Release the plan (its graph, worklists and counters). */
 int uwshcu_batch_destroy(void *plan);
 
+/* ---- tangent-linear model ---------------------------------------------------------------------- */
+
+/* Directions and tangent outputs of a tangent-linear call.  The direction arrays have the layout of
+ * the call's inputs (t0, qv0: (mix, mkx); tke: (mix, mkx+1); pblh: (mix)); NULL means zero.  The
+ * tangent outputs have the layout of the outputs of the same name. */
+typedef struct uwshcu_tangent {
+    const double *dt0, *dqv0, *dtke, *dpblh;
+    double drpen, drle, drkm, dcriqc;     /* directions in the tuning parameters */
+    double *cush, *umf, *slflx, *qtflx, *flxprc1, *flxsnow1, *qvten, *qlten, *qiten, *sten, *uten,
+        *vten, *trten, *qrten, *qsten, *precip, *snow, *evapc, *cufrc, *qcu, *qlu, *qiu, *cbmf, *qc,
+        *rliq, *wu;
+} uwshcu_tangent;
+
+/* No counterpart in the reference.  Tangent-linear model of compute_uwshcu: the outputs of `m`
+ * (bit for bit those of uwshcu_compute_device) and their derivatives along the direction in `t`
+ * (forward mode through every statement of the scheme, the Newton iterations included; the
+ * derivative is that of the branch the FP64 path takes).  Device arrays, enqueued on `stream`;
+ * FP64 precision setting only; mkx + 1 <= 64, ncnst <= 5. */
+int uwshcu_tangent_device(const uwshcu_member *m, const uwshcu_tangent *t, void *stream);
+
 /* Column limit of uwshcu_compute_device_noalloc: its worklist is one fixed device array of
  * 64 + UWSHCU_NOALLOC_MAX_COLUMNS ints (4 MiB + 256 B) that every GPU which loads the library holds
  * until the process exits. */
