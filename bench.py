@@ -128,6 +128,27 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def shard_seed(rank):
+    """Seed of rank `rank`'s columns: every rank generates and computes its own 259,200 columns (the
+    columns are independent, so there is no exchange step and no collective on the data path)."""
+    return 1 + rank
+
+
+def max_over_ranks(dist, value, device):
+    """The largest `value` over all ranks (device times are reported as the max over ranks)."""
+    if dist is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(world, ncol_per_rank, seconds):
+    """Whole-job columns/s: the columns of all ranks over the slowest rank's time (weak scaling)."""
+    return world * ncol_per_rank / seconds
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -367,7 +388,7 @@ def main():
     two_phase = args.schedule == "two-phase"
     assert uw.set_schedule(uw.SCHED_TWO_PHASE if two_phase else uw.SCHED_SINGLE_PASS) == 0
     n = args.ncol
-    s = soundings.make_soundings(n, PVER, seed=1 + rank, rh_pbl=RH_PBL)
+    s = soundings.make_soundings(n, PVER, seed=shard_seed(rank), rh_pbl=RH_PBL)
     case = uw.DeviceCase(s)
     stream = torch.cuda.Stream()
     nbytes_in, nbytes_out = bytes_per_column()
@@ -404,11 +425,8 @@ def main():
         uw.set_profiling(False)
         phases = {"trigger_ms": trig_ms / max(calls, 1), "worklist_ms": list_ms / max(calls, 1),
                   "worklist_columns": ncand, "calls": calls}
-    if pg:
-        t = torch.tensor([ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * n / (ms * 1e-3)
+    ms = max_over_ranks(pg, ms, "cuda")
+    value = job_throughput(world, n, ms * 1e-3)
     # the dominant kernel: the worklist launch of the two-phase schedule, else the single pass
     kernel_ms = phases["worklist_ms"] if phases else ms
 
@@ -427,11 +445,8 @@ def main():
             out["cush"][:] = s["cush"]
             rc, _ = uw.compute_host(s, out=out)
         sec = (time.perf_counter() - t0) / ksteps
-        if pg:
-            t = torch.tensor([sec], device="cuda")
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            sec = float(t.item())
-        e2e = {"value": world * n / sec, "unit": "columns/s",
+        sec = max_over_ranks(pg, sec, "cuda")
+        e2e = {"value": job_throughput(world, n, sec), "unit": "columns/s",
                "h2d_bytes_per_step": int(n * (nbytes_in + 8 * PVER)),
                "d2h_bytes_per_step": int(n * nbytes_out), "ms_per_step": sec * 1e3,
                "status": int(rc)}
