@@ -48,6 +48,11 @@ TL_HD double tl_val(double x) { return x; }
 TL_HD double tl_der(Tl x) { return x.d; }
 TL_HD double tl_der(double) { return 0.0; }
 
+TL_HD Tl uw_div_by(Tl a, Tl b, Tl y)
+{
+    const double q = uw_div_by(a.v, b.v, y.v);
+    return Tl(q, (a.d - q * b.d) / b.v);
+}
 TL_HD Tl uw_exp(Tl x)
 {
     const double e = uw_exp(x.v);

@@ -39,6 +39,18 @@
 #define UW_SUB(a, b) ((a) - (b))
 #endif
 
+// a / b from the correctly rounded reciprocal y = RN(1/b): q = RN(a y), e = a - b q (exact with an
+// FMA), RN(q + e y) = RN(a / b) for operands and quotient in the normal range (P. Markstein, IBM J.
+// Res. Dev. 34 (1990) 111-119; J.-M. Muller et al., Handbook of Floating-Point Arithmetic, the
+// division theorems of ch. 5): the IEEE quotient from one multiply and two FMAs once 1/b is known.
+// Used where one divisor serves several divisions.
+UW_HD double uw_div_by(double a, double b, double y)
+{
+    const double q = UW_MUL(a, y);
+    const double e = fma(-b, q, a);
+    return fma(e, y, q);
+}
+
 UW_HD double uw_exp(double x)
 {
     if (x != x) return x;

@@ -67,6 +67,7 @@ struct UwConst {
     // uwshcu module (uwshcu.F90:25-37)
     double xlv, xlf, xls, cp, zvir, r, g, ep2, p00, rovcp, rpen;
     double rle, rkm, criqc;   // compute_uwshcu parameters (uwshcu.F90:1036, 1038, 1065)
+    double rinv;              // 1 / r, correctly rounded (divisions by r in conden)
     // wv_saturation module (wv_saturation.F90:48-59)
     double tmin, tmax, ttrice, epsqs, rgasv, hlatf, hlatv, cpws, tmelt;
     double pcf[6];

@@ -563,6 +563,7 @@ int uwshcu_init(double xlv, double cp, double xlf, double zvir, double r, double
     k.ep2 = ep2;
     k.p00 = 1.e5;
     k.rovcp = k.r / k.cp;
+    k.rinv = 1.0 / k.r;
     k.rpen = rpen;
     k.rle = s.init ? s.k.rle : 0.1;       // uwshcu.F90:1036
     k.rkm = s.init ? s.k.rkm : 14.0;      // uwshcu.F90:1038

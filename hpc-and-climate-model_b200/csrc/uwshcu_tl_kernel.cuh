@@ -91,10 +91,15 @@ __device__ __noinline__ int conden(Tl p, Tl ex, Tl thl, Tl qt, Tl& th, Tl& qv,
         th = tc / ex;
     } else {
         Tl qs = rvls;
+        // the Fortran's divisions by leff, r and (twice per step) temps go through their
+        // correctly rounded reciprocals: the same quotients, bit for bit (uw_div_by)
+        const Tl rleff = 1.0 / leff;
+        const Tl cpl = uw_div_by(c.cp, leff, rleff);
 #pragma unroll 1
         for (int it = 0; it < 10; it++) {
-            temps = temps + ((tc - temps) * c.cp / leff + qt - rvls) /
-                                (c.cp / leff + c.ep2 * leff * rvls / c.r / temps / temps);
+            const Tl rt = 1.0 / temps;
+            temps = temps + (uw_div_by((tc - temps) * c.cp, leff, rleff) + qt - rvls) /
+                                (cpl + uw_div_by(uw_div_by(uw_div_by(c.ep2 * leff * rvls, c.r, c.rinv), temps, rt), temps, rt));
             qs = qsat_qs(temps, p, tbl);
             rvls = qs;
         }
