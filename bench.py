@@ -278,6 +278,48 @@ def run_batched(args):
         ach = sum(ops) / (ms * 1e-3) / 1e12
         fp64_alg = {"ops_per_step": sum(ops), "achieved": ach, "peak": pk, "unit": "TFLOP/s",
                     "frac": ach / pk, "t_roof_ms": sum(ops) / (pk * 1e12) * 1e3}
+    # the same members in the reduced-precision modes, side by side with FP64: speed and error
+    G = 9.80616
+
+    def col_quantities():
+        return [((c.out["sten"] * c.inp["dp0"]).sum(0) / G, (c.out["qvten"] * c.inp["dp0"]).sum(0) / G,
+                 c.out["precip"].clone(), c.out["cnt"].clone(), (c.out["cush"] != -1.0)) for c in cases]
+
+    ref_q = col_quantities()
+    plan.close()
+    others = {}
+    for name, mode in (("fast", uw.PREC_FAST), ("mixed", uw.PREC_MIXED)):
+        assert uw.set_precision(mode) == 0
+        p2 = uw.BatchPlan(cases)
+        tuned2 = p2.autotune(stream)
+        assert p2.capture(stream) == 0, uw.last_cuda_error()
+        with torch.cuda.stream(stream):
+            for _ in range(max(args.warmup, 3)):
+                for c in cases:
+                    c.out["cush"].copy_(c.cush0, non_blocking=True)
+                assert p2.run(stream) == 0
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                for c in cases:
+                    c.out["cush"].copy_(c.cush0, non_blocking=True)
+                assert p2.run(stream) == 0
+            e1.record(stream)
+        e1.synchronize()
+        ms2 = e0.elapsed_time(e1) / args.steps
+        q = col_quantities()
+        err = {}
+        for j, nm in enumerate(("heating", "moistening", "precipitation")):
+            a = torch.cat([x[j] for x in q]).double()
+            b = torch.cat([x[j] for x in ref_q]).double()
+            err[nm] = float(torch.sqrt(torch.mean((a - b) ** 2)) / torch.sqrt(torch.mean(b ** 2)))
+        flips_top = int(sum(int((x[3] != y[3]).sum()) for x, y in zip(q, ref_q)))
+        flips_trig = int(sum(int((x[4] != y[4]).sum()) for x, y in zip(q, ref_q)))
+        others[name] = {"value": ncol / (ms2 * 1e-3), "ms_per_step": ms2, "speedup_vs_fp64": ms / ms2,
+                        "column_rel_rms_vs_fp64": err, "cloud_top_flips": flips_top,
+                        "trigger_flips": flips_trig, "autotuned": list(tuned2)}
+        p2.close()
+    assert uw.set_precision(uw.PREC_FP64) == 0
     line = {
         "metric": "columns/s (batched uneven compute_uwshcu, FP64, 4 members x 262,144 columns)",
         "value": ncol / (ms * 1e-3), "unit": "columns/s", "n_gpus": 1, "steps": args.steps,
@@ -291,11 +333,11 @@ def run_batched(args):
                              "per lane per task" % tuned},
         "gpu_launches": args.steps * 2 * nclass, "status": st,
         "roofline": {"fp64_algorithmic": fp64_alg},
+        "precisions": others,
     }
     if clk is not None:
         line["clocks"] = clk.summary()
     print(json.dumps(line), flush=True)
-    plan.close()
 
 
 def run_tangent(args):

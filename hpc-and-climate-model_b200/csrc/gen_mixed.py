@@ -22,12 +22,12 @@ if old in head:
     head = head.replace(old, '''        if (__all_sync(__activemask(), fabs(dT) < 1.e-9)) break;''')
 head = head.replace('__device__ __forceinline__ int conden(R p, R ex, R thl, R qt, R& th, R& qv, R& ql, R& qi,',
                     '__device__ __noinline__ int conden(R p, R ex, R thl, R qt, R& th, R& qv, R& ql, R& qi,')
-head = head.replace('''// temperature change is below 1e-9 K; this kernel''', '''// temperature change is below 1e-9 K on every lane of the warp; this kernel''')
+
 src = open(D + 'uwshcu_fp64_kernel.cuh').read()
 b = src[src.index(marker):]
 # keep uw_column and the plain kernel only
 cut = b.index('// The fast-FP64 precision mode: same launch shapes as uwshcu_fp64_kernel.')
-b = b[:cut].rstrip() + '\n'
+b = b[:cut].rstrip() + '\n\n}  // namespace\n'
 b = b.replace('uwshcu_fp64_kernel', 'uwshcu_mixed_kernel')
 b = b.replace('#define CONDEN(...) (FAST ? conden_fast(__VA_ARGS__) : conden(__VA_ARGS__))', '#define CONDEN(...) conden(__VA_ARGS__)')
 b = re.sub(r'\bdouble\b', 'R', b)
@@ -53,8 +53,10 @@ rep('''    __shared__ R tbl[UW_TBL];
     for (int t = threadIdx.x; t < UW_TBL; t += blockDim.x) {
         tbld[t] = c_estbl[t];
         tblf[t] = (float)c_estbl[t];
-    }''')
+    }''', 3)
 rep('uw_column<KP, NC, MODE, 0>(A, tbl, i, active, wl, wl_count);', 'uw_column<KP, NC, MODE, 0>(A, tbld, tblf, i, active, wl, wl_count);')
+rep('(B.m[m], tbl, tid, active, B.wl[m], B.count + m);', '(B.m[m], tbld, tblf, tid, active, B.wl[m], B.count + m);')
+rep('(B.m[m], tbl, i, active, nullptr, nullptr);', '(B.m[m], tbld, tblf, i, active, nullptr, nullptr);')
 b = b.replace(', tbl)', ', tbld, tblf)')
 rep("""    R cin = 0, cinlcl = 0, plcl = 0,""", """    double cin = 0, cinlcl = 0;
     R plcl = 0,""")

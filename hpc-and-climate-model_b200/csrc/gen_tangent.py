@@ -30,8 +30,8 @@ def main():
     s = open(SRC).read()
     head_end = s.index("#pragma once")
     s = s[head_end:]
-    # drop the fast-mode and batched kernels: the tangent kernel is one single-pass launch
-    s = s[: s.index("// The fast-FP64 precision mode: same launch shapes as uwshcu_fp64_kernel.")].rstrip() + "\n"
+    # drop the batched and fast-mode kernels: the tangent kernel has its own launches
+    s = s[: s.index("// Batched trigger pass: every column of every member of B")].rstrip() + "\n\n}  // namespace\n"
     s = rep(s, '#include "uw_math.h"', '#include "uw_math.h"\n#include "uw_dual.h"')
     s = re.sub(r"\bdouble\b", "Tl", s)
     # tables stay double
@@ -41,7 +41,8 @@ def main():
     # the tangent argument block
     s = rep(s, '#include "uwshcu_common.cuh"', '#include "uwshcu_common.cuh"\n#include "uwshcu.h"')
     # directions and tangent outputs of one launch: the ABI's uwshcu_tangent
-    s = rep(s, "namespace {\n", "namespace {\n\ntypedef uwshcu_tangent UwTangent;\n", 1)
+    assert s.count("namespace {\n") >= 1
+    s = s.replace("namespace {\n", "namespace {\n\ntypedef uwshcu_tangent UwTangent;\n", 1)
     s = rep(s, "const bool active, int* __restrict__ wl, int* __restrict__ wl_count)",
             "const bool active, int* __restrict__ wl, int* __restrict__ wl_count,\n"
             "                                          const UwTangent& T)")

@@ -19,3 +19,28 @@ extern "C" cudaError_t uw_fast_launch_k32n32(const UwArgs* a, int mode, int* wl,
     else uwshcu_fast_kernel<32, 32, UW_MODE_LIST><<<grid, block, 0, stream>>>(*a, wl, wl_count);
     return cudaGetLastError();
 }
+
+// Batched trigger (phase 0) and persistent worklist (phase 1) launches of this precision mode;
+// minb selects the worklist instantiation (only the ones compiled here).
+extern "C" cudaError_t uw_fast_batch_k32n32(const UwBatch* b, int phase, int grid, int block, int minb,
+                                          cudaStream_t stream)
+{
+    if (grid <= 0) return cudaSuccess;
+    if (phase == 0) {
+        uwshcu_batch_trigger<32, 32, 1><<<grid, block, 0, stream>>>(*b);
+        return cudaGetLastError();
+    }
+    if (minb == 4) {
+        uwshcu_batch_list<32, 32, 4, 1><<<grid, block, 0, stream>>>(*b);
+        return cudaGetLastError();
+    }
+    return cudaErrorInvalidValue;
+}
+
+extern "C" cudaError_t uw_fast_batch_occupancy_k32n32(int minb, int block, int* blocks_per_sm)
+{
+    *blocks_per_sm = 0;
+    if (minb == 4)
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, uwshcu_batch_list<32, 32, 4, 1>, block, 0);
+    return cudaSuccess;
+}

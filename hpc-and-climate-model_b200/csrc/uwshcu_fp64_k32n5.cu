@@ -30,19 +30,19 @@ extern "C" cudaError_t uw_fp64_batch_k32n5(const UwBatch* b, int phase, int grid
 {
     if (grid <= 0) return cudaSuccess;
     if (phase == 0) {
-        uwshcu_batch_trigger<32, 5><<<grid, block, 0, stream>>>(*b);
+        uwshcu_batch_trigger<32, 5, 0><<<grid, block, 0, stream>>>(*b);
         return cudaGetLastError();
     }
     if (minb == 3) {
-        uwshcu_batch_list<32, 5, 3><<<grid, block, 0, stream>>>(*b);
+        uwshcu_batch_list<32, 5, 3, 0><<<grid, block, 0, stream>>>(*b);
         return cudaGetLastError();
     }
     if (minb == 4) {
-        uwshcu_batch_list<32, 5, 4><<<grid, block, 0, stream>>>(*b);
+        uwshcu_batch_list<32, 5, 4, 0><<<grid, block, 0, stream>>>(*b);
         return cudaGetLastError();
     }
     if (minb == 6) {
-        uwshcu_batch_list<32, 5, 6><<<grid, block, 0, stream>>>(*b);
+        uwshcu_batch_list<32, 5, 6, 0><<<grid, block, 0, stream>>>(*b);
         return cudaGetLastError();
     }
     return cudaErrorInvalidValue;
@@ -53,10 +53,10 @@ extern "C" cudaError_t uw_fp64_batch_occupancy_k32n5(int minb, int block, int* b
 {
     *blocks_per_sm = 0;
     if (minb == 3)
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, uwshcu_batch_list<32, 5, 3>, block, 0);
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, uwshcu_batch_list<32, 5, 3, 0>, block, 0);
     if (minb == 4)
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, uwshcu_batch_list<32, 5, 4>, block, 0);
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, uwshcu_batch_list<32, 5, 4, 0>, block, 0);
     if (minb == 6)
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, uwshcu_batch_list<32, 5, 6>, block, 0);
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, uwshcu_batch_list<32, 5, 6, 0>, block, 0);
     return cudaSuccess;
 }

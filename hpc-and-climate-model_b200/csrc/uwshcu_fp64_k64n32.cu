@@ -30,11 +30,11 @@ extern "C" cudaError_t uw_fp64_batch_k64n32(const UwBatch* b, int phase, int gri
 {
     if (grid <= 0) return cudaSuccess;
     if (phase == 0) {
-        uwshcu_batch_trigger<64, 32><<<grid, block, 0, stream>>>(*b);
+        uwshcu_batch_trigger<64, 32, 0><<<grid, block, 0, stream>>>(*b);
         return cudaGetLastError();
     }
     if (minb == 4) {
-        uwshcu_batch_list<64, 32, 4><<<grid, block, 0, stream>>>(*b);
+        uwshcu_batch_list<64, 32, 4, 0><<<grid, block, 0, stream>>>(*b);
         return cudaGetLastError();
     }
     return cudaErrorInvalidValue;
@@ -45,6 +45,6 @@ extern "C" cudaError_t uw_fp64_batch_occupancy_k64n32(int minb, int block, int* 
 {
     *blocks_per_sm = 0;
     if (minb == 4)
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, uwshcu_batch_list<64, 32, 4>, block, 0);
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, uwshcu_batch_list<64, 32, 4, 0>, block, 0);
     return cudaSuccess;
 }

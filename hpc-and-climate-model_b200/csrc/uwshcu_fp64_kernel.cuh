@@ -136,11 +136,11 @@ __device__ __noinline__ int conden(double p, double ex, double thl, double qt, d
 }
 
 // conden for the fast-FP64 precision mode: the same saturation adjustment with one reciprocal of the
-// temperature per Newton step (2 divisions instead of 5) and a stop once every lane of the warp has
-// taken a step smaller than 1e-10 T.  The Fortran always takes 10 steps; the steps shrink about
-// 100x per iteration and fall below 1e-10 T after 5-7, so the result differs from conden by about
-// 1e-12 relative.  The warp-wide vote (__all_sync over the lanes active at the call) keeps the
-// lanes of a warp together.
+// temperature per Newton step (2 divisions instead of 5), each lane stopping after its first step
+// smaller than 1e-10 T.  The Fortran always takes 10 steps; the steps shrink about 100x per
+// iteration and fall below 1e-10 T after 5-7, so the result differs from conden by about 1e-12
+// relative.  A lane's result depends only on its own column; the warp leaves the loop when every
+// lane is done (__all_sync over the lanes active at the call), so the lanes stay together.
 __device__ __noinline__ int conden_fast(double p, double ex, double thl, double qt, double& th, double& qv,
                                         double& ql, double& qi, const double* __restrict__ tbl)
 {
@@ -159,15 +159,18 @@ __device__ __noinline__ int conden_fast(double p, double ex, double thl, double 
         const double cpl = c.cp / leff;
         const double a2 = c.ep2 * leff / c.r;
         double qs = rvls;
+        bool done = false;
 #pragma unroll 1
         for (int it = 0; it < 10; it++) {
-            const double rt = 1.0 / temps;
-            const double dT = ((tc - temps) * cpl + qt - rvls) / (cpl + a2 * rvls * rt * rt);
-            temps = temps + dT;
-            qs = qsat_qs(temps, p, tbl);
-            rvls = qs;
-            const bool conv = fabs(dT) < 1.e-10 * temps;
-            if (__all_sync(__activemask(), conv)) break;
+            if (!done) {
+                const double rt = 1.0 / temps;
+                const double dT = ((tc - temps) * cpl + qt - rvls) / (cpl + a2 * rvls * rt * rt);
+                temps = temps + dT;
+                qs = qsat_qs(temps, p, tbl);
+                rvls = qs;
+                done = fabs(dT) < 1.e-10 * temps;
+            }
+            if (__all_sync(__activemask(), done)) break;
         }
         double qc = MX(qt - qs, 0.0);
         qv = qt - qc;
@@ -459,6 +462,10 @@ __device__ double findsp_point(double q, double t, double p, unsigned int& errbi
 #define UW_MODE_ALL 0
 #define UW_MODE_TRIGGER 1
 #define UW_MODE_LIST 2
+
+// The column code and the kernels have internal linkage: every unit that includes a column-code
+// header (FP64, fast, mixed, tangent) carries its own copies under the same names.
+namespace {
 
 // One column per lane: column i of A when `active`.  All 32 lanes of the warp must call it together
 // (it starts with a warp ballot).  `tbl` is the saturation table in shared memory.  In
@@ -2016,32 +2023,10 @@ uwshcu_fp64_kernel(const __grid_constant__ UwArgs A, int* __restrict__ wl, int* 
     uw_column<KP, NC, MODE, 0>(A, tbl, i, active, wl, wl_count);
 }
 
-// The fast-FP64 precision mode: same launch shapes as uwshcu_fp64_kernel.
-template <int KP, int NC, int MODE>
-__global__ void __launch_bounds__(128, MODE == UW_MODE_LIST ? 4 : (MODE == UW_MODE_TRIGGER ? 5 : 3))
-uwshcu_fast_kernel(const __grid_constant__ UwArgs A, int* __restrict__ wl, int* __restrict__ wl_count)
-{
-    __shared__ double tbl[UW_TBL];
-    for (int t = threadIdx.x; t < UW_TBL; t += blockDim.x) tbl[t] = c_estbl[t];
-    __syncthreads();
-
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    int i;
-    bool active;
-    if (MODE == UW_MODE_LIST) {
-        active = tid < *wl_count;
-        i = active ? wl[tid] : 0;
-    } else {
-        active = tid < A.iend;
-        i = tid;
-    }
-    uw_column<KP, NC, MODE, 1>(A, tbl, i, active, wl, wl_count);
-}
-
 // Batched trigger pass: every column of every member of B (members of one level/tracer class).
 // Blocks [block_start[m], block_start[m+1]) cover member m; its convecting columns go to
-// wl[m] / count[m].
-template <int KP, int NC>
+// wl[m] / count[m].  FAST selects the column code of the fast-FP64 mode.
+template <int KP, int NC, int FAST>
 __global__ void __launch_bounds__(128, 5) uwshcu_batch_trigger(const __grid_constant__ UwBatch B)
 {
     __shared__ double tbl[UW_TBL];
@@ -2052,14 +2037,14 @@ __global__ void __launch_bounds__(128, 5) uwshcu_batch_trigger(const __grid_cons
     while (m + 1 < B.nm && (int)blockIdx.x >= B.block_start[m + 1]) m++;
     const int tid = ((int)blockIdx.x - B.block_start[m]) * blockDim.x + threadIdx.x;
     const bool active = tid < B.m[m].iend;
-    uw_column<KP, NC, UW_MODE_TRIGGER, 0>(B.m[m], tbl, tid, active, B.wl[m], B.count + m);
+    uw_column<KP, NC, UW_MODE_TRIGGER, FAST>(B.m[m], tbl, tid, active, B.wl[m], B.count + m);
 }
 
 // Batched worklist pass, persistent: each warp takes the next task (32 * B.chunk consecutive queue
 // entries of one member) from the device counter *B.task_head until the queues are drained, so a
 // warp never mixes members (their level counts differ).  Task t of member m covers entries
 // [t * 32 * chunk, (t + 1) * 32 * chunk) of wl[m].
-template <int KP, int NC, int MINB>
+template <int KP, int NC, int MINB, int FAST>
 __global__ void __launch_bounds__(128, MINB) uwshcu_batch_list(const __grid_constant__ UwBatch B)
 {
     __shared__ double tbl[UW_TBL];
@@ -2090,7 +2075,31 @@ __global__ void __launch_bounds__(128, MINB) uwshcu_batch_list(const __grid_cons
             const int idx = first + c * 32 + lane;
             const bool active = idx < n;
             const int i = active ? B.wl[m][idx] : 0;
-            uw_column<KP, NC, UW_MODE_LIST, 0>(B.m[m], tbl, i, active, nullptr, nullptr);
+            uw_column<KP, NC, UW_MODE_LIST, FAST>(B.m[m], tbl, i, active, nullptr, nullptr);
         }
     }
 }
+
+// The fast-FP64 precision mode: same launch shapes as uwshcu_fp64_kernel.
+template <int KP, int NC, int MODE>
+__global__ void __launch_bounds__(128, MODE == UW_MODE_LIST ? 4 : (MODE == UW_MODE_TRIGGER ? 5 : 3))
+uwshcu_fast_kernel(const __grid_constant__ UwArgs A, int* __restrict__ wl, int* __restrict__ wl_count)
+{
+    __shared__ double tbl[UW_TBL];
+    for (int t = threadIdx.x; t < UW_TBL; t += blockDim.x) tbl[t] = c_estbl[t];
+    __syncthreads();
+
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    int i;
+    bool active;
+    if (MODE == UW_MODE_LIST) {
+        active = tid < *wl_count;
+        i = active ? wl[tid] : 0;
+    } else {
+        active = tid < A.iend;
+        i = tid;
+    }
+    uw_column<KP, NC, MODE, 1>(A, tbl, i, active, wl, wl_count);
+}
+
+}  // namespace

@@ -1096,34 +1096,69 @@ UW_DECL_BATCH(64, 5)
 UW_DECL_BATCH(32, 32)
 UW_DECL_BATCH(64, 32)
 #undef UW_DECL_BATCH
+#define UW_DECL_BATCH_P(P, KP, NC)                                                                     \
+    extern "C" cudaError_t uw_##P##_batch_k##KP##n##NC(const UwBatch* b, int phase, int grid, int block, \
+                                                       int minb, cudaStream_t stream);                 \
+    extern "C" cudaError_t uw_##P##_batch_occupancy_k##KP##n##NC(int minb, int block, int* blocks_per_sm);
+UW_DECL_BATCH_P(fast, 32, 5)
+UW_DECL_BATCH_P(fast, 64, 5)
+UW_DECL_BATCH_P(fast, 32, 32)
+UW_DECL_BATCH_P(fast, 64, 32)
+UW_DECL_BATCH_P(mixed, 32, 5)
+UW_DECL_BATCH_P(mixed, 64, 5)
+#undef UW_DECL_BATCH_P
 
 namespace {
 
 // Level/tracer classes of the compiled instantiations: bit 0 = 64-level bound, bit 1 = 32 tracers.
 constexpr int kClasses = 4;
-cudaError_t batch_launch(int cls, const UwBatch* b, int phase, int grid, int block, int minb, cudaStream_t st)
+typedef cudaError_t (*BatchFn)(const UwBatch*, int, int, int, int, cudaStream_t);
+typedef cudaError_t (*BatchOccFn)(int, int, int*);
+// the batch launch hooks of a precision mode and class (null: not compiled)
+BatchFn batch_fn(int prec, int cls)
 {
-    switch (cls) {
-    case 0: return uw_fp64_batch_k32n5(b, phase, grid, block, minb, st);
-    case 1: return uw_fp64_batch_k64n5(b, phase, grid, block, minb, st);
-    case 2: return uw_fp64_batch_k32n32(b, phase, grid, block, minb, st);
-    default: return uw_fp64_batch_k64n32(b, phase, grid, block, minb, st);
-    }
+    static const BatchFn fp64[kClasses] = {uw_fp64_batch_k32n5, uw_fp64_batch_k64n5, uw_fp64_batch_k32n32,
+                                           uw_fp64_batch_k64n32};
+    static const BatchFn fast[kClasses] = {uw_fast_batch_k32n5, uw_fast_batch_k64n5, uw_fast_batch_k32n32,
+                                           uw_fast_batch_k64n32};
+    static const BatchFn mixed[kClasses] = {uw_mixed_batch_k32n5, uw_mixed_batch_k64n5, nullptr, nullptr};
+    return prec == UWSHCU_PREC_FAST ? fast[cls] : prec == UWSHCU_PREC_MIXED ? mixed[cls] : fp64[cls];
 }
-cudaError_t batch_occupancy(int cls, int minb, int block, int* per_sm)
+BatchOccFn batch_occ_fn(int prec, int cls)
 {
-    switch (cls) {
-    case 0: return uw_fp64_batch_occupancy_k32n5(minb, block, per_sm);
-    case 1: return uw_fp64_batch_occupancy_k64n5(minb, block, per_sm);
-    case 2: return uw_fp64_batch_occupancy_k32n32(minb, block, per_sm);
-    default: return uw_fp64_batch_occupancy_k64n32(minb, block, per_sm);
-    }
+    static const BatchOccFn fp64[kClasses] = {uw_fp64_batch_occupancy_k32n5, uw_fp64_batch_occupancy_k64n5,
+                                              uw_fp64_batch_occupancy_k32n32, uw_fp64_batch_occupancy_k64n32};
+    static const BatchOccFn fast[kClasses] = {uw_fast_batch_occupancy_k32n5, uw_fast_batch_occupancy_k64n5,
+                                              uw_fast_batch_occupancy_k32n32, uw_fast_batch_occupancy_k64n32};
+    static const BatchOccFn mixed[kClasses] = {uw_mixed_batch_occupancy_k32n5, uw_mixed_batch_occupancy_k64n5,
+                                               nullptr, nullptr};
+    return prec == UWSHCU_PREC_FAST ? fast[cls] : prec == UWSHCU_PREC_MIXED ? mixed[cls] : fp64[cls];
 }
-// register caps compiled per class (the 32-tracer classes carry only the 128-register one)
-bool batch_has_minb(int cls, int minb) { return cls < 2 ? (minb == 3 || minb == 4 || minb == 6) : minb == 4; }
+cudaError_t batch_launch(int prec, int cls, const UwBatch* b, int phase, int grid, int block, int minb, cudaStream_t st)
+{
+    BatchFn f = batch_fn(prec, cls);
+    return f ? f(b, phase, grid, block, minb, st) : cudaErrorInvalidValue;
+}
+cudaError_t batch_occupancy(int prec, int cls, int minb, int block, int* per_sm)
+{
+    BatchOccFn f = batch_occ_fn(prec, cls);
+    if (!f) {
+        *per_sm = 0;
+        return cudaErrorInvalidValue;
+    }
+    return f(minb, block, per_sm);
+}
+// register caps compiled per precision and class: FP64 with 5 tracers carries 168/128/80 registers,
+// the others only the 128-register one
+bool batch_has_minb(int prec, int cls, int minb)
+{
+    if (prec == UWSHCU_PREC_FP64 && cls < 2) return minb == 3 || minb == 4 || minb == 6;
+    return minb == 4;
+}
 
 struct BatchPlan {
     int dev = 0;
+    int prec = UWSHCU_PREC_FP64;  // precision mode at creation
     int nm = 0;
     uwshcu_member mem[UWSHCU_MAX_MEMBERS];
     int ncls = 0;
@@ -1145,13 +1180,14 @@ int plan_enqueue(BatchPlan& P, cudaStream_t st)
     if ((e = cudaMemsetAsync(P.d_scratch, 0, (64 + kClasses) * sizeof(int), st)) != cudaSuccess) return cuda_fail(e);
     for (int c = 0; c < P.ncls; c++) {
         P.b[c].chunk = P.chunk;
-        if ((e = batch_launch(P.cls_id[c], &P.b[c], 0, P.trig_grid[c], P.block, 0, st)) != cudaSuccess) return cuda_fail(e);
+        if ((e = batch_launch(P.prec, P.cls_id[c], &P.b[c], 0, P.trig_grid[c], P.block, 0, st)) != cudaSuccess)
+            return cuda_fail(e);
     }
     for (int c = 0; c < P.ncls; c++) {
         int per_sm = 0;
-        if ((e = batch_occupancy(P.cls_id[c], P.minb, P.block, &per_sm)) != cudaSuccess) return cuda_fail(e);
+        if ((e = batch_occupancy(P.prec, P.cls_id[c], P.minb, P.block, &per_sm)) != cudaSuccess) return cuda_fail(e);
         if (per_sm <= 0) return UWSHCU_ERR_BAD_ARGS;
-        if ((e = batch_launch(P.cls_id[c], &P.b[c], 1, P.nsm * per_sm, P.block, P.minb, st)) != cudaSuccess)
+        if ((e = batch_launch(P.prec, P.cls_id[c], &P.b[c], 1, P.nsm * per_sm, P.block, P.minb, st)) != cudaSuccess)
             return cuda_fail(e);
     }
     return UWSHCU_OK;
@@ -1176,7 +1212,7 @@ extern "C" int uwshcu_batch_create(int nmembers, const uwshcu_member* members, v
     *plan = nullptr;
     if (!s.init) return UWSHCU_ERR_NOT_INITIALIZED;
     if (nmembers < 1 || nmembers > UWSHCU_MAX_MEMBERS || !members) return UWSHCU_ERR_BAD_ARGS;
-    if (s.precision != UWSHCU_PREC_FP64) return UWSHCU_ERR_BAD_ARGS;   // the batch path is FP64
+    // the plan keeps the precision mode in force now (FP64, FAST, or MIXED with ncnst <= 5)
     const int ncnst = s.k.ncnst;
     size_t total = 0;
     for (int j = 0; j < nmembers; j++) {
@@ -1196,6 +1232,7 @@ extern "C" int uwshcu_batch_create(int nmembers, const uwshcu_member* members, v
     if (rc != UWSHCU_OK) return rc;
     BatchPlan* P = new BatchPlan();
     P->nm = nmembers;
+    P->prec = s.precision;
     cudaError_t e;
     if ((e = cudaGetDevice(&P->dev)) != cudaSuccess || (e = cudaDeviceGetAttribute(&P->nsm, cudaDevAttrMultiProcessorCount, P->dev)) != cudaSuccess) {
         plan_free(P);
@@ -1366,7 +1403,7 @@ extern "C" int uwshcu_batch_autotune(void* plan, void* stream, int* block_out, i
     for (int block : blocks) {
         for (int minb : minbs) {
             bool ok = true;
-            for (int c = 0; c < P.ncls; c++) ok = ok && batch_has_minb(P.cls_id[c], minb);
+            for (int c = 0; c < P.ncls; c++) ok = ok && batch_has_minb(P.prec, P.cls_id[c], minb);
             if (!ok) continue;
             for (int chunk : chunks) {
                 plan_set_block(P, block);

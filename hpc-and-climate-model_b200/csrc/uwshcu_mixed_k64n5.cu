@@ -19,3 +19,28 @@ extern "C" cudaError_t uw_mixed_launch_k64n5(const UwArgs* a, int mode, int* wl,
     else uwshcu_mixed_kernel<64, 5, UW_MODE_LIST><<<grid, block, 0, stream>>>(*a, wl, wl_count);
     return cudaGetLastError();
 }
+
+// Batched trigger (phase 0) and persistent worklist (phase 1) launches of this precision mode;
+// minb selects the worklist instantiation (only the ones compiled here).
+extern "C" cudaError_t uw_mixed_batch_k64n5(const UwBatch* b, int phase, int grid, int block, int minb,
+                                          cudaStream_t stream)
+{
+    if (grid <= 0) return cudaSuccess;
+    if (phase == 0) {
+        uwshcu_batch_trigger<64, 5, 0><<<grid, block, 0, stream>>>(*b);
+        return cudaGetLastError();
+    }
+    if (minb == 4) {
+        uwshcu_batch_list<64, 5, 4, 0><<<grid, block, 0, stream>>>(*b);
+        return cudaGetLastError();
+    }
+    return cudaErrorInvalidValue;
+}
+
+extern "C" cudaError_t uw_mixed_batch_occupancy_k64n5(int minb, int block, int* blocks_per_sm)
+{
+    *blocks_per_sm = 0;
+    if (minb == 4)
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, uwshcu_batch_list<64, 5, 4, 0>, block, 0);
+    return cudaSuccess;
+}

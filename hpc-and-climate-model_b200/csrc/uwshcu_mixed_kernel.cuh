@@ -12,7 +12,8 @@
 //
 // The FP64 islands use algebraically equal but cheaper forms than the Fortran (one division per
 // Newton step instead of six, FMA contraction allowed) and stop the conden iteration once the
-// temperature change is below 1e-9 K on every lane of the warp; this kernel is checked against the FP64 oracle with error
+// temperature change is below 1e-9 K (each lane at its own step, so results do not depend on which
+// columns share a warp); this kernel is checked against the FP64 oracle with error
 // statistics, not bit for bit.
 #pragma once
 #include <cuda_runtime.h>
@@ -122,15 +123,19 @@ __device__ __noinline__ int conden(R p, R ex, R thl, R qt, R& th, R& qv, R& ql, 
     const double cpl = c.cp / leff;
     const double a = c.ep2 * leff / c.r;
     double temps = tc;
+    bool done = false;
 #pragma unroll 1
     for (int it = 0; it < 10; it++) {
-        const double rt = 1.0 / temps;
-        const double dT = ((tc - temps) * cpl + qtd - rvls) / (cpl + a * rvls * rt * rt);
-        temps += dT;
-        es = estblf_d(temps, tbld);
-        rvls = MN(1.0, c.epsqs * es / (pd - c.omeps * es));
-        if (rvls < 0.0) rvls = 1.0;
-        if (__all_sync(__activemask(), fabs(dT) < 1.e-9)) break;
+        if (!done) {
+            const double rt = 1.0 / temps;
+            const double dT = ((tc - temps) * cpl + qtd - rvls) / (cpl + a * rvls * rt * rt);
+            temps += dT;
+            es = estblf_d(temps, tbld);
+            rvls = MN(1.0, c.epsqs * es / (pd - c.omeps * es));
+            if (rvls < 0.0) rvls = 1.0;
+            done = fabs(dT) < 1.e-9;
+        }
+        if (__all_sync(__activemask(), done)) break;
     }
     const double qc = MX(qtd - rvls, 0.0);
     qv = (R)(qtd - qc);
@@ -408,6 +413,10 @@ __device__ R findsp_point(R q, R t, R p, unsigned int& errbits, const double* __
 //   UW_MODE_LIST     thread t runs the whole scheme for column wl[t], t < *wl_count.
 // The worklist path recomputes the phase-1 part of a convecting column instead of storing it: the
 // heavy buoyancy-sorting work then runs in warps made only of convecting columns.
+
+// The column code and the kernels have internal linkage: every unit that includes a column-code
+// header (FP64, fast, mixed, tangent) carries its own copies under the same names.
+namespace {
 
 // One column per lane: column i of A when `active`.  All 32 lanes of the warp must call it together
 // (it starts with a warp ballot).  `tbl` is the saturation table in shared memory.  In
@@ -1975,3 +1984,70 @@ uwshcu_mixed_kernel(const __grid_constant__ UwArgs A, int* __restrict__ wl, int*
     }
     uw_column<KP, NC, MODE, 0>(A, tbld, tblf, i, active, wl, wl_count);
 }
+
+// Batched trigger pass: every column of every member of B (members of one level/tracer class).
+// Blocks [block_start[m], block_start[m+1]) cover member m; its convecting columns go to
+// wl[m] / count[m].  FAST selects the column code of the fast-FP64 mode.
+template <int KP, int NC, int FAST>
+__global__ void __launch_bounds__(128, 5) uwshcu_batch_trigger(const __grid_constant__ UwBatch B)
+{
+    __shared__ double tbld[UW_TBL];
+    __shared__ float tblf[UW_TBL];
+    for (int t = threadIdx.x; t < UW_TBL; t += blockDim.x) {
+        tbld[t] = c_estbl[t];
+        tblf[t] = (float)c_estbl[t];
+    }
+    __syncthreads();
+
+    int m = 0;
+    while (m + 1 < B.nm && (int)blockIdx.x >= B.block_start[m + 1]) m++;
+    const int tid = ((int)blockIdx.x - B.block_start[m]) * blockDim.x + threadIdx.x;
+    const bool active = tid < B.m[m].iend;
+    uw_column<KP, NC, UW_MODE_TRIGGER, FAST>(B.m[m], tbld, tblf, tid, active, B.wl[m], B.count + m);
+}
+
+// Batched worklist pass, persistent: each warp takes the next task (32 * B.chunk consecutive queue
+// entries of one member) from the device counter *B.task_head until the queues are drained, so a
+// warp never mixes members (their level counts differ).  Task t of member m covers entries
+// [t * 32 * chunk, (t + 1) * 32 * chunk) of wl[m].
+template <int KP, int NC, int MINB, int FAST>
+__global__ void __launch_bounds__(128, MINB) uwshcu_batch_list(const __grid_constant__ UwBatch B)
+{
+    __shared__ double tbld[UW_TBL];
+    __shared__ float tblf[UW_TBL];
+    for (int t = threadIdx.x; t < UW_TBL; t += blockDim.x) {
+        tbld[t] = c_estbl[t];
+        tblf[t] = (float)c_estbl[t];
+    }
+    __syncthreads();
+
+    const int lane = threadIdx.x & 31;
+    const int per_task = 32 * B.chunk;
+    for (;;) {
+        int task = 0;
+        if (lane == 0) task = atomicAdd(B.task_head, 1);
+        task = __shfl_sync(0xffffffffu, task, 0);
+        int m = -1, first = 0;
+        for (int j = 0; j < B.nm; j++) {
+            const int nt = (B.count[j] + per_task - 1) / per_task;
+            if (m < 0) {
+                if (task < nt) {
+                    m = j;
+                    first = task * per_task;
+                } else {
+                    task -= nt;
+                }
+            }
+        }
+        if (m < 0) break;   // same task on every lane: the whole warp leaves
+        const int n = B.count[m];
+        for (int c = 0; c < B.chunk; c++) {
+            const int idx = first + c * 32 + lane;
+            const bool active = idx < n;
+            const int i = active ? B.wl[m][idx] : 0;
+            uw_column<KP, NC, UW_MODE_LIST, FAST>(B.m[m], tbld, tblf, i, active, nullptr, nullptr);
+        }
+    }
+}
+
+}  // namespace

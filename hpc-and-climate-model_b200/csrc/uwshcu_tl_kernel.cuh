@@ -114,11 +114,11 @@ __device__ __noinline__ int conden(Tl p, Tl ex, Tl thl, Tl qt, Tl& th, Tl& qv,
 }
 
 // conden for the fast-FP64 precision mode: the same saturation adjustment with one reciprocal of the
-// temperature per Newton step (2 divisions instead of 5) and a stop once every lane of the warp has
-// taken a step smaller than 1e-10 T.  The Fortran always takes 10 steps; the steps shrink about
-// 100x per iteration and fall below 1e-10 T after 5-7, so the result differs from conden by about
-// 1e-12 relative.  The warp-wide vote (__all_sync over the lanes active at the call) keeps the
-// lanes of a warp together.
+// temperature per Newton step (2 divisions instead of 5), each lane stopping after its first step
+// smaller than 1e-10 T.  The Fortran always takes 10 steps; the steps shrink about 100x per
+// iteration and fall below 1e-10 T after 5-7, so the result differs from conden by about 1e-12
+// relative.  A lane's result depends only on its own column; the warp leaves the loop when every
+// lane is done (__all_sync over the lanes active at the call), so the lanes stay together.
 __device__ __noinline__ int conden_fast(Tl p, Tl ex, Tl thl, Tl qt, Tl& th, Tl& qv,
                                         Tl& ql, Tl& qi, const double* __restrict__ tbl)
 {
@@ -137,15 +137,18 @@ __device__ __noinline__ int conden_fast(Tl p, Tl ex, Tl thl, Tl qt, Tl& th, Tl& 
         const Tl cpl = c.cp / leff;
         const Tl a2 = c.ep2 * leff / c.r;
         Tl qs = rvls;
+        bool done = false;
 #pragma unroll 1
         for (int it = 0; it < 10; it++) {
-            const Tl rt = 1.0 / temps;
-            const Tl dT = ((tc - temps) * cpl + qt - rvls) / (cpl + a2 * rvls * rt * rt);
-            temps = temps + dT;
-            qs = qsat_qs(temps, p, tbl);
-            rvls = qs;
-            const bool conv = fabs(dT) < 1.e-10 * temps;
-            if (__all_sync(__activemask(), conv)) break;
+            if (!done) {
+                const Tl rt = 1.0 / temps;
+                const Tl dT = ((tc - temps) * cpl + qt - rvls) / (cpl + a2 * rvls * rt * rt);
+                temps = temps + dT;
+                qs = qsat_qs(temps, p, tbl);
+                rvls = qs;
+                done = fabs(dT) < 1.e-10 * temps;
+            }
+            if (__all_sync(__activemask(), done)) break;
         }
         Tl qc = MX(qt - qs, 0.0);
         qv = qt - qc;
@@ -437,6 +440,10 @@ __device__ Tl findsp_point(Tl q, Tl t, Tl p, unsigned int& errbits, const double
 #define UW_MODE_ALL 0
 #define UW_MODE_TRIGGER 1
 #define UW_MODE_LIST 2
+
+// The column code and the kernels have internal linkage: every unit that includes a column-code
+// header (FP64, fast, mixed, tangent) carries its own copies under the same names.
+namespace {
 
 // One column per lane: column i of A when `active`.  All 32 lanes of the warp must call it together
 // (it starts with a warp ballot).  `tbl` is the saturation table in shared memory.  In
@@ -2005,3 +2012,5 @@ uwshcu_tl_kernel(const __grid_constant__ UwArgs A, int* __restrict__ wl, int* __
     }
     uw_column<KP, NC, MODE, 0>(A, tbl, i, active, wl, wl_count, T);
 }
+
+}  // namespace

@@ -37,13 +37,14 @@ extern "C" {
 #define UWSHCU_PREC_FP64 0               /* FP64 throughout, Fortran evaluation order, no FMA      */
 #define UWSHCU_PREC_MIXED 1              /* FP32 bulk, FP64 conden/roots/qsinvert/implicit CIN/
                                             positive_moisture, Kahan vertical sums (ncnst <= 5).
-                                            1.67x the FP64 path; column heating/moistening/precip
+                                            1.5x the FP64 path; column heating/moistening/precip
                                             ~0.9 % relative RMS (cloud tops of ~0.6 % of the
                                             convecting columns move)                            */
-#define UWSHCU_PREC_FAST 2               /* FP64 throughout with a Newton conden that stops once the
-                                            warp's steps are below 1e-10 T and divides twice per
-                                            step instead of five times; FMA contraction allowed.
-                                            Not bit-exact: ~1e-12 relative per conden call     */
+#define UWSHCU_PREC_FAST 2               /* FP64 throughout with a Newton conden that stops each
+                                            lane after its first step below 1e-10 T and divides
+                                            twice per step; FMA contraction allowed.  Not
+                                            bit-exact (~1e-12 relative per conden call); about
+                                            the FP64 path's speed                              */
 
 /* ---- set-up -------------------------------------------------------------------------------- */
 
@@ -230,7 +231,9 @@ typedef struct uwshcu_member {
  * the plan's worklists and counters here, once.  A run makes one trigger launch and one persistent
  * worklist launch per level class (mkx + 1 <= 32 or <= 64): the worklist kernel pulls warps of
  * one member's convecting columns from a device counter until every member's queue is drained.
- * Results are the same bits as uwshcu_compute_device on each member. */
+ * The plan runs in the precision mode set when it is created (uwshcu_set_precision: FP64, FAST, or
+ * MIXED with ncnst <= 5).  Results are the same bits as uwshcu_compute_device on each member in
+ * that mode. */
 int uwshcu_batch_create(int nmembers, const uwshcu_member *members, void **plan);
 
 /* Enqueue one run of the plan on `stream` (the captured CUDA graph when there is one). */
@@ -241,8 +244,8 @@ int uwshcu_batch_run(void *plan, void *stream);
 int uwshcu_batch_capture(void *plan, void *stream);
 
 /* Time the compiled launch shapes of the worklist pass (block of 64 or 128 threads, register cap
- * 168/128/80 = 3/4/6 blocks of 128 per SM, 32 or 64 columns per warp task) on this plan's data
- * and keep the fastest in the plan (it drops a captured graph).  Runs the scheme several times:
+ * 168/128/80 = 3/4/6 blocks of 128 per SM in FP64, 128 in the other modes, 32 or 64 columns per
+ * warp task) on this plan's data and keep the fastest in the plan (it drops a captured graph).  Runs the scheme several times:
  * the outputs are overwritten and cush is restored to its value on entry.  Reports the choice. */
 int uwshcu_batch_autotune(void *plan, void *stream, int *block, int *regcap_blocks, int *chunk);
 
