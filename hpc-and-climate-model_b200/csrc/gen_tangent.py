@@ -77,6 +77,7 @@ def main():
         return "A.%s[i] = tl_val(%s);" % (f, x)
     s = re.sub(r"\bA\.(precip|snow|cush|cbmf|rliq|cnt|cnb)\[i\] = ([^;]+);", col_store, s)
     s = re.sub(r"(A\.diag_real\[[^\]]+\]) = ([^;]+);", lambda m: "%s = tl_val(%s);" % (m.group(1), m.group(2)), s)
+    s = re.sub(r"\bDLV\(([^()]*)\) = ([^;]+);", lambda m: "DLV(%s) = tl_val(%s);" % (m.group(1), m.group(2)), s)
     # the kernel
     s = s.replace("uwshcu_fp64_kernel", "uwshcu_tl_kernel")
     s = rep(s, "uwshcu_tl_kernel(const __grid_constant__ UwArgs A, int* __restrict__ wl, int* __restrict__ wl_count)",

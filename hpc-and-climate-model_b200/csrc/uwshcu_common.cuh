@@ -32,6 +32,23 @@
 #define UW_DR_PPEN 6
 #define UW_DR_TKEAVG 7
 #define UW_NDR 8
+// Per-level diagnostics, array (UW_NDL, mkx + 1, mix): the history fields of compute_uwshcu
+// (uwshcu.F90:1945-1990, :4383-4433), levels bottom-up k = 0 .. mkx for both level orders.  Interface
+// fields fill k = 0 .. mkx; layer fields (UW_DL_FER and after) fill k = 1 .. mkx and hold 0 at k = 0.
+#define UW_DL_UFRC 0
+#define UW_DL_QTU 1
+#define UW_DL_THLU 2
+#define UW_DL_THVU 3
+#define UW_DL_UU 4
+#define UW_DL_VU 5
+#define UW_DL_UEMF 6
+#define UW_DL_FLXRAIN 7
+#define UW_DL_FLXSNOW 8
+#define UW_DL_FER 9
+#define UW_DL_FDR 10
+#define UW_DL_DWTEN 11
+#define UW_DL_DITEN 12
+#define UW_NDL 13
 
 // exit_* bits
 #define UW_X_UWCU (1 << 0)
@@ -94,6 +111,7 @@ struct UwArgs {
     double *wu;
     int *diag_int;       // optional (UW_NDI, mix)
     double *diag_real;   // optional (UW_NDR, mix)
+    double *diag_level;  // optional (UW_NDL, mkx + 1, mix)
     unsigned int *err;   // device error word
 };
 

@@ -502,6 +502,30 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
 #define OL(a, k) A.a[(size_t)RL(k) * mix + i]
 #define OT(m, k) A.trten[((size_t)((m) - 1) * mkx + RL(k)) * mix + i]
 #define CNT(x) (inv ? (double)(mkx + 1) - (x) : (x))
+#define DLV(j, k) A.diag_level[((size_t)(j) * (mkx + 1) + (k)) * mix + i]
+// per-level diagnostics of the current state, levels bottom-up in both level orders
+// (uwshcu.F90:1945-1990 and :4383-4433)
+#define PUT_DIAG_LEVEL()                                                                                  \
+    if (A.diag_level) {                                                                                   \
+        for (int k = 0; k <= mkx; k++) {                                                                  \
+            DLV(UW_DL_UFRC, k) = ufrc[k];                                                                 \
+            DLV(UW_DL_QTU, k) = qtu[k];                                                                   \
+            DLV(UW_DL_THLU, k) = thlu[k];                                                                 \
+            DLV(UW_DL_THVU, k) = thvu[k];                                                                 \
+            DLV(UW_DL_UU, k) = uu[k];                                                                     \
+            DLV(UW_DL_VU, k) = vu[k];                                                                     \
+            DLV(UW_DL_UEMF, k) = UEMF(k);                                                                 \
+            DLV(UW_DL_FLXRAIN, k) = flxrain[k];                                                           \
+            DLV(UW_DL_FLXSNOW, k) = flxsnow[k];                                                           \
+        }                                                                                                 \
+        for (int j = UW_DL_FER; j < UW_NDL; j++) DLV(j, 0) = 0.0;                                         \
+        for (int k = 1; k <= mkx; k++) {                                                                  \
+            DLV(UW_DL_FER, k) = fer[k];                                                                   \
+            DLV(UW_DL_FDR, k) = fdr[k];                                                                   \
+            DLV(UW_DL_DWTEN, k) = dwten[k];                                                               \
+            DLV(UW_DL_DITEN, k) = diten[k];                                                               \
+        }                                                                                                 \
+    }
 
     // ---- thread-private profiles ---------------------------------------------------------------
     double ps0[KP], p0[KP], dp0[KP], zs0[KP], exn0[KP], exns0[KP];
@@ -1486,7 +1510,6 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                 } while (0);
                 if (stop) ldone = true;
             }
-#undef UEMF
         }
         UW_SYNC();
         if (!stop) do {
@@ -1834,6 +1857,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
             A.rliq[i] = rliq;
             A.cnt[i] = CNT(cnt);
             A.cnb[i] = CNT(cnb);
+            PUT_DIAG_LEVEL();
             cin_s = cin; cinlcl_s = cinlcl; plcl_s = plcl; pinv_s = ps0[kinv - 1]; plfc_s = plfc;
             pbup_s = ps0[kbup]; ppen_s = ps0[kpen - 1] + ppen; tkeavg_s = tkeavg;
             kinv_s = kinv; klcl_s = klcl; klfc_s = klfc; krel_s = krel; kbup_s = kbup; kpen_s = kpen;
@@ -1924,6 +1948,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
         A.diag_real[UW_DR_PPEN * (size_t)mix + i] = ps0[kpen - 1] + ppen;
         A.diag_real[UW_DR_TKEAVG * (size_t)mix + i] = tkeavg;
     }
+    PUT_DIAG_LEVEL();
     }
 
     // (label 333, :4448-4549)
@@ -1957,6 +1982,9 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
             A.diag_real[UW_DR_CINLCL * (size_t)mix + i] = -1.0;
             for (int j = UW_DR_PLCL; j < UW_NDR; j++) A.diag_real[j * (size_t)mix + i] = 0.0;
         }
+        if (A.diag_level)
+            for (int j = 0; j < UW_NDL; j++)
+                for (int k = 0; k <= mkx; k++) DLV(j, k) = 0.0;
         kinv = klcl = klfc = krel = kbup = kpen = 0;
     }
     if (A.diag_int) {
@@ -1995,6 +2023,9 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
 #undef OI
 #undef OL
 #undef OT
+#undef DLV
+#undef PUT_DIAG_LEVEL
+#undef UEMF
 }
 
 // ---- kernels ---------------------------------------------------------------------------------------

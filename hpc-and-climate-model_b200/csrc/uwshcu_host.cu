@@ -842,6 +842,49 @@ int bxcompute_uwshcu_inv_(const int* pcols, const int* pver, const int* ncol, co
                                rliq, cnt_inv, cnb_inv, nullptr, lchnk, dpdry0_inv, wu_inv);
 }
 
+// A member's arrays are all given (the diagnostics are optional) and its sizes are valid.
+static bool member_ok(const uwshcu_member& m, int ncnst)
+{
+    if (bad_dims(m.mix, m.mkx, m.iend, ncnst) || (m.inv != 0 && m.inv != 1)) return false;
+    const void* need[] = {m.ps0, m.zs0, m.p0, m.z0, m.dp0, m.u0, m.v0, m.qv0, m.ql0, m.qi0, m.t0, m.s0, m.tr0,
+                          m.tke, m.pblh, m.cush, m.umf, m.slflx, m.qtflx, m.flxprc1, m.flxsnow1, m.qvten,
+                          m.qlten, m.qiten, m.sten, m.uten, m.vten, m.trten, m.qrten, m.qsten, m.precip,
+                          m.snow, m.evapc, m.cufrc, m.qcu, m.qlu, m.qiu, m.cbmf, m.qc, m.rliq, m.cnt,
+                          m.cnb, m.dpdry0, m.wu};
+    for (const void* p : need)
+        if (!p) return false;
+    return true;
+}
+
+// The kernel arguments of one member.
+static UwArgs member_args(const uwshcu_member& m, int ncnst, unsigned int* err)
+{
+    UwArgs A{};
+    A.mix = m.mix; A.mkx = m.mkx; A.iend = m.iend; A.ncnst = ncnst; A.inv = m.inv; A.dt = m.dt;
+    A.ps0 = m.ps0; A.zs0 = m.zs0; A.p0 = m.p0; A.z0 = m.z0; A.dp0 = m.dp0; A.u0 = m.u0; A.v0 = m.v0;
+    A.qv0 = m.qv0; A.ql0 = m.ql0; A.qi0 = m.qi0; A.t0 = m.t0; A.s0 = m.s0; A.tr0 = m.tr0; A.tke = m.tke;
+    A.pblh = m.pblh; A.cush = m.cush; A.umf = m.umf; A.slflx = m.slflx; A.qtflx = m.qtflx;
+    A.flxprc1 = m.flxprc1; A.flxsnow1 = m.flxsnow1; A.qvten = m.qvten; A.qlten = m.qlten; A.qiten = m.qiten;
+    A.sten = m.sten; A.uten = m.uten; A.vten = m.vten; A.trten = m.trten; A.qrten = m.qrten;
+    A.qsten = m.qsten; A.precip = m.precip; A.snow = m.snow; A.evapc = m.evapc; A.cufrc = m.cufrc;
+    A.qcu = m.qcu; A.qlu = m.qlu; A.qiu = m.qiu; A.cbmf = m.cbmf; A.qc = m.qc; A.rliq = m.rliq;
+    A.cnt = m.cnt; A.cnb = m.cnb; A.dpdry0 = m.dpdry0; A.wu = m.wu; A.diag_int = m.diag_int;
+    A.diag_real = m.diag_real; A.diag_level = m.diag_level; A.err = err;
+    return A;
+}
+
+int uwshcu_compute_member(const uwshcu_member* m, void* stream)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    if (!s.init) return UWSHCU_ERR_NOT_INITIALIZED;
+    if (!m || !member_ok(*m, s.k.ncnst)) return UWSHCU_ERR_BAD_ARGS;
+    DeviceState* d = nullptr;
+    int rc = ensure_device(&d);
+    if (rc != UWSHCU_OK) return rc;
+    return enqueue(*d, member_args(*m, s.k.ncnst, d->d_err), (cudaStream_t)stream);
+}
+
 int uwshcu_compute_device(int mix, int mkx, int iend, int ncnst, double dt, int inv, const double* ps0,
                           const double* zs0, const double* p0, const double* z0, const double* dp0,
                           const double* u0, const double* v0, const double* qv0, const double* ql0,
@@ -910,13 +953,8 @@ int uwshcu_tangent_device(const uwshcu_member* m, const uwshcu_tangent* t, void*
     if (!m || !t) return UWSHCU_ERR_BAD_ARGS;
     const int ncnst = s.k.ncnst;
     if (s.precision != UWSHCU_PREC_FP64 || ncnst > 5 || m->mkx + 1 > 64) return UWSHCU_ERR_BAD_ARGS;
-    if (bad_dims(m->mix, m->mkx, m->iend, ncnst) || (m->inv != 0 && m->inv != 1)) return UWSHCU_ERR_BAD_ARGS;
-    const void* need[] = {m->ps0, m->zs0, m->p0, m->z0, m->dp0, m->u0, m->v0, m->qv0, m->ql0, m->qi0, m->t0,
-                          m->s0, m->tr0, m->tke, m->pblh, m->cush, m->umf, m->slflx, m->qtflx, m->flxprc1,
-                          m->flxsnow1, m->qvten, m->qlten, m->qiten, m->sten, m->uten, m->vten, m->trten,
-                          m->qrten, m->qsten, m->precip, m->snow, m->evapc, m->cufrc, m->qcu, m->qlu, m->qiu,
-                          m->cbmf, m->qc, m->rliq, m->cnt, m->cnb, m->dpdry0, m->wu,
-                          t->cush, t->umf, t->slflx, t->qtflx, t->flxprc1, t->flxsnow1, t->qvten, t->qlten,
+    if (!member_ok(*m, ncnst)) return UWSHCU_ERR_BAD_ARGS;
+    const void* need[] = {t->cush, t->umf, t->slflx, t->qtflx, t->flxprc1, t->flxsnow1, t->qvten, t->qlten,
                           t->qiten, t->sten, t->uten, t->vten, t->trten, t->qrten, t->qsten, t->precip,
                           t->snow, t->evapc, t->cufrc, t->qcu, t->qlu, t->qiu, t->cbmf, t->qc, t->rliq, t->wu};
     for (const void* p : need)
@@ -924,17 +962,7 @@ int uwshcu_tangent_device(const uwshcu_member* m, const uwshcu_tangent* t, void*
     DeviceState* d = nullptr;
     int rc = ensure_device(&d);
     if (rc != UWSHCU_OK) return rc;
-    UwArgs A{};
-    A.mix = m->mix; A.mkx = m->mkx; A.iend = m->iend; A.ncnst = ncnst; A.inv = m->inv; A.dt = m->dt;
-    A.ps0 = m->ps0; A.zs0 = m->zs0; A.p0 = m->p0; A.z0 = m->z0; A.dp0 = m->dp0; A.u0 = m->u0; A.v0 = m->v0;
-    A.qv0 = m->qv0; A.ql0 = m->ql0; A.qi0 = m->qi0; A.t0 = m->t0; A.s0 = m->s0; A.tr0 = m->tr0; A.tke = m->tke;
-    A.pblh = m->pblh; A.cush = m->cush; A.umf = m->umf; A.slflx = m->slflx; A.qtflx = m->qtflx;
-    A.flxprc1 = m->flxprc1; A.flxsnow1 = m->flxsnow1; A.qvten = m->qvten; A.qlten = m->qlten;
-    A.qiten = m->qiten; A.sten = m->sten; A.uten = m->uten; A.vten = m->vten; A.trten = m->trten;
-    A.qrten = m->qrten; A.qsten = m->qsten; A.precip = m->precip; A.snow = m->snow; A.evapc = m->evapc;
-    A.cufrc = m->cufrc; A.qcu = m->qcu; A.qlu = m->qlu; A.qiu = m->qiu; A.cbmf = m->cbmf; A.qc = m->qc;
-    A.rliq = m->rliq; A.cnt = m->cnt; A.cnb = m->cnb; A.dpdry0 = m->dpdry0; A.wu = m->wu;
-    A.diag_int = m->diag_int; A.diag_real = m->diag_real; A.err = d->d_err;
+    UwArgs A = member_args(*m, ncnst, d->d_err);
     // the forward path's two-phase schedule: trigger pass, then the convecting columns
     auto launch = (m->mkx + 1 <= 32) ? uw_tl_launch_k32n5 : uw_tl_launch_k64n5;
     cudaStream_t st = (cudaStream_t)stream;
@@ -1217,14 +1245,7 @@ extern "C" int uwshcu_batch_create(int nmembers, const uwshcu_member* members, v
     size_t total = 0;
     for (int j = 0; j < nmembers; j++) {
         const uwshcu_member& m = members[j];
-        if (bad_dims(m.mix, m.mkx, m.iend, ncnst) || (m.inv != 0 && m.inv != 1)) return UWSHCU_ERR_BAD_ARGS;
-        const void* need[] = {m.ps0, m.zs0, m.p0, m.z0, m.dp0, m.u0, m.v0, m.qv0, m.ql0, m.qi0, m.t0, m.s0, m.tr0,
-                              m.tke, m.pblh, m.cush, m.umf, m.slflx, m.qtflx, m.flxprc1, m.flxsnow1, m.qvten,
-                              m.qlten, m.qiten, m.sten, m.uten, m.vten, m.trten, m.qrten, m.qsten, m.precip,
-                              m.snow, m.evapc, m.cufrc, m.qcu, m.qlu, m.qiu, m.cbmf, m.qc, m.rliq, m.cnt,
-                              m.cnb, m.dpdry0, m.wu};
-        for (const void* p : need)
-            if (!p) return UWSHCU_ERR_BAD_ARGS;
+        if (!member_ok(m, ncnst)) return UWSHCU_ERR_BAD_ARGS;
         total += (size_t)m.iend;
     }
     DeviceState* d = nullptr;
@@ -1262,18 +1283,7 @@ extern "C" int uwshcu_batch_create(int nmembers, const uwshcu_member* members, v
         const int c = cls_slot[cls];
         UwBatch& b = P->b[c];
         const int slot = b.nm++;
-        UwArgs& A = b.m[slot];
-        A = UwArgs{};
-        A.mix = m.mix; A.mkx = m.mkx; A.iend = m.iend; A.ncnst = ncnst; A.inv = m.inv; A.dt = m.dt;
-        A.ps0 = m.ps0; A.zs0 = m.zs0; A.p0 = m.p0; A.z0 = m.z0; A.dp0 = m.dp0; A.u0 = m.u0; A.v0 = m.v0;
-        A.qv0 = m.qv0; A.ql0 = m.ql0; A.qi0 = m.qi0; A.t0 = m.t0; A.s0 = m.s0; A.tr0 = m.tr0; A.tke = m.tke;
-        A.pblh = m.pblh; A.cush = m.cush; A.umf = m.umf; A.slflx = m.slflx; A.qtflx = m.qtflx;
-        A.flxprc1 = m.flxprc1; A.flxsnow1 = m.flxsnow1; A.qvten = m.qvten; A.qlten = m.qlten; A.qiten = m.qiten;
-        A.sten = m.sten; A.uten = m.uten; A.vten = m.vten; A.trten = m.trten; A.qrten = m.qrten;
-        A.qsten = m.qsten; A.precip = m.precip; A.snow = m.snow; A.evapc = m.evapc; A.cufrc = m.cufrc;
-        A.qcu = m.qcu; A.qlu = m.qlu; A.qiu = m.qiu; A.cbmf = m.cbmf; A.qc = m.qc; A.rliq = m.rliq;
-        A.cnt = m.cnt; A.cnb = m.cnb; A.dpdry0 = m.dpdry0; A.wu = m.wu; A.diag_int = m.diag_int;
-        A.diag_real = m.diag_real; A.err = P->d_err;
+        b.m[slot] = member_args(m, ncnst, P->d_err);
         b.wl[slot] = P->d_scratch + wl_off;
         wl_off += (size_t)m.iend;
     }

@@ -486,6 +486,30 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
 #define SEEDL(a, da, k) Tl(GL(a, k), T.da ? __ldg(&T.da[(size_t)RL(k) * mix + i]) : 0.0)
 #define SEEDI(a, da, k) Tl(GI(a, k), T.da ? __ldg(&T.da[(size_t)RI(k) * mix + i]) : 0.0)
 #define CNT(x) (inv ? (Tl)(mkx + 1) - (x) : (x))
+#define DLV(j, k) A.diag_level[((size_t)(j) * (mkx + 1) + (k)) * mix + i]
+// per-level diagnostics of the current state, levels bottom-up in both level orders
+// (uwshcu.F90:1945-1990 and :4383-4433)
+#define PUT_DIAG_LEVEL()                                                                                  \
+    if (A.diag_level) {                                                                                   \
+        for (int k = 0; k <= mkx; k++) {                                                                  \
+            DLV(UW_DL_UFRC, k) = tl_val(ufrc[k]);                                                                 \
+            DLV(UW_DL_QTU, k) = tl_val(qtu[k]);                                                                   \
+            DLV(UW_DL_THLU, k) = tl_val(thlu[k]);                                                                 \
+            DLV(UW_DL_THVU, k) = tl_val(thvu[k]);                                                                 \
+            DLV(UW_DL_UU, k) = tl_val(uu[k]);                                                                     \
+            DLV(UW_DL_VU, k) = tl_val(vu[k]);                                                                     \
+            DLV(UW_DL_UEMF, k) = tl_val(UEMF(k));                                                                 \
+            DLV(UW_DL_FLXRAIN, k) = tl_val(flxrain[k]);                                                           \
+            DLV(UW_DL_FLXSNOW, k) = tl_val(flxsnow[k]);                                                           \
+        }                                                                                                 \
+        for (int j = UW_DL_FER; j < UW_NDL; j++) DLV(j, 0) = tl_val(0.0);                                         \
+        for (int k = 1; k <= mkx; k++) {                                                                  \
+            DLV(UW_DL_FER, k) = tl_val(fer[k]);                                                                   \
+            DLV(UW_DL_FDR, k) = tl_val(fdr[k]);                                                                   \
+            DLV(UW_DL_DWTEN, k) = tl_val(dwten[k]);                                                               \
+            DLV(UW_DL_DITEN, k) = tl_val(diten[k]);                                                               \
+        }                                                                                                 \
+    }
 
     // ---- thread-private profiles ---------------------------------------------------------------
     Tl ps0[KP], p0[KP], dp0[KP], zs0[KP], exn0[KP], exns0[KP];
@@ -1470,7 +1494,6 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                 } while (0);
                 if (stop) ldone = true;
             }
-#undef UEMF
         }
         UW_SYNC();
         if (!stop) do {
@@ -1818,6 +1841,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
             { const Tl v_ = (rliq); A.rliq[i] = tl_val(v_); T.rliq[i] = tl_der(v_); }
             A.cnt[i] = tl_val(CNT(cnt));
             A.cnb[i] = tl_val(CNT(cnb));
+            PUT_DIAG_LEVEL();
             cin_s = cin; cinlcl_s = cinlcl; plcl_s = plcl; pinv_s = ps0[kinv - 1]; plfc_s = plfc;
             pbup_s = ps0[kbup]; ppen_s = ps0[kpen - 1] + ppen; tkeavg_s = tkeavg;
             kinv_s = kinv; klcl_s = klcl; klfc_s = klfc; krel_s = krel; kbup_s = kbup; kpen_s = kpen;
@@ -1908,6 +1932,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
         A.diag_real[UW_DR_PPEN * (size_t)mix + i] = tl_val(ps0[kpen - 1] + ppen);
         A.diag_real[UW_DR_TKEAVG * (size_t)mix + i] = tl_val(tkeavg);
     }
+    PUT_DIAG_LEVEL();
     }
 
     // (label 333, :4448-4549)
@@ -1941,6 +1966,9 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
             A.diag_real[UW_DR_CINLCL * (size_t)mix + i] = tl_val(-1.0);
             for (int j = UW_DR_PLCL; j < UW_NDR; j++) A.diag_real[j * (size_t)mix + i] = tl_val(0.0);
         }
+        if (A.diag_level)
+            for (int j = 0; j < UW_NDL; j++)
+                for (int k = 0; k <= mkx; k++) DLV(j, k) = tl_val(0.0);
         kinv = klcl = klfc = krel = kbup = kpen = 0;
     }
     if (A.diag_int) {
@@ -1984,6 +2012,9 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
 #undef TOT
 #undef TOL
 #undef TOI
+#undef DLV
+#undef PUT_DIAG_LEVEL
+#undef UEMF
 }
 
 // ---- kernels ---------------------------------------------------------------------------------------

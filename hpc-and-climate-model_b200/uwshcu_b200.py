@@ -32,6 +32,10 @@ ERR_NO_DEVICE = -4
 ERR_ALLOC = -5
 ERR_TOO_LARGE = -6
 NOALLOC_MAX_COLUMNS = 1048576
+# per-level diagnostic rows of uwshcu_member.diag_level, array (NDL, mkx + 1, mix), levels bottom-up
+DL_NAMES = ("ufrc", "qtu", "thlu", "thvu", "uu", "vu", "uemf", "flxrain", "flxsnow", "fer", "fdr",
+            "dwten", "diten")
+NDL = len(DL_NAMES)
 
 EXPORTS = ("uwshcu_init", "uwshcu_set_rpen", "uwshcu_init_default", "uwshcu_set_precision",
            "uwshcu_set_block", "uwshcu_set_schedule", "uwshcu_set_profiling",
@@ -41,7 +45,7 @@ EXPORTS = ("uwshcu_init", "uwshcu_set_rpen", "uwshcu_init_default", "uwshcu_set_
            "uwshcu_compute_device_noalloc", "uwshcu_batch_create", "uwshcu_batch_run",
            "uwshcu_batch_capture", "uwshcu_batch_autotune", "uwshcu_batch_status",
            "uwshcu_batch_destroy", "uwshcu_set_pipeline", "uwshcu_set_params",
-           "uwshcu_budget_device", "uwshcu_tangent_device")
+           "uwshcu_budget_device", "uwshcu_tangent_device", "uwshcu_compute_member")
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
@@ -210,6 +214,8 @@ class DeviceCase:
         self.out["cush"].copy_(self.cush0)
         self.diag_int = torch.zeros((8, n), dtype=torch.int32, device=device) if diag else None
         self.diag_real = torch.zeros((8, n), dtype=torch.float64, device=device) if diag else None
+        self.diag_level = (torch.zeros((NDL, mkx + 1, n), dtype=torch.float64, device=device)
+                           if diag else None)
 
     def reset_cush(self):
         self.out["cush"].copy_(self.cush0)
@@ -234,6 +240,12 @@ class DeviceCase:
             P(self.diag_int) if self.diag_int is not None else None,
             P(self.diag_real) if self.diag_real is not None else None,
             ctypes.c_void_p(st.cuda_stream))
+
+    def launch_member(self, inv=0, stream=None):
+        """Enqueue one call of uwshcu_compute_member (which also fills diag_level) on `stream`."""
+        st = stream if stream is not None else self.torch.cuda.current_stream()
+        m = member_of(self, inv)
+        return lib().uwshcu_compute_member(ctypes.byref(m), ctypes.c_void_p(st.cuda_stream))
 
     def launch_noalloc(self, inv=0, stream=None, status_bits=None):
         """Enqueue one call of uwshcu_compute_device_noalloc on `stream`; status_bits is None or a
@@ -288,6 +300,7 @@ class DeviceCase:
         if self.diag_int is not None:
             o["diag_int"] = self.diag_int.cpu().numpy()
             o["diag_real"] = self.diag_real.cpu().numpy()
+            o["diag_level"] = self.diag_level.cpu().numpy()
         return o
 
 
@@ -311,7 +324,7 @@ def eval_math_device(fn, x, y=None):
 MAX_MEMBERS = 8
 _MEMBER_PTRS = ("ps0 zs0 p0 z0 dp0 u0 v0 qv0 ql0 qi0 t0 s0 tr0 tke pblh cush umf slflx qtflx flxprc1 "
                 "flxsnow1 qvten qlten qiten sten uten vten trten qrten qsten precip snow evapc cufrc qcu "
-                "qlu qiu cbmf qc rliq cnt cnb dpdry0 wu diag_int diag_real").split()
+                "qlu qiu cbmf qc rliq cnt cnb dpdry0 wu diag_int diag_real diag_level").split()
 
 
 class Member(ctypes.Structure):
@@ -328,7 +341,7 @@ def member_of(case, inv=0):
     m.inv = inv
     m.dt = case.dt
     for name in _MEMBER_PTRS:
-        if name in ("diag_int", "diag_real"):
+        if name in ("diag_int", "diag_real", "diag_level"):
             t = getattr(case, name)
         elif name in case.out:
             t = case.out[name]

@@ -221,7 +221,35 @@ typedef struct uwshcu_member {
     double *wu;
     int *diag_int;      /* optional, as in uwshcu_compute_device */
     double *diag_real;  /* optional */
+    double *diag_level; /* optional per-level diagnostics (UWSHCU_NDL, mkx + 1, mix), see below */
 } uwshcu_member;
+
+/* Per-level diagnostics: the history fields compute_uwshcu writes for every column
+ * (uwshcu.F90:1945-1990 after the explicit-CIN fallback, :4383-4433 otherwise, zeros at the exit
+ * :4484-4529).  Array (UWSHCU_NDL, mkx + 1, mix), element (j, k, i) at (j * (mkx + 1) + k) * mix + i,
+ * levels bottom-up (k = 0 at the surface) for both level orders.  Rows 0..8 are interface fields
+ * (k = 0..mkx), rows 9..12 layer fields (k = 1..mkx; k = 0 holds 0).  The Fortran stores them
+ * top-down in its *_out arrays (ufrc_out(i, mkx:0:-1) = ufrc(0:mkx)); reverse k to get that order. */
+#define UWSHCU_DL_UFRC 0     /* updraft fractional area */
+#define UWSHCU_DL_QTU 1      /* updraft total water */
+#define UWSHCU_DL_THLU 2     /* updraft liquid-water potential temperature */
+#define UWSHCU_DL_THVU 3     /* updraft virtual potential temperature */
+#define UWSHCU_DL_UU 4       /* updraft zonal wind */
+#define UWSHCU_DL_VU 5       /* updraft meridional wind */
+#define UWSHCU_DL_UEMF 6     /* net updraft mass flux including penetrative entrainment */
+#define UWSHCU_DL_FLXRAIN 7  /* rain flux */
+#define UWSHCU_DL_FLXSNOW 8  /* snow flux */
+#define UWSHCU_DL_FER 9      /* lateral fractional entrainment rate */
+#define UWSHCU_DL_FDR 10     /* lateral fractional detrainment rate */
+#define UWSHCU_DL_DWTEN 11   /* detrained liquid water tendency */
+#define UWSHCU_DL_DITEN 12   /* detrained ice tendency */
+#define UWSHCU_NDL 13
+
+/* uwshcu_compute_device with its arguments in a member struct (ncnst from uwshcu_init), which also
+ * carries the optional per-level diagnostics.  No counterpart in the reference: compute_uwshcu
+ * writes these fields to module arrays for CAM's history output (outfld), which a C caller cannot
+ * reach.  Same status codes, stream semantics and results as uwshcu_compute_device. */
+int uwshcu_compute_member(const uwshcu_member *m, void *stream);
 
 #define UWSHCU_MAX_MEMBERS 8
 

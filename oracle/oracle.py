@@ -23,6 +23,11 @@ OUT_LAYER = ("qvten", "qlten", "qiten", "sten", "uten", "vten", "qrten", "qsten"
              "cufrc", "qcu", "qlu", "qiu", "qc")
 OUT_COL = ("precip", "snow", "cbmf", "rliq", "cnt", "cnb", "cush")
 NDI, NDR = 8, 8
+# per-level diagnostic rows: ufrc qtu thlu thvu uu vu uemf flxrain flxsnow (interfaces), fer fdr dwten
+# diten (layers, rows 1..mkx); array (NDL, mkx + 1, ncol), levels bottom-up
+NDL = 13
+DL_NAMES = ("ufrc", "qtu", "thlu", "thvu", "uu", "vu", "uemf", "flxrain", "flxsnow", "fer", "fdr",
+            "dwten", "diten")
 
 _lib = None
 _libs = {}
@@ -104,12 +109,14 @@ def alloc_outputs(mkx, ncnst, mix, cush_in):
 
 def compute(s, nthreads=0, diag=True, inv=False):
     """Run the oracle on a sounding dict (all columns, mix = iend = ncol).  Returns the output
-    dict; with diag=True also 'diag_int' (8, ncol) and 'diag_real' (8, ncol)."""
+    dict; with diag=True also 'diag_int' (8, ncol), 'diag_real' (8, ncol) and 'diag_level'
+    (13, mkx + 1, ncol)."""
     L = lib()
     mkx, ncnst, n = s["mkx"], s["ncnst"], s["ncol"]
     o = alloc_outputs(mkx, ncnst, n, s["cush"])
     di = np.zeros((NDI, n), dtype=np.int32)
     dr = np.zeros((NDR, n))
+    dl = np.zeros((NDL, mkx + 1, n))
     ci, cd = ctypes.c_int, ctypes.c_double
     if not inv:
         rc = L.uwo_compute_uwshcu(
@@ -123,7 +130,8 @@ def compute(s, nthreads=0, diag=True, inv=False):
             _p(o["precip"]), _p(o["snow"]), _p(o["evapc"]), _p(o["cufrc"]), _p(o["qcu"]),
             _p(o["qlu"]), _p(o["qiu"]), _p(o["cbmf"]), _p(o["qc"]), _p(o["rliq"]),
             _p(s["massflx_sh"]), _p(o["cnt"]), _p(o["cnb"]), _p(s["dpdry0"]), _p(o["wu"]),
-            di.ctypes.data_as(_I) if diag else None, _p(dr) if diag else None, ci(nthreads))
+            di.ctypes.data_as(_I) if diag else None, _p(dr) if diag else None,
+            _p(dl) if diag else None, ci(nthreads))
     else:
         z = np.zeros(n)
         rc = L.uwo_compute_uwshcu_inv(
@@ -143,6 +151,7 @@ def compute(s, nthreads=0, diag=True, inv=False):
     if diag:
         o["diag_int"] = di
         o["diag_real"] = dr
+        o["diag_level"] = dl
     return o
 
 

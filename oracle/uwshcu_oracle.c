@@ -585,7 +585,25 @@ typedef struct {
     const double *qw0;
     int *diag_int;
     double *diag_real;
+    double *diag_level;
 } uwo_io;
+
+/* Per-level diagnostics (the Fortran's history fields, uwshcu.F90:4383-4433), array
+ * (UWO_NDL, mkx+1, mix), levels bottom-up (k = 0..mkx as in compute_uwshcu) for both entries;
+ * layer fields use rows 1..mkx and leave row 0 at zero. */
+enum { UWO_DL_UFRC, UWO_DL_QTU, UWO_DL_THLU, UWO_DL_THVU, UWO_DL_UU, UWO_DL_VU, UWO_DL_UEMF,
+       UWO_DL_FLXRAIN, UWO_DL_FLXSNOW, UWO_DL_FER, UWO_DL_FDR, UWO_DL_DWTEN, UWO_DL_DITEN, UWO_NDL };
+
+static void put_diag_level(const uwo_io *A, int i, int mkx, const double *const *f)
+{
+    int j, k;
+    if (!A->diag_level) return;
+    for (j = 0; j < UWO_NDL; j++)
+        for (k = 0; k <= mkx; k++) {
+            const int layer = j >= UWO_DL_FER;
+            A->diag_level[((size_t)j * (mkx + 1) + k) * A->mix + (i - 1)] = (layer && k == 0) ? 0.0 : (f ? f[j][k] : 0.0);
+        }
+}
 
 /* Fortran (mix,0:mkx), (mix,mkx) and (mix,mkx,ncnst) element addresses; i and k as in Fortran. */
 #define AI(a, i, k) (a)[(size_t)(k) * (size_t)A->mix + (size_t)((i) - 1)]
@@ -668,6 +686,12 @@ static int uw_column(const uwo_io *A, int i)
         sten_s[mkx + 1], evapc_s[mkx + 1], uten_s[mkx + 1], vten_s[mkx + 1], cufrc_s[mkx + 1],
         qcu_s[mkx + 1], qlu_s[mkx + 1], qiu_s[mkx + 1], qc_s[mkx + 1], umf_s[mkx + 1],
         slflx_s[mkx + 1], qtflx_s[mkx + 1], trten_s[ncnst + 1][mkx + 1];
+    /* iteration-1 copies of the per-level diagnostics (:919-931) */
+    double ufrc_s[mkx + 1], qtu_s[mkx + 1], thlu_s[mkx + 1], thvu_s[mkx + 1], uu_s[mkx + 1], vu_s[mkx + 1],
+        uemf_s[mkx + 1], flxrain_s[mkx + 1], flxsnow_s[mkx + 1], fer_s[mkx + 1], fdr_s[mkx + 1],
+        dwten_s[mkx + 1], diten_s[mkx + 1];
+    const double *const diag_s[UWO_NDL] = {ufrc_s, qtu_s, thlu_s, thvu_s, uu_s, vu_s, uemf_s, flxrain_s,
+                                           flxsnow_s, fer_s, fdr_s, dwten_s, diten_s};
     double cush_s = 0, precip_s = 0, snow_s = 0, cin_s = 0, rliq_s = 0, cbmf_s = 0, cnt_s = 0,
            cnb_s = 0, cinlcl_s = 0, plcl_s = 0, plfc_s = 0, pinv_s = 0, pbup_s = 0, ppen_s = 0,
            tkeavg_s = 0;
@@ -1184,6 +1208,7 @@ static int uw_column(const uwo_io *A, int i)
                     dr[UWO_DR_PPEN * ds] = ppen_s;
                     dr[UWO_DR_TKEAVG * ds] = tkeavg_s;
                 }
+                put_diag_level(A, i, mkx, diag_s);
                 kinv = kinv_s;
                 klcl = klcl_s;
                 klfc = klfc_s;
@@ -2032,6 +2057,19 @@ static int uw_column(const uwo_io *A, int i)
                 umf_s[k] = umf[k];
                 slflx_s[k] = slflx[k];
                 qtflx_s[k] = qtflx[k];
+                ufrc_s[k] = ufrc[k];
+                qtu_s[k] = qtu[k];
+                thlu_s[k] = thlu[k];
+                thvu_s[k] = thvu[k];
+                uu_s[k] = uu[k];
+                vu_s[k] = vu[k];
+                uemf_s[k] = uemf[k];
+                flxrain_s[k] = flxrain[k];
+                flxsnow_s[k] = flxsnow[k];
+                fer_s[k] = fer[k];
+                fdr_s[k] = fdr[k];
+                dwten_s[k] = dwten[k];
+                diten_s[k] = diten[k];
             }
             precip_s = precip;
             snow_s = snow;
@@ -2139,6 +2177,11 @@ static int uw_column(const uwo_io *A, int i)
         dr[UWO_DR_PPEN * ds] = ps0[kpen - 1] + ppen;
         dr[UWO_DR_TKEAVG * ds] = tkeavg;
     }
+    {
+        const double *const fin[UWO_NDL] = {ufrc, qtu, thlu, thvu, uu, vu, uemf, flxrain, flxsnow, fer, fdr,
+                                            dwten, diten};
+        put_diag_level(A, i, mkx, fin);
+    }
 
 l333:
     if (id_exit) {
@@ -2179,6 +2222,7 @@ l333:
             dr[UWO_DR_CINLCL * ds] = -1.0;
             for (k = UWO_DR_PLCL; k < UWO_NDR; k++) dr[k * ds] = 0.0;
         }
+        put_diag_level(A, i, mkx, 0);
         kinv = klcl = klfc = krel = kbup = kpen = 0;
     }
     if (A->diag_int) {
@@ -2293,7 +2337,7 @@ int uwo_compute_uwshcu(int mix, int mkx, int iend, int ncnst, double dt,
                        double *snow, double *evapc, double *cufrc, double *qcu, double *qlu,
                        double *qiu, double *cbmf, double *qc, double *rliq, const double *massflx_sh,
                        double *cnt, double *cnb, const double *dpdry0, double *wu,
-                       int *diag_int, double *diag_real, int nthreads)
+                       int *diag_int, double *diag_real, double *diag_level, int nthreads)
 {
     int st = 0, i;
     int nthr = nthreads > 0 ? nthreads : UWO_MAXTHREADS();
@@ -2335,7 +2379,7 @@ int uwo_compute_uwshcu(int mix, int mkx, int iend, int ncnst, double dt,
         A.qrten = qrten; A.qsten = qsten; A.precip = precip; A.snow = snow; A.evapc = evapc;
         A.cufrc = cufrc; A.qcu = qcu; A.qlu = qlu; A.qiu = qiu; A.cbmf = cbmf; A.qc = qc;
         A.rliq = rliq; A.cnt = cnt; A.cnb = cnb; A.dpdry0 = dpdry0; A.wu = wu; A.qw0 = qwcol;
-        A.diag_int = diag_int; A.diag_real = diag_real;
+        A.diag_int = diag_int; A.diag_real = diag_real; A.diag_level = diag_level;
         s = uw_column(&A, i);
         if (s > st) st = s;
     }
@@ -2402,7 +2446,7 @@ int uwo_compute_uwshcu_inv(int mix, int mkx, int iend, int ncnst, double dt,
                             t0, s0, tr0, tke, cf, ccf, pblh, cush, umf, slflx, qtflx, fp1, fs1,
                             qvten, qlten, qiten, sten, uten, vten, trten, qrten, qsten, precip, snow,
                             evapc, cufrc, qcu, qlu, qiu, cbmf, qc, rliq, massflx_sh, cnt, cnb, dpdry0,
-                            wu, NULL, NULL, nthreads);
+                            wu, NULL, NULL, NULL, nthreads);
     for (i = 0; i < iend; i++) {
         cnti[i] = mkx + 1 - cnt[i];
         cnbi[i] = mkx + 1 - cnb[i];

@@ -58,6 +58,10 @@ void uwo_get_estbl(double *out250);
  * tmelt pcf1..pcf5 (22 values). */
 void uwo_get_consts(double *out22);
 
+/* Per-level diagnostics (the Fortran's history fields ufrc, qtu, thlu, thvu, uu, vu, uemf, flxrain,
+ * flxsnow on interfaces and fer, fdr, dwten, diten on layers; uwshcu.F90:4383-4433 and the explicit-CIN
+ * copies :1945-1989): optional diag_level array (13, mkx+1, mix), levels bottom-up k = 0..mkx, layer
+ * fields in rows 1..mkx. */
 /* compute_uwshcu (uwshcu.F90:478-492) with the Fortran argument list; qsat/lchnk are not needed
  * (the built-in fqsatd semantics are used).  Optional diagnostics may be null.  nthreads <= 0 uses
  * the OpenMP default.  Returns 0, or a positive status for the reference's endrun cases
@@ -75,7 +79,7 @@ int uwo_compute_uwshcu(int mix, int mkx, int iend, int ncnst, double dt,
                        double *snow, double *evapc, double *cufrc, double *qcu, double *qlu,
                        double *qiu, double *cbmf, double *qc, double *rliq, const double *massflx_sh,
                        double *cnt, double *cnb, const double *dpdry0, double *wu,
-                       int *diag_int, double *diag_real, int nthreads);
+                       int *diag_int, double *diag_real, double *diag_level, int nthreads);
 
 /* compute_uwshcu_inv (uwshcu.F90:251-476): CAM top-down level order in and out. */
 int uwo_compute_uwshcu_inv(int mix, int mkx, int iend, int ncnst, double dt,

@@ -1,7 +1,7 @@
 """Batched uneven launches (uwshcu_batch_*): members with different level counts and trigger
 fractions in one trigger launch and one persistent worklist launch per level class.  Every member's
-outputs must be the bits uwshcu_compute_device gives for that member alone, for a plain run, a
-CUDA-graph replay and a run with the autotuned launch shape."""
+outputs, per-level diagnostics included, must be the bits uwshcu_compute_member gives for that
+member alone, for a plain run, a CUDA-graph replay and a run with the autotuned launch shape."""
 import ctypes
 
 import numpy as np
@@ -33,6 +33,7 @@ def _poison(case):
         t.fill_(-777.0)
     case.diag_int.fill_(-7)
     case.diag_real.fill_(-777.0)
+    case.diag_level.fill_(-777.0)
     case.reset_cush()
 
 
@@ -49,7 +50,7 @@ def test_batch_matches_single_member_calls(uw, cuda, prec):
     ref, bat = _cases(uw)
     want = []
     for r in ref:
-        assert r.launch() == 0, uw.last_cuda_error()
+        assert r.launch_member() == 0, uw.last_cuda_error()
         assert r.status() == 0
         want.append(r.outputs_numpy())
     trig = [float(np.mean(w["cush"] != -1.0)) for w in want]
