@@ -398,7 +398,7 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=32768)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--schedule", default="two-phase", choices=["two-phase", "single-pass"])
+    ap.add_argument("--schedule", default="two-phase", choices=["two-phase", "sorted", "single-pass"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fast", "mixed"],
                     help="fp64: bit-exact (default); fast: FP64 with the early-stopping conden; "
                          "mixed: FP32 bulk with FP64 islands")
@@ -427,8 +427,10 @@ def main():
     assert uw.init_default() == 0
     prec = {"fp64": uw.PREC_FP64, "fast": uw.PREC_FAST, "mixed": uw.PREC_MIXED}[args.precision]
     assert uw.set_precision(prec) == 0, "precision %s not available" % args.precision
-    two_phase = args.schedule == "two-phase"
-    assert uw.set_schedule(uw.SCHED_TWO_PHASE if two_phase else uw.SCHED_SINGLE_PASS) == 0
+    two_phase = args.schedule in ("two-phase", "sorted")
+    sorted_pass = args.schedule == "sorted" and args.precision != "mixed"
+    assert uw.set_schedule({"two-phase": uw.SCHED_TWO_PHASE, "sorted": uw.SCHED_SORTED,
+                            "single-pass": uw.SCHED_SINGLE_PASS}[args.schedule]) == 0
     n = args.ncol
     s = soundings.make_soundings(n, PVER, seed=shard_seed(rank), rh_pbl=RH_PBL)
     case = uw.DeviceCase(s)
@@ -552,7 +554,8 @@ def main():
                                 if (phases and prec == uw.PREC_FP64) else None,
                      "peak_kind": peak_kind,
                      "kernel": "uwshcu_%s_kernel<32,5,%s>" % ({"fp64": "fp64", "fast": "fast", "mixed": "mixed"}[args.precision],
-                                                              "UW_MODE_LIST" if phases else "UW_MODE_ALL"),
+                                                              ("UW_MODE_LIST1 + UW_MODE_RESUME" if sorted_pass else "UW_MODE_LIST")
+                                                              if phases else "UW_MODE_ALL"),
                      "kernel_ms": kernel_ms, "columns_per_launch": ncols_dom,
                      "fp64": fp64, "fp64_algorithmic": fp64_alg,
                      "note": "branchy FP64 column physics: neither HBM nor the FP64 pipe is the bound "
@@ -562,7 +565,8 @@ def main():
         "schedule": args.schedule,
         "precision": args.precision,
         "phases": phases,
-        "gpu_launches": args.steps * (2 if two_phase else 1),
+        # trigger + worklist; sorted: trigger, first worklist launch, 3 sort kernels, second launch
+        "gpu_launches": args.steps * ((6 if sorted_pass else 2) if two_phase else 1),
         "status": st,
     }
     if e2e is not None:

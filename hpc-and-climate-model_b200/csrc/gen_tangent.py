@@ -54,8 +54,8 @@ def main():
             "#define TOT(m, k) T.trten[((size_t)((m) - 1) * mkx + RL(k)) * mix + i]\n"
             "#define SEEDL(a, da, k) Tl(GL(a, k), T.da ? __ldg(&T.da[(size_t)RL(k) * mix + i]) : 0.0)\n"
             "#define SEEDI(a, da, k) Tl(GI(a, k), T.da ? __ldg(&T.da[(size_t)RI(k) * mix + i]) : 0.0)")
-    s = rep(s, "t0[k] = GL(t0, k);", "t0[k] = SEEDL(t0, dt0, k);", 2)
-    s = rep(s, "qv0[k] = GL(qv0, k);", "qv0[k] = SEEDL(qv0, dqv0, k);", 2)
+    s = rep(s, "t0[k] = GL(t0, k);", "t0[k] = SEEDL(t0, dt0, k);", 3)
+    s = rep(s, "qv0[k] = GL(qv0, k);", "qv0[k] = SEEDL(qv0, dqv0, k);", 3)
     s = rep(s, "tkeavg = tkeavg + dpi * GI(tke, k);", "tkeavg = tkeavg + dpi * SEEDI(tke, dtke, k);")
     s = rep(s, "const Tl pblh = __ldg(&A.pblh[i]);",
             "const Tl pblh = Tl(__ldg(&A.pblh[i]), T.dpblh ? __ldg(&T.dpblh[i]) : 0.0);")
@@ -85,8 +85,10 @@ def main():
             "                 const __grid_constant__ UwTangent T)")
     s = rep(s, "uw_column<KP, NC, MODE, 0>(A, tbl, i, active, wl, wl_count);",
             "uw_column<KP, NC, MODE, 0>(A, tbl, i, active, wl, wl_count, T);")
-    s = s.replace("__launch_bounds__(128, MODE == UW_MODE_LIST ? 4 : (MODE == UW_MODE_TRIGGER ? 5 : 3))",
-                  "__launch_bounds__(128)")
+    s = rep(s, "__launch_bounds__(128, UW_MODE_IS_LIST(MODE) ? 4 : (MODE == UW_MODE_TRIGGER ? 5 : 3))",
+            "__launch_bounds__(128)")
+    # the split worklist pass (UW_MODE_LIST1 / UW_MODE_RESUME) is FP64 and FAST only: no state copies here
+    s = re.sub(r"\n[ ]*UW_(SAVE|LOAD)_STATE\([^;]*\);", "", s)
     for u in ("TOI", "TOL", "TOT", "SEEDL", "SEEDI"):
         s = s.replace("#undef OT\n", "#undef OT\n#undef %s\n" % u, 1)
     header = ("// uwshcu_tl_kernel.cuh -- tangent-linear (forward-mode) kernel of compute_uwshcu\n"

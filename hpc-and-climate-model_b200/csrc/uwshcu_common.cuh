@@ -96,6 +96,20 @@ struct UwConst {
     int wet[UW_NCMAX];
 };
 
+// Hand-off between the two launches of the split worklist pass (UW_MODE_LIST1 -> UW_MODE_RESUME),
+// one region of device memory per stream that runs the pass.  Slots beyond cap are not handed off:
+// those columns finish in the first launch.
+#define UW_HAND_KEYS 64   // sort keys: 63 - iteration-1 updraft depth (deepest first)
+struct UwHand {
+    double* state;   // (uw_state_words, cap): word w of slot s at state[w * cap + s]
+    int cap;         // slots
+    int* count;      // slots requested by the first launch (may exceed cap)
+    int* col;        // column of each slot
+    int* key;        // sort key of each slot
+    int* order;      // slots in key order (counting sort)
+    int* hist;       // UW_HAND_KEYS counters of the sort
+};
+
 // Pointers of one compute_uwshcu call (device addresses), in the Fortran argument order.
 struct UwArgs {
     int mix, mkx, iend, ncnst;
@@ -113,6 +127,7 @@ struct UwArgs {
     double *diag_real;   // optional (UW_NDR, mix)
     double *diag_level;  // optional (UW_NDL, mkx + 1, mix)
     unsigned int *err;   // device error word
+    const UwHand *hand;  // UW_MODE_LIST1 / UW_MODE_RESUME only: device copy of the hand-off region
 };
 
 // ---- batched launches --------------------------------------------------------------------------

@@ -32,6 +32,7 @@
 #include <math.h>
 #include "uwshcu_common.cuh"
 #include "uw_math.h"
+#include "uw_state.cuh"
 
 namespace {
 
@@ -456,25 +457,36 @@ __device__ double findsp_point(double q, double t, double p, unsigned int& errbi
 //                    Columns that leave the scheme on the way write their final outputs (the
 //                    label-333 zeroes); the others are appended to the worklist `wl` (warp ballot,
 //                    one atomicAdd per warp) and write nothing;
-//   UW_MODE_LIST     thread t runs the whole scheme for column wl[t], t < *wl_count.
+//   UW_MODE_LIST     thread t runs the whole scheme for column wl[t], t < *wl_count;
+//   UW_MODE_LIST1    as UW_MODE_LIST, except that a column taking the implicit-CIN branch of
+//                    iteration 2 (uwshcu.F90:1759-1889) stores its state in the hand-off region
+//                    A.hand (a free slot permitting) and stops there;
+//   UW_MODE_RESUME   thread t continues hand-off slot order[t] from that point to the end.
 // The worklist path recomputes the phase-1 part of a convecting column instead of storing it: the
-// heavy buoyancy-sorting work then runs in warps made only of convecting columns.
+// heavy buoyancy-sorting work then runs in warps made only of convecting columns.  The split at the
+// CIN decision drops the columns that end in iteration 1 or take the explicit-CIN branch from the
+// warps of iteration 2, and sorts the rest by their iteration-1 updraft depth, which predicts the
+// iteration-2 depth (lanes whose updraft has stopped wait for the deepest one in their warp).
 #define UW_MODE_ALL 0
 #define UW_MODE_TRIGGER 1
 #define UW_MODE_LIST 2
+#define UW_MODE_LIST1 3
+#define UW_MODE_RESUME 4
+#define UW_MODE_IS_LIST(m) ((m) == UW_MODE_LIST || (m) == UW_MODE_LIST1 || (m) == UW_MODE_RESUME)
 
 // The column code and the kernels have internal linkage: every unit that includes a column-code
 // header (FP64, fast, mixed, tangent) carries its own copies under the same names.
 namespace {
 
-// One column per lane: column i of A when `active`.  All 32 lanes of the warp must call it together
-// (it starts with a warp ballot).  `tbl` is the saturation table in shared memory.  In
+// One column per lane: column i_in of A when `active` (in UW_MODE_RESUME, i_in is a hand-off slot).
+// All 32 lanes of the warp must call it together (it starts with a warp ballot).  `tbl` is the saturation table in shared memory.  In
 // UW_MODE_TRIGGER, convecting columns are appended to wl / *wl_count.
 // FAST = 1: the fast-FP64 precision mode (conden_fast in place of conden), not bit-exact.
 template <int KP, int NC, int MODE, int FAST>
-__device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restrict__ tbl, const int i,
+__device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restrict__ tbl, const int i_in,
                                           const bool active, int* __restrict__ wl, int* __restrict__ wl_count)
 {
+    const int i = (MODE == UW_MODE_RESUME && active) ? A.hand->col[i_in] : i_in;
 #define CONDEN(...) (FAST ? conden_fast(__VA_ARGS__) : conden(__VA_ARGS__))
     bool cand = false;
     // lanes of this warp that run a column; UW_SYNC() joins them where every one of them arrives
@@ -562,9 +574,14 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
     double cbmf = 0, wlcl = 0, ufrclcl = 0, ppen = 0, precip = 0, snow = 0, rliq = 0, cush, cnt, cnb;
     double thlu_top = 0, qtu_top = 0, exntop = 1.0, drage = 0, bogbot = 0, bogtop = 0, rho0j = 0,
            wtwb = 0, wtw = 0, xs1 = 0, xs2 = 0, xc1 = 0, xc2 = 0;
-    double thj, qvj, qlj, qij;
+    double thj = 0, qvj = 0, qlj = 0, qij = 0;
     double rainflx = 0, snowflx = 0;
     (void)kinv_o_d;
+    const double pblh = __ldg(&A.pblh[i]);
+    double tscaleh_r = 0.0;   // UW_MODE_RESUME: tscaleh of the iteration handed over
+    bool handed = false;      // UW_MODE_LIST1: the column continues in UW_MODE_RESUME
+
+    if constexpr (MODE != UW_MODE_RESUME) {   // uniform
 
     // ---- output initialisation (uwshcu.F90:1087-1124) ------------------------------------------
     if (MODE != UW_MODE_TRIGGER) {
@@ -610,7 +627,6 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
         thl0[k] = (t0[k] - xlv * ql0[k] / cp - xls * qi0[k] / cp) / exn0[k];
         qw0[k] = findsp_point(qv0[k], t0[k], p0[k], errbits, tbl);
     }
-    const double pblh = __ldg(&A.pblh[i]);
     cush = A.cush[i];
     {
         double tmpf[KP];
@@ -676,6 +692,65 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
     cnt = (double)mkx;
     cnb = 0.0;
     }
+    } else {   // uniform
+        // the state UW_MODE_LIST1 stored at the implicit-CIN branch of iteration 2 (uw_state.cuh),
+        // and the arrays that the set-up and that branch's restore build from the inputs, rebuilt
+        // with the same operations
+        UW_LOAD_STATE(A.hand->state + i_in, (size_t)A.hand->cap, tscaleh_r);
+        for (int k = 0; k <= mkx; k++) {
+            ps0[k] = GI(ps0, k);
+            zs0[k] = GI(zs0, k);
+        }
+        for (int k = 1; k <= mkx; k++) {
+            p0[k] = GL(p0, k);
+            dp0[k] = GL(dp0, k);
+        }
+        {
+            double tmpf[KP];
+            for (int k = 1; k <= mkx; k++) tmpf[k] = GL(u0, k);
+            slope<KP>(mkx, tmpf, p0, ssu0);
+            for (int k = 1; k <= mkx; k++) tmpf[k] = GL(v0, k);
+            slope<KP>(mkx, tmpf, p0, ssv0);
+            for (int m = 1; m <= ncnst; m++) {
+                for (int k = 1; k <= mkx; k++) tmpf[k] = GT(m, k);
+                slope<KP>(mkx, tmpf, p0, sstr0[m - 1]);
+            }
+        }
+        for (int k = 1; k <= mkx; k++) {
+            qv0[k] = GL(qv0, k);
+            ql0[k] = GL(ql0, k);
+            qi0[k] = GL(qi0, k);
+            t0[k] = GL(t0, k);
+            s0[k] = GL(s0, k);
+            qt0[k] = (qv0[k] + ql0[k] + qi0[k]);
+            thl0[k] = (t0[k] - xlv * ql0[k] / cp - xls * qi0[k] / cp) / exn0[k];
+            thv0bot[k] = thv0bot_o[k];
+            thv0top[k] = thv0top_o[k];
+            thvl0bot[k] = thvl0bot_o[k];
+            thvl0top[k] = thvl0top_o[k];
+        }
+        slope<KP>(mkx, thl0, p0, ssthl0);
+        slope<KP>(mkx, qt0, p0, ssqt0);
+        for (int k = 0; k <= mkx; k++) {
+            umf[k] = 0.0; emf[k] = 0.0; slflx[k] = 0.0; qtflx[k] = 0.0; uflx[k] = 0.0;
+            vflx[k] = 0.0; ufrc[k] = 0.0; thlu[k] = 0.0; qtu[k] = 0.0; uu[k] = 0.0;
+            vu[k] = 0.0; wu[k] = 0.0; thvu[k] = 0.0; thlu_emf[k] = 0.0; qtu_emf[k] = 0.0;
+            uu_emf[k] = 0.0; vu_emf[k] = 0.0;
+            for (int m = 0; m < ncnst; m++) {
+                trflx[m][k] = 0.0;
+                tru[m][k] = 0.0;
+                tru_emf[m][k] = 0.0;
+            }
+        }
+        for (int k = 1; k <= mkx; k++) {
+            qvten[k] = 0.0; qlten[k] = 0.0; qiten[k] = 0.0; sten[k] = 0.0; uten[k] = 0.0;
+            vten[k] = 0.0; qrten[k] = 0.0; qsten[k] = 0.0; dwten[k] = 0.0; diten[k] = 0.0;
+            evapc[k] = 0.0; cufrc[k] = 0.0; qcu[k] = 0.0; qlu[k] = 0.0; qiu[k] = 0.0;
+            fer[k] = 0.0; fdr[k] = 0.0; qc[k] = 0.0; qc_l[k] = 0.0; qc_i[k] = 0.0;
+            qtten[k] = 0.0; slten[k] = 0.0;
+            for (int m = 0; m < ncnst; m++) trten[m][k] = 0.0;
+        }
+    }
 
     UW_SYNC();
 
@@ -687,8 +762,9 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
     // sections.  (Lanes that leave a loop at different iterations otherwise run apart for the rest
     // of the column: the worklist kernel ran with 1.9 of 32 lanes active.)  Loops marked `uniform`
     // have the same trip count on every live lane; UW_SYNC() appears only directly inside them.
-    for (int iter = 1; iter <= (MODE == UW_MODE_TRIGGER ? 1 : 2); iter++) {   // uniform
-        double tscaleh = 0.0;
+    for (int iter = (MODE == UW_MODE_RESUME ? 2 : 1); iter <= (MODE == UW_MODE_TRIGGER ? 1 : 2); iter++) {   // uniform
+        double tscaleh = tscaleh_r;
+        if constexpr (MODE != UW_MODE_RESUME) {   // uniform
         if (!stop) do {
         tscaleh = cush;
         cush = -1.0;
@@ -923,6 +999,30 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
 
         } while (0);
         UW_SYNC();
+        }   // MODE != UW_MODE_RESUME
+        if constexpr (MODE == UW_MODE_LIST1) {   // uniform
+        if (iter == 2) {   // uniform
+            // implicit CIN: the rest of the column runs in the UW_MODE_RESUME launch; without a free
+            // slot it goes on here
+            const unsigned want = __ballot_sync(live, !stop);
+            if (want) {
+                const UwHand& H = *A.hand;
+                const unsigned ln = threadIdx.x & 31u;
+                const int leader = __ffs(want) - 1;
+                int base = 0;
+                if ((int)ln == leader) base = atomicAdd(H.count, __popc(want));
+                base = __shfl_sync(live, base, leader);
+                const int slot = base + __popc(want & ((1u << ln) - 1u));
+                if (!stop && slot < H.cap) {
+                    H.col[slot] = i;
+                    H.key[slot] = UW_HAND_KEYS - 1 - MN(MX(kpen_s - krel_s, 0), UW_HAND_KEYS - 1);
+                    UW_SAVE_STATE(H.state + slot, (size_t)H.cap, tscaleh);
+                    handed = true;
+                    stop = true;
+                }
+            }
+        }
+        }
         // ---- release level and closure (:2035-2184) ------------------------------------------
         if (!stop) do {
         if (klcl < kinv) {
@@ -1952,7 +2052,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
     }
 
     // (label 333, :4448-4549)
-    if (!cand) {
+    if (!cand && !handed) {
     if (id_exit) {
         xflags |= UW_X_UWCU;
         for (int k = 0; k <= mkx; k++) {
@@ -2034,7 +2134,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
 // 168): the extra resident warps hide more FP64 and local-memory latency than the added spills
 // cost (-10 % time on the benchmark workload).
 template <int KP, int NC, int MODE>
-__global__ void __launch_bounds__(128, MODE == UW_MODE_LIST ? 4 : (MODE == UW_MODE_TRIGGER ? 5 : 3))
+__global__ void __launch_bounds__(128, UW_MODE_IS_LIST(MODE) ? 4 : (MODE == UW_MODE_TRIGGER ? 5 : 3))
 uwshcu_fp64_kernel(const __grid_constant__ UwArgs A, int* __restrict__ wl, int* __restrict__ wl_count)
 {
     __shared__ double tbl[UW_TBL];
@@ -2044,9 +2144,13 @@ uwshcu_fp64_kernel(const __grid_constant__ UwArgs A, int* __restrict__ wl, int* 
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     int i;
     bool active;
-    if (MODE == UW_MODE_LIST) {
+    if (MODE == UW_MODE_LIST || MODE == UW_MODE_LIST1) {
         active = tid < *wl_count;
         i = active ? wl[tid] : 0;
+    } else if (MODE == UW_MODE_RESUME) {
+        const int n = MN(*A.hand->count, A.hand->cap);
+        active = tid < n;
+        i = active ? A.hand->order[tid] : 0;   // a hand-off slot
     } else {
         active = tid < A.iend;
         i = tid;
@@ -2113,7 +2217,7 @@ __global__ void __launch_bounds__(128, MINB) uwshcu_batch_list(const __grid_cons
 
 // The fast-FP64 precision mode: same launch shapes as uwshcu_fp64_kernel.
 template <int KP, int NC, int MODE>
-__global__ void __launch_bounds__(128, MODE == UW_MODE_LIST ? 4 : (MODE == UW_MODE_TRIGGER ? 5 : 3))
+__global__ void __launch_bounds__(128, UW_MODE_IS_LIST(MODE) ? 4 : (MODE == UW_MODE_TRIGGER ? 5 : 3))
 uwshcu_fast_kernel(const __grid_constant__ UwArgs A, int* __restrict__ wl, int* __restrict__ wl_count)
 {
     __shared__ double tbl[UW_TBL];
@@ -2123,9 +2227,13 @@ uwshcu_fast_kernel(const __grid_constant__ UwArgs A, int* __restrict__ wl, int* 
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     int i;
     bool active;
-    if (MODE == UW_MODE_LIST) {
+    if (MODE == UW_MODE_LIST || MODE == UW_MODE_LIST1) {
         active = tid < *wl_count;
         i = active ? wl[tid] : 0;
+    } else if (MODE == UW_MODE_RESUME) {
+        const int n = MN(*A.hand->count, A.hand->cap);
+        active = tid < n;
+        i = active ? A.hand->order[tid] : 0;   // a hand-off slot
     } else {
         active = tid < A.iend;
         i = tid;

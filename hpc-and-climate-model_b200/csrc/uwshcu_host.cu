@@ -18,6 +18,7 @@
 
 #include "uwshcu.h"
 #include "uwshcu_common.cuh"
+#include "uw_state.cuh"
 #include "uw_math.h"
 
 #define UW_DECL(KP, NC)                                                                              \
@@ -63,7 +64,10 @@ UW_DECL_MIXED(64, 5)
 namespace {
 
 constexpr int kMaxDev = 16;
-constexpr int kModeAll = 0, kModeTrigger = 1, kModeList = 2;
+constexpr int kModeAll = 0, kModeTrigger = 1, kModeList = 2, kModeList1 = 3, kModeResume = 4;
+// Largest hand-off region of the split worklist pass (bytes of column state per region); a call
+// with more implicit-CIN columns than fit finishes the rest in the first launch.
+constexpr size_t kHandBytes = (size_t)4 << 30;
 
 cudaError_t set_constants_all(const UwConst* k, const double* tbl)
 {
@@ -104,6 +108,12 @@ cudaError_t launch_mode(const UwArgs* a, int prec, int mode, int* wl, int* wl_co
     return cudaErrorInvalidValue;
 }
 
+// One hand-off region of the split worklist pass: [UwHand][count, hist][col][key][order][state].
+struct HandRegion {
+    char* base = nullptr;
+    size_t cap = 0, words = 0;
+};
+
 struct DeviceState {
     unsigned uploaded_gen = 0;   // generation of the constants in this device's __constant__ bank
     unsigned int* d_err = nullptr;
@@ -124,6 +134,8 @@ struct DeviceState {
     static constexpr int kPipe = 8;
     cudaStream_t pipe[kPipe] = {};
     std::vector<cudaEvent_t> done;   // one per chunk, grown on demand
+    // hand-off regions of the split worklist pass: [0] device-array calls, [1 + j] pipe stream j
+    HandRegion hand[1 + kPipe];
 };
 
 struct State {
@@ -134,6 +146,7 @@ struct State {
     double tbl[UW_TBL];
     int precision = UWSHCU_PREC_FP64;
     int schedule = UWSHCU_SCHED_TWO_PHASE;
+    int hand_slots = 0;          // cap of the hand-off slots per region (0: by kHandBytes only)
     int block = 128;
     bool profiling = false;
     int chunk_columns = 32768;   // host-array calls: columns per pipeline chunk (0: one chunk)
@@ -307,6 +320,104 @@ int grow_worklist(DeviceState& d, size_t ncol)
     return UWSHCU_OK;
 }
 
+// ---- split worklist pass -----------------------------------------------------------------------
+// Counting sort of the hand-off slots by key: histogram, exclusive scan, scatter.  The order inside
+// a key is that of the atomics; a column's result does not depend on which columns share its warp.
+__global__ void hand_hist_kernel(const UwHand* __restrict__ H)
+{
+    const int n = min(*H->count, H->cap);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+        atomicAdd(&H->hist[H->key[t]], 1);
+}
+
+__global__ void hand_scan_kernel(const UwHand* __restrict__ H)
+{
+    if (threadIdx.x != 0) return;
+    int acc = 0;
+    for (int b = 0; b < UW_HAND_KEYS; b++) {
+        const int c = H->hist[b];
+        H->hist[b] = acc;
+        acc += c;
+    }
+}
+
+__global__ void hand_scatter_kernel(const UwHand* __restrict__ H)
+{
+    const int n = min(*H->count, H->cap);
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+        H->order[atomicAdd(&H->hist[H->key[t]], 1)] = t;
+}
+
+// Hand-off region r sized for calls of iend columns with mkx levels and ncnst tracers; nullptr when
+// the device has no room for it (the caller then runs the unsplit worklist pass).
+const UwHand* hand_region(DeviceState& d, int r, int iend, int mkx, int ncnst)
+{
+    HandRegion& h = d.hand[r];
+    const size_t words = uw_state_words(mkx, ncnst);
+    size_t cap = std::min((size_t)iend, kHandBytes / (words * sizeof(double)));
+    if (S().hand_slots > 0) cap = std::min(cap, (size_t)S().hand_slots);
+    cap = std::max(cap, (size_t)32);
+    if (S().hand_slots > 0 && h.base && h.cap > cap) {   // a smaller limit applies to this region now
+        cudaFree(h.base);
+        h = HandRegion{};
+    }
+    if (h.base && h.cap >= cap && h.words >= words) return reinterpret_cast<const UwHand*>(h.base);
+    cap = std::max(cap, h.cap);
+    const size_t nw = std::max(words, h.words);
+    auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t o_cnt = up(sizeof(UwHand)), o_col = o_cnt + up((1 + UW_HAND_KEYS) * sizeof(int)),
+                 o_key = o_col + up(cap * sizeof(int)), o_ord = o_key + up(cap * sizeof(int)),
+                 o_st = o_ord + up(cap * sizeof(int)), bytes = o_st + nw * cap * sizeof(double);
+    if (h.base) cudaFree(h.base);
+    h = HandRegion{};
+    char* base = nullptr;
+    if (cudaMalloc(&base, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    UwHand u{};
+    u.state = reinterpret_cast<double*>(base + o_st);
+    u.cap = (int)cap;
+    u.count = reinterpret_cast<int*>(base + o_cnt);
+    u.hist = u.count + 1;
+    u.col = reinterpret_cast<int*>(base + o_col);
+    u.key = reinterpret_cast<int*>(base + o_key);
+    u.order = reinterpret_cast<int*>(base + o_ord);
+    if (cudaMemcpy(base, &u, sizeof(u), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(base);
+        return nullptr;
+    }
+    h.base = base;
+    h.cap = cap;
+    h.words = nw;
+    return reinterpret_cast<const UwHand*>(base);
+}
+
+// The worklist pass over list[0 .. *count): one UW_MODE_LIST launch, or with the sorted schedule
+// (FP64 and FAST) the split pass through hand-off region r: UW_MODE_LIST1, the sort of the handed-off
+// columns by iteration-1 updraft depth, UW_MODE_RESUME.
+cudaError_t worklist_pass(DeviceState& d, int r, UwArgs A, int* list, int* count, cudaStream_t st)
+{
+    State& s = S();
+    const UwHand* H = nullptr;
+    if (s.schedule == UWSHCU_SCHED_SORTED && s.precision != UWSHCU_PREC_MIXED)
+        H = hand_region(d, r, A.iend, A.mkx, A.ncnst);
+    if (!H) return launch_mode(&A, s.precision, kModeList, list, count, A.iend, s.block, st);
+    cudaError_t e;
+    A.hand = H;
+    const HandRegion& h = d.hand[r];
+    int* cnt = reinterpret_cast<int*>(h.base + ((sizeof(UwHand) + 255) & ~(size_t)255));
+    if ((e = cudaMemsetAsync(cnt, 0, (1 + UW_HAND_KEYS) * sizeof(int), st)) != cudaSuccess) return e;
+    if ((e = launch_mode(&A, s.precision, kModeList1, list, count, A.iend, s.block, st)) != cudaSuccess) return e;
+    const int nb = (int)std::min((h.cap + 255) / 256, (size_t)1184);
+    hand_hist_kernel<<<nb, 256, 0, st>>>(H);
+    hand_scan_kernel<<<1, 32, 0, st>>>(H);
+    hand_scatter_kernel<<<nb, 256, 0, st>>>(H);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    return launch_mode(&A, s.precision, kModeResume, nullptr, nullptr, (int)h.cap, s.block, st);
+}
+
 // Enqueue the column computation for A on st with the selected schedule.
 int enqueue(DeviceState& d, const UwArgs& A, cudaStream_t st)
 {
@@ -331,7 +442,7 @@ int enqueue(DeviceState& d, const UwArgs& A, cudaStream_t st)
     if (ev && (e = cudaEventRecord(ev[0], st)) != cudaSuccess) return cuda_fail(e);
     if ((e = launch_mode(&A, s.precision, kModeTrigger, list, count, A.iend, s.block, st)) != cudaSuccess) return cuda_fail(e);
     if (ev && (e = cudaEventRecord(ev[1], st)) != cudaSuccess) return cuda_fail(e);
-    if ((e = launch_mode(&A, s.precision, kModeList, list, count, A.iend, s.block, st)) != cudaSuccess) return cuda_fail(e);
+    if ((e = worklist_pass(d, 0, A, list, count, st)) != cudaSuccess) return cuda_fail(e);
     if (ev && (e = cudaEventRecord(ev[2], st)) != cudaSuccess) return cuda_fail(e);
     return UWSHCU_OK;
 }
@@ -498,7 +609,7 @@ int host_call(int inv, int mix, int mkx, int iend, int ncnst, double dt, const d
         } else {
             if ((e = launch_mode(&A, s.precision, kModeTrigger, wreg + 2, wreg, A.iend, s.block, st)) != cudaSuccess)
                 return cuda_fail(e);
-            if ((e = launch_mode(&A, s.precision, kModeList, wreg + 2, wreg, A.iend, s.block, st)) != cudaSuccess)
+            if ((e = worklist_pass(*d, 1 + (int)(c % (size_t)s.pipe_streams), A, wreg + 2, wreg, st)) != cudaSuccess)
                 return cuda_fail(e);
         }
         if ((e = cudaMemcpyAsync(hout, dout, per_out * nc * sizeof(double), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
@@ -652,8 +763,19 @@ int uwshcu_set_schedule(int schedule)
 {
     State& s = S();
     std::lock_guard<std::mutex> lock(s.mu);
-    if (schedule != UWSHCU_SCHED_SINGLE_PASS && schedule != UWSHCU_SCHED_TWO_PHASE) return UWSHCU_ERR_BAD_ARGS;
+    if (schedule != UWSHCU_SCHED_SINGLE_PASS && schedule != UWSHCU_SCHED_TWO_PHASE &&
+        schedule != UWSHCU_SCHED_SORTED)
+        return UWSHCU_ERR_BAD_ARGS;
     s.schedule = schedule;
+    return UWSHCU_OK;
+}
+
+int uwshcu_set_hand_slots(int slots)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    if (slots < 0) return UWSHCU_ERR_BAD_ARGS;
+    s.hand_slots = slots == 0 ? 0 : std::max(slots, 32);
     return UWSHCU_OK;
 }
 
@@ -740,6 +862,8 @@ int uwshcu_finalize(void)
         if (d.h_buf) cudaFreeHost(d.h_buf);
         if (d.d_err) cudaFree(d.d_err);
         if (d.d_wl) cudaFree(d.d_wl);
+        for (HandRegion& h : d.hand)
+            if (h.base) cudaFree(h.base);
         for (int n = 0; n < DeviceState::kSlots; n++)
             for (int j = 0; j < 3; j++)
                 if (d.ev[n][j]) cudaEventDestroy(d.ev[n][j]);

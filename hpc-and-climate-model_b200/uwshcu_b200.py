@@ -45,7 +45,8 @@ EXPORTS = ("uwshcu_init", "uwshcu_set_rpen", "uwshcu_init_default", "uwshcu_set_
            "uwshcu_compute_device_noalloc", "uwshcu_batch_create", "uwshcu_batch_run",
            "uwshcu_batch_capture", "uwshcu_batch_autotune", "uwshcu_batch_status",
            "uwshcu_batch_destroy", "uwshcu_set_pipeline", "uwshcu_set_params",
-           "uwshcu_budget_device", "uwshcu_tangent_device", "uwshcu_compute_member")
+           "uwshcu_budget_device", "uwshcu_tangent_device", "uwshcu_compute_member",
+           "uwshcu_set_hand_slots")
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
@@ -101,6 +102,7 @@ def set_precision(mode):
 
 SCHED_SINGLE_PASS = 0
 SCHED_TWO_PHASE = 1
+SCHED_SORTED = 2
 
 
 def set_schedule(schedule):
@@ -122,6 +124,10 @@ def profile_read():
 
 def set_pipeline(chunk_columns, streams):
     return lib().uwshcu_set_pipeline(ctypes.c_int(chunk_columns), ctypes.c_int(streams))
+
+
+def set_hand_slots(slots):
+    return lib().uwshcu_set_hand_slots(ctypes.c_int(slots))
 
 
 def set_block(threads):

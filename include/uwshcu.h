@@ -80,9 +80,21 @@ int uwshcu_set_precision(int mode);
 #define UWSHCU_SCHED_SINGLE_PASS 0       /* one launch, every column runs the whole scheme          */
 #define UWSHCU_SCHED_TWO_PHASE 1         /* default: trigger pass over all columns, then the
                                             convecting columns from a device worklist             */
+#define UWSHCU_SCHED_SORTED 2            /* two-phase with the worklist pass split at the CIN
+                                            decision of iteration 2: the implicit-CIN columns
+                                            finish in a second launch, in warps sorted by their
+                                            iteration-1 updraft depth (FP64 and FAST; MIXED runs
+                                            the two-phase schedule).  Holds up to 4 GiB of device
+                                            memory per stream for the column state.             */
 
-/* Select the kernel schedule; both give identical results. */
+/* Select the kernel schedule; all give identical results. */
 int uwshcu_set_schedule(int schedule);
+
+/* Cap on the columns one call of the sorted schedule hands to its second launch (per stream;
+ * 0 = default, bounded by 4 GiB of state, about 160,000 columns at 30 levels and 5 tracers;
+ * values below 32 count as 32).  Columns beyond the cap finish in the first launch: the results are
+ * the same, the memory smaller, the sorting partial.  No counterpart in the reference. */
+int uwshcu_set_hand_slots(int slots);
 
 /* Opt-in timing of the two-phase schedule: when on, every call records CUDA events on its stream
  * around the trigger launch and the worklist launch (up to 256 calls between reads). */
