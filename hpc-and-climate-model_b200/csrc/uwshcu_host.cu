@@ -133,7 +133,8 @@ struct DeviceState {
     // overlap the later chunks' computation
     static constexpr int kPipe = 8;
     cudaStream_t pipe[kPipe] = {};
-    std::vector<cudaEvent_t> done;   // one per chunk, grown on demand
+    cudaStream_t pin = nullptr, pout = nullptr;   // copy-in and copy-out streams
+    std::vector<cudaEvent_t> done, ev_in, ev_comp;   // per chunk: copied out, copied in, computed
     // hand-off regions of the split worklist pass: [0] device-array calls, [1 + j] pipe stream j
     HandRegion hand[1 + kPipe];
 };
@@ -145,7 +146,7 @@ struct State {
     UwConst k{};
     double tbl[UW_TBL];
     int precision = UWSHCU_PREC_FP64;
-    int schedule = UWSHCU_SCHED_TWO_PHASE;
+    int schedule = UWSHCU_SCHED_SORTED;
     int hand_slots = 0;          // cap of the hand-off slots per region (0: by kHandBytes only)
     int block = 128;
     bool profiling = false;
@@ -279,7 +280,25 @@ struct Plane {
     double* dst;
     size_t rows;
     size_t src_ld, dst_ld, n;
+    double* dev;   // device address of the compact (staging-side) end
 };
+
+// Whether [p, p + bytes) is page-locked host memory (cudaMallocHost, cudaHostAlloc,
+// cudaHostRegister): its first and last bytes are.
+bool pinned_range(const void* p, size_t bytes)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess || a.type != cudaMemoryTypeHost) {
+        cudaGetLastError();
+        return false;
+    }
+    if (cudaPointerGetAttributes(&a, static_cast<const char*>(p) + bytes - 1) != cudaSuccess ||
+        a.type != cudaMemoryTypeHost) {
+        cudaGetLastError();
+        return false;
+    }
+    return true;
+}
 
 void copy_planes(const std::vector<Plane>& planes)
 {
@@ -484,16 +503,34 @@ int host_call(int inv, int mix, int mkx, int iend, int ncnst, double dt, const d
 
     const size_t n = (size_t)iend, ld = (size_t)mix, KI = (size_t)mkx + 1, KL = (size_t)mkx;
     const size_t KT = KL * (size_t)ncnst;
-    // Column chunks, each a compact (nc-column) copy of its inputs and outputs in the arena and the
-    // pinned staging area.  Chunk c runs on pipe[c % kPipe]: copy in, trigger + worklist pass, copy
-    // out.  The host packs chunk c+1 while the GPU works on chunk c and unpacks chunk c while the
-    // GPU works on the later ones.  Each chunk has its own worklist and endrun word.
+    // Column chunks, each a compact (nc-column) copy of its inputs and outputs in the arena (and, for
+    // pageable caller arrays, in the pinned staging area).  Three-stage pipeline: the copy-in stream
+    // takes every chunk's inputs back to back, chunk c computes (trigger + worklist pass) on
+    // pipe[c % pipe_streams] once its inputs are in, and the copy-out stream takes its outputs once
+    // it is computed.  The host packs chunk c+1 while the GPU works on chunk c and unpacks the
+    // chunks in order as they arrive.  Each chunk has its own worklist and endrun word.
     const size_t per_in = 3 * KI + 11 * KL + KT + 2;     // doubles per column, input block
     const size_t per_out = 6 * KI + 14 * KL + KT + 7;    // doubles per column, output block
     const size_t csz = s.chunk_columns > 0 ? (size_t)s.chunk_columns : n;
     const size_t nch = (n + csz - 1) / csz;
     const size_t nin = per_in * n, nout = per_out * n;
-    if ((rc = grow(*d, nin + nout, nin + nout + 2 * nch)) != UWSHCU_OK) return rc;
+    // Page-locked caller arrays: every plane goes straight between them and the device with a
+    // strided copy (no host packing, no staging); otherwise through the pinned staging area.
+    bool direct = true;
+    {
+        const double* arrays[] = {ps0, zs0, tke, p0, z0, dp0, u0, v0, qv0, ql0, qi0, t0, s0, dpdry0, tr0, pblh,
+                                  cush, umf, slflx, qtflx, flxprc1, flxsnow1, wu, qvten, qlten, qiten, sten,
+                                  uten, vten, qrten, qsten, evapc, cufrc, qcu, qlu, qiu, qc, trten, precip,
+                                  snow, cbmf, rliq, cnt, cnb};
+        const size_t rows[] = {KI, KI, KI, KL, KL, KL, KL, KL, KL, KL, KL, KL, KL, KL, KT, 1,
+                               1, KI, KI, KI, KI, KI, KI, KL, KL, KL, KL,
+                               KL, KL, KL, KL, KL, KL, KL, KL, KL, KL, KT, 1,
+                               1, 1, 1, 1, 1};
+        static_assert(sizeof(arrays) / sizeof(arrays[0]) == sizeof(rows) / sizeof(rows[0]), "one row count per array");
+        for (size_t a = 0; a < sizeof(rows) / sizeof(rows[0]) && direct; a++)
+            direct = pinned_range(arrays[a], ((rows[a] - 1) * ld + n) * sizeof(double));
+    }
+    if ((rc = grow(*d, nin + nout, direct ? 2 * nch : nin + nout + 2 * nch)) != UWSHCU_OK) return rc;
     if ((rc = grow_worklist(*d, n + 2 * nch)) != UWSHCU_OK) return rc;
     cudaError_t e;
     if (!d->pipe[0]) {
@@ -505,19 +542,24 @@ int host_call(int inv, int mix, int mkx, int iend, int ncnst, double dt, const d
                 return cuda_fail(e);
         }
     }
-    while (d->done.size() < nch) {
-        cudaEvent_t ev;
-        if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return cuda_fail(e);
-        d->done.push_back(ev);
+    if (!d->pin) {
+        if ((e = cudaStreamCreateWithFlags(&d->pin, cudaStreamNonBlocking)) != cudaSuccess) return cuda_fail(e);
+        if ((e = cudaStreamCreateWithFlags(&d->pout, cudaStreamNonBlocking)) != cudaSuccess) return cuda_fail(e);
     }
-    unsigned int* hbits = reinterpret_cast<unsigned int*>(d->h_buf + nin + nout);   // nch words
+    for (std::vector<cudaEvent_t>* v : {&d->done, &d->ev_in, &d->ev_comp})
+        while (v->size() < nch) {
+            cudaEvent_t ev;
+            if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return cuda_fail(e);
+            v->push_back(ev);
+        }
+    unsigned int* hbits = reinterpret_cast<unsigned int*>(d->h_buf + (direct ? 0 : nin + nout));   // nch words
 
     std::vector<std::vector<Plane>> outs(nch);
     size_t base_in = 0, base_out = 0;
     for (size_t c = 0; c < nch; c++) {
         const size_t c0 = c * csz, nc = std::min(csz, n - c0);
-        double* hin = d->h_buf + base_in;
-        double* hout = d->h_buf + nin + base_out;
+        double* hin = direct ? nullptr : d->h_buf + base_in;
+        double* hout = direct ? nullptr : d->h_buf + nin + base_out;
         double* din = d->d_buf + base_in;
         double* dout = d->d_buf + nin + base_out;
         base_in += per_in * nc;
@@ -525,7 +567,7 @@ int host_call(int inv, int mix, int mkx, int iend, int ncnst, double dt, const d
         std::vector<Plane> in;
         size_t off = 0;
         auto add_in = [&](const double* a, size_t rows) -> const double* {
-            in.push_back(Plane{a + c0, hin + off, rows, ld, nc, nc});
+            in.push_back(Plane{a + c0, direct ? nullptr : hin + off, rows, ld, nc, nc, din + off});
             const double* dp = din + off;
             off += rows * nc;
             return dp;
@@ -554,12 +596,12 @@ int host_call(int inv, int mix, int mkx, int iend, int ncnst, double dt, const d
         A.tr0 = add_in(tr0, KT);   // (mix, mkx, ncnst): mkx*ncnst rows of mix
         A.pblh = add_in(pblh, 1);
         A.cush = const_cast<double*>(add_in(cush, 1));
-        copy_planes(in);
+        if (!direct) copy_planes(in);
 
         std::vector<Plane>& out = outs[c];
         size_t oo = 0;
         auto add_out = [&](double* a, size_t rows) -> double* {
-            out.push_back(Plane{hout + oo, a + c0, rows, nc, ld, nc});
+            out.push_back(Plane{direct ? nullptr : hout + oo, a + c0, rows, nc, ld, nc, dout + oo});
             double* dp = dout + oo;
             oo += rows * nc;
             return dp;
@@ -592,7 +634,7 @@ int host_call(int inv, int mix, int mkx, int iend, int ncnst, double dt, const d
         A.cnt = add_out(cnt, 1);
         A.cnb = add_out(cnb, 1);
         // cush is in/out: the kernel rewrites it in place in the input block
-        out.push_back(Plane{hin + (A.cush - din), cush + c0, 1, nc, ld, nc});
+        out.push_back(Plane{direct ? nullptr : hin + (A.cush - din), cush + c0, 1, nc, ld, nc, A.cush});
         // this chunk's worklist region: [0] count, [1] endrun bits, [2 ..] column ids
         int* wreg = d->d_wl + (c0 + 2 * c);
         A.err = reinterpret_cast<unsigned int*>(wreg + 1);
@@ -600,9 +642,17 @@ int host_call(int inv, int mix, int mkx, int iend, int ncnst, double dt, const d
         A.diag_real = nullptr;
 
         cudaStream_t st = d->pipe[c % (size_t)s.pipe_streams];
-        if ((e = cudaMemsetAsync(wreg, 0, 2 * sizeof(int), st)) != cudaSuccess) return cuda_fail(e);
-        if ((e = cudaMemcpyAsync(din, hin, per_in * nc * sizeof(double), cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        if ((e = cudaMemsetAsync(wreg, 0, 2 * sizeof(int), d->pin)) != cudaSuccess) return cuda_fail(e);
+        if (direct) {
+            for (const Plane& p : in)
+                if ((e = cudaMemcpy2DAsync(p.dev, p.dst_ld * sizeof(double), p.src, p.src_ld * sizeof(double),
+                                           p.n * sizeof(double), p.rows, cudaMemcpyHostToDevice, d->pin)) != cudaSuccess)
+                    return cuda_fail(e);
+        } else if ((e = cudaMemcpyAsync(din, hin, per_in * nc * sizeof(double), cudaMemcpyHostToDevice, d->pin)) != cudaSuccess) {
             return cuda_fail(e);
+        }
+        if ((e = cudaEventRecord(d->ev_in[c], d->pin)) != cudaSuccess) return cuda_fail(e);
+        if ((e = cudaStreamWaitEvent(st, d->ev_in[c], 0)) != cudaSuccess) return cuda_fail(e);
         if (s.schedule == UWSHCU_SCHED_SINGLE_PASS) {
             if ((e = launch_mode(&A, s.precision, kModeAll, nullptr, nullptr, A.iend, s.block, st)) != cudaSuccess)
                 return cuda_fail(e);
@@ -612,18 +662,27 @@ int host_call(int inv, int mix, int mkx, int iend, int ncnst, double dt, const d
             if ((e = worklist_pass(*d, 1 + (int)(c % (size_t)s.pipe_streams), A, wreg + 2, wreg, st)) != cudaSuccess)
                 return cuda_fail(e);
         }
-        if ((e = cudaMemcpyAsync(hout, dout, per_out * nc * sizeof(double), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        if ((e = cudaEventRecord(d->ev_comp[c], st)) != cudaSuccess) return cuda_fail(e);
+        if ((e = cudaStreamWaitEvent(d->pout, d->ev_comp[c], 0)) != cudaSuccess) return cuda_fail(e);
+        if (direct) {
+            for (const Plane& p : out)
+                if ((e = cudaMemcpy2DAsync(p.dst, p.dst_ld * sizeof(double), p.dev, p.src_ld * sizeof(double),
+                                           p.n * sizeof(double), p.rows, cudaMemcpyDeviceToHost, d->pout)) != cudaSuccess)
+                    return cuda_fail(e);
+        } else {
+            if ((e = cudaMemcpyAsync(hout, dout, per_out * nc * sizeof(double), cudaMemcpyDeviceToHost, d->pout)) != cudaSuccess)
+                return cuda_fail(e);
+            if ((e = cudaMemcpyAsync(hin + (A.cush - din), A.cush, nc * sizeof(double), cudaMemcpyDeviceToHost, d->pout)) != cudaSuccess)
+                return cuda_fail(e);
+        }
+        if ((e = cudaMemcpyAsync(hbits + c, wreg + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, d->pout)) != cudaSuccess)
             return cuda_fail(e);
-        if ((e = cudaMemcpyAsync(hin + (A.cush - din), A.cush, nc * sizeof(double), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
-            return cuda_fail(e);
-        if ((e = cudaMemcpyAsync(hbits + c, wreg + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
-            return cuda_fail(e);
-        if ((e = cudaEventRecord(d->done[c], st)) != cudaSuccess) return cuda_fail(e);
+        if ((e = cudaEventRecord(d->done[c], d->pout)) != cudaSuccess) return cuda_fail(e);
     }
     unsigned int bits = 0;
     for (size_t c = 0; c < nch; c++) {
         if ((e = cudaEventSynchronize(d->done[c])) != cudaSuccess) return cuda_fail(e);
-        copy_planes(outs[c]);
+        if (!direct) copy_planes(outs[c]);
         bits |= hbits[c];
     }
     return status_from_bits(bits);
@@ -871,6 +930,10 @@ int uwshcu_finalize(void)
         for (int j = 0; j < DeviceState::kPipe; j++)
             if (d.pipe[j]) cudaStreamDestroy(d.pipe[j]);
         for (cudaEvent_t ev : d.done) cudaEventDestroy(ev);
+        for (cudaEvent_t ev : d.ev_in) cudaEventDestroy(ev);
+        for (cudaEvent_t ev : d.ev_comp) cudaEventDestroy(ev);
+        if (d.pin) cudaStreamDestroy(d.pin);
+        if (d.pout) cudaStreamDestroy(d.pout);
         d = DeviceState{};
     }
     if (have) cudaSetDevice(cur);

@@ -103,6 +103,7 @@ def set_precision(mode):
 SCHED_SINGLE_PASS = 0
 SCHED_TWO_PHASE = 1
 SCHED_SORTED = 2
+SCHED_DEFAULT = SCHED_SORTED
 
 
 def set_schedule(schedule):

@@ -78,9 +78,9 @@ int uwshcu_set_precision(int mode);
 
 /* Kernel schedules (uwshcu_set_schedule). */
 #define UWSHCU_SCHED_SINGLE_PASS 0       /* one launch, every column runs the whole scheme          */
-#define UWSHCU_SCHED_TWO_PHASE 1         /* default: trigger pass over all columns, then the
-                                            convecting columns from a device worklist             */
-#define UWSHCU_SCHED_SORTED 2            /* two-phase with the worklist pass split at the CIN
+#define UWSHCU_SCHED_TWO_PHASE 1         /* trigger pass over all columns, then the convecting
+                                            columns from a device worklist                        */
+#define UWSHCU_SCHED_SORTED 2            /* default: two-phase with the worklist pass split at the CIN
                                             decision of iteration 2: the implicit-CIN columns
                                             finish in a second launch, in warps sorted by their
                                             iteration-1 updraft depth (FP64 and FAST; MIXED runs

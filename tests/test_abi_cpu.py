@@ -54,7 +54,7 @@ def test_bad_arguments_are_rejected(uw):
     assert L.uwshcu_set_block(ctypes.c_int(48)) == uw.ERR_BAD_ARGS
     assert L.uwshcu_set_precision(ctypes.c_int(7)) == uw.ERR_BAD_ARGS
     assert uw.set_schedule(3) == uw.ERR_BAD_ARGS
-    assert uw.set_schedule(uw.SCHED_SORTED) == 0 and uw.set_schedule(uw.SCHED_TWO_PHASE) == 0
+    assert uw.set_schedule(uw.SCHED_TWO_PHASE) == 0 and uw.set_schedule(uw.SCHED_DEFAULT) == 0
     assert uw.set_hand_slots(-1) == uw.ERR_BAD_ARGS
     assert uw.set_hand_slots(100) == 0 and uw.set_hand_slots(0) == 0
     assert L.uwshcu_compute_member(None, None) == uw.ERR_BAD_ARGS

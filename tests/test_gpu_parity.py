@@ -95,18 +95,18 @@ def test_repeat_calls_are_deterministic(uw, cuda):
 
 
 def test_schedules_agree_bit_for_bit(uw, cuda):
-    """The single-pass and the two-phase (trigger pass + worklist) schedules compute the same
-    column code on the same inputs."""
+    """The single-pass, the two-phase (trigger pass + worklist) and the sorted (worklist split at the
+    iteration-2 CIN decision) schedules compute the same column code on the same inputs."""
     s = soundings.make_soundings(5000, 30, seed=61)
     outs = []
     try:
-        for sched in (uw.SCHED_SINGLE_PASS, uw.SCHED_TWO_PHASE):
+        for sched in (uw.SCHED_SINGLE_PASS, uw.SCHED_TWO_PHASE, uw.SCHED_SORTED):
             assert uw.set_schedule(sched) == 0
             rc, o = uw.compute_host(s)
             assert rc == 0
             outs.append(o)
     finally:
-        uw.set_schedule(uw.SCHED_TWO_PHASE)
+        uw.set_schedule(uw.SCHED_DEFAULT)
     for f in FIELDS:
         assert np.array_equal(outs[0][f], outs[1][f]), f
 
@@ -170,3 +170,34 @@ def test_tuning_parameters_match_oracle(uw, oracle_pm, cuda):
     finally:
         assert uw.init_default() == 0
         oracle_pm.init_default()
+
+
+@pytest.mark.gpu
+def test_page_locked_host_arrays_match_pageable(uw, cuda):
+    """Page-locked caller arrays take the direct path (strided copies between them and the device,
+    no staging): the same bits as pageable arrays, for both level orders, with mix > iend and with
+    several chunks over several streams."""
+    import torch
+
+    keep = []
+
+    def pinned(x):
+        t = torch.from_numpy(np.ascontiguousarray(x)).pin_memory()
+        keep.append(t)
+        return t.numpy()
+
+    s = soundings.make_soundings(5000, 30, seed=63)
+    try:
+        for entry in ("compute_uwshcu_", "compute_uwshcu_inv_"):
+            si = s if entry == "compute_uwshcu_" else soundings.to_inv(s)
+            sp = {k: pinned(v) if isinstance(v, np.ndarray) else v for k, v in si.items()}
+            for chunk, streams in ((0, 1), (1024, 3)):
+                assert uw.set_pipeline(chunk, streams) == 0
+                rc0, o0 = uw.compute_host(si, entry=entry, iend=4700)
+                outp = {k: pinned(v) for k, v in uw.alloc_outputs(30, 5, 5000, si["cush"]).items()}
+                rc, o = uw.compute_host(sp, entry=entry, iend=4700, out=outp)
+                assert rc == rc0 == 0
+                bad = [k for k in o0 if not np.array_equal(o[k], o0[k])]
+                assert not bad, (entry, chunk, streams, bad)
+    finally:
+        assert uw.set_pipeline(32768, 4) == 0

@@ -49,7 +49,7 @@ def test_device_entry_sorted_matches_two_phase(uw, cuda, prec, pver):
                 assert case.status() == 0
             out[name] = case.outputs_numpy()
     finally:
-        _settings(uw, uw.SCHED_TWO_PHASE, 0)
+        _settings(uw, uw.SCHED_DEFAULT, 0)
         uw.set_precision(uw.PREC_FP64)
     ref = out["two_phase"]
     # the workload reaches the hand-off: convecting columns that took the implicit branch
@@ -76,7 +76,7 @@ def test_host_entries_sorted_match_two_phase(uw, cuda):
                 assert rc == rc0
                 assert not _diff(o0, o), (entry, chunk, streams, slots, _diff(o0, o))
     finally:
-        _settings(uw, uw.SCHED_TWO_PHASE, 0)
+        _settings(uw, uw.SCHED_DEFAULT, 0)
         assert uw.set_pipeline(32768, 4) == 0
 
 
@@ -92,7 +92,7 @@ def test_sorted_schedule_matches_oracle(uw, oracle_pm, cuda):
         assert case.status() == ref["status"]
         out = case.outputs_numpy()
     finally:
-        _settings(uw, uw.SCHED_TWO_PHASE, 0)
+        _settings(uw, uw.SCHED_DEFAULT, 0)
     same = [k for k in ("umf", "qvten", "sten", "precip", "cush", "cnt", "cnb", "diag_int", "diag_real",
                         "diag_level") if np.mean(np.all((out[k] == ref[k]).reshape(-1, s["ncol"]), axis=0)) < 0.9999]
     assert not same, same
