@@ -85,8 +85,7 @@ def main():
             "                 const __grid_constant__ UwTangent T)")
     s = rep(s, "uw_column<KP, NC, MODE, 0>(A, tbl, i, active, wl, wl_count);",
             "uw_column<KP, NC, MODE, 0>(A, tbl, i, active, wl, wl_count, T);")
-    s = rep(s, "__launch_bounds__(128, UW_MODE_IS_LIST(MODE) ? 4 : (MODE == UW_MODE_TRIGGER ? 5 : 3))",
-            "__launch_bounds__(128)")
+    s = rep(s, "__launch_bounds__(128, UW_LIST_MINB(MODE))", "__launch_bounds__(128)")
     # the split worklist pass (UW_MODE_LIST1 / UW_MODE_RESUME) is FP64 and FAST only: no state copies here
     s = re.sub(r"\n[ ]*UW_(SAVE|LOAD)_STATE\([^;]*\);", "", s)
     for u in ("TOI", "TOL", "TOT", "SEEDL", "SEEDI"):
