@@ -40,13 +40,14 @@ RH_PBL = (0.675, 0.93)
 METRIC = "columns/s (compute_uwshcu, FP64, 259,200 x 30 levels)"
 
 
-# From the ncu capture of the worklist kernel on the 65,536-column case of this workload (29,956
+# From the ncu capture of the worklist pass on the 65,536-column case of this workload (29,956
 # worklist columns; summary in profiles/uwshcu_fp64_kernel_bench65k.txt): DRAM bytes read + written
-# per worklist column, and FP64 operations executed per worklist column (2 x DFMA + DADD + DMUL
-# thread instructions, Newton steps of the IEEE divisions included).  Both scale with the columns
-# a launch processes.
-NCU_DRAM_BYTES_PER_LIST_COLUMN = 10.494e9 / 29_956
-NCU_FP64_OPS_PER_LIST_COLUMN = 776.1 * 17.77e-3 * 1.858e9 / 29_956
+# per worklist column by its two launches (UW_MODE_LIST1 7.362 GB + UW_MODE_RESUME 3.868 GB), and
+# FP64 operations executed per worklist column (2 x DFMA + DADD + DMUL thread instructions per
+# cycle x cycles of each launch: 731.26 x 17,665,035 + 559.94 x 14,018,129; the Newton steps of the
+# IEEE divisions included).  Both scale with the columns a launch processes.
+NCU_DRAM_BYTES_PER_LIST_COLUMN = 11.2301e9 / 29_956
+NCU_FP64_OPS_PER_LIST_COLUMN = (731.26 * 17_665_035 + 559.94 * 14_018_129) / 29_956
 FP64_DFMA_PER_CYCLE = 9472    # ncu sm__sass_thread_inst_executed_op_dfma_pred_on.sum.peak_sustained
 # Algorithmic FP64 operations per convecting / other column of each workload, counted by the
 # oracle's operation-counting build (written by oracle/opcount.py; a data file, read as text).
@@ -544,7 +545,7 @@ def main():
                     "what": "algorithmic FP64 operations of the whole step (oracle operation count "
                             "per convecting / other column x columns) / step time, against 2 x 9472 "
                             "DFMA/cycle x median SM clock"}
-    if phases and prec == uw.PREC_FP64 and clk is not None and clk.summary().get("sm_mhz"):
+    if phases and sorted_pass and prec == uw.PREC_FP64 and clk is not None and clk.summary().get("sm_mhz"):
         hz = clk.summary()["sm_mhz"] * 1e6
         ach = NCU_FP64_OPS_PER_LIST_COLUMN * ncols_dom / (kernel_ms * 1e-3) / 1e12
         pk = 2 * FP64_DFMA_PER_CYCLE * hz / 1e12
@@ -568,7 +569,7 @@ def main():
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak,
                      "traffic": (NCU_DRAM_BYTES_PER_LIST_COLUMN * ncols_dom)
-                                if (phases and prec == uw.PREC_FP64) else None,
+                                if (phases and sorted_pass and prec == uw.PREC_FP64) else None,
                      "peak_kind": peak_kind,
                      "kernel": "uwshcu_%s_kernel<32,5,%s>" % ({"fp64": "fp64", "fast": "fast", "mixed": "mixed"}[args.precision],
                                                               ("UW_MODE_LIST1 + UW_MODE_RESUME" if sorted_pass else "UW_MODE_LIST")
