@@ -429,7 +429,7 @@ def main():
     prec = {"fp64": uw.PREC_FP64, "fast": uw.PREC_FAST, "mixed": uw.PREC_MIXED}[args.precision]
     assert uw.set_precision(prec) == 0, "precision %s not available" % args.precision
     two_phase = args.schedule in ("two-phase", "sorted")
-    sorted_pass = args.schedule == "sorted" and args.precision != "mixed"
+    sorted_pass = args.schedule == "sorted"
     assert uw.set_schedule({"two-phase": uw.SCHED_TWO_PHASE, "sorted": uw.SCHED_SORTED,
                             "single-pass": uw.SCHED_SINGLE_PASS}[args.schedule]) == 0
     n = args.ncol

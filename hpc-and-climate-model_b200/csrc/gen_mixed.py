@@ -46,8 +46,7 @@ rep('#define GL(a, k) __ldg(&A.a[(size_t)RL(k) * mix + i])', '#define GL(a, k) (
 rep('#define GT(m, k) __ldg(&A.tr0[((size_t)((m) - 1) * mkx + RL(k)) * mix + i])', '#define GT(m, k) ((R)__ldg(&A.tr0[((size_t)((m) - 1) * mkx + RL(k)) * mix + i]))')
 rep('#define CNT(x) (inv ? (R)(mkx + 1) - (x) : (x))', '#define CNT(x) (inv ? (double)(mkx + 1) - (double)(x) : (double)(x))')
 rep('const R* __restrict__ tbl, const int i_in,', 'const double* __restrict__ tbld, const float* __restrict__ tblf, const int i_in,')
-# the split worklist pass (UW_MODE_LIST1 / UW_MODE_RESUME) is FP64 and FAST only: no state copies here
-b = re.sub(r'\n[ ]*UW_(SAVE|LOAD)_STATE\([^;]*\);', '', b)
+
 rep('''    __shared__ R tbl[UW_TBL];
     for (int t = threadIdx.x; t < UW_TBL; t += blockDim.x) tbl[t] = c_estbl[t];''',
 '''    __shared__ double tbld[UW_TBL];

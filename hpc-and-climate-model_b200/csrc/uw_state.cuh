@@ -45,20 +45,40 @@
     X(krel_s) X(kbup_s) X(kpen_s) X(kinv_o) X(klcl_o) X(klfc_o)
 
 #define UW_ST_ONE(x) +1
+// Extra words for scalars that take two (the compensated sums rliq, rainflx, snowflx of the
+// mixed-precision column code).
+#define UW_ST_WIDE 3
 // words of one slot: the lists above, plus tscaleh and errbits
 __host__ __device__ inline size_t uw_state_words(int mkx, int ncnst)
 {
     const size_t lv = (size_t)mkx + 1;
     return (0 UW_ST_FULL(UW_ST_ONE)) * lv + (0 UW_ST_LEV0(UW_ST_ONE)) + (0 UW_ST_TRA(UW_ST_ONE)) * (size_t)ncnst +
-           (0 UW_ST_VEC(UW_ST_ONE)) * (size_t)ncnst + (0 UW_ST_DBL(UW_ST_ONE)) + (0 UW_ST_INT(UW_ST_ONE)) + 2;
+           (0 UW_ST_VEC(UW_ST_ONE)) * (size_t)ncnst + (0 UW_ST_DBL(UW_ST_ONE)) + (0 UW_ST_INT(UW_ST_ONE)) + 2 +
+           UW_ST_WIDE;
 }
+
+// One scalar to / from the buffer, whatever its type (every integer and float is exact in a
+// double).  A type of two words provides its own overloads next to its definition.
+#if defined(__CUDACC__)
+__device__ __forceinline__ void uw_st_put(double* st, size_t& w, size_t cs, double x) { st[w++ * cs] = x; }
+__device__ __forceinline__ void uw_st_put(double* st, size_t& w, size_t cs, float x) { st[w++ * cs] = (double)x; }
+__device__ __forceinline__ void uw_st_put(double* st, size_t& w, size_t cs, int x) { st[w++ * cs] = (double)x; }
+__device__ __forceinline__ void uw_st_put(double* st, size_t& w, size_t cs, unsigned int x) { st[w++ * cs] = (double)x; }
+__device__ __forceinline__ void uw_st_get(const double* st, size_t& w, size_t cs, double& x) { x = st[w++ * cs]; }
+__device__ __forceinline__ void uw_st_get(const double* st, size_t& w, size_t cs, float& x) { x = (float)st[w++ * cs]; }
+__device__ __forceinline__ void uw_st_get(const double* st, size_t& w, size_t cs, int& x) { x = (int)st[w++ * cs]; }
+__device__ __forceinline__ void uw_st_get(const double* st, size_t& w, size_t cs, unsigned int& x)
+{
+    x = (unsigned int)st[w++ * cs];
+}
+#endif
 
 // Column code only (names mkx, ncnst, errbits and the listed variables in scope).
 #define UW_SV_FULL(a) for (int k_ = 0; k_ <= mkx; k_++) st_[(w_ + k_) * cs_] = a[k_]; w_ += mkx + 1;
 #define UW_SV_LEV0(a) st_[w_ * cs_] = a[0]; w_++;
 #define UW_SV_TRA(a) for (int m_ = 0; m_ < ncnst; m_++) st_[(w_ + m_) * cs_] = a[m_][0]; w_ += ncnst;
 #define UW_SV_VEC(a) for (int m_ = 0; m_ < ncnst; m_++) st_[(w_ + m_) * cs_] = a[m_]; w_ += ncnst;
-#define UW_SV_ONE(x) st_[w_ * cs_] = (double)(x); w_++;
+#define UW_SV_ONE(x) uw_st_put(st_, w_, cs_, x);
 #define UW_SAVE_STATE(ST, CS, TSCALEH)                                                                    \
     do {                                                                                                  \
         double* const st_ = (ST);                                                                         \
@@ -72,13 +92,12 @@ __host__ __device__ inline size_t uw_state_words(int mkx, int ncnst)
 #define UW_LD_LEV0(a) a[0] = st_[w_ * cs_]; w_++;
 #define UW_LD_TRA(a) for (int m_ = 0; m_ < ncnst; m_++) a[m_][0] = st_[(w_ + m_) * cs_]; w_ += ncnst;
 #define UW_LD_VEC(a) for (int m_ = 0; m_ < ncnst; m_++) a[m_] = st_[(w_ + m_) * cs_]; w_ += ncnst;
-#define UW_LD_DBL(x) x = st_[w_ * cs_]; w_++;
-#define UW_LD_INT(x) x = (int)st_[w_ * cs_]; w_++;
+#define UW_LD_ONE(x) uw_st_get(st_, w_, cs_, x);
 #define UW_LOAD_STATE(ST, CS, TSCALEH)                                                                    \
     do {                                                                                                  \
         const double* const st_ = (ST);                                                                   \
         const size_t cs_ = (CS);                                                                          \
         size_t w_ = 0;                                                                                    \
         UW_ST_FULL(UW_LD_FULL) UW_ST_LEV0(UW_LD_LEV0) UW_ST_TRA(UW_LD_TRA) UW_ST_VEC(UW_LD_VEC)          \
-        UW_ST_DBL(UW_LD_DBL) UW_ST_INT(UW_LD_INT) UW_LD_DBL(TSCALEH) errbits = (unsigned int)st_[w_ * cs_]; \
+        UW_ST_DBL(UW_LD_ONE) UW_ST_INT(UW_LD_ONE) UW_LD_ONE(TSCALEH) UW_LD_ONE(errbits)                  \
     } while (0)

@@ -414,14 +414,13 @@ const UwHand* hand_region(DeviceState& d, int r, int iend, int mkx, int ncnst)
 }
 
 // The worklist pass over list[0 .. *count): one UW_MODE_LIST launch, or with the sorted schedule
-// (FP64 and FAST) the split pass through hand-off region r: UW_MODE_LIST1, the sort of the handed-off
+// the split pass through hand-off region r: UW_MODE_LIST1, the sort of the handed-off
 // columns by iteration-1 updraft depth, UW_MODE_RESUME.
 cudaError_t worklist_pass(DeviceState& d, int r, UwArgs A, int* list, int* count, cudaStream_t st)
 {
     State& s = S();
     const UwHand* H = nullptr;
-    if (s.schedule == UWSHCU_SCHED_SORTED && s.precision != UWSHCU_PREC_MIXED)
-        H = hand_region(d, r, A.iend, A.mkx, A.ncnst);
+    if (s.schedule == UWSHCU_SCHED_SORTED) H = hand_region(d, r, A.iend, A.mkx, A.ncnst);
     if (!H) return launch_mode(&A, s.precision, kModeList, list, count, A.iend, s.block, st);
     cudaError_t e;
     A.hand = H;

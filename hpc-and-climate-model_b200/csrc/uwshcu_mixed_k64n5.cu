@@ -16,6 +16,8 @@ extern "C" cudaError_t uw_mixed_launch_k64n5(const UwArgs* a, int mode, int* wl,
     dim3 grid((unsigned)((nthreads + block - 1) / block));
     if (mode == UW_MODE_ALL) uwshcu_mixed_kernel<64, 5, UW_MODE_ALL><<<grid, block, 0, stream>>>(*a, wl, wl_count);
     else if (mode == UW_MODE_TRIGGER) uwshcu_mixed_kernel<64, 5, UW_MODE_TRIGGER><<<grid, block, 0, stream>>>(*a, wl, wl_count);
+    else if (mode == UW_MODE_LIST1) uwshcu_mixed_kernel<64, 5, UW_MODE_LIST1><<<grid, block, 0, stream>>>(*a, wl, wl_count);
+    else if (mode == UW_MODE_RESUME) uwshcu_mixed_kernel<64, 5, UW_MODE_RESUME><<<grid, block, 0, stream>>>(*a, wl, wl_count);
     else uwshcu_mixed_kernel<64, 5, UW_MODE_LIST><<<grid, block, 0, stream>>>(*a, wl, wl_count);
     return cudaGetLastError();
 }

@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include "uwshcu_common.cuh"
+#include "uw_state.cuh"
 
 namespace {
 
@@ -42,6 +43,20 @@ struct Kahan {
         s = t;
     }
 };
+// Kahan sums in the hand-off state of the sorted schedule (uw_state.cuh): two words (the scalar
+// overloads there stay visible next to these).
+using ::uw_st_get;
+using ::uw_st_put;
+__device__ __forceinline__ void uw_st_put(double* st, size_t& w, size_t cs, const Kahan& x)
+{
+    st[w++ * cs] = (double)x.s;
+    st[w++ * cs] = (double)x.e;
+}
+__device__ __forceinline__ void uw_st_get(const double* st, size_t& w, size_t cs, Kahan& x)
+{
+    x.s = (float)st[w++ * cs];
+    x.e = (float)st[w++ * cs];
+}
 
 __device__ __forceinline__ float estblf_f(float td, const float* __restrict__ tf)
 {
@@ -650,6 +665,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
         // the state UW_MODE_LIST1 stored at the implicit-CIN branch of iteration 2 (uw_state.cuh),
         // and the arrays that the set-up and that branch's restore build from the inputs, rebuilt
         // with the same operations
+        UW_LOAD_STATE(A.hand->state + i_in, (size_t)A.hand->cap, tscaleh_r);
         for (int k = 0; k <= mkx; k++) {
             ps0[k] = GI(ps0, k);
             zs0[k] = GI(zs0, k);
@@ -968,6 +984,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                 if (!stop && slot < H.cap) {
                     H.col[slot] = i;
                     H.key[slot] = UW_HAND_KEYS - 1 - MN(MX(kpen_s - krel_s, 0), UW_HAND_KEYS - 1);
+                    UW_SAVE_STATE(H.state + slot, (size_t)H.cap, tscaleh);
                     handed = true;
                     stop = true;
                 }

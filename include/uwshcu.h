@@ -83,9 +83,9 @@ int uwshcu_set_precision(int mode);
 #define UWSHCU_SCHED_SORTED 2            /* default: two-phase with the worklist pass split at the CIN
                                             decision of iteration 2: the implicit-CIN columns
                                             finish in a second launch, in warps sorted by their
-                                            iteration-1 updraft depth (FP64 and FAST; MIXED runs
-                                            the two-phase schedule).  Holds up to 4 GiB of device
-                                            memory per stream for the column state.             */
+                                            iteration-1 updraft depth (every precision mode).
+                                            Holds up to 4 GiB of device memory per stream for the
+                                            column state.                                        */
 
 /* Select the kernel schedule; all give identical results. */
 int uwshcu_set_schedule(int schedule);

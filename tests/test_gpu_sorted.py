@@ -4,7 +4,7 @@ Its worklist pass runs in two launches: the first computes iteration 1 of the im
 iteration 2 up to the CIN decision (uwshcu.F90:1759-1889); a column taking the implicit branch stores
 its whole state and a second launch continues it, in warps sorted by iteration-1 updraft depth.
 Each column computes the same operations in the same order whichever launch finishes it, so every
-output and diagnostic must be the bits of the two-phase schedule: in the FP64 and FAST modes,
+output and diagnostic must be the bits of the two-phase schedule: in the FP64, FAST and MIXED modes,
 through the device entry with all diagnostics, through the host entries chunked over streams, for
 30 and 51 levels, and with a slot cap small enough that most columns finish in the first launch.
 """
@@ -27,11 +27,11 @@ def _settings(uw, sched, slots):
     assert uw.set_hand_slots(slots) == 0
 
 
-@pytest.mark.parametrize("prec", ["fp64", "fast"])
+@pytest.mark.parametrize("prec", ["fp64", "fast", "mixed"])
 @pytest.mark.parametrize("pver", [30, 51])
 def test_device_entry_sorted_matches_two_phase(uw, cuda, prec, pver):
     assert uw.init_default() == 0
-    mode = {"fp64": uw.PREC_FP64, "fast": uw.PREC_FAST}[prec]
+    mode = {"fp64": uw.PREC_FP64, "fast": uw.PREC_FAST, "mixed": uw.PREC_MIXED}[prec]
     s = soundings.make_soundings(12000, pver, seed=111 + pver, rh_pbl=(0.6, 0.95))
     out = {}
     try:
