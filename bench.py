@@ -227,8 +227,10 @@ BATCH_MEMBERS = ((262_144, 30, (0.55, 0.757)), (262_144, 35, (0.625, 0.86)),
 
 
 def run_batched(args):
-    """One step = one replay of the captured batch plan (trigger + persistent worklist launch per
-    level class) over all members, inputs resident in HBM."""
+    """One step = one replay of the captured batch plan over all members, inputs resident in HBM:
+    per level class a trigger launch and the worklist pass (sorted schedule, the default: a
+    persistent first worklist launch, the per-member sort of the handed-off columns, a persistent
+    resume launch; --schedule two-phase: one persistent worklist launch)."""
     import torch
     import soundings
     import uwshcu_b200 as uw
@@ -236,6 +238,8 @@ def run_batched(args):
     world, rank, local = dist_setup()
     torch.cuda.set_device(local)
     assert uw.init_default() == 0
+    sorted_plan = args.schedule == "sorted"
+    assert uw.set_schedule(uw.SCHED_SORTED if sorted_plan else uw.SCHED_TWO_PHASE) == 0
     cases = []
     for j, (n, pver, rh) in enumerate(BATCH_MEMBERS):
         s = soundings.make_soundings(n, pver, seed=100 + 10 * rank + j, rh_pbl=rh)
@@ -329,10 +333,17 @@ def run_batched(args):
         "config": {"workload": "batched uneven launch: 4 members x 262,144 columns, pver 30/35/51/30, "
                                "5 tracers, dt=1800 s", "pver": [m[1] for m in BATCH_MEMBERS],
                    "trigger_fraction": trig, "l2": "inputs larger than L2",
-                   "launch": "CUDA graph: per level class one trigger launch + one persistent worklist "
-                             "launch; autotuned block %d, register cap %d blocks/SM, %d column(s) "
-                             "per lane per task" % tuned},
-        "gpu_launches": args.steps * 2 * nclass, "status": st,
+                   "launch": ("CUDA graph: per level class one trigger launch, a persistent first "
+                              "worklist launch (4 blocks/SM) and a persistent resume launch (5 blocks/SM), "
+                              "3 sort kernels per member; autotuned block %d, %d column(s) per lane per "
+                              "task" % (tuned[0], tuned[2])
+                              if sorted_plan else
+                              "CUDA graph: per level class one trigger launch + one persistent worklist "
+                              "launch; autotuned block %d, register cap %d blocks/SM, %d column(s) "
+                              "per lane per task" % tuned),
+                   "schedule": args.schedule},
+        "gpu_launches": args.steps * ((3 * nclass + 3 * len(BATCH_MEMBERS)) if sorted_plan else 2 * nclass),
+        "status": st,
         "roofline": {"fp64_algorithmic": fp64_alg},
         "precisions": others,
     }

@@ -54,10 +54,11 @@ rep('''    __shared__ R tbl[UW_TBL];
     for (int t = threadIdx.x; t < UW_TBL; t += blockDim.x) {
         tbld[t] = c_estbl[t];
         tblf[t] = (float)c_estbl[t];
-    }''', 3)
+    }''', 4)
 rep('uw_column<KP, NC, MODE, 0>(A, tbl, i, active, wl, wl_count);', 'uw_column<KP, NC, MODE, 0>(A, tbld, tblf, i, active, wl, wl_count);')
 rep('(B.m[m], tbl, tid, active, B.wl[m], B.count + m);', '(B.m[m], tbld, tblf, tid, active, B.wl[m], B.count + m);')
 rep('(B.m[m], tbl, i, active, nullptr, nullptr);', '(B.m[m], tbld, tblf, i, active, nullptr, nullptr);')
+rep('(B.m[m], tbl, slot, active, nullptr, nullptr);', '(B.m[m], tbld, tblf, slot, active, nullptr, nullptr);')
 b = b.replace(', tbl)', ', tbld, tblf)')
 rep("""    R cin = 0, cinlcl = 0, plcl = 0,""", """    double cin = 0, cinlcl = 0;
     R plcl = 0,""")

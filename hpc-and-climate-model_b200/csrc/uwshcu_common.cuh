@@ -140,6 +140,7 @@ struct UwBatch {
     int block_start[UW_MAXM + 1];    // trigger launch: first block of each member
     int *count;                      // per-member worklist counts (device, nm ints)
     int *task_head;                  // device task counter of the persistent worklist launch
+    int *task_head2;                 // the same for the resume launch of the sorted schedule
     int *wl[UW_MAXM];                // per-member worklists (device)
     UwArgs m[UW_MAXM];
 };

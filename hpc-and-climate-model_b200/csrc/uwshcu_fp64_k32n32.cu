@@ -24,7 +24,8 @@ extern "C" cudaError_t uw_fp64_launch_k32n32(const UwArgs* a, int mode, int* wl,
     return cudaGetLastError();
 }
 
-// Batched trigger (phase 0) and persistent worklist (phase 1) launches; minb selects the
+// Batched trigger (phase 0), persistent worklist (phase 1), and for the sorted schedule the
+// persistent first worklist (phase 2) and resume (phase 3) launches; minb selects the
 // worklist instantiation (register cap = 65536 / (128 * minb)).  Returns cudaErrorInvalidValue
 // for a minb that is not compiled here.
 extern "C" cudaError_t uw_fp64_batch_k32n32(const UwBatch* b, int phase, int grid, int block, int minb,
@@ -33,6 +34,14 @@ extern "C" cudaError_t uw_fp64_batch_k32n32(const UwBatch* b, int phase, int gri
     if (grid <= 0) return cudaSuccess;
     if (phase == 0) {
         uwshcu_batch_trigger<32, 32, 0><<<grid, block, 0, stream>>>(*b);
+        return cudaGetLastError();
+    }
+    if (phase == 2) {   // sorted schedule: first worklist launch (register cap of minb 4)
+        uwshcu_batch_list<32, 32, 4, 0, UW_MODE_LIST1><<<grid, block, 0, stream>>>(*b);
+        return cudaGetLastError();
+    }
+    if (phase == 3) {   // sorted schedule: resume launch
+        uwshcu_batch_resume<32, 32, 0><<<grid, block, 0, stream>>>(*b);
         return cudaGetLastError();
     }
     if (minb == 4) {

@@ -2181,8 +2181,9 @@ __global__ void __launch_bounds__(128, 5) uwshcu_batch_trigger(const __grid_cons
 // Batched worklist pass, persistent: each warp takes the next task (32 * B.chunk consecutive queue
 // entries of one member) from the device counter *B.task_head until the queues are drained, so a
 // warp never mixes members (their level counts differ).  Task t of member m covers entries
-// [t * 32 * chunk, (t + 1) * 32 * chunk) of wl[m].
-template <int KP, int NC, int MINB, int FAST>
+// [t * 32 * chunk, (t + 1) * 32 * chunk) of wl[m].  LMODE: UW_MODE_LIST, or UW_MODE_LIST1 for the
+// sorted schedule (each member hands its implicit-CIN columns to its own region, B.m[m].hand).
+template <int KP, int NC, int MINB, int FAST, int LMODE = UW_MODE_LIST>
 __global__ void __launch_bounds__(128, MINB) uwshcu_batch_list(const __grid_constant__ UwBatch B)
 {
     __shared__ double tbl[UW_TBL];
@@ -2213,8 +2214,44 @@ __global__ void __launch_bounds__(128, MINB) uwshcu_batch_list(const __grid_cons
             const int idx = first + c * 32 + lane;
             const bool active = idx < n;
             const int i = active ? B.wl[m][idx] : 0;
-            uw_column<KP, NC, UW_MODE_LIST, FAST>(B.m[m], tbl, i, active, nullptr, nullptr);
+            uw_column<KP, NC, LMODE, FAST>(B.m[m], tbl, i, active, nullptr, nullptr);
         }
+    }
+}
+
+// Batched resume launch of the sorted schedule, persistent: each warp takes the next task (32
+// consecutive entries of one member's hand-off slots in sorted order) from *B.task_head2 until every
+// member's slots are done.  Member m has min(*count, cap) slots in its region B.m[m].hand.
+template <int KP, int NC, int FAST>
+__global__ void __launch_bounds__(128, 5) uwshcu_batch_resume(const __grid_constant__ UwBatch B)
+{
+    __shared__ double tbl[UW_TBL];
+    for (int t = threadIdx.x; t < UW_TBL; t += blockDim.x) tbl[t] = c_estbl[t];
+    __syncthreads();
+
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int task = 0;
+        if (lane == 0) task = atomicAdd(B.task_head2, 1);
+        task = __shfl_sync(0xffffffffu, task, 0);
+        int m = -1, first = 0;
+        for (int j = 0; j < B.nm; j++) {
+            const int nt = (MN(*B.m[j].hand->count, B.m[j].hand->cap) + 31) / 32;
+            if (m < 0) {
+                if (task < nt) {
+                    m = j;
+                    first = task * 32;
+                } else {
+                    task -= nt;
+                }
+            }
+        }
+        if (m < 0) break;   // same task on every lane: the whole warp leaves
+        const UwHand& H = *B.m[m].hand;
+        const int idx = first + lane;
+        const bool active = idx < MN(*H.count, H.cap);
+        const int slot = active ? H.order[idx] : 0;
+        uw_column<KP, NC, UW_MODE_RESUME, FAST>(B.m[m], tbl, slot, active, nullptr, nullptr);
     }
 }
 

@@ -369,26 +369,17 @@ __global__ void hand_scatter_kernel(const UwHand* __restrict__ H)
 
 // Hand-off region r sized for calls of iend columns with mkx levels and ncnst tracers; nullptr when
 // the device has no room for it (the caller then runs the unsplit worklist pass).
-const UwHand* hand_region(DeviceState& d, int r, int iend, int mkx, int ncnst)
+// Offset of the [count, hist] block in a hand-off region.
+constexpr size_t kHandCountOffset = (sizeof(UwHand) + 255) & ~(size_t)255;
+
+// One hand-off region of cap slots of words doubles: its device UwHand at the start; nullptr when
+// the device has no room for it.
+char* hand_alloc(size_t cap, size_t words)
 {
-    HandRegion& h = d.hand[r];
-    const size_t words = uw_state_words(mkx, ncnst);
-    size_t cap = std::min((size_t)iend, kHandBytes / (words * sizeof(double)));
-    if (S().hand_slots > 0) cap = std::min(cap, (size_t)S().hand_slots);
-    cap = std::max(cap, (size_t)32);
-    if (S().hand_slots > 0 && h.base && h.cap > cap) {   // a smaller limit applies to this region now
-        cudaFree(h.base);
-        h = HandRegion{};
-    }
-    if (h.base && h.cap >= cap && h.words >= words) return reinterpret_cast<const UwHand*>(h.base);
-    cap = std::max(cap, h.cap);
-    const size_t nw = std::max(words, h.words);
     auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
-    const size_t o_cnt = up(sizeof(UwHand)), o_col = o_cnt + up((1 + UW_HAND_KEYS) * sizeof(int)),
+    const size_t o_cnt = kHandCountOffset, o_col = o_cnt + up((1 + UW_HAND_KEYS) * sizeof(int)),
                  o_key = o_col + up(cap * sizeof(int)), o_ord = o_key + up(cap * sizeof(int)),
-                 o_st = o_ord + up(cap * sizeof(int)), bytes = o_st + nw * cap * sizeof(double);
-    if (h.base) cudaFree(h.base);
-    h = HandRegion{};
+                 o_st = o_ord + up(cap * sizeof(int)), bytes = o_st + words * cap * sizeof(double);
     char* base = nullptr;
     if (cudaMalloc(&base, bytes) != cudaSuccess) {
         cudaGetLastError();
@@ -407,6 +398,33 @@ const UwHand* hand_region(DeviceState& d, int r, int iend, int mkx, int ncnst)
         cudaFree(base);
         return nullptr;
     }
+    return base;
+}
+
+// Slots of a region for calls of iend columns with state of words doubles per slot.
+size_t hand_slots_for(int iend, size_t words)
+{
+    size_t cap = std::min((size_t)iend, kHandBytes / (words * sizeof(double)));
+    if (S().hand_slots > 0) cap = std::min(cap, (size_t)S().hand_slots);
+    return std::max(cap, (size_t)32);
+}
+
+const UwHand* hand_region(DeviceState& d, int r, int iend, int mkx, int ncnst)
+{
+    HandRegion& h = d.hand[r];
+    const size_t words = uw_state_words(mkx, ncnst);
+    size_t cap = hand_slots_for(iend, words);
+    if (S().hand_slots > 0 && h.base && h.cap > cap) {   // a smaller limit applies to this region now
+        cudaFree(h.base);
+        h = HandRegion{};
+    }
+    if (h.base && h.cap >= cap && h.words >= words) return reinterpret_cast<const UwHand*>(h.base);
+    cap = std::max(cap, h.cap);
+    const size_t nw = std::max(words, h.words);
+    if (h.base) cudaFree(h.base);
+    h = HandRegion{};
+    char* base = hand_alloc(cap, nw);
+    if (!base) return nullptr;
     h.base = base;
     h.cap = cap;
     h.words = nw;
@@ -425,7 +443,7 @@ cudaError_t worklist_pass(DeviceState& d, int r, UwArgs A, int* list, int* count
     cudaError_t e;
     A.hand = H;
     const HandRegion& h = d.hand[r];
-    int* cnt = reinterpret_cast<int*>(h.base + ((sizeof(UwHand) + 255) & ~(size_t)255));
+    int* cnt = reinterpret_cast<int*>(h.base + kHandCountOffset);
     if ((e = cudaMemsetAsync(cnt, 0, (1 + UW_HAND_KEYS) * sizeof(int), st)) != cudaSuccess) return e;
     if ((e = launch_mode(&A, s.precision, kModeList1, list, count, A.iend, s.block, st)) != cudaSuccess) return e;
     const int nb = (int)std::min((h.cap + 255) / 256, (size_t)1184);
@@ -1380,7 +1398,9 @@ struct BatchPlan {
     UwBatch b[kClasses];           // per used class
     int trig_grid[kClasses];
     int* d_scratch = nullptr;      // [0, 64): counts of all members, [64, 64 + kClasses): task heads,
-                                   // then the worklists
+                                   // [64 + kClasses, 64 + 2 kClasses): resume task heads, worklists
+    bool sorted = false;           // created under the sorted schedule, with a region per member
+    char* hand[UWSHCU_MAX_MEMBERS] = {};
     unsigned int* d_err = nullptr;
     double* d_cush_save = nullptr; // autotune only
     int block = 128, minb = 4, chunk = 1;
@@ -1391,11 +1411,36 @@ struct BatchPlan {
 int plan_enqueue(BatchPlan& P, cudaStream_t st)
 {
     cudaError_t e;
-    if ((e = cudaMemsetAsync(P.d_scratch, 0, (64 + kClasses) * sizeof(int), st)) != cudaSuccess) return cuda_fail(e);
+    if ((e = cudaMemsetAsync(P.d_scratch, 0, (64 + 2 * kClasses) * sizeof(int), st)) != cudaSuccess) return cuda_fail(e);
+    for (int j = 0; j < P.nm && P.sorted; j++)
+        if ((e = cudaMemsetAsync(P.hand[j] + kHandCountOffset, 0, (1 + UW_HAND_KEYS) * sizeof(int), st)) != cudaSuccess)
+            return cuda_fail(e);
     for (int c = 0; c < P.ncls; c++) {
         P.b[c].chunk = P.chunk;
         if ((e = batch_launch(P.prec, P.cls_id[c], &P.b[c], 0, P.trig_grid[c], P.block, 0, st)) != cudaSuccess)
             return cuda_fail(e);
+    }
+    if (P.sorted) {
+        // first worklist launch per class, the sort of each member's hand-off slots, resume launch
+        for (int c = 0; c < P.ncls; c++) {
+            int per_sm = 0;
+            if ((e = batch_occupancy(P.prec, P.cls_id[c], 4, P.block, &per_sm)) != cudaSuccess) return cuda_fail(e);
+            if (per_sm <= 0) return UWSHCU_ERR_BAD_ARGS;
+            if ((e = batch_launch(P.prec, P.cls_id[c], &P.b[c], 2, P.nsm * per_sm, P.block, 4, st)) != cudaSuccess)
+                return cuda_fail(e);
+        }
+        for (int j = 0; j < P.nm; j++) {
+            const UwHand* H = reinterpret_cast<const UwHand*>(P.hand[j]);
+            const int nb = (int)std::min(((size_t)P.mem[j].iend + 255) / 256, (size_t)1184);
+            hand_hist_kernel<<<nb, 256, 0, st>>>(H);
+            hand_scan_kernel<<<1, 32, 0, st>>>(H);
+            hand_scatter_kernel<<<nb, 256, 0, st>>>(H);
+        }
+        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e);
+        for (int c = 0; c < P.ncls; c++)   // 5 resident blocks of 128 threads per SM (launch bounds)
+            if ((e = batch_launch(P.prec, P.cls_id[c], &P.b[c], 3, P.nsm * 5 * (128 / P.block), P.block, 0, st)) != cudaSuccess)
+                return cuda_fail(e);
+        return UWSHCU_OK;
     }
     for (int c = 0; c < P.ncls; c++) {
         int per_sm = 0;
@@ -1413,6 +1458,8 @@ void plan_free(BatchPlan* P)
     if (P->d_scratch) cudaFree(P->d_scratch);
     if (P->d_err) cudaFree(P->d_err);
     if (P->d_cush_save) cudaFree(P->d_cush_save);
+    for (char* h : P->hand)
+        if (h) cudaFree(h);
     delete P;
 }
 
@@ -1445,14 +1492,28 @@ extern "C" int uwshcu_batch_create(int nmembers, const uwshcu_member* members, v
         plan_free(P);
         return cuda_fail(e);
     }
-    if ((e = cudaMalloc(&P->d_scratch, (64 + kClasses + total) * sizeof(int))) != cudaSuccess ||
+    if ((e = cudaMalloc(&P->d_scratch, (64 + 2 * kClasses + total) * sizeof(int))) != cudaSuccess ||
         (e = cudaMalloc(&P->d_err, sizeof(unsigned int))) != cudaSuccess ||
         (e = cudaMemset(P->d_err, 0, sizeof(unsigned int))) != cudaSuccess) {
         plan_free(P);
         return cuda_fail(e);
     }
     int cls_slot[kClasses] = {-1, -1, -1, -1};
-    size_t wl_off = 64 + kClasses;
+    size_t wl_off = 64 + 2 * kClasses;
+    // sorted schedule: a hand-off region per member (a plan without room for them runs two-phase)
+    P->sorted = s.schedule == UWSHCU_SCHED_SORTED;
+    for (int j = 0; j < nmembers && P->sorted; j++) {
+        const size_t words = uw_state_words(members[j].mkx, ncnst);
+        P->hand[j] = hand_alloc(hand_slots_for(members[j].iend, words), words);
+        if (!P->hand[j]) {
+            for (char*& h : P->hand)
+                if (h) {
+                    cudaFree(h);
+                    h = nullptr;
+                }
+            P->sorted = false;
+        }
+    }
     for (int j = 0; j < nmembers; j++) {
         const uwshcu_member& m = members[j];
         P->mem[j] = m;
@@ -1463,6 +1524,7 @@ extern "C" int uwshcu_batch_create(int nmembers, const uwshcu_member* members, v
             UwBatch& b = P->b[P->ncls];
             b = UwBatch{};
             b.task_head = P->d_scratch + 64 + P->ncls;
+            b.task_head2 = P->d_scratch + 64 + kClasses + P->ncls;
             P->trig_grid[P->ncls] = 0;
             P->ncls++;
         }
@@ -1470,6 +1532,7 @@ extern "C" int uwshcu_batch_create(int nmembers, const uwshcu_member* members, v
         UwBatch& b = P->b[c];
         const int slot = b.nm++;
         b.m[slot] = member_args(m, ncnst, P->d_err);
+        b.m[slot].hand = reinterpret_cast<const UwHand*>(P->hand[j]);
         b.wl[slot] = P->d_scratch + wl_off;
         wl_off += (size_t)m.iend;
     }

@@ -22,7 +22,8 @@ extern "C" cudaError_t uw_mixed_launch_k64n5(const UwArgs* a, int mode, int* wl,
     return cudaGetLastError();
 }
 
-// Batched trigger (phase 0) and persistent worklist (phase 1) launches of this precision mode;
+// Batched trigger (phase 0), persistent worklist (phase 1), and for the sorted schedule the
+// persistent first worklist (phase 2) and resume (phase 3) launches of this precision mode;
 // minb selects the worklist instantiation (only the ones compiled here).
 extern "C" cudaError_t uw_mixed_batch_k64n5(const UwBatch* b, int phase, int grid, int block, int minb,
                                           cudaStream_t stream)
@@ -30,6 +31,14 @@ extern "C" cudaError_t uw_mixed_batch_k64n5(const UwBatch* b, int phase, int gri
     if (grid <= 0) return cudaSuccess;
     if (phase == 0) {
         uwshcu_batch_trigger<64, 5, 0><<<grid, block, 0, stream>>>(*b);
+        return cudaGetLastError();
+    }
+    if (phase == 2) {   // sorted schedule: first worklist launch (register cap of minb 4)
+        uwshcu_batch_list<64, 5, 4, 0, UW_MODE_LIST1><<<grid, block, 0, stream>>>(*b);
+        return cudaGetLastError();
+    }
+    if (phase == 3) {   // sorted schedule: resume launch
+        uwshcu_batch_resume<64, 5, 0><<<grid, block, 0, stream>>>(*b);
         return cudaGetLastError();
     }
     if (minb == 4) {

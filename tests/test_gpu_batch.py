@@ -38,15 +38,19 @@ def _poison(case):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("sched", ["sorted", "two_phase"])
 @pytest.mark.parametrize("prec", ["fp64", "fast", "mixed"])
-def test_batch_matches_single_member_calls(uw, cuda, prec):
-    """In every precision mode: the reduced-precision conden iterations stop per lane, so a column's
+def test_batch_matches_single_member_calls(uw, cuda, prec, sched):
+    """In every precision mode and both worklist schedules (a plan takes the schedule in force when
+    it is created: sorted plans hand each member's implicit-CIN columns to its own region and resume
+    them in depth order): the reduced-precision conden iterations stop per lane, so a column's
     result does not depend on which columns share its warp and the batch reproduces the single calls."""
     import torch
 
     assert uw.init_default() == 0
     mode = {"fp64": uw.PREC_FP64, "fast": uw.PREC_FAST, "mixed": uw.PREC_MIXED}[prec]
     assert uw.set_precision(mode) == 0
+    assert uw.set_schedule(uw.SCHED_SORTED if sched == "sorted" else uw.SCHED_TWO_PHASE) == 0
     ref, bat = _cases(uw)
     want = []
     for r in ref:
@@ -87,6 +91,7 @@ def test_batch_matches_single_member_calls(uw, cuda, prec):
     finally:
         plan.close()
         uw.set_precision(uw.PREC_FP64)
+        uw.set_schedule(uw.SCHED_DEFAULT)
 
 
 def test_batch_rejects_bad_plans_before_touching_the_device(uw):
