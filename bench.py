@@ -400,6 +400,53 @@ def run_tangent(args):
     print(json.dumps(line), flush=True)
 
 
+def run_adjoint(args):
+    """Cost of the adjoint model against the forward pass: 65,536 columns x 30 levels, cotangents on
+    every differentiable output, gradients in t0, qv0, tke, pblh and the four tuning parameters."""
+    import torch
+    import soundings
+    import uwshcu_b200 as uw
+
+    torch.cuda.set_device(0)
+    assert uw.init_default() == 0
+    n = 65_536
+    s = soundings.make_soundings(n, PVER, seed=301, rh_pbl=RH_PBL)
+    case = uw.DeviceCase(s)
+    g = torch.Generator(device="cpu").manual_seed(11)
+    cot = {k: torch.randn(v.shape, generator=g, dtype=torch.float64).cuda() for k, v in case.out.items()
+           if k in uw.ADJ_OUTPUTS}
+    stream = torch.cuda.Stream()
+
+    def timed(fn, steps):
+        with torch.cuda.stream(stream):
+            for _ in range(max(args.warmup, 3)):
+                case.reset_cush()
+                fn()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                case.reset_cush()
+                fn()
+            e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    def adjoint():
+        rc, _ = uw.adjoint_launch(case, cot, stream=stream)
+        assert rc == 0, (rc, uw.last_cuda_error())
+
+    fwd = timed(lambda: case.launch(stream=stream), args.steps)
+    adj = timed(adjoint, max(1, min(args.steps, 5)))
+    line = {"metric": "adjoint cost / forward cost (compute_uwshcu, 65,536 x 30, FP64)",
+            "value": adj / fwd, "unit": "ratio", "higher_is_better": False, "n_gpus": 1,
+            "steps": max(1, min(args.steps, 5)), "warmup": max(args.warmup, 3), "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "65,536 columns x 30 levels, random cotangents on every differentiable "
+                                   "output"},
+            "forward_ms": fwd, "adjoint_ms": adj, "tape_rows_per_warp": uw.adjoint_last_records()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -414,7 +461,7 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fast", "mixed"],
                     help="fp64: bit-exact (default); fast: FP64 with the early-stopping conden; "
                          "mixed: FP32 bulk with FP64 islands")
-    ap.add_argument("--config", default="fp64", choices=["fp64", "batched", "tangent"],
+    ap.add_argument("--config", default="fp64", choices=["fp64", "batched", "tangent", "adjoint"],
                     help="fp64: the 259,200-column workload (default); batched: 4 uneven members")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -423,6 +470,8 @@ def main():
         return run_batched(args)
     if args.config == "tangent":
         return run_tangent(args)
+    if args.config == "adjoint":
+        return run_adjoint(args)
 
     import torch
     import soundings

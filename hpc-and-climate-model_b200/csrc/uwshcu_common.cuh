@@ -110,6 +110,25 @@ struct UwHand {
     int* hist;       // UW_HAND_KEYS counters of the sort
 };
 
+// One batch of the adjoint model (device addresses): slot t is worklist entry wl[b0 + t], t < nb, and
+// warp w holds slots 32w .. 32w+31.  Warp w's tape (uw_adj.h) has rcap rows, its adjoints
+// (index x of lane l at x * 32 + l) start at adj + w * astride; slot t's output-index table entry
+// (f, k) is ids[(f * KP + k) * cap + t].
+struct UwAdjHost {
+    const int* wl;
+    int b0, nb;
+    void* ab;            // int2 operand indices, warp w at w * rcap * 32
+    void* d;             // double2 partials, same layout
+    int rcap;            // tape rows per warp
+    int* ids;
+    int cap;
+    int* nrow;           // rows taken per warp
+    int* ovf;            // tape overflow per warp
+    double* adj;
+    size_t astride;      // doubles of adjoints per warp
+    unsigned int* status;
+};
+
 // Pointers of one compute_uwshcu call (device addresses), in the Fortran argument order.
 struct UwArgs {
     int mix, mkx, iend, ncnst;

@@ -7,6 +7,7 @@
 // every column-physics step (findsp included) runs on the GPU, and a call costs one H2D copy of the
 // packed inputs, one kernel launch and one D2H copy of the packed outputs.
 #include <cuda_runtime.h>
+#include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
 #include <cmath>
@@ -47,6 +48,10 @@ extern "C" cudaError_t uw_budget_launch(int mix, int mkx, int iend, int inv, dou
                                         const double* uten, const double* vten, const double* precip,
                                         const double* snow, const double* rliq, double* te_rer,
                                         double* tw_rer, cudaStream_t stream);
+extern "C" cudaError_t uw_adj_set_constants_k32n5(const UwConst* h, const double* tbl);
+extern "C" cudaError_t uw_adj_launch_k32n5(const UwArgs* a, const void* slots, const uwshcu_adjoint* c, int phase,
+                                           cudaStream_t stream);
+extern "C" size_t uw_adj_row_bytes_k32n5();
 extern "C" cudaError_t uw_tl_set_constants_k32n5(const UwConst* h, const double* tbl);
 extern "C" cudaError_t uw_tl_set_constants_k64n5(const UwConst* h, const double* tbl);
 extern "C" cudaError_t uw_tl_launch_k32n5(const UwArgs* a, const uwshcu_tangent* t, int mode, int* wl,
@@ -81,6 +86,7 @@ cudaError_t set_constants_all(const UwConst* k, const double* tbl)
     if ((e = uw_fast_set_constants_k32n32(k, tbl)) != cudaSuccess) return e;
     if ((e = uw_fast_set_constants_k64n32(k, tbl)) != cudaSuccess) return e;
     if ((e = uw_tl_set_constants_k32n5(k, tbl)) != cudaSuccess) return e;
+    if ((e = uw_adj_set_constants_k32n5(k, tbl)) != cudaSuccess) return e;
     if ((e = uw_tl_set_constants_k64n5(k, tbl)) != cudaSuccess) return e;
     if ((e = uw_mixed_set_constants_k32n5(k, tbl)) != cudaSuccess) return e;
     return uw_mixed_set_constants_k64n5(k, tbl);
@@ -137,6 +143,9 @@ struct DeviceState {
     std::vector<cudaEvent_t> done, ev_in, ev_comp;   // per chunk: copied out, copied in, computed
     // hand-off regions of the split worklist pass: [0] device-array calls, [1 + j] pipe stream j
     HandRegion hand[1 + kPipe];
+    // adjoint tapes, adjoints and tables, kept between adjoint calls (uwshcu_adjoint_release)
+    void* adj_buf = nullptr;
+    size_t adj_bytes = 0;
 };
 
 struct State {
@@ -148,6 +157,8 @@ struct State {
     int precision = UWSHCU_PREC_FP64;
     int schedule = UWSHCU_SCHED_SORTED;
     int hand_slots = 0;          // cap of the hand-off slots per region (0: by kHandBytes only)
+    int adj_records = 0;         // largest tape of the last adjoint call (rows per warp)
+    int adj_rows = 0;            // tape rows per warp for the next adjoint call (0: kAdjRows)
     int block = 128;
     bool profiling = false;
     int chunk_columns = 32768;   // host-array calls: columns per pipeline chunk (0: one chunk)
@@ -705,6 +716,17 @@ int host_call(int inv, int mix, int mkx, int iend, int ncnst, double dt, const d
     return status_from_bits(bits);
 }
 
+// Zeroes the adjoints of the index space warp w used: (nin + rows of the warp) x 32 doubles at
+// adj + w * astride, one block per warp.
+__global__ void adj_zero_kernel(double* __restrict__ adj, size_t astride, const int* __restrict__ nrow, int nin,
+                                int rcap)
+{
+    const int w = blockIdx.x;
+    const size_t n = (size_t)(nin + min(nrow[w], rcap)) * 32 / 2;
+    double2* p = reinterpret_cast<double2*>(adj + (size_t)w * astride);
+    for (size_t j = threadIdx.x; j < n; j += blockDim.x) p[j] = make_double2(0.0, 0.0);
+}
+
 __global__ void eval_math_kernel(int fn, const double* __restrict__ x, const double* __restrict__ y,
                                  double* __restrict__ out, int n)
 {
@@ -932,7 +954,7 @@ int uwshcu_finalize(void)
     bool have = cudaGetDevice(&cur) == cudaSuccess;
     for (int dv = 0; dv < kMaxDev; dv++) {
         DeviceState& d = s.dev[dv];
-        if (!d.d_err && !d.d_buf && !d.h_buf && !d.stream && !d.pipe[0]) continue;
+        if (!d.d_err && !d.d_buf && !d.h_buf && !d.stream && !d.pipe[0] && !d.adj_buf) continue;
         cudaSetDevice(dv);
         if (d.d_buf) cudaFree(d.d_buf);
         if (d.h_buf) cudaFreeHost(d.h_buf);
@@ -940,6 +962,7 @@ int uwshcu_finalize(void)
         if (d.d_wl) cudaFree(d.d_wl);
         for (HandRegion& h : d.hand)
             if (h.base) cudaFree(h.base);
+        if (d.adj_buf) cudaFree(d.adj_buf);
         for (int n = 0; n < DeviceState::kSlots; n++)
             for (int j = 0; j < 3; j++)
                 if (d.ev[n][j]) cudaEventDestroy(d.ev[n][j]);
@@ -1177,6 +1200,177 @@ int uwshcu_tangent_device(const uwshcu_member* m, const uwshcu_tangent* t, void*
     if ((e = launch(&A, t, kModeList, d->d_wl + 1, d->d_wl, m->iend, 128, st)) != cudaSuccess) return cuda_fail(e);
     return UWSHCU_OK;
 }
+
+// Tape rows per warp of the adjoint model (32 records of 24 B each): a warp of
+// convecting 30-level columns takes ~1.5e5 rows.
+constexpr int kAdjRows = 1 << 18;
+
+int uwshcu_adjoint_device(const uwshcu_member* m, const uwshcu_adjoint* a, void* stream)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    if (!s.init) return UWSHCU_ERR_NOT_INITIALIZED;
+    if (!m || !a) return UWSHCU_ERR_BAD_ARGS;
+    const int ncnst = s.k.ncnst;
+    if (s.precision != UWSHCU_PREC_FP64 || ncnst > 5 || m->mkx + 1 > 32) return UWSHCU_ERR_BAD_ARGS;
+    if (!member_ok(*m, ncnst)) return UWSHCU_ERR_BAD_ARGS;
+    DeviceState* d = nullptr;
+    int rc = ensure_device(&d);
+    if (rc != UWSHCU_OK) return rc;
+    const UwArgs A = member_args(*m, ncnst, d->d_err);
+    const size_t mix = (size_t)m->mix, mkx = (size_t)m->mkx;
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e;
+    // gradients start at zero: the columns that leave the scheme in the trigger pass keep it
+    const std::pair<double*, size_t> grads[] = {{a->t0, mix * mkx}, {a->qv0, mix * mkx}, {a->tke, mix * (mkx + 1)},
+                                                {a->pblh, mix}, {a->rpen, mix}, {a->rle, mix}, {a->rkm, mix},
+                                                {a->criqc, mix}};
+    for (const auto& g : grads)
+        if (g.first && (e = cudaMemsetAsync(g.first, 0, g.second * sizeof(double), st)) != cudaSuccess) return cuda_fail(e);
+    if (m->iend == 0) return UWSHCU_OK;
+    // trigger pass of the FP64 path: the exit columns' outputs and the worklist of the others
+    if ((rc = grow_worklist(*d, (size_t)m->iend)) != UWSHCU_OK) return rc;
+    if ((e = cudaMemsetAsync(d->d_wl, 0, sizeof(int), st)) != cudaSuccess) return cuda_fail(e);
+    if ((e = launch_mode(&A, UWSHCU_PREC_FP64, kModeTrigger, d->d_wl + 1, d->d_wl, m->iend, 128, st)) != cudaSuccess)
+        return cuda_fail(e);
+    int ncand = 0;
+    if ((e = cudaMemcpyAsync(&ncand, d->d_wl, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return cuda_fail(e);
+    s.adj_records = 0;
+    if (ncand == 0) return UWSHCU_OK;
+    // Batches of warps (32 slots each) whose tapes fit 3/4 of the device memory that is free or
+    // already held by the adjoint buffer.  The tape capacity is sized from the previous call's largest
+    // tape (+1/8); a batch that overflows it makes the call start again at the full capacity.
+    const size_t nin = 3 * mkx + 6, rowb = uw_adj_row_bytes_k32n5();
+    const size_t nids = (size_t)(25 + 5) * 32;   // output-index table entries per slot (KP = 32, NC = 5)
+    const size_t nw_need = ((size_t)ncand + 31) / 32;
+    auto up = [](size_t x) { return (x + 255) / 256 * 256; };
+    // the candidates in ascending column order: the warps' columns, and with them the tapes and the
+    // order of every reduction, do not depend on the order the trigger pass appended them in
+    int end_bit = 1;
+    while (end_bit < 31 && ((size_t)1 << end_bit) < (size_t)m->iend) end_bit++;
+    size_t sort_bytes = 0;
+    if ((e = cub::DeviceRadixSort::SortKeys(nullptr, sort_bytes, d->d_wl + 1, d->d_wl + 1, ncand, 0, end_bit, st)) !=
+        cudaSuccess)
+        return cuda_fail(e);
+    bool restart = false;
+    double* cush_saved = nullptr;
+    for (size_t rcap = s.adj_rows > 0 ? (size_t)s.adj_rows : (size_t)kAdjRows;; restart = true) {
+        const size_t astride = (nin + rcap) * 32;
+        const size_t per_warp = rcap * rowb + astride * sizeof(double) + 32 * nids * sizeof(int) + 2 * sizeof(int) + 1024;
+        size_t freeb = 0, totalb = 0;
+        if ((e = cudaMemGetInfo(&freeb, &totalb)) != cudaSuccess) return cuda_fail(e);
+        const size_t avail = (freeb + d->adj_bytes) / 4 * 3;
+        const size_t nw = std::min(nw_need, std::max((size_t)1, avail / per_warp)), nb = 32 * nw;
+        // carve the buffer: tapes (operand indices, partials), adjoints, tables, counters, status
+        const size_t o_ab = 0, o_d = o_ab + up(nw * rcap * 32 * 8), o_adj = o_d + up(nw * rcap * 32 * 16);
+        const size_t o_ids = o_adj + up(nw * astride * sizeof(double)), o_nrow = o_ids + up(nb * nids * sizeof(int));
+        const size_t o_st = o_nrow + up(2 * nw * sizeof(int)), o_wl = o_st + 256, o_tmp = o_wl + up(ncand * sizeof(int));
+        const size_t o_cush = o_tmp + up(sort_bytes), bytes = o_cush + up((size_t)m->iend * sizeof(double));
+        // cush is read and written by the forward sweep: a call that starts again puts back the values
+        // the trigger pass left (saved in the buffer before it may be replaced), then saves them anew
+        if (restart && (e = cudaMemcpyAsync(m->cush, cush_saved, (size_t)m->iend * sizeof(double),
+                                            cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
+            return cuda_fail(e);
+        if (bytes > d->adj_bytes) {   // grown with 1/16 to spare, so that calls of similar size reuse it
+            const size_t held = freeb + d->adj_bytes;
+            if (d->adj_buf) cudaFree(d->adj_buf);
+            d->adj_buf = nullptr;
+            d->adj_bytes = 0;
+            const size_t want = std::min(bytes + bytes / 16, std::max(bytes, held - held / 8));
+            if ((e = cudaMalloc(&d->adj_buf, want)) != cudaSuccess) return cuda_fail(e);
+            d->adj_bytes = want;
+        }
+        char* base = static_cast<char*>(d->adj_buf);
+        cush_saved = reinterpret_cast<double*>(base + o_cush);
+        if ((e = cudaMemcpyAsync(cush_saved, m->cush, (size_t)m->iend * sizeof(double), cudaMemcpyDeviceToDevice, st)) !=
+            cudaSuccess)
+            return cuda_fail(e);
+        int* nrow = reinterpret_cast<int*>(base + o_nrow);
+        unsigned int* status = reinterpret_cast<unsigned int*>(base + o_st);
+        int* wl = reinterpret_cast<int*>(base + o_wl);
+        size_t tmp_bytes = sort_bytes;
+        if ((e = cudaMemsetAsync(status, 0, sizeof(unsigned int), st)) != cudaSuccess ||
+            (e = cub::DeviceRadixSort::SortKeys(base + o_tmp, tmp_bytes, d->d_wl + 1, wl, ncand, 0, end_bit, st)) !=
+                cudaSuccess)
+            return cuda_fail(e);
+        std::vector<int> counts(nw);
+        int most = 0;
+        unsigned int bits = 0;
+        for (size_t b0 = 0; b0 < (size_t)ncand && !bits; b0 += nb) {
+            UwAdjHost h{};
+            h.wl = wl;
+            h.b0 = (int)b0;
+            h.nb = (int)std::min(nb, (size_t)ncand - b0);
+            h.ab = base + o_ab;
+            h.d = base + o_d;
+            h.rcap = (int)rcap;
+            h.ids = reinterpret_cast<int*>(base + o_ids);
+            h.cap = (int)nb;
+            h.nrow = nrow;
+            h.ovf = nrow + nw;
+            h.adj = reinterpret_cast<double*>(base + o_adj);
+            h.astride = astride;
+            h.status = status;
+            const size_t used = ((size_t)h.nb + 31) / 32;   // warps holding a slot
+            if ((e = cudaMemsetAsync(h.ids, 0xff, nb * nids * sizeof(int), st)) != cudaSuccess ||
+                (e = uw_adj_launch_k32n5(&A, &h, a, 0, st)) != cudaSuccess)
+                return cuda_fail(e);
+            adj_zero_kernel<<<(unsigned)used, 512, 0, st>>>(h.adj, astride, nrow, (int)nin, (int)rcap);
+            if ((e = cudaGetLastError()) != cudaSuccess || (e = uw_adj_launch_k32n5(&A, &h, a, 1, st)) != cudaSuccess ||
+                (e = cudaMemcpyAsync(counts.data(), nrow, used * sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+                (e = cudaMemcpyAsync(&bits, status, sizeof(unsigned int), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+                (e = cudaStreamSynchronize(st)) != cudaSuccess)
+                return cuda_fail(e);
+            for (size_t j = 0; j < used; j++) most = std::max(most, counts[j]);
+        }
+        s.adj_records = most;
+        if (bits && rcap < (size_t)kAdjRows) {   // the sized capacity was too small: again at the full one
+            rcap = kAdjRows;
+            continue;
+        }
+        s.adj_rows = (int)std::min((size_t)kAdjRows, ((size_t)most + most / 8 + 4095) / 4096 * 4096);
+        if (bits) {
+            s.adj_rows = 0;
+            std::snprintf(s.lasterr, sizeof(s.lasterr),
+                          "uwshcu_adjoint_device: a warp's tape exceeds %d rows (largest %d)", kAdjRows, most);
+            return UWSHCU_ERR_TOO_LARGE;
+        }
+        return UWSHCU_OK;
+    }
+}
+
+int uwshcu_set_adjoint_rows(int rows)
+{
+    if (rows < 0 || rows > kAdjRows) return UWSHCU_ERR_BAD_ARGS;
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    s.adj_rows = rows;
+    return UWSHCU_OK;
+}
+
+int uwshcu_adjoint_release(void)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    int cur = 0;
+    const bool have = cudaGetDevice(&cur) == cudaSuccess;
+    cudaError_t e = cudaSuccess;
+    for (int dv = 0; dv < kMaxDev; dv++) {
+        DeviceState& d = s.dev[dv];
+        if (!d.adj_buf) continue;
+        cudaSetDevice(dv);
+        const cudaError_t f = cudaFree(d.adj_buf);
+        if (f != cudaSuccess) e = f;
+        d.adj_buf = nullptr;
+        d.adj_bytes = 0;
+    }
+    if (have) cudaSetDevice(cur);
+    return e == cudaSuccess ? UWSHCU_OK : cuda_fail(e);
+}
+
+int uwshcu_adjoint_last_records(void) { return S().adj_records; }
 
 int uwshcu_eval_math(int fn, const double* x, const double* y, double* out, int n, void* stream)
 {

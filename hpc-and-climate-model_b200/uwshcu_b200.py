@@ -46,7 +46,8 @@ EXPORTS = ("uwshcu_init", "uwshcu_set_rpen", "uwshcu_init_default", "uwshcu_set_
            "uwshcu_batch_capture", "uwshcu_batch_autotune", "uwshcu_batch_status",
            "uwshcu_batch_destroy", "uwshcu_set_pipeline", "uwshcu_set_params",
            "uwshcu_budget_device", "uwshcu_tangent_device", "uwshcu_compute_member",
-           "uwshcu_set_hand_slots")
+           "uwshcu_set_hand_slots", "uwshcu_adjoint_device", "uwshcu_adjoint_last_records",
+           "uwshcu_adjoint_release", "uwshcu_set_adjoint_rows")
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
@@ -431,3 +432,50 @@ def tangent_launch(case, dirs=None, dparams=(0.0, 0.0, 0.0, 0.0), inv=0, stream=
     if rc != 0:
         raise RuntimeError("uwshcu_tangent_device: %d %s" % (rc, last_cuda_error()))
     return tout
+
+
+# ---- adjoint model -----------------------------------------------------------------------------------
+_ADJ_GRAD = ("t0", "qv0", "tke", "pblh", "rpen", "rle", "rkm", "criqc")
+# outputs that take a cotangent in adjoint_launch
+ADJ_OUTPUTS = tuple(_TANGENT_OUT)
+
+
+class Adjoint(ctypes.Structure):
+    """uwshcu_adjoint of include/uwshcu.h."""
+    _fields_ = [(n, ctypes.c_void_p) for n in _TANGENT_OUT] + [(n, ctypes.c_void_p) for n in _ADJ_GRAD]
+
+
+def adjoint_launch(case, cot, inv=0, stream=None):
+    """One uwshcu_adjoint_device call on a DeviceCase: `cot` maps output names to device tensors
+    shaped like case.out (the cotangents; missing ones are zero).  Returns (status, gradients): t0,
+    qv0 (mkx, n), tke (mkx + 1, n), pblh (n) and the per-column parameter gradients rpen, rle, rkm,
+    criqc (n), as torch tensors; the case's own outputs get the FP64 values."""
+    import torch
+    st = stream if stream is not None else torch.cuda.current_stream()
+    dev = case.out["umf"].device
+    n, mkx = case.n, case.mkx
+    grads = {"t0": torch.zeros((mkx, n), dtype=torch.float64, device=dev),
+             "qv0": torch.zeros((mkx, n), dtype=torch.float64, device=dev),
+             "tke": torch.zeros((mkx + 1, n), dtype=torch.float64, device=dev)}
+    grads.update({k: torch.zeros(n, dtype=torch.float64, device=dev) for k in _ADJ_GRAD[3:]})
+    a = Adjoint()
+    for k in _TANGENT_OUT:
+        c = cot.get(k)
+        setattr(a, k, c.data_ptr() if c is not None else None)
+    for k in _ADJ_GRAD:
+        setattr(a, k, grads[k].data_ptr())
+    m = member_of(case, inv)
+    rc = lib().uwshcu_adjoint_device(ctypes.byref(m), ctypes.byref(a), ctypes.c_void_p(st.cuda_stream))
+    return rc, grads
+
+
+def adjoint_last_records():
+    return lib().uwshcu_adjoint_last_records()
+
+
+def adjoint_release():
+    return lib().uwshcu_adjoint_release()
+
+
+def set_adjoint_rows(rows):
+    return lib().uwshcu_set_adjoint_rows(ctypes.c_int(rows))

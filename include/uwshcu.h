@@ -315,6 +315,48 @@ typedef struct uwshcu_tangent {
  * FP64 precision setting only; mkx + 1 <= 64, ncnst <= 5. */
 int uwshcu_tangent_device(const uwshcu_member *m, const uwshcu_tangent *t, void *stream);
 
+/* ---- adjoint model ------------------------------------------------------------------------------ */
+
+/* Cotangents and gradients of an adjoint call (device arrays).  The cotangents ("output weights")
+ * have the layouts of the outputs of the same name; NULL means zero.  The gradients have the layouts
+ * of the inputs (t0, qv0: (mix, mkx); tke: (mix, mkx+1); pblh: (mix)); the tuning-parameter
+ * gradients are per column (mix): the gradient of the whole call is their sum over the columns.
+ * A NULL gradient is not computed. */
+typedef struct uwshcu_adjoint {
+    const double *cush, *umf, *slflx, *qtflx, *flxprc1, *flxsnow1, *qvten, *qlten, *qiten, *sten,
+        *uten, *vten, *trten, *qrten, *qsten, *precip, *snow, *evapc, *cufrc, *qcu, *qlu, *qiu, *cbmf,
+        *qc, *rliq, *wu;
+    double *t0, *qv0, *tke, *pblh;
+    double *rpen, *rle, *rkm, *criqc;
+} uwshcu_adjoint;
+
+/* No counterpart in the reference.  Adjoint (reverse mode) of compute_uwshcu: for the member `m` it
+ * computes the outputs (bit for bit those of uwshcu_compute_device) and the gradient of
+ * J = sum over outputs of (cotangent x output) with respect to t0, qv0, tke, pblh and, per column,
+ * rpen, rle, rkm and criqc -- the transpose of uwshcu_tangent_device (the derivative is that of the
+ * branch the FP64 path takes; a saturation adjustment's derivative is taken at its converged
+ * state).  The columns that leave the scheme in the trigger pass have constant outputs and zero
+ * gradients; the others run a taped forward sweep (a tape per warp of 32 columns) and a reverse
+ * sweep, in batches that fit 3/4 of the device memory that is free or already held by the adjoint
+ * buffer.  The library keeps that buffer between calls (release it with uwshcu_adjoint_release) and
+ * sizes the tapes from the previous call's largest tape.  Waits for `stream` before it returns.
+ * FP64 precision setting; mkx + 1 <= 32, ncnst <= 5.  UWSHCU_ERR_TOO_LARGE if a warp's tape exceeds
+ * 2^18 rows. */
+int uwshcu_adjoint_device(const uwshcu_member *m, const uwshcu_adjoint *a, void *stream);
+
+/* Largest tape of the last uwshcu_adjoint_device call, in rows per warp of 32 columns (a sizing
+ * aid). */
+int uwshcu_adjoint_last_records(void);
+
+/* No counterpart in the reference.  Tape capacity of the next uwshcu_adjoint_device call, in rows per
+ * warp (1 .. 2^18; 0: the library's choice).  A batch that overflows it makes that call start again at
+ * 2^18 rows; later calls size the tapes from the largest tape seen. */
+int uwshcu_set_adjoint_rows(int rows);
+
+/* No counterpart in the reference.  Frees the adjoint buffer on every device (uwshcu_finalize
+ * frees it too); the next adjoint call allocates it again. */
+int uwshcu_adjoint_release(void);
+
 /* Column limit of uwshcu_compute_device_noalloc: its worklist is one fixed device array of
  * 64 + UWSHCU_NOALLOC_MAX_COLUMNS ints (4 MiB + 256 B) that every GPU which loads the library holds
  * until the process exits. */
