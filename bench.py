@@ -409,7 +409,7 @@ def run_adjoint(args):
 
     torch.cuda.set_device(0)
     assert uw.init_default() == 0
-    n = 65_536
+    n = args.columns
     s = soundings.make_soundings(n, PVER, seed=301, rh_pbl=RH_PBL)
     case = uw.DeviceCase(s)
     g = torch.Generator(device="cpu").manual_seed(11)
@@ -437,12 +437,12 @@ def run_adjoint(args):
 
     fwd = timed(lambda: case.launch(stream=stream), args.steps)
     adj = timed(adjoint, max(1, min(args.steps, 5)))
-    line = {"metric": "adjoint cost / forward cost (compute_uwshcu, 65,536 x 30, FP64)",
+    line = {"metric": "adjoint cost / forward cost (compute_uwshcu, %s x 30, FP64)" % f"{n:,}",
             "value": adj / fwd, "unit": "ratio", "higher_is_better": False, "n_gpus": 1,
             "steps": max(1, min(args.steps, 5)), "warmup": max(args.warmup, 3), "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": "65,536 columns x 30 levels, random cotangents on every differentiable "
-                                   "output"},
+            "config": {"workload": "%s columns x 30 levels, random cotangents on every differentiable "
+                                   "output" % f"{n:,}"},
             "forward_ms": fwd, "adjoint_ms": adj, "tape_rows_per_warp": uw.adjoint_last_records()}
     print(json.dumps(line), flush=True)
 
@@ -454,6 +454,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--ncol", type=int, default=NCOL)
+    ap.add_argument("--columns", type=int, default=65536,
+                    help="columns of the tangent and adjoint cost configs (65,536 by default)")
     ap.add_argument("--cpu-sample", type=int, default=32768)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")

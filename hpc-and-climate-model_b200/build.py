@@ -39,6 +39,7 @@ UNITS = {
     "uwshcu_tl_k64n5.cu": ["-fmad=false"],
     # adjoint kernels: no FMA contraction, so their forward values are the FP64 path's bits
     "uwshcu_adj_k32n5.cu": ["-fmad=false"],
+    "uwshcu_adj_k64n5.cu": ["-fmad=false"],
     "uwshcu_host.cu": [],
 }
 

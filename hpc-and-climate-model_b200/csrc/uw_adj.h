@@ -62,7 +62,7 @@ struct Ad {
 // The row of a record with operands (a, da) and (b, db): the lane's next row.  Called, not inlined:
 // the column code records from ~10^4 sites, and one shared copy keeps the kernel's code inside the
 // instruction cache.
-__device__ __noinline__ int ad_row(int a, double da, int b, double db)
+static __device__ __noinline__ int ad_row(int a, double da, int b, double db)
 {
     AdWarpTape& t = uw_adj_tape();
     const int lane = threadIdx.x & 31;

@@ -52,6 +52,9 @@ extern "C" cudaError_t uw_adj_set_constants_k32n5(const UwConst* h, const double
 extern "C" cudaError_t uw_adj_launch_k32n5(const UwArgs* a, const void* slots, const uwshcu_adjoint* c, int phase,
                                            cudaStream_t stream);
 extern "C" size_t uw_adj_row_bytes_k32n5();
+extern "C" cudaError_t uw_adj_set_constants_k64n5(const UwConst* h, const double* tbl);
+extern "C" cudaError_t uw_adj_launch_k64n5(const UwArgs* a, const void* slots, const uwshcu_adjoint* c, int phase,
+                                           cudaStream_t stream);
 extern "C" cudaError_t uw_tl_set_constants_k32n5(const UwConst* h, const double* tbl);
 extern "C" cudaError_t uw_tl_set_constants_k64n5(const UwConst* h, const double* tbl);
 extern "C" cudaError_t uw_tl_launch_k32n5(const UwArgs* a, const uwshcu_tangent* t, int mode, int* wl,
@@ -87,6 +90,7 @@ cudaError_t set_constants_all(const UwConst* k, const double* tbl)
     if ((e = uw_fast_set_constants_k64n32(k, tbl)) != cudaSuccess) return e;
     if ((e = uw_tl_set_constants_k32n5(k, tbl)) != cudaSuccess) return e;
     if ((e = uw_adj_set_constants_k32n5(k, tbl)) != cudaSuccess) return e;
+    if ((e = uw_adj_set_constants_k64n5(k, tbl)) != cudaSuccess) return e;
     if ((e = uw_tl_set_constants_k64n5(k, tbl)) != cudaSuccess) return e;
     if ((e = uw_mixed_set_constants_k32n5(k, tbl)) != cudaSuccess) return e;
     return uw_mixed_set_constants_k64n5(k, tbl);
@@ -158,7 +162,7 @@ struct State {
     int schedule = UWSHCU_SCHED_SORTED;
     int hand_slots = 0;          // cap of the hand-off slots per region (0: by kHandBytes only)
     int adj_records = 0;         // largest tape of the last adjoint call (rows per warp)
-    int adj_rows = 0;            // tape rows per warp for the next adjoint call (0: kAdjRows)
+    int adj_rows = 0;            // tape rows per warp for the next adjoint call (0: the unit's full capacity)
     int block = 128;
     bool profiling = false;
     int chunk_columns = 32768;   // host-array calls: columns per pipeline chunk (0: one chunk)
@@ -1201,9 +1205,9 @@ int uwshcu_tangent_device(const uwshcu_member* m, const uwshcu_tangent* t, void*
     return UWSHCU_OK;
 }
 
-// Tape rows per warp of the adjoint model (32 records of 24 B each): a warp of
-// convecting 30-level columns takes ~1.5e5 rows.
-constexpr int kAdjRows = 1 << 18;
+// Tape rows per warp of the adjoint model (32 records of 24 B each) at full capacity: a warp of
+// convecting 30-level columns takes ~1.3e5 rows, of 51-level columns about twice that.
+constexpr int kAdjRows32 = 1 << 18, kAdjRows64 = 1 << 19;
 
 int uwshcu_adjoint_device(const uwshcu_member* m, const uwshcu_adjoint* a, void* stream)
 {
@@ -1212,13 +1216,17 @@ int uwshcu_adjoint_device(const uwshcu_member* m, const uwshcu_adjoint* a, void*
     if (!s.init) return UWSHCU_ERR_NOT_INITIALIZED;
     if (!m || !a) return UWSHCU_ERR_BAD_ARGS;
     const int ncnst = s.k.ncnst;
-    if (s.precision != UWSHCU_PREC_FP64 || ncnst > 5 || m->mkx + 1 > 32) return UWSHCU_ERR_BAD_ARGS;
+    if (s.precision != UWSHCU_PREC_FP64 || ncnst > 5 || m->mkx + 1 > 64) return UWSHCU_ERR_BAD_ARGS;
     if (!member_ok(*m, ncnst)) return UWSHCU_ERR_BAD_ARGS;
     DeviceState* d = nullptr;
     int rc = ensure_device(&d);
     if (rc != UWSHCU_OK) return rc;
     const UwArgs A = member_args(*m, ncnst, d->d_err);
     const size_t mix = (size_t)m->mix, mkx = (size_t)m->mkx;
+    // the unit for the level count: KP = 32 or 64 levels
+    const bool k32 = m->mkx + 1 <= 32;
+    auto adj_launch = k32 ? uw_adj_launch_k32n5 : uw_adj_launch_k64n5;
+    const int full_rows = k32 ? kAdjRows32 : kAdjRows64, kp = k32 ? 32 : 64;
     cudaStream_t st = (cudaStream_t)stream;
     cudaError_t e;
     // gradients start at zero: the columns that leave the scheme in the trigger pass keep it
@@ -1239,11 +1247,13 @@ int uwshcu_adjoint_device(const uwshcu_member* m, const uwshcu_adjoint* a, void*
         return cuda_fail(e);
     s.adj_records = 0;
     if (ncand == 0) return UWSHCU_OK;
-    // Batches of warps (32 slots each) whose tapes fit 3/4 of the device memory that is free or
+    // Batches of warps (32 slots each) whose tapes fit 85 % of the device memory that is free or
     // already held by the adjoint buffer.  The tape capacity is sized from the previous call's largest
-    // tape (+1/8); a batch that overflows it makes the call start again at the full capacity.
+    // tape (+1/16); a batch that overflows it makes the call start again at the full capacity.  A
+    // batch costs about one warp's forward sweep whatever its size (the sweep is a latency chain per
+    // warp), so one batch for all candidates is what the sizing aims at.
     const size_t nin = 3 * mkx + 6, rowb = uw_adj_row_bytes_k32n5();
-    const size_t nids = (size_t)(25 + 5) * 32;   // output-index table entries per slot (KP = 32, NC = 5)
+    const size_t nids = (size_t)(25 + 5) * kp;   // output-index table entries per slot (NC = 5)
     const size_t nw_need = ((size_t)ncand + 31) / 32;
     auto up = [](size_t x) { return (x + 255) / 256 * 256; };
     // the candidates in ascending column order: the warps' columns, and with them the tapes and the
@@ -1256,12 +1266,13 @@ int uwshcu_adjoint_device(const uwshcu_member* m, const uwshcu_adjoint* a, void*
         return cuda_fail(e);
     bool restart = false;
     double* cush_saved = nullptr;
-    for (size_t rcap = s.adj_rows > 0 ? (size_t)s.adj_rows : (size_t)kAdjRows;; restart = true) {
+    for (size_t rcap = s.adj_rows > 0 ? std::min((size_t)s.adj_rows, (size_t)full_rows) : (size_t)full_rows;;
+         restart = true) {
         const size_t astride = (nin + rcap) * 32;
         const size_t per_warp = rcap * rowb + astride * sizeof(double) + 32 * nids * sizeof(int) + 2 * sizeof(int) + 1024;
         size_t freeb = 0, totalb = 0;
         if ((e = cudaMemGetInfo(&freeb, &totalb)) != cudaSuccess) return cuda_fail(e);
-        const size_t avail = (freeb + d->adj_bytes) / 4 * 3;
+        const size_t avail = (freeb + d->adj_bytes) / 20 * 17;
         const size_t nw = std::min(nw_need, std::max((size_t)1, avail / per_warp)), nb = 32 * nw;
         // carve the buffer: tapes (operand indices, partials), adjoints, tables, counters, status
         const size_t o_ab = 0, o_d = o_ab + up(nw * rcap * 32 * 8), o_adj = o_d + up(nw * rcap * 32 * 16);
@@ -1273,12 +1284,12 @@ int uwshcu_adjoint_device(const uwshcu_member* m, const uwshcu_adjoint* a, void*
         if (restart && (e = cudaMemcpyAsync(m->cush, cush_saved, (size_t)m->iend * sizeof(double),
                                             cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
             return cuda_fail(e);
-        if (bytes > d->adj_bytes) {   // grown with 1/16 to spare, so that calls of similar size reuse it
+        if (bytes > d->adj_bytes) {   // grown with 1/32 to spare, so that calls of similar size reuse it
             const size_t held = freeb + d->adj_bytes;
             if (d->adj_buf) cudaFree(d->adj_buf);
             d->adj_buf = nullptr;
             d->adj_bytes = 0;
-            const size_t want = std::min(bytes + bytes / 16, std::max(bytes, held - held / 8));
+            const size_t want = std::min(bytes + bytes / 32, std::max(bytes, held / 20 * 18));
             if ((e = cudaMalloc(&d->adj_buf, want)) != cudaSuccess) return cuda_fail(e);
             d->adj_bytes = want;
         }
@@ -1315,10 +1326,10 @@ int uwshcu_adjoint_device(const uwshcu_member* m, const uwshcu_adjoint* a, void*
             h.status = status;
             const size_t used = ((size_t)h.nb + 31) / 32;   // warps holding a slot
             if ((e = cudaMemsetAsync(h.ids, 0xff, nb * nids * sizeof(int), st)) != cudaSuccess ||
-                (e = uw_adj_launch_k32n5(&A, &h, a, 0, st)) != cudaSuccess)
+                (e = adj_launch(&A, &h, a, 0, st)) != cudaSuccess)
                 return cuda_fail(e);
             adj_zero_kernel<<<(unsigned)used, 512, 0, st>>>(h.adj, astride, nrow, (int)nin, (int)rcap);
-            if ((e = cudaGetLastError()) != cudaSuccess || (e = uw_adj_launch_k32n5(&A, &h, a, 1, st)) != cudaSuccess ||
+            if ((e = cudaGetLastError()) != cudaSuccess || (e = adj_launch(&A, &h, a, 1, st)) != cudaSuccess ||
                 (e = cudaMemcpyAsync(counts.data(), nrow, used * sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
                 (e = cudaMemcpyAsync(&bits, status, sizeof(unsigned int), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
                 (e = cudaStreamSynchronize(st)) != cudaSuccess)
@@ -1326,15 +1337,15 @@ int uwshcu_adjoint_device(const uwshcu_member* m, const uwshcu_adjoint* a, void*
             for (size_t j = 0; j < used; j++) most = std::max(most, counts[j]);
         }
         s.adj_records = most;
-        if (bits && rcap < (size_t)kAdjRows) {   // the sized capacity was too small: again at the full one
-            rcap = kAdjRows;
+        if (bits && rcap < (size_t)full_rows) {   // the sized capacity was too small: again at the full one
+            rcap = full_rows;
             continue;
         }
-        s.adj_rows = (int)std::min((size_t)kAdjRows, ((size_t)most + most / 8 + 4095) / 4096 * 4096);
+        s.adj_rows = (int)std::min((size_t)full_rows, ((size_t)most + most / 16 + 4095) / 4096 * 4096);
         if (bits) {
             s.adj_rows = 0;
             std::snprintf(s.lasterr, sizeof(s.lasterr),
-                          "uwshcu_adjoint_device: a warp's tape exceeds %d rows (largest %d)", kAdjRows, most);
+                          "uwshcu_adjoint_device: a warp's tape exceeds %d rows (largest %d)", full_rows, most);
             return UWSHCU_ERR_TOO_LARGE;
         }
         return UWSHCU_OK;
@@ -1343,7 +1354,7 @@ int uwshcu_adjoint_device(const uwshcu_member* m, const uwshcu_adjoint* a, void*
 
 int uwshcu_set_adjoint_rows(int rows)
 {
-    if (rows < 0 || rows > kAdjRows) return UWSHCU_ERR_BAD_ARGS;
+    if (rows < 0 || rows > kAdjRows64) return UWSHCU_ERR_BAD_ARGS;
     State& s = S();
     std::lock_guard<std::mutex> lock(s.mu);
     s.adj_rows = rows;

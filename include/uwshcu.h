@@ -337,11 +337,11 @@ typedef struct uwshcu_adjoint {
  * branch the FP64 path takes; a saturation adjustment's derivative is taken at its converged
  * state).  The columns that leave the scheme in the trigger pass have constant outputs and zero
  * gradients; the others run a taped forward sweep (a tape per warp of 32 columns) and a reverse
- * sweep, in batches that fit 3/4 of the device memory that is free or already held by the adjoint
+ * sweep, in batches that fit 85 % of the device memory that is free or already held by the adjoint
  * buffer.  The library keeps that buffer between calls (release it with uwshcu_adjoint_release) and
  * sizes the tapes from the previous call's largest tape.  Waits for `stream` before it returns.
- * FP64 precision setting; mkx + 1 <= 32, ncnst <= 5.  UWSHCU_ERR_TOO_LARGE if a warp's tape exceeds
- * 2^18 rows. */
+ * FP64 precision setting; mkx + 1 <= 64, ncnst <= 5.  UWSHCU_ERR_TOO_LARGE if a warp's tape exceeds
+ * 2^18 rows (mkx + 1 <= 32) or 2^19 rows (33 .. 64 levels). */
 int uwshcu_adjoint_device(const uwshcu_member *m, const uwshcu_adjoint *a, void *stream);
 
 /* Largest tape of the last uwshcu_adjoint_device call, in rows per warp of 32 columns (a sizing
@@ -349,8 +349,9 @@ int uwshcu_adjoint_device(const uwshcu_member *m, const uwshcu_adjoint *a, void 
 int uwshcu_adjoint_last_records(void);
 
 /* No counterpart in the reference.  Tape capacity of the next uwshcu_adjoint_device call, in rows per
- * warp (1 .. 2^18; 0: the library's choice).  A batch that overflows it makes that call start again at
- * 2^18 rows; later calls size the tapes from the largest tape seen. */
+ * warp (1 .. 2^19, at most the full capacity of the call's level count; 0: the library's choice).  A
+ * batch that overflows it makes that call start again at the full capacity; later calls size the
+ * tapes from the largest tape seen. */
 int uwshcu_set_adjoint_rows(int rows);
 
 /* No counterpart in the reference.  Frees the adjoint buffer on every device (uwshcu_finalize

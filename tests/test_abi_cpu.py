@@ -60,7 +60,7 @@ def test_bad_arguments_are_rejected(uw):
     assert L.uwshcu_compute_member(None, None) == uw.ERR_BAD_ARGS
     assert L.uwshcu_tangent_device(None, None, None) == uw.ERR_BAD_ARGS
     assert L.uwshcu_adjoint_device(None, None, None) == uw.ERR_BAD_ARGS
-    assert uw.set_adjoint_rows(-1) == uw.ERR_BAD_ARGS and uw.set_adjoint_rows((1 << 18) + 1) == uw.ERR_BAD_ARGS
+    assert uw.set_adjoint_rows(-1) == uw.ERR_BAD_ARGS and uw.set_adjoint_rows((1 << 19) + 1) == uw.ERR_BAD_ARGS
     assert uw.set_adjoint_rows(0) == 0
     assert uw.adjoint_release() == 0
 

@@ -6,12 +6,14 @@ gives <ADJ w, d>, column by column.  Both linearise the same FP64 computation (t
 path takes) and multiply the same partial derivatives in opposite orders, so they agree to the
 rounding of that product.  Most columns agree to ~1e-15 of the column's sum of |terms|; a column
 whose derivative is ill-conditioned (intermediate derivatives many orders above the outputs', which
-cancel) amplifies rounding in both models alike.  The bar measures that amplification with the
-tangent-linear model alone: its defect of linearity under a split of the direction, d = d1 + d2,
-|<w, TL d> - <w, TL d1> - <w, TL d2>|.  Every convecting column must satisfy
-|<w, TL d> - <ADJ w, d>| <= 1e-9 |terms| + 100 x that defect, and the median column 1e-13.  The
-adjoint's forward sweep also reproduces the FP64 outputs bit for bit.  The tangent-linear model itself
-is checked against finite differences in test_gpu_tangent.py.
+cancel) amplifies rounding, and the two models amplify it differently (the tangent model in its
+tangents, the adjoint in its adjoints).  The bar measures each model's amplification on the column
+with that model alone, by its defect of linearity under a split of its argument:
+|<w, TL d> - <w, TL d1> - <w, TL d2>| for d = d1 + d2, and |<ADJ w, d> - <ADJ w1, d> - <ADJ w2, d>| for
+w = w1 + w2.  Every convecting column must satisfy |<w, TL d> - <ADJ w, d>| <= 1e-9 |terms| + 100 x
+(the sum of the two defects), and the median column 1e-13.  The adjoint's forward sweep also
+reproduces the FP64 outputs bit for bit.  The tangent-linear model itself is checked against finite
+differences in test_gpu_tangent.py.
 """
 import numpy as np
 import pytest
@@ -24,11 +26,11 @@ OUTS = ("cush umf slflx qtflx flxprc1 flxsnow1 qvten qlten qiten sten uten vten 
         "snow evapc cufrc qcu qlu qiu cbmf qc rliq wu").split()
 
 
-@pytest.mark.parametrize("inv", [0, 1])
-def test_adjoint_dot_product(uw, cuda, inv):
+@pytest.mark.parametrize("inv,pver", [(0, 30), (1, 30), (0, 51)])
+def test_adjoint_dot_product(uw, cuda, inv, pver):
     import torch
     assert uw.init_default() == 0
-    s = soundings.make_soundings(2048, 30, seed=301 + inv, rh_pbl=(0.6, 0.95))
+    s = soundings.make_soundings(2048, pver, seed=301 + inv + pver, rh_pbl=(0.6, 0.95))
     if inv:
         s = soundings.to_inv(s)
     ref = uw.DeviceCase(s)
@@ -74,13 +76,23 @@ def test_adjoint_dot_product(uw, cuda, inv):
     t2 = uw.tangent_launch(uw.DeviceCase(s, inputs=ref.inp), d2, p2, inv=inv)
     torch.cuda.synchronize()
     lin = (lhs - sum(per_col(cot[k] * (t1[k] + t2[k])) for k in OUTS)).abs()
+    # the adjoint's own defect of linearity: w = w1 + w2 (w2 = w - w1)
+    w1 = {k: v * torch.rand(v.shape, generator=g, dtype=torch.float64).to(v.device) for k, v in cot.items()}
+    w2 = {k: cot[k] - w1[k] for k in cot}
+    ga = [uw.adjoint_launch(uw.DeviceCase(s, inputs=ref.inp), w, inv=inv) for w in (w1, w2)]
+    assert all(rc_ == 0 for rc_, _ in ga)
+
+    def dot_adj(gr):
+        r = sum(per_col(gr[k] * dirs[k]) for k in ("t0", "qv0", "tke", "pblh"))
+        return r + sum(gr[k] * p for k, p in zip(("rpen", "rle", "rkm", "criqc"), dparams))
+    lin_adj = (rhs - dot_adj(ga[0][1]) - dot_adj(ga[1][1])).abs()
     conv = torch.from_numpy(want["cush"] != -1.0).to(lhs.device) & (scl > 0)
     assert int(conv.sum()) > 200, int(conv.sum())
     assert bool(torch.isfinite(lhs).all()) and bool(torch.isfinite(rhs).all())
     err = (lhs - rhs).abs()
-    bound = 1e-9 * scl + 100.0 * lin
+    bound = 1e-9 * scl + 100.0 * (lin + lin_adj)
     bad = torch.nonzero(conv & (err > bound)).flatten().tolist()
-    assert not bad, [(c, float(err[c] / scl[c]), float(lin[c] / scl[c])) for c in bad[:8]]
+    assert not bad, [(c, float(err[c] / scl[c]), float(lin[c] / scl[c]), float(lin_adj[c] / scl[c])) for c in bad[:8]]
     rel = (err / scl.clamp(min=1e-300))[conv].cpu().numpy()
     assert np.median(rel) <= 1e-13, np.median(rel)
     # the columns that leave the scheme in the trigger pass have zero gradients
