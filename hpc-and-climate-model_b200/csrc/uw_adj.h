@@ -92,8 +92,20 @@ __device__ __forceinline__ Ad ad_rec(double v, int a, double da, int b, double d
     return Ad(v, ad_row(a, da, b, db));
 }
 
-__device__ __forceinline__ Ad operator+(Ad a, Ad b) { return ad_rec(a.v + b.v, a.i, 1.0, b.i, 1.0); }
-__device__ __forceinline__ Ad operator-(Ad a, Ad b) { return ad_rec(a.v - b.v, a.i, 1.0, b.i, -1.0); }
+// A result whose derivative is exactly 1 in its only active operand (x + c, c + x, x - c, |x| for
+// x >= 0) takes that operand's index instead of a record: an adjoint added to the index is the
+// chain rule with factor 1.
+__device__ __forceinline__ Ad operator+(Ad a, Ad b)
+{
+    if (b.i < 0) return Ad(a.v + b.v, a.i);
+    if (a.i < 0) return Ad(a.v + b.v, b.i);
+    return ad_rec(a.v + b.v, a.i, 1.0, b.i, 1.0);
+}
+__device__ __forceinline__ Ad operator-(Ad a, Ad b)
+{
+    if (b.i < 0) return Ad(a.v - b.v, a.i);
+    return ad_rec(a.v - b.v, a.i, 1.0, b.i, -1.0);
+}
 __device__ __forceinline__ Ad operator*(Ad a, Ad b) { return ad_rec(a.v * b.v, a.i, b.v, b.i, a.v); }
 __device__ __forceinline__ Ad operator/(Ad a, Ad b)
 {
@@ -140,7 +152,11 @@ __device__ __forceinline__ Ad sqrt(Ad x)
     const double s = sqrt(x.v);
     return ad_rec(s, x.i, x.i >= 0 ? 1.0 / (2.0 * s) : 0.0, -1, 0.0);
 }
-__device__ __forceinline__ Ad fabs(Ad x) { return ad_rec(fabs(x.v), x.i, x.v < 0.0 ? -1.0 : 1.0, -1, 0.0); }
+__device__ __forceinline__ Ad fabs(Ad x)
+{
+    if (!(x.v < 0.0)) return Ad(fabs(x.v), x.i);
+    return ad_rec(fabs(x.v), x.i, -1.0, -1, 0.0);
+}
 __device__ __forceinline__ Ad trunc(Ad x) { return Ad(trunc(x.v)); }
 __device__ __forceinline__ Ad floor(Ad x) { return Ad(floor(x.v)); }
 __device__ __forceinline__ Ad copysign(Ad a, Ad b)
