@@ -103,11 +103,14 @@ __global__ void __launch_bounds__(UW_ADJ_RBLOCK) uwshcu_adj_reverse(const __grid
 #define RI(k) (inv ? (mkx - (k)) : (k))
 #define RL(k) (inv ? (mkx - (k)) : ((k) - 1))
 #define AID(f, k) G.ids[((size_t)(f) * KP + (k)) * G.cap + slot]
-#define SEED(f, k, row)                                                                                   \
-    if (C.f) {                                                                                            \
-        const int id_ = AID(UW_AO_##f, k);                                                                \
-        if (id_ >= 0 && id_ < nin + rows) atomicAdd(&af[(size_t)id_ * 32 + lane], C.f[(size_t)(row) * mix + i]); \
+// a seed at an index with the sign bit goes to the index, negated
+#define SEED_AT(id, w)                                                                                    \
+    {                                                                                                     \
+        const int id_ = (id), ix_ = id_ & ~AD_NEG;                                                        \
+        if (id_ >= 0 && ix_ < nin + rows) atomicAdd(&af[(size_t)ix_ * 32 + lane], (id_ & AD_NEG) ? -(w) : (w)); \
     }
+#define SEED(f, k, row)                                                                                   \
+    if (C.f) SEED_AT(AID(UW_AO_##f, k), C.f[(size_t)(row) * mix + i])
     if (active) {
         for (int k = 0; k <= mkx; k++) {
             SEED(umf, k, RI(k)) SEED(slflx, k, RI(k)) SEED(qtflx, k, RI(k)) SEED(flxprc1, k, RI(k))
@@ -122,11 +125,7 @@ __global__ void __launch_bounds__(UW_ADJ_RBLOCK) uwshcu_adj_reverse(const __grid
         SEED(cush, 0, 0) SEED(precip, 0, 0) SEED(snow, 0, 0) SEED(cbmf, 0, 0) SEED(rliq, 0, 0)
         if (C.trten)
             for (int m = 1; m <= ncnst; m++)
-                for (int k = 1; k <= mkx; k++) {
-                    const int id_ = AID(UW_AO_N + m - 1, k);
-                    if (id_ >= 0 && id_ < nin + rows)
-                        atomicAdd(&af[(size_t)id_ * 32 + lane], C.trten[((size_t)(m - 1) * mkx + RL(k)) * mix + i]);
-                }
+                for (int k = 1; k <= mkx; k++) SEED_AT(AID(UW_AO_N + m - 1, k), C.trten[((size_t)(m - 1) * mkx + RL(k)) * mix + i])
     }
     __syncwarp();
     uw_adj_sweep(G.ab + (size_t)w * G.rcap * 32, G.d + (size_t)w * G.rcap * 32, rows, nin, af, nr,
@@ -146,6 +145,7 @@ __global__ void __launch_bounds__(UW_ADJ_RBLOCK) uwshcu_adj_reverse(const __grid
     if (C.criqc) C.criqc[i] = GR(3 * mkx + 5);
 #undef GR
 #undef SEED
+#undef SEED_AT
 #undef AID
 #undef RI
 #undef RL

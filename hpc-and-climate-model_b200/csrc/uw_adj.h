@@ -86,15 +86,30 @@ __device__ __forceinline__ void ad_align(unsigned live)
     t.n[lane] = __reduce_max_sync(live, t.n[lane]);
 }
 
+// Bit 30 of an index marks a value that is minus the one the index names (negations record
+// nothing); a record takes the sign into its partial.  Indices stay below 2^20.
+#define AD_NEG (1 << 30)
+
 __device__ __forceinline__ Ad ad_rec(double v, int a, double da, int b, double db)
 {
     if (a < 0 && b < 0) return Ad(v);
+    if (a >= 0 && (a & AD_NEG)) {
+        a ^= AD_NEG;
+        da = -da;
+    }
+    if (b >= 0 && (b & AD_NEG)) {
+        b ^= AD_NEG;
+        db = -db;
+    }
     return Ad(v, ad_row(a, da, b, db));
 }
 
-// A result whose derivative is exactly 1 in its only active operand (x + c, c + x, x - c, |x| for
-// x >= 0) takes that operand's index instead of a record: an adjoint added to the index is the
-// chain rule with factor 1.
+// the index of -x
+__device__ __forceinline__ int ad_neg(int i) { return i < 0 ? i : i ^ AD_NEG; }
+
+// A result whose derivative is exactly 1 or -1 in its only active operand (x + c, c + x, x - c, c - x,
+// -x, |x|) takes that operand's index, with the sign, instead of a record: an adjoint added to the
+// index is the chain rule with factor +-1.
 __device__ __forceinline__ Ad operator+(Ad a, Ad b)
 {
     if (b.i < 0) return Ad(a.v + b.v, a.i);
@@ -104,6 +119,7 @@ __device__ __forceinline__ Ad operator+(Ad a, Ad b)
 __device__ __forceinline__ Ad operator-(Ad a, Ad b)
 {
     if (b.i < 0) return Ad(a.v - b.v, a.i);
+    if (a.i < 0) return Ad(a.v - b.v, ad_neg(b.i));
     return ad_rec(a.v - b.v, a.i, 1.0, b.i, -1.0);
 }
 __device__ __forceinline__ Ad operator*(Ad a, Ad b) { return ad_rec(a.v * b.v, a.i, b.v, b.i, a.v); }
@@ -112,7 +128,7 @@ __device__ __forceinline__ Ad operator/(Ad a, Ad b)
     const double q = a.v / b.v;
     return ad_rec(q, a.i, 1.0 / b.v, b.i, -q / b.v);
 }
-__device__ __forceinline__ Ad operator-(Ad a) { return ad_rec(-a.v, a.i, -1.0, -1, 0.0); }
+__device__ __forceinline__ Ad operator-(Ad a) { return Ad(-a.v, ad_neg(a.i)); }
 __device__ __forceinline__ Ad operator+(Ad a) { return a; }
 __device__ __forceinline__ Ad& operator+=(Ad& a, Ad b) { return a = a + b; }
 __device__ __forceinline__ Ad& operator-=(Ad& a, Ad b) { return a = a - b; }
@@ -152,17 +168,13 @@ __device__ __forceinline__ Ad sqrt(Ad x)
     const double s = sqrt(x.v);
     return ad_rec(s, x.i, x.i >= 0 ? 1.0 / (2.0 * s) : 0.0, -1, 0.0);
 }
-__device__ __forceinline__ Ad fabs(Ad x)
-{
-    if (!(x.v < 0.0)) return Ad(fabs(x.v), x.i);
-    return ad_rec(fabs(x.v), x.i, -1.0, -1, 0.0);
-}
+__device__ __forceinline__ Ad fabs(Ad x) { return Ad(fabs(x.v), x.v < 0.0 ? ad_neg(x.i) : x.i); }
 __device__ __forceinline__ Ad trunc(Ad x) { return Ad(trunc(x.v)); }
 __device__ __forceinline__ Ad floor(Ad x) { return Ad(floor(x.v)); }
 __device__ __forceinline__ Ad copysign(Ad a, Ad b)
 {
     const double r = copysign(a.v, b.v);
-    return ad_rec(r, a.i, r == a.v ? 1.0 : -1.0, -1, 0.0);
+    return Ad(r, r == a.v ? a.i : ad_neg(a.i));
 }
 
 // A value with its derivatives along 4 directions (forward mode, no tape), for the inner iterations of
