@@ -45,6 +45,3 @@ extern "C" cudaError_t uw_adj_launch_k64n5(const UwArgs* a, const void* slots, c
     }
     return cudaGetLastError();
 }
-
-// bytes of one tape row of a warp: 32 records of operand indices and partials
-extern "C" size_t uw_adj_row_bytes_k64n5() { return 32 * (sizeof(int2) + sizeof(double2)); }

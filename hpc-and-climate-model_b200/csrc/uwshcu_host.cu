@@ -51,7 +51,7 @@ extern "C" cudaError_t uw_budget_launch(int mix, int mkx, int iend, int inv, dou
 extern "C" cudaError_t uw_adj_set_constants_k32n5(const UwConst* h, const double* tbl);
 extern "C" cudaError_t uw_adj_launch_k32n5(const UwArgs* a, const void* slots, const uwshcu_adjoint* c, int phase,
                                            cudaStream_t stream);
-extern "C" size_t uw_adj_row_bytes_k32n5();
+extern "C" size_t uw_adj_row_bytes_k32n5();   // the same for both units: 32 records per row
 extern "C" cudaError_t uw_adj_set_constants_k64n5(const UwConst* h, const double* tbl);
 extern "C" cudaError_t uw_adj_launch_k64n5(const UwArgs* a, const void* slots, const uwshcu_adjoint* c, int phase,
                                            cudaStream_t stream);
