@@ -1,23 +1,30 @@
 #!/usr/bin/env python
 """Benchmark of the UW shallow-cumulus driver compute_uwshcu on B200.
 
-Workload: 259,200 independent columns (a 720 x 360 grid) x 30 levels, 5 tracers (qv, ql, qi, nl,
-ni), dt = 1800 s, seeded synthetic soundings (hpc-and-climate-model_b200/soundings.py) with the
-PBL relative humidity drawn from U(0.675, 0.93) so that about 40 % of the columns convect.
-A step is one compute_uwshcu call over all columns.  Metric: columns per second.
+Workload: 1,048,576 independent columns x 30 levels, 5 tracers (qv, ql, qi, nl, ni), dt = 1800 s,
+seeded synthetic soundings (hpc-and-climate-model_b200/soundings.py) with the PBL relative humidity
+drawn from U(0.675, 0.93) so that about 40 % of the columns convect.  A step is one compute_uwshcu
+call over all columns.  Metric: columns per second.
 
-  value : device-resident throughput (inputs already in HBM, uwshcu_compute_device), CUDA events
-          on the launching stream around exactly K steps; inputs (1.2 GB) exceed the 126 MB L2.
+  value : device-resident throughput of the FP64 path (inputs already in HBM,
+          uwshcu_compute_device), CUDA events on the launching stream around exactly K steps;
+          inputs (4.6 GB) exceed the 126 MB L2.
   e2e   : the same metric through the reference-facing C ABI compute_uwshcu_ with host arrays:
           the timed region includes the host->device copy of each step's inputs and the
           device->host copy of its outputs.
+  mixed : the mixed-precision path on the same columns: columns/s, speed-up over FP64, relative
+          RMS error of column heating, moistening and precipitation against the FP64 path (which is
+          the FP64 oracle bit for bit), and the columns whose decisions change.
+  adjoint: the adjoint model against the forward pass on 65,536 x 30 columns (cost ratio, tape).
+  parity: the FP64 path on the 259,200 x 30 grid (720 x 360) against the oracle builds: decision
+          agreement and the fraction of columns within 1e-11 on every output.
   --impl reference : the reference algorithm's CPU implementation (the C restatement in
           oracle/, compiled with -O2 -ffp-contract=off, OpenMP over all host cores) on a bounded
           sample of the same workload.
 
-Multi-GPU (torchrun): every rank processes its own 259,200 columns (different seeds); columns are
-independent, so there is no collective on the data path ("scaling": "weak").  Timing is the max
-over ranks of the device time.
+Multi-GPU (torchrun): every rank processes its own 1,048,576 columns (different seeds); columns
+are independent, so there is no collective on the data path ("scaling": "weak").  Timing is the max
+over ranks of the device time.  The mixed, adjoint and parity legs run at N = 1 only.
 """
 import argparse
 import json
@@ -33,11 +40,13 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.join(REPO, "hpc-and-climate-model_b200")
 sys.path.insert(0, PKG)
 
-NCOL = 259_200
+NCOL = 1_048_576
+NCOL_GRID = 259_200       # the 720 x 360 grid of the parity leg
 PVER = 30
 NCNST = 5
 RH_PBL = (0.675, 0.93)
-METRIC = "columns/s (compute_uwshcu, FP64, 259,200 x 30 levels)"
+METRIC = "columns/s (compute_uwshcu, FP64, 1,048,576 x 30 levels)"
+G = 9.80616
 
 
 # From the ncu capture of the worklist pass on the 65,536-column case of this workload (29,956
@@ -130,7 +139,7 @@ class ClockSampler:
 
 
 def shard_seed(rank):
-    """Seed of rank `rank`'s columns: every rank generates and computes its own 259,200 columns (the
+    """Seed of rank `rank`'s columns: every rank generates and computes its own columns (the
     columns are independent, so there is no exchange step and no collective on the data path)."""
     return 1 + rank
 
@@ -177,7 +186,7 @@ def run_reference(args):
     oracle.init_default()
     cores = os.cpu_count() or 1
     sample = int(args.cpu_sample)
-    s = soundings.make_soundings(sample, PVER, seed=1, rh_pbl=RH_PBL)
+    s = soundings.make_soundings(sample, PVER, seed=shard_seed(0), rh_pbl=RH_PBL)
     for _ in range(args.warmup if args.warmup < 1 else 1):
         oracle.compute(s, nthreads=cores, diag=False)
     times = []
@@ -192,32 +201,188 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded soundings)",
-        "config": {"workload": "compute_uwshcu 259,200 x 30 levels, 5 tracers, dt=1800 s; each "
+        "config": {"workload": "compute_uwshcu 1,048,576 x 30 levels, 5 tracers, dt=1800 s; each "
                                "step a %d-column sample" % sample,
                    "ncol_sample": sample, "pver": PVER, "ncnst": NCNST},
         "cpu_baseline": {"value": val, "unit": "columns/s", "cores": cores, "kind": "port",
-                         "sample": "%d columns of the 259,200-column workload per step" % sample},
+                         "sample": "the first %d columns of the 1,048,576-column workload "
+                                   "per step" % sample},
         "e2e": {"value": val, "unit": "columns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
-def cpu_baseline_leg(seconds=10.0):
+OUT_FIELDS = ("umf", "slflx", "qtflx", "flxprc1", "flxsnow1", "wu", "qvten", "qlten", "qiten",
+              "sten", "uten", "vten", "qrten", "qsten", "evapc", "cufrc", "qcu", "qlu", "qiu", "qc",
+              "trten", "precip", "snow", "cbmf", "rliq", "cnt", "cnb", "cush")
+
+
+def _column_errors(out, ref):
+    """Worst norm-wise relative column error over all outputs (max_k |a-b| / max_k |b| per field)
+    and the per-field fraction of columns within 1e-11."""
+    worst, per = None, {}
+    for f in OUT_FIELDS:
+        a = np.asarray(out[f], dtype=np.float64)
+        b = np.asarray(ref[f], dtype=np.float64)
+        n = b.shape[-1]
+        a, b = a.reshape(-1, n), b.reshape(-1, n)
+        num = np.abs(a - b).max(axis=0)
+        den = np.abs(b).max(axis=0)
+        with np.errstate(invalid="ignore", divide="ignore"):
+            e = np.where(den > 0, num / np.where(den > 0, den, 1.0), np.where(num > 0, np.inf, 0.0))
+        per[f] = float(np.mean(e <= 1e-11))
+        worst = e if worst is None else np.maximum(worst, e)
+    return worst, per
+
+
+def grid_case(uw):
+    """The FP64 path on the 259,200-column grid (seed 0) with diagnostics: inputs and outputs."""
+    import soundings
+    s = soundings.make_soundings(NCOL_GRID, PVER, seed=0, rh_pbl=RH_PBL)
+    case = uw.DeviceCase(s, diag=True)
+    rc = case.launch()
+    st = case.status()
+    out = case.outputs_numpy()
+    del case
+    return s, out, rc, st
+
+
+def cpu_baseline_leg(s, gpu_out):
+    """The oracle (the C restatement of the reference algorithm, OpenMP over all host cores) timed
+    on the 259,200-column grid, and, as the checker, compared with the FP64 path's outputs of the
+    same inputs (gpu_out): the glibc build (pinned to the reference's C++ drop-in), the build with
+    the Fortran's own math (glibc exp/log/pow, CALERF erfc) and the build with the kernel's math
+    routines.  Returns (cpu_baseline, parity)."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle
-    import soundings
-    oracle.init_default()
     cores = os.cpu_count() or 1
-    n = 32768
-    s = soundings.make_soundings(n, PVER, seed=3, rh_pbl=RH_PBL)
-    oracle.compute(s, nthreads=cores, diag=False)
-    done, t0 = 0, time.perf_counter()
-    while time.perf_counter() - t0 < seconds:
-        oracle.compute(s, nthreads=cores, diag=False)
-        done += n
-    sec = time.perf_counter() - t0
-    return {"value": done / sec, "unit": "columns/s", "cores": cores, "kind": "port",
-            "sample": "%d passes over a %d-column slice of the workload (%.1f s)" % (done // n, n, sec)}
+    n = s["ncol"]
+    parity, base = {"workload": "259,200 columns (720 x 360) x 30 levels, seed 0, ~40 % convecting",
+                    "column_error": "max_k |gpu - oracle| / max_k |oracle| per output field"}, None
+    try:
+        for name in ("glibc", "fortran", "portable"):
+            oracle.set_variant(name)
+            oracle.init_default()
+            t0 = time.perf_counter()
+            ref = oracle.compute(s, nthreads=cores, diag=True)
+            sec = time.perf_counter() - t0
+            if name == "glibc":
+                base = {"value": n / sec, "unit": "columns/s", "cores": cores, "kind": "port",
+                        "sample": "one pass over the %d-column grid (%.1f s); the 1,048,576-column "
+                                  "workload has the same column distribution" % (n, sec)}
+            worst, per = _column_errors(gpu_out, ref)
+            trig = float(np.mean((gpu_out["cush"] != -1.0) == (ref["cush"] != -1.0)))
+            parity[name] = {
+                "columns_within_1e-11_all_outputs": float(np.mean(worst <= 1e-11)),
+                "columns_bit_identical": float(np.mean(worst == 0.0)),
+                "trigger_agree": trig, "cloud_base_agree": float(np.mean(gpu_out["cnb"] == ref["cnb"])),
+                "cloud_top_agree": float(np.mean(gpu_out["cnt"] == ref["cnt"])),
+                "level_indices_agree": float(np.mean(np.all(gpu_out["diag_int"][2:] == ref["diag_int"][2:], axis=0))),
+                "worst_fields_within_1e-11": dict(sorted(per.items(), key=lambda kv: kv[1])[:3])}
+            del ref
+    finally:
+        oracle.set_variant("glibc")
+    parity["builds"] = {"glibc": "exp/log/pow/erfc from glibc; pinned bit for bit to the reference's "
+                                 "C++ drop-in (bxcompute_uwshcu_inv.cpp) built for the host",
+                        "fortran": "glibc exp/log/pow and CAM's CALERF erfc: the functions a Fortran "
+                                   "build of uwshcu.F90 calls",
+                        "portable": "the kernel's own math routines (correctly rounded exp/log/pow, "
+                                    "CALERF erfc): expected bit for bit"}
+    return base, parity
+
+
+def column_quantities_dev(case):
+    """Column heating, moistening and precipitation and the decisions of the last call, on the
+    device (errstats.py's definitions)."""
+    o, dp0 = case.out, case.inp["dp0"]
+    return {"heating": (o["sten"] * dp0).sum(0) / G, "moistening": (o["qvten"] * dp0).sum(0) / G,
+            "precipitation": o["precip"].clone(), "cnt": o["cnt"].clone(), "cnb": o["cnb"].clone(),
+            "trigger": o["cush"] != -1.0}
+
+
+def mixed_leg(uw, case, stream, steps, warmup, fp64_ms):
+    """The mixed-precision path on the columns of `case`, whose outputs hold the FP64 path's: speed
+    and the error of column heating, moistening and precipitation against FP64."""
+    import torch
+    ref = column_quantities_dev(case)
+    assert uw.set_precision(uw.PREC_MIXED) == 0
+    try:
+        def step():
+            case.out["cush"].copy_(case.cush0, non_blocking=True)
+            rc = case.launch(stream=stream)
+            if rc != 0:
+                raise RuntimeError("mixed: %d %s" % (rc, uw.last_cuda_error()))
+        with torch.cuda.stream(stream):
+            for _ in range(warmup):
+                step()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                step()
+            e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        q = column_quantities_dev(case)
+    finally:
+        assert uw.set_precision(uw.PREC_FP64) == 0
+    err = {}
+    for k in ("heating", "moistening", "precipitation"):
+        a, b = q[k].double(), ref[k].double()
+        err[k] = float(torch.sqrt(torch.mean((a - b) ** 2)) / torch.sqrt(torch.mean(b ** 2)))
+    n = case.n
+    return {"value": n / (ms * 1e-3), "unit": "columns/s", "ms_per_step": ms,
+            "speedup_vs_fp64": fp64_ms / ms, "column_rel_rms_vs_fp64": err,
+            "flips": {"trigger": int((q["trigger"] != ref["trigger"]).sum()),
+                      "cloud_base": int((q["cnb"] != ref["cnb"]).sum()),
+                      "cloud_top": int((q["cnt"] != ref["cnt"]).sum()),
+                      "convecting_columns": int(ref["trigger"].sum())},
+            "targets": "north_star: >= 2x the FP64 path at <= 1e-4 relative RMS"}
+
+
+def adjoint_leg(uw, steps, warmup, n=65_536):
+    """The adjoint model against the forward pass on n x 30 columns (random cotangents on every
+    differentiable output): cost ratio and tape size."""
+    import torch
+    import soundings
+    s = soundings.make_soundings(n, PVER, seed=301, rh_pbl=RH_PBL)
+    case = uw.DeviceCase(s)
+    g = torch.Generator(device="cpu").manual_seed(11)
+    cot = {k: torch.randn(v.shape, generator=g, dtype=torch.float64).cuda() for k, v in case.out.items()
+           if k in uw.ADJ_OUTPUTS}
+    stream = torch.cuda.Stream()
+
+    def timed(fn, k):
+        with torch.cuda.stream(stream):
+            for _ in range(warmup):
+                case.reset_cush()
+                fn()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(k):
+                case.reset_cush()
+                fn()
+            e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / k
+
+    def adjoint():
+        rc, _ = uw.adjoint_launch(case, cot, stream=stream)
+        if rc != 0:
+            raise RuntimeError("adjoint: %d %s" % (rc, uw.last_cuda_error()))
+
+    fwd = timed(lambda: case.launch(stream=stream), steps)
+    ka = max(1, min(steps, 5))
+    adj = timed(adjoint, ka)
+    rows = uw.adjoint_last_records()
+    conv = int((case.out["cush"] != -1.0).sum())
+    uw.adjoint_release()
+    del case, cot
+    torch.cuda.empty_cache()
+    return {"value": adj / fwd, "unit": "adjoint ms / forward ms", "forward_ms": fwd,
+            "adjoint_ms": adj, "steps": ka, "workload": "%s columns x 30 levels (seed 301)" % f"{n:,}",
+            "convecting_columns": conv, "tape_rows_per_warp": rows,
+            "tape_bytes_per_convecting_column": rows * 32,
+            "target": "north_star: <= 4x the forward"}
 
 
 # Batched uneven workload: 4 members of 262,144 columns (1,048,576 in all) with 30, 35, 51 and 30
@@ -456,7 +621,9 @@ def main():
     ap.add_argument("--ncol", type=int, default=NCOL)
     ap.add_argument("--columns", type=int, default=65536,
                     help="columns of the tangent and adjoint cost configs (65,536 by default)")
-    ap.add_argument("--cpu-sample", type=int, default=32768)
+    ap.add_argument("--cpu-sample", type=int, default=65536)
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the mixed-precision, adjoint and parity legs of the default run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--schedule", default="sorted", choices=["two-phase", "sorted", "single-pass"])
@@ -464,7 +631,7 @@ def main():
                     help="fp64: bit-exact (default); fast: FP64 with the early-stopping conden; "
                          "mixed: FP32 bulk with FP64 islands")
     ap.add_argument("--config", default="fp64", choices=["fp64", "batched", "tangent", "adjoint"],
-                    help="fp64: the 259,200-column workload (default); batched: 4 uneven members")
+                    help="fp64: the 1,048,576-column workload (default); batched: 4 uneven members")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -594,10 +761,24 @@ def main():
                "flips": rep["flips"],
                "field_rel_rms_max": max(v["rel_rms"] for v in rep["fields"].values())}
 
+    extras = rank == 0 and world == 1 and not args.no_extras and prec == uw.PREC_FP64
+    mixed = adjoint = None
+    if extras:
+        mixed = mixed_leg(uw, case, stream, args.steps, max(args.warmup, 3), ms)
+    if extras or (rank == 0 and world == 1 and not args.no_cpu_baseline):
+        # free the large workload before the grid run, the adjoint buffer and the oracle
+        del case
+        torch.cuda.empty_cache()
+        grid_s, grid_out, grid_rc, grid_st = grid_case(uw)
+        if extras:
+            adjoint = adjoint_leg(uw, args.steps, max(args.warmup, 3))
+
     peak, peak_kind = peaks()
     ncols_dom = phases["worklist_columns"] if phases else n
     fp64 = None
     fp64_alg = None
+    # operation counts per convecting / other column of this column distribution (counted on the
+    # 259,200-column grid of the same generator)
     ops = algorithmic_ops("fp64_259200x30", world * n, trig) if PVER == 30 else None
     if ops and clk is not None and clk.summary().get("sm_mhz"):
         pk = 2 * FP64_DFMA_PER_CYCLE * clk.summary()["sm_mhz"] * 1e6 / 1e12
@@ -618,15 +799,17 @@ def main():
     alg = ncols_dom * (nbytes_in + nbytes_out)
     achieved = alg / (kernel_ms * 1e-3) / 1e9
     line = {
-        "metric": METRIC if prec == uw.PREC_FP64 else METRIC.replace("FP64", args.precision),
+        "metric": "columns/s (compute_uwshcu, %s, %s x 30 levels)" % (
+            "FP64" if prec == uw.PREC_FP64 else args.precision, f"{n:,}"),
         "value": value, "unit": "columns/s", "n_gpus": world,
         "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64" if prec == uw.PREC_MIXED else "f64",
         "data": "synthetic (seeded soundings, PCG64 seed 1+rank)",
-        "config": {"workload": "compute_uwshcu 259,200 columns (720x360) x 30 levels, 5 tracers, "
-                               "dt=1800 s, ~40% convecting", "ncol_per_gpu": n, "pver": PVER,
-                   "ncnst": NCNST, "trigger_fraction": trig, "l2": "inputs (1.2 GB) larger than L2",
+        "config": {"workload": "compute_uwshcu %s columns x 30 levels, 5 tracers, dt=1800 s, ~40%% "
+                               "convecting" % f"{n:,}", "ncol_per_gpu": n, "pver": PVER,
+                   "ncnst": NCNST, "trigger_fraction": trig,
+                   "l2": "inputs (%.1f GB) larger than L2" % (n * nbytes_in / 1e9),
                    "parallelism": "column shards, %d rank(s), no collective" % world},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak,
@@ -656,8 +839,15 @@ def main():
     line["budgets"] = budget
     if clk is not None:
         line["clocks"] = clk.summary()
+    if mixed is not None:
+        line["mixed"] = mixed
+    if adjoint is not None:
+        line["adjoint"] = adjoint
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_leg()
+        base, parity = cpu_baseline_leg(grid_s, grid_out)
+        parity["gpu_status"] = [int(grid_rc), int(grid_st)]
+        line["cpu_baseline"] = base
+        line["parity"] = parity
     if rank == 0:
         print(json.dumps(line), flush=True)
     if pg:

@@ -3,21 +3,19 @@
 // The scheme amplifies last-bit differences of the transcendental functions strongly (for example
 // wu = sqrt(wtw) with wtw near 0, or 1 - thvj/thv0j multiplied by 2 g cridis / wue^2 ~ 1e4): two
 // libms that differ by one ulp give column differences of up to 1e-5.  These routines use only
-// operations that IEEE 754 rounds exactly the same way everywhere (+ - * /, sqrt, fma, floor,
-// frexp, ldexp, comparisons), so a host build (-ffp-contract=off) and a device build
-// (-fmad=false) of the same expression produce identical results.  Accuracy is about 1 ulp
-// (exp, log), a few ulp (pow with |y log x| < 1) and about 1e-16 relative (erfc).
+// operations that IEEE 754 rounds exactly the same way everywhere (+ - * /, sqrt, fma, rint,
+// floor, frexp, ldexp, comparisons), so a host build (-ffp-contract=off) and a device build
+// (-fmad=false, or explicit __dmul_rn/__dadd_rn where contraction is on) of the same expression
+// produce identical results.
 //
 // Methods:
-//   exp  -- Cody-Waite argument reduction x = k ln2 + r with a two-part ln2, Taylor polynomial of
-//           degree 13 for e^r on |r| <= ln2/2 (Horner with fma), scaling by 2^k.
-//   log  -- x = m 2^e with m in [sqrt(1/2), sqrt(2)), f = m - 1, s = f / (2 + f),
-//           log(1+f) = f - (f^2/2 - s (f^2/2 + R)), R = z (2/3 + 2/5 z + ... + 2/25 z^11), z = s^2
-//           (the atanh series), plus e ln2 in two parts.
-//   pow  -- exp(y log x) for x > 0.
+//   exp, log, pow -- correctly rounded (Ziv's fast path, rounding test and accurate double-double
+//           path; description and references below), so that they return what every correctly
+//           rounding libm returns, and glibc's exp/log/pow (the functions a Fortran build of the
+//           scheme calls on Linux) in all but the few cases in 10^3 that glibc rounds the other way.
 //   erfc -- W. J. Cody, "Rational Chebyshev approximations for the error function", Math. Comp.
 //           23 (1969) 631-637: the three-interval rational approximations of CALERF (SPECFUN), the
-//           algorithm of CAM's error_function module that uwshcu.F90:5 uses.
+//           algorithm of CAM's error_function module that uwshcu.F90:5 uses, with the exp above.
 #pragma once
 #include <math.h>
 
@@ -51,34 +49,291 @@ UW_HD double uw_div_by(double a, double b, double y)
     return fma(e, y, q);
 }
 
+// ---------------------------------------------------------------------------------------------
+// Correctly rounded exp, log and pow (round to nearest), after Ziv's strategy (A. Ziv, "Fast
+// evaluation of elementary mathematical functions with correctly rounded last bit", ACM TOMS 17
+// (1991) 410-423): a fast evaluation to about 2^-64 relative as an unevaluated sum hi + lo, a
+// rounding test that proves RN(hi + lo) is the rounding of the exact value, and otherwise an
+// accurate double-double evaluation to about 2^-100 whose rounding is wrong only if the exact
+// value lies within 2^-100 of a midpoint between two doubles.  Double-double arithmetic uses the
+// error-free transformations TwoSum (Knuth), Fast2Sum (Dekker) and TwoProd with an FMA.  Table
+// reduction (J.-M. Muller, Elementary Functions, 3rd ed., ch. 6): exp(x) = 2^m 2^(j/64) e^r with
+// |r| <= ln2/128 and a 64-entry double-double table of 2^(j/64); log(x) = e ln2 - log(INVC) +
+// log1p(m INVC - 1) with m in [sqrt(1/2), sqrt(2)), a 7-bit reciprocal INVC per 1/128-wide bin
+// (so the reduced argument is exact), and Taylor series of e^r and log1p.  The constants are
+// computed from their definitions by gen_crmath_tables.py.  Subnormal results of exp and pow are
+// scaled after rounding (one extra rounding; the scheme never produces them).
+//
+// Agreement with other correctly rounding libraries is what these routines are for: a libm whose
+// results are correctly rounded in all but a few cases in 10^3 (glibc's exp, log and pow) then
+// gives the same bits in all but those cases.
+#include "uw_crmath_tables.h"
+
+#if defined(__CUDACC__)
+#define UW_HD_SLOW static __host__ __device__ __noinline__
+static __device__ const double uw_cr_expt_d[128] = UW_CR_EXPT_INIT;
+static __device__ const double uw_cr_logt_d[276] = UW_CR_LOGT_INIT;
+#else
+#define UW_HD_SLOW static
+#endif
+static const double uw_cr_expt_h[128] = UW_CR_EXPT_INIT;
+static const double uw_cr_logt_h[276] = UW_CR_LOGT_INIT;
+#if defined(__CUDA_ARCH__)
+#define UW_CR_EXPT(i) __ldg(&uw_cr_expt_d[(i)])
+#define UW_CR_LOGT(i) __ldg(&uw_cr_logt_d[(i)])
+#else
+#define UW_CR_EXPT(i) (uw_cr_expt_h[(i)])
+#define UW_CR_LOGT(i) (uw_cr_logt_h[(i)])
+#endif
+
+// s + e = a + b exactly (TwoSum).
+UW_HD void uw_two_sum(double a, double b, double* s, double* e)
+{
+    const double ss = UW_ADD(a, b);
+    const double v = UW_SUB(ss, a);
+    *e = UW_ADD(UW_SUB(a, UW_SUB(ss, v)), UW_SUB(b, v));
+    *s = ss;
+}
+
+// s + e = a + b exactly when |a| >= |b| or a = 0 (Fast2Sum).
+UW_HD void uw_fast_two_sum(double a, double b, double* s, double* e)
+{
+    const double ss = UW_ADD(a, b);
+    *e = UW_SUB(b, UW_SUB(ss, a));
+    *s = ss;
+}
+
+// (h, l) = (h, l) (bh, bl) + (ch, cl) in double-double, for |(h, l) (bh, bl)| well below |c|.
+UW_HD void uw_dd_mul_add(double* h, double* l, double bh, double bl, double ch, double cl)
+{
+    const double p = UW_MUL(*h, bh);
+    const double q = UW_ADD(fma(*h, bh, -p), UW_ADD(UW_MUL(*h, bl), UW_MUL(*l, bh)));
+    double s, e;
+    uw_two_sum(ch, p, &s, &e);
+    e = UW_ADD(e, UW_ADD(q, cl));
+    uw_fast_two_sum(s, e, h, l);
+}
+
+// Ziv's rounding test: RN(h + l) is the correctly rounded value of every number within err of
+// h + l when both ends of that interval round to the same double.
+UW_HD int uw_cr_rounds(double h, double l, double err)
+{
+    return UW_ADD(h, UW_ADD(l, err)) == UW_ADD(h, UW_SUB(l, err));
+}
+
+// rh + rl = xh + xl - kd ln2/64 (error below 2^-100 absolute for |k| < 2^17), with
+// kd = RN(xh * 64/ln2) rounded to an integer.  xh - kd*C1 is exact (kd*C1 is exact and the
+// operands are within a factor 2), the rest is collected by TwoSum.
+UW_HD void uw_exp_reduce(double xh, double xl, double* kd, double* rh, double* rl)
+{
+    const double k = rint(UW_MUL(xh, UW_CR_INVL));
+    const double t = fma(-k, UW_CR_C1, xh);
+    double h, e;
+    uw_two_sum(t, UW_MUL(-k, UW_CR_C2), &h, &e);
+    e = UW_ADD(e, UW_SUB(xl, UW_MUL(k, UW_CR_C3)));
+    uw_two_sum(h, e, rh, rl);
+    *kd = k;
+}
+
+// Bit patterns of doubles (exact on both sides).
+#if defined(__CUDA_ARCH__)
+#define UW_D2LL(x) __double_as_longlong(x)
+#define UW_LL2D(x) __longlong_as_double(x)
+#else
+#include <string.h>
+UW_HD long long UW_D2LL(double x)
+{
+    long long i;
+    memcpy(&i, &x, sizeof i);
+    return i;
+}
+UW_HD double UW_LL2D(long long i)
+{
+    double x;
+    memcpy(&x, &i, sizeof x);
+    return x;
+}
+#endif
+
+// 2^m y for y in [0.98, 2.03] (|m| <= 1076): one exact multiplication by 2^m where 2^m and the
+// result are normal, ldexp otherwise (subnormal results, overflow).
+UW_HD double uw_cr_scale(double y, int m)
+{
+    if (m >= -1021 && m <= 1022) return UW_MUL(y, UW_LL2D((long long)(m + 1023) << 52));
+    return ldexp(y, m);
+}
+
+// Accurate exp(xh + xl), |xh + xl| <= 746: e^r by its Taylor series to degree 11 (truncation
+// below 2^-119 for |r| <= ln2/128), degrees 6..11 in double, 0..5 by double-double Horner steps,
+// times the double-double table entry; relative error about 2^-100.
+UW_HD double uw_exp_accurate_core(double xh, double xl)
+{
+    double kd, rh, rl;
+    uw_exp_reduce(xh, xl, &kd, &rh, &rl);
+    const int k = (int)kd;
+    const int j = k & 63;
+    const int m = (k - j) / 64;
+    double q = UW_CR_F11_H;
+    q = fma(q, rh, UW_CR_F10_H);
+    q = fma(q, rh, UW_CR_F9_H);
+    q = fma(q, rh, UW_CR_F8_H);
+    q = fma(q, rh, UW_CR_F7_H);
+    q = fma(q, rh, UW_CR_F6_H);
+    double h = q, l = 0.0;
+    uw_dd_mul_add(&h, &l, rh, rl, UW_CR_F5_H, UW_CR_F5_L);
+    uw_dd_mul_add(&h, &l, rh, rl, UW_CR_F4_H, UW_CR_F4_L);
+    uw_dd_mul_add(&h, &l, rh, rl, UW_CR_F3_H, UW_CR_F3_L);
+    uw_dd_mul_add(&h, &l, rh, rl, 0.5, 0.0);
+    uw_dd_mul_add(&h, &l, rh, rl, 1.0, 0.0);
+    uw_dd_mul_add(&h, &l, rh, rl, 1.0, 0.0);
+    const double th = UW_CR_EXPT(2 * j), tl = UW_CR_EXPT(2 * j + 1);
+    double H, L;
+    {
+        const double p = UW_MUL(th, h);
+        const double e = UW_ADD(fma(th, h, -p), UW_ADD(UW_MUL(th, l), UW_MUL(tl, h)));
+        uw_fast_two_sum(p, e, &H, &L);
+    }
+    return uw_cr_scale(UW_ADD(H, L), m);
+}
+
+UW_HD_SLOW double uw_exp_accurate(double x) { return uw_exp_accurate_core(x, 0.0); }
+
+// Fast exp(xh + xl): e^r = 1 + r + r^2 P(r) with P to degree 5 in double (absolute error below
+// 2^-66), times the table entry.  Returns 1 and sets *y when the rounding test passes with the
+// relative error bound err_rel (at least 2^-63).
+UW_HD int uw_exp_fast(double xh, double xl, double err_rel, double* y)
+{
+    double kd, rh, rl;
+    uw_exp_reduce(xh, xl, &kd, &rh, &rl);
+    const int k = (int)kd;
+    const int j = k & 63;
+    const int m = (k - j) / 64;
+    double p = UW_CR_F7_H;
+    p = fma(p, rh, UW_CR_F6_H);
+    p = fma(p, rh, UW_CR_F5_H);
+    p = fma(p, rh, UW_CR_F4_H);
+    p = fma(p, rh, UW_CR_F3_H);
+    p = fma(p, rh, 0.5);
+    const double q = UW_MUL(UW_MUL(rh, rh), p);
+    double h, l;
+    uw_fast_two_sum(1.0, rh, &h, &l);
+    l = UW_ADD(l, UW_ADD(rl, q));
+    const double th = UW_CR_EXPT(2 * j), tl = UW_CR_EXPT(2 * j + 1);
+    const double H = UW_MUL(th, h);
+    const double L = UW_ADD(fma(th, h, -H), UW_ADD(UW_MUL(th, l), UW_MUL(tl, h)));
+    if (!uw_cr_rounds(H, L, UW_MUL(err_rel, H))) return 0;
+    *y = uw_cr_scale(UW_ADD(H, L), m);
+    return 1;
+}
+
 UW_HD double uw_exp(double x)
 {
     if (x != x) return x;
-    if (x > 709.782712893384) return HUGE_VAL;
-    if (x < -745.1332191019412) return 0.0;
-    const double LOG2E = 1.4426950408889634074;
-    const double LN2_HI = 6.93147180369123816490e-01;
-    const double LN2_LO = 1.90821492927058770002e-10;
-    const double kd = floor(fma(x, LOG2E, 0.5));
-    double r = fma(-kd, LN2_HI, x);
-    r = fma(-kd, LN2_LO, r);
-    double p = 1.0 / 6227020800.0;          // 1/13!
-    p = fma(p, r, 1.0 / 479001600.0);       // 1/12!
-    p = fma(p, r, 1.0 / 39916800.0);        // 1/11!
-    p = fma(p, r, 1.0 / 3628800.0);         // 1/10!
-    p = fma(p, r, 1.0 / 362880.0);          // 1/9!
-    p = fma(p, r, 1.0 / 40320.0);           // 1/8!
-    p = fma(p, r, 1.0 / 5040.0);            // 1/7!
-    p = fma(p, r, 1.0 / 720.0);             // 1/6!
-    p = fma(p, r, 1.0 / 120.0);             // 1/5!
-    p = fma(p, r, 1.0 / 24.0);              // 1/4!
-    p = fma(p, r, 1.0 / 6.0);               // 1/3!
-    p = fma(p, r, 0.5);
-    p = fma(p, r, 1.0);
-    p = fma(p, r, 1.0);
-    int k = (int)kd;
-    if (k < -1020) return ldexp(ldexp(p, k + 60), -60);
-    return ldexp(p, k);
+    if (x > 709.8) return HUGE_VAL;
+    if (x < -745.2) return 0.0;
+    double y;
+    if (uw_exp_fast(x, 0.0, 0x1p-63, &y)) return y;
+    return uw_exp_accurate(x);
+}
+
+// Reduction of log: x = 2^e m, m in [sqrt(1/2), sqrt(2)), bin i = floor(128 m) - 90, t = m INVC - 1
+// (exact, |t| < 2^-6).  x must be positive and finite.
+UW_HD void uw_log_reduce(double x, int* e, int* i, double* t)
+{
+    int ea = 0;
+    if (x < 0x1p-1022) {
+        x = UW_MUL(x, 0x1p54);
+        ea = -54;
+    }
+    // x = 2^e m with m in [1/2, 1) (x positive and normal here): frexp by its bits
+    const long long b = UW_D2LL(x);
+    *e = (int)((b >> 52) & 0x7ff) - 1022;
+    double m = UW_LL2D((b & 0x000fffffffffffffLL) | 0x3fe0000000000000LL);
+    if (m < UW_CR_SQRTH) {
+        m = UW_MUL(m, 2.0);
+        *e = *e - 1;
+    }
+    *e = *e + ea;
+    *i = (int)UW_MUL(m, 128.0) - 90;
+    *t = fma(m, UW_CR_LOGT(3 * *i), -1.0);
+}
+
+// Accurate log as a double-double (relative error about 2^-100): log1p(t) = t S(t) with the
+// Taylor coefficients of degrees 9..17 of S in double and 1..8 by double-double Horner steps.
+UW_HD void uw_log_accurate_dd(double x, double* H, double* L)
+{
+    int e, i;
+    double t;
+    uw_log_reduce(x, &e, &i, &t);
+    double q = UW_CR_L17_H;
+    q = fma(q, t, UW_CR_L16_H);
+    q = fma(q, t, UW_CR_L15_H);
+    q = fma(q, t, UW_CR_L14_H);
+    q = fma(q, t, UW_CR_L13_H);
+    q = fma(q, t, UW_CR_L12_H);
+    q = fma(q, t, UW_CR_L11_H);
+    q = fma(q, t, UW_CR_L10_H);
+    q = fma(q, t, UW_CR_L9_H);
+    double h = q, l = 0.0;
+    uw_dd_mul_add(&h, &l, t, 0.0, UW_CR_L8_H, UW_CR_L8_L);
+    uw_dd_mul_add(&h, &l, t, 0.0, UW_CR_L7_H, UW_CR_L7_L);
+    uw_dd_mul_add(&h, &l, t, 0.0, UW_CR_L6_H, UW_CR_L6_L);
+    uw_dd_mul_add(&h, &l, t, 0.0, UW_CR_L5_H, UW_CR_L5_L);
+    uw_dd_mul_add(&h, &l, t, 0.0, UW_CR_L4_H, UW_CR_L4_L);
+    uw_dd_mul_add(&h, &l, t, 0.0, UW_CR_L3_H, UW_CR_L3_L);
+    uw_dd_mul_add(&h, &l, t, 0.0, UW_CR_L2_H, UW_CR_L2_L);
+    uw_dd_mul_add(&h, &l, t, 0.0, 1.0, 0.0);
+    // log1p(t) = t (h + l)
+    double ph = UW_MUL(t, h);
+    double pl = UW_ADD(fma(t, h, -ph), UW_MUL(t, l));
+    // e ln2 - log(INVC): e*LN2H is exact (42-bit constant, |e| < 2^11)
+    const double ed = (double)e;
+    double sh, sl;
+    uw_two_sum(UW_MUL(ed, UW_CR_LN2H), UW_CR_LOGT(3 * i + 1), &sh, &sl);
+    sl = UW_ADD(sl, UW_ADD(UW_MUL(ed, UW_CR_LN2L), UW_CR_LOGT(3 * i + 2)));
+    uw_fast_two_sum(sh, sl, &sh, &sl);
+    double rh, rl;
+    uw_two_sum(sh, ph, &rh, &rl);
+    rl = UW_ADD(rl, UW_ADD(sl, pl));
+    uw_fast_two_sum(rh, rl, H, L);
+}
+
+UW_HD_SLOW double uw_log_accurate(double x)
+{
+    double H, L;
+    uw_log_accurate_dd(x, &H, &L);
+    return UW_ADD(H, L);
+}
+
+// Fast log as a double-double, relative error below 2^-64: t - t^2/2 exactly (TwoProd), t^3 P(t)
+// in double with P to degree 9 (truncation below 2^-75 relative).
+UW_HD void uw_log_fast(double x, double* H, double* L)
+{
+    int e, i;
+    double t;
+    uw_log_reduce(x, &e, &i, &t);
+    double p = UW_CR_L12_H;
+    p = fma(p, t, UW_CR_L11_H);
+    p = fma(p, t, UW_CR_L10_H);
+    p = fma(p, t, UW_CR_L9_H);
+    p = fma(p, t, UW_CR_L8_H);
+    p = fma(p, t, UW_CR_L7_H);
+    p = fma(p, t, UW_CR_L6_H);
+    p = fma(p, t, UW_CR_L5_H);
+    p = fma(p, t, UW_CR_L4_H);
+    p = fma(p, t, UW_CR_L3_H);
+    const double t3p = UW_MUL(UW_MUL(t, t), UW_MUL(t, p));
+    const double t2h = UW_MUL(t, t);
+    const double t2l = fma(t, t, -t2h);
+    const double ed = (double)e;
+    double s1, e1, s2, e2, s3, e3;
+    uw_two_sum(UW_MUL(ed, UW_CR_LN2H), UW_CR_LOGT(3 * i + 1), &s1, &e1);
+    uw_two_sum(s1, t, &s2, &e2);
+    uw_two_sum(s2, UW_MUL(-0.5, t2h), &s3, &e3);
+    double lo = UW_ADD(UW_ADD(e1, e2), e3);
+    lo = UW_ADD(lo, UW_ADD(UW_MUL(ed, UW_CR_LN2L), UW_CR_LOGT(3 * i + 2)));
+    lo = UW_ADD(lo, UW_SUB(t3p, UW_MUL(0.5, t2l)));
+    uw_fast_two_sum(s3, lo, H, L);
 }
 
 UW_HD double uw_log(double x)
@@ -88,44 +343,46 @@ UW_HD double uw_log(double x)
         return (x != x) ? x : (x - x) / (x - x);   // NaN for x < 0
     }
     if (x == HUGE_VAL) return x;
-    const double LN2_HI = 6.93147180369123816490e-01;
-    const double LN2_LO = 1.90821492927058770002e-10;
-    int e;
-    double m = frexp(x, &e);                 // m in [0.5, 1)
-    if (m < 0.70710678118654752440) {
-        m = m * 2.0;
-        e = e - 1;
-    }
-    const double f = m - 1.0;                // exact
-    const double s = f / (2.0 + f);
-    const double z = UW_MUL(s, s);
-    double q = 2.0 / 25.0;
-    q = fma(q, z, 2.0 / 23.0);
-    q = fma(q, z, 2.0 / 21.0);
-    q = fma(q, z, 2.0 / 19.0);
-    q = fma(q, z, 2.0 / 17.0);
-    q = fma(q, z, 2.0 / 15.0);
-    q = fma(q, z, 2.0 / 13.0);
-    q = fma(q, z, 2.0 / 11.0);
-    q = fma(q, z, 2.0 / 9.0);
-    q = fma(q, z, 2.0 / 7.0);
-    q = fma(q, z, 2.0 / 5.0);
-    q = fma(q, z, 2.0 / 3.0);
-    const double R = UW_MUL(z, q);
-    const double hfsq = UW_MUL(UW_MUL(0.5, f), f);
-    const double dk = (double)e;
-    const double t = UW_ADD(UW_MUL(s, UW_ADD(hfsq, R)), UW_MUL(dk, LN2_LO));
-    return UW_SUB(UW_MUL(dk, LN2_HI), UW_SUB(UW_SUB(hfsq, t), f));
+    double H, L;
+    uw_log_fast(x, &H, &L);
+    if (uw_cr_rounds(H, L, UW_MUL(0x1p-62, fabs(H)))) return UW_ADD(H, L);
+    return uw_log_accurate(x);
 }
 
+UW_HD_SLOW double uw_pow_accurate(double x, double y)
+{
+    double Lh, Ll;
+    uw_log_accurate_dd(x, &Lh, &Ll);
+    const double zh = UW_MUL(y, Lh);
+    const double zl = UW_ADD(fma(y, Lh, -zh), UW_MUL(y, Ll));
+    return uw_exp_accurate_core(zh, zl);
+}
+
+// pow(x, y) for x >= 0: exp(y log x) with log and the product in double-double.
 UW_HD double uw_pow(double x, double y)
 {
     if (x != x || y != y) return x + y;
     if (y == 0.0) return 1.0;
     if (x == 0.0) return (y > 0.0) ? 0.0 : HUGE_VAL;
     if (x < 0.0) return (x - x) / (x - x);
-    return uw_exp(UW_MUL(y, uw_log(x)));
+    if (x == HUGE_VAL) return (y > 0.0) ? HUGE_VAL : 0.0;
+    double Lh, Ll;
+    uw_log_fast(x, &Lh, &Ll);
+    const double zh = UW_MUL(y, Lh);
+    if (zh > 709.8) return HUGE_VAL;
+    if (zh < -745.2) return 0.0;
+    const double zl = UW_ADD(fma(y, Lh, -zh), UW_MUL(y, Ll));
+    // |z| 2^-64 from the logarithm plus 2^-66 from the exponential, with a factor 4 to spare
+    double r;
+    if (uw_exp_fast(zh, zl, UW_MUL(0x1p-62, UW_ADD(1.0, fabs(zh))), &r)) return r;
+    return uw_pow_accurate(x, y);
 }
+
+// The exponential CALERF calls: this file's correctly rounded exp unless the includer names another
+// (the oracle's Fortran-math build names the C library's exp, as a Fortran build of CALERF calls it).
+#ifndef UW_ERFC_EXP
+#define UW_ERFC_EXP uw_exp
+#endif
 
 // erfc(x), Cody's CALERF with jint = 1.
 UW_HD double uw_erfc(double x)
@@ -165,7 +422,7 @@ UW_HD double uw_erfc(double x)
         result = UW_ADD(xnum, C[7]) / UW_ADD(xden, D[7]);
         const double ysq = floor(UW_MUL(y, 16.0)) / 16.0;
         const double del = UW_MUL(UW_SUB(y, ysq), UW_ADD(y, ysq));
-        result = UW_MUL(UW_MUL(uw_exp(-UW_MUL(ysq, ysq)), uw_exp(-del)), result);
+        result = UW_MUL(UW_MUL(UW_ERFC_EXP(-UW_MUL(ysq, ysq)), UW_ERFC_EXP(-del)), result);
     } else if (y >= xbig) {
         result = 0.0;
     } else {
@@ -179,7 +436,7 @@ UW_HD double uw_erfc(double x)
         result = UW_SUB(sqrpi, result) / y;
         const double ysq2 = floor(UW_MUL(y, 16.0)) / 16.0;
         const double del = UW_MUL(UW_SUB(y, ysq2), UW_ADD(y, ysq2));
-        result = UW_MUL(UW_MUL(uw_exp(-UW_MUL(ysq2, ysq2)), uw_exp(-del)), result);
+        result = UW_MUL(UW_MUL(UW_ERFC_EXP(-UW_MUL(ysq2, ysq2)), UW_ERFC_EXP(-del)), result);
     }
     if (x < 0.0) result = UW_SUB(2.0, result);
     return result;

@@ -62,6 +62,7 @@
 #define UW_X_CUFILTER (1 << 8)
 #define UW_X_KINV1 (1 << 9)
 #define UW_X_REI (1 << 10)
+#define UW_X_NONFINITE (1 << 11)   // a non-finite input (no counterpart in the Fortran)
 // limit_* bits
 #define UW_L_SHCU (1 << 0)
 #define UW_L_NEGCON (1 << 1)
@@ -78,6 +79,7 @@
 #define UW_ERRBIT_MU 1        // 'Critical error in mu calculation' (uwshcu.F90:2119-2122)
 #define UW_ERRBIT_FINDSP 2    // findsp did not converge (uwshcu.F90:5423-5431)
 #define UW_ERRBIT_ENTHALPY 4  // findsp enthalpy not conserved (uwshcu.F90:5435-5447)
+#define UW_ERRBIT_NONFINITE 8 // a column had a non-finite input and took the exit path
 
 // Physical constants and tables, set once by uwshcu_init and copied to __constant__ memory.
 struct UwConst {

@@ -124,15 +124,33 @@ struct HandRegion {
     size_t cap = 0, words = 0;
 };
 
+// What a device-array call (uwshcu_compute_device, uwshcu_compute_member, the tangent-linear and
+// adjoint entries) needs besides its arguments, one set per caller stream, so that calls on different
+// streams whose GPU work overlaps do not share a worklist, a hand-off region or an endrun word.
+struct StreamCtx {
+    cudaStream_t stream = nullptr;
+    bool used = false;
+    unsigned long long last = 0;   // LRU tick of the last call
+    unsigned int* err = nullptr;   // endrun bits of the calls since the last uwshcu_device_status
+    int* wl = nullptr;             // worklist of convecting columns: [0] = count, [1..] = column ids
+    size_t wl_cap = 0;
+    HandRegion hand;               // hand-off region of the sorted schedule
+};
+
 struct DeviceState {
     unsigned uploaded_gen = 0;   // generation of the constants in this device's __constant__ bank
-    unsigned int* d_err = nullptr;
+    // per caller stream; a call on a new stream when all are taken reuses the least recently used
+    // one after a cudaDeviceSynchronize (that stream's uncollected endrun bits are dropped)
+    static constexpr int kStreamCtx = 32;
+    StreamCtx sctx[kStreamCtx];
+    unsigned long long tick = 0;
+    int* last_count = nullptr;   // worklist count of the last device-array call (profiling)
     cudaStream_t stream = nullptr;
     double* d_buf = nullptr;     // device arena (doubles)
     size_t d_cap = 0;
     double* h_buf = nullptr;     // pinned staging (doubles)
     size_t h_cap = 0;
-    int* d_wl = nullptr;         // worklist of convecting columns: [0] = count, [1..] = column ids
+    int* d_wl = nullptr;         // host-array calls: per chunk [count, endrun bits, column ids]
     size_t wl_cap = 0;
     // opt-in per-launch timing: events around the trigger and worklist launches of each call
     static constexpr int kSlots = 256;
@@ -145,7 +163,8 @@ struct DeviceState {
     cudaStream_t pipe[kPipe] = {};
     cudaStream_t pin = nullptr, pout = nullptr;   // copy-in and copy-out streams
     std::vector<cudaEvent_t> done, ev_in, ev_comp;   // per chunk: copied out, copied in, computed
-    // hand-off regions of the split worklist pass: [0] device-array calls, [1 + j] pipe stream j
+    // hand-off regions of the split worklist pass of host-array calls: [1 + j] pipe stream j ([0]
+    // unused: device-array calls use their stream's StreamCtx)
     HandRegion hand[1 + kPipe];
     // adjoint tapes, adjoints and tables, kept between adjoint calls (uwshcu_adjoint_release)
     void* adj_buf = nullptr;
@@ -236,6 +255,7 @@ int status_from_bits(unsigned bits)
     if (bits & UW_ERRBIT_ENTHALPY) return UWSHCU_ERR_FINDSP_ENTHALPY;
     if (bits & UW_ERRBIT_FINDSP) return UWSHCU_ERR_FINDSP_NONCONVERGED;
     if (bits & UW_ERRBIT_MU) return UWSHCU_ERR_MU_INCONSISTENT;
+    if (bits & UW_ERRBIT_NONFINITE) return UWSHCU_WARN_NONFINITE_INPUT;
     return UWSHCU_OK;
 }
 
@@ -253,10 +273,6 @@ int ensure_device(DeviceState** out)
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return cuda_fail(e);
     if (dev < 0 || dev >= kMaxDev) return UWSHCU_ERR_NO_DEVICE;
     DeviceState& d = s.dev[dev];
-    if (!d.d_err) {
-        if ((e = cudaMalloc(&d.d_err, sizeof(unsigned int))) != cudaSuccess) return cuda_fail(e);
-        if ((e = cudaMemset(d.d_err, 0, sizeof(unsigned int))) != cudaSuccess) return cuda_fail(e);
-    }
     if (!d.stream) {
         if ((e = cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking)) != cudaSuccess) return cuda_fail(e);
     }
@@ -342,15 +358,45 @@ void copy_planes(const std::vector<Plane>& planes)
     for (auto& t : th) t.join();
 }
 
-int grow_worklist(DeviceState& d, size_t ncol)
+// A worklist of at least n ints (cudaFree waits for the device, so no call still uses the old one).
+int grow_ints(int*& buf, size_t& cap, size_t n)
 {
-    if (ncol + 1 <= d.wl_cap) return UWSHCU_OK;
-    if (d.d_wl) cudaFree(d.d_wl);
-    d.d_wl = nullptr;
-    d.wl_cap = 0;
-    cudaError_t e = cudaMalloc(&d.d_wl, (ncol + 1) * sizeof(int));
+    if (n <= cap) return UWSHCU_OK;
+    if (buf) cudaFree(buf);
+    buf = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc(&buf, n * sizeof(int));
     if (e != cudaSuccess) return cuda_fail(e);
-    d.wl_cap = ncol + 1;
+    cap = n;
+    return UWSHCU_OK;
+}
+
+int grow_worklist(DeviceState& d, size_t ncol) { return grow_ints(d.d_wl, d.wl_cap, ncol + 1); }
+
+// The context of caller stream st on device d (created on first use).
+int stream_ctx(DeviceState& d, cudaStream_t st, StreamCtx** out)
+{
+    StreamCtx* c = nullptr;
+    for (StreamCtx& x : d.sctx)
+        if (x.used && x.stream == st) c = &x;
+    if (!c) {
+        for (StreamCtx& x : d.sctx)
+            if (!x.used && (!c || x.err)) c = &x;   // a free slot, one with buffers first
+        if (!c) {
+            c = &d.sctx[0];
+            for (StreamCtx& x : d.sctx)
+                if (x.last < c->last) c = &x;
+            cudaError_t e = cudaDeviceSynchronize();   // its stream's work may still use its buffers
+            if (e != cudaSuccess) return cuda_fail(e);
+        }
+        cudaError_t e;
+        if (!c->err && (e = cudaMalloc(&c->err, sizeof(unsigned int))) != cudaSuccess) return cuda_fail(e);
+        if ((e = cudaMemset(c->err, 0, sizeof(unsigned int))) != cudaSuccess) return cuda_fail(e);
+        c->stream = st;
+        c->used = true;
+    }
+    c->last = ++d.tick;
+    *out = c;
     return UWSHCU_OK;
 }
 
@@ -424,9 +470,8 @@ size_t hand_slots_for(int iend, size_t words)
     return std::max(cap, (size_t)32);
 }
 
-const UwHand* hand_region(DeviceState& d, int r, int iend, int mkx, int ncnst)
+const UwHand* hand_region(HandRegion& h, int iend, int mkx, int ncnst)
 {
-    HandRegion& h = d.hand[r];
     const size_t words = uw_state_words(mkx, ncnst);
     size_t cap = hand_slots_for(iend, words);
     if (S().hand_slots > 0 && h.base && h.cap > cap) {   // a smaller limit applies to this region now
@@ -449,15 +494,14 @@ const UwHand* hand_region(DeviceState& d, int r, int iend, int mkx, int ncnst)
 // The worklist pass over list[0 .. *count): one UW_MODE_LIST launch, or with the sorted schedule
 // the split pass through hand-off region r: UW_MODE_LIST1, the sort of the handed-off
 // columns by iteration-1 updraft depth, UW_MODE_RESUME.
-cudaError_t worklist_pass(DeviceState& d, int r, UwArgs A, int* list, int* count, cudaStream_t st)
+cudaError_t worklist_pass(HandRegion& h, UwArgs A, int* list, int* count, cudaStream_t st)
 {
     State& s = S();
     const UwHand* H = nullptr;
-    if (s.schedule == UWSHCU_SCHED_SORTED) H = hand_region(d, r, A.iend, A.mkx, A.ncnst);
+    if (s.schedule == UWSHCU_SCHED_SORTED) H = hand_region(h, A.iend, A.mkx, A.ncnst);
     if (!H) return launch_mode(&A, s.precision, kModeList, list, count, A.iend, s.block, st);
     cudaError_t e;
     A.hand = H;
-    const HandRegion& h = d.hand[r];
     int* cnt = reinterpret_cast<int*>(h.base + kHandCountOffset);
     if ((e = cudaMemsetAsync(cnt, 0, (1 + UW_HAND_KEYS) * sizeof(int), st)) != cudaSuccess) return e;
     if ((e = launch_mode(&A, s.precision, kModeList1, list, count, A.iend, s.block, st)) != cudaSuccess) return e;
@@ -470,18 +514,21 @@ cudaError_t worklist_pass(DeviceState& d, int r, UwArgs A, int* list, int* count
 }
 
 // Enqueue the column computation for A on st with the selected schedule.
-int enqueue(DeviceState& d, const UwArgs& A, cudaStream_t st)
+// A device-array call on stream st with the stream's context c (A.err is set here).
+int enqueue(DeviceState& d, StreamCtx& c, UwArgs A, cudaStream_t st)
 {
     State& s = S();
     cudaError_t e;
+    A.err = c.err;
     if (s.schedule == UWSHCU_SCHED_SINGLE_PASS) {
         if ((e = launch_mode(&A, s.precision, kModeAll, nullptr, nullptr, A.iend, s.block, st)) != cudaSuccess) return cuda_fail(e);
         return UWSHCU_OK;
     }
-    int rc = grow_worklist(d, (size_t)A.iend);
+    int rc = grow_ints(c.wl, c.wl_cap, (size_t)A.iend + 1);
     if (rc != UWSHCU_OK) return rc;
-    int* count = d.d_wl;
-    int* list = d.d_wl + 1;
+    int* count = c.wl;
+    int* list = c.wl + 1;
+    d.last_count = count;
     cudaEvent_t* ev = nullptr;
     if (s.profiling && d.nrec < DeviceState::kSlots) {
         ev = d.ev[d.nrec];
@@ -493,7 +540,7 @@ int enqueue(DeviceState& d, const UwArgs& A, cudaStream_t st)
     if (ev && (e = cudaEventRecord(ev[0], st)) != cudaSuccess) return cuda_fail(e);
     if ((e = launch_mode(&A, s.precision, kModeTrigger, list, count, A.iend, s.block, st)) != cudaSuccess) return cuda_fail(e);
     if (ev && (e = cudaEventRecord(ev[1], st)) != cudaSuccess) return cuda_fail(e);
-    if ((e = worklist_pass(d, 0, A, list, count, st)) != cudaSuccess) return cuda_fail(e);
+    if ((e = worklist_pass(c.hand, A, list, count, st)) != cudaSuccess) return cuda_fail(e);
     if (ev && (e = cudaEventRecord(ev[2], st)) != cudaSuccess) return cuda_fail(e);
     return UWSHCU_OK;
 }
@@ -691,7 +738,7 @@ int host_call(int inv, int mix, int mkx, int iend, int ncnst, double dt, const d
         } else {
             if ((e = launch_mode(&A, s.precision, kModeTrigger, wreg + 2, wreg, A.iend, s.block, st)) != cudaSuccess)
                 return cuda_fail(e);
-            if ((e = worklist_pass(*d, 1 + (int)(c % (size_t)s.pipe_streams), A, wreg + 2, wreg, st)) != cudaSuccess)
+            if ((e = worklist_pass(d->hand[1 + c % (size_t)s.pipe_streams], A, wreg + 2, wreg, st)) != cudaSuccess)
                 return cuda_fail(e);
         }
         if ((e = cudaEventRecord(d->ev_comp[c], st)) != cudaSuccess) return cuda_fail(e);
@@ -913,7 +960,8 @@ int uwshcu_profile_read(int* calls, double* trigger_ms, double* list_ms, int* li
     *calls = d.nrec;
     if (list_columns) {
         int cnt = 0;
-        if (d.d_wl && (e = cudaMemcpy(&cnt, d.d_wl, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess) return cuda_fail(e);
+        if (d.last_count && (e = cudaMemcpy(&cnt, d.last_count, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess)
+            return cuda_fail(e);
         *list_columns = cnt;
     }
     d.nrec = 0;
@@ -958,12 +1006,16 @@ int uwshcu_finalize(void)
     bool have = cudaGetDevice(&cur) == cudaSuccess;
     for (int dv = 0; dv < kMaxDev; dv++) {
         DeviceState& d = s.dev[dv];
-        if (!d.d_err && !d.d_buf && !d.h_buf && !d.stream && !d.pipe[0] && !d.adj_buf) continue;
+        if (!d.d_buf && !d.h_buf && !d.stream && !d.pipe[0] && !d.adj_buf && !d.sctx[0].err) continue;
         cudaSetDevice(dv);
         if (d.d_buf) cudaFree(d.d_buf);
         if (d.h_buf) cudaFreeHost(d.h_buf);
-        if (d.d_err) cudaFree(d.d_err);
         if (d.d_wl) cudaFree(d.d_wl);
+        for (StreamCtx& c : d.sctx) {
+            if (c.err) cudaFree(c.err);
+            if (c.wl) cudaFree(c.wl);
+            if (c.hand.base) cudaFree(c.hand.base);
+        }
         for (HandRegion& h : d.hand)
             if (h.base) cudaFree(h.base);
         if (d.adj_buf) cudaFree(d.adj_buf);
@@ -1113,7 +1165,9 @@ int uwshcu_compute_member(const uwshcu_member* m, void* stream)
     DeviceState* d = nullptr;
     int rc = ensure_device(&d);
     if (rc != UWSHCU_OK) return rc;
-    return enqueue(*d, member_args(*m, s.k.ncnst, d->d_err), (cudaStream_t)stream);
+    StreamCtx* c = nullptr;
+    if ((rc = stream_ctx(*d, (cudaStream_t)stream, &c)) != UWSHCU_OK) return rc;
+    return enqueue(*d, *c, member_args(*m, s.k.ncnst, c->err), (cudaStream_t)stream);
 }
 
 int uwshcu_compute_device(int mix, int mkx, int iend, int ncnst, double dt, int inv, const double* ps0,
@@ -1151,8 +1205,9 @@ int uwshcu_compute_device(int mix, int mkx, int iend, int ncnst, double dt, int 
     A.trten = trten; A.qrten = qrten; A.qsten = qsten; A.precip = precip; A.snow = snow; A.evapc = evapc;
     A.cufrc = cufrc; A.qcu = qcu; A.qlu = qlu; A.qiu = qiu; A.cbmf = cbmf; A.qc = qc; A.rliq = rliq;
     A.cnt = cnt; A.cnb = cnb; A.dpdry0 = dpdry0; A.wu = wu; A.diag_int = diag_int; A.diag_real = diag_real;
-    A.err = d->d_err;
-    return enqueue(*d, A, (cudaStream_t)stream);
+    StreamCtx* c = nullptr;
+    if ((rc = stream_ctx(*d, (cudaStream_t)stream, &c)) != UWSHCU_OK) return rc;
+    return enqueue(*d, *c, A, (cudaStream_t)stream);
 }
 
 int uwshcu_budget_device(int mix, int mkx, int iend, int inv, double dt, const double* s0,
@@ -1193,15 +1248,18 @@ int uwshcu_tangent_device(const uwshcu_member* m, const uwshcu_tangent* t, void*
     DeviceState* d = nullptr;
     int rc = ensure_device(&d);
     if (rc != UWSHCU_OK) return rc;
-    UwArgs A = member_args(*m, ncnst, d->d_err);
+    cudaStream_t st = (cudaStream_t)stream;
+    StreamCtx* c = nullptr;
+    if ((rc = stream_ctx(*d, st, &c)) != UWSHCU_OK) return rc;
+    UwArgs A = member_args(*m, ncnst, c->err);
     // the forward path's two-phase schedule: trigger pass, then the convecting columns
     auto launch = (m->mkx + 1 <= 32) ? uw_tl_launch_k32n5 : uw_tl_launch_k64n5;
-    cudaStream_t st = (cudaStream_t)stream;
     cudaError_t e;
-    if ((rc = grow_worklist(*d, (size_t)m->iend)) != UWSHCU_OK) return rc;
-    if ((e = cudaMemsetAsync(d->d_wl, 0, sizeof(int), st)) != cudaSuccess) return cuda_fail(e);
-    if ((e = launch(&A, t, kModeTrigger, d->d_wl + 1, d->d_wl, m->iend, 128, st)) != cudaSuccess) return cuda_fail(e);
-    if ((e = launch(&A, t, kModeList, d->d_wl + 1, d->d_wl, m->iend, 128, st)) != cudaSuccess) return cuda_fail(e);
+    if ((rc = grow_ints(c->wl, c->wl_cap, (size_t)m->iend + 1)) != UWSHCU_OK) return rc;
+    int* wl = c->wl;
+    if ((e = cudaMemsetAsync(wl, 0, sizeof(int), st)) != cudaSuccess) return cuda_fail(e);
+    if ((e = launch(&A, t, kModeTrigger, wl + 1, wl, m->iend, 128, st)) != cudaSuccess) return cuda_fail(e);
+    if ((e = launch(&A, t, kModeList, wl + 1, wl, m->iend, 128, st)) != cudaSuccess) return cuda_fail(e);
     return UWSHCU_OK;
 }
 
@@ -1221,7 +1279,9 @@ int uwshcu_adjoint_device(const uwshcu_member* m, const uwshcu_adjoint* a, void*
     DeviceState* d = nullptr;
     int rc = ensure_device(&d);
     if (rc != UWSHCU_OK) return rc;
-    const UwArgs A = member_args(*m, ncnst, d->d_err);
+    StreamCtx* sc = nullptr;
+    if ((rc = stream_ctx(*d, (cudaStream_t)stream, &sc)) != UWSHCU_OK) return rc;
+    const UwArgs A = member_args(*m, ncnst, sc->err);
     const size_t mix = (size_t)m->mix, mkx = (size_t)m->mkx;
     // the unit for the level count: KP = 32 or 64 levels
     const bool k32 = m->mkx + 1 <= 32;
@@ -1237,12 +1297,12 @@ int uwshcu_adjoint_device(const uwshcu_member* m, const uwshcu_adjoint* a, void*
         if (g.first && (e = cudaMemsetAsync(g.first, 0, g.second * sizeof(double), st)) != cudaSuccess) return cuda_fail(e);
     if (m->iend == 0) return UWSHCU_OK;
     // trigger pass of the FP64 path: the exit columns' outputs and the worklist of the others
-    if ((rc = grow_worklist(*d, (size_t)m->iend)) != UWSHCU_OK) return rc;
-    if ((e = cudaMemsetAsync(d->d_wl, 0, sizeof(int), st)) != cudaSuccess) return cuda_fail(e);
-    if ((e = launch_mode(&A, UWSHCU_PREC_FP64, kModeTrigger, d->d_wl + 1, d->d_wl, m->iend, 128, st)) != cudaSuccess)
+    if ((rc = grow_ints(sc->wl, sc->wl_cap, (size_t)m->iend + 1)) != UWSHCU_OK) return rc;
+    if ((e = cudaMemsetAsync(sc->wl, 0, sizeof(int), st)) != cudaSuccess) return cuda_fail(e);
+    if ((e = launch_mode(&A, UWSHCU_PREC_FP64, kModeTrigger, sc->wl + 1, sc->wl, m->iend, 128, st)) != cudaSuccess)
         return cuda_fail(e);
     int ncand = 0;
-    if ((e = cudaMemcpyAsync(&ncand, d->d_wl, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+    if ((e = cudaMemcpyAsync(&ncand, sc->wl, sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
         (e = cudaStreamSynchronize(st)) != cudaSuccess)
         return cuda_fail(e);
     s.adj_records = 0;
@@ -1261,7 +1321,7 @@ int uwshcu_adjoint_device(const uwshcu_member* m, const uwshcu_adjoint* a, void*
     int end_bit = 1;
     while (end_bit < 31 && ((size_t)1 << end_bit) < (size_t)m->iend) end_bit++;
     size_t sort_bytes = 0;
-    if ((e = cub::DeviceRadixSort::SortKeys(nullptr, sort_bytes, d->d_wl + 1, d->d_wl + 1, ncand, 0, end_bit, st)) !=
+    if ((e = cub::DeviceRadixSort::SortKeys(nullptr, sort_bytes, sc->wl + 1, sc->wl + 1, ncand, 0, end_bit, st)) !=
         cudaSuccess)
         return cuda_fail(e);
     bool restart = false;
@@ -1303,7 +1363,7 @@ int uwshcu_adjoint_device(const uwshcu_member* m, const uwshcu_adjoint* a, void*
         int* wl = reinterpret_cast<int*>(base + o_wl);
         size_t tmp_bytes = sort_bytes;
         if ((e = cudaMemsetAsync(status, 0, sizeof(unsigned int), st)) != cudaSuccess ||
-            (e = cub::DeviceRadixSort::SortKeys(base + o_tmp, tmp_bytes, d->d_wl + 1, wl, ncand, 0, end_bit, st)) !=
+            (e = cub::DeviceRadixSort::SortKeys(base + o_tmp, tmp_bytes, sc->wl + 1, wl, ncand, 0, end_bit, st)) !=
                 cudaSuccess)
             return cuda_fail(e);
         std::vector<int> counts(nw);
@@ -1406,8 +1466,12 @@ int uwshcu_device_status(void* stream)
     cudaError_t e;
     unsigned int bits = 0;
     if ((e = cudaStreamSynchronize((cudaStream_t)stream)) != cudaSuccess) return cuda_fail(e);
-    if ((e = cudaMemcpy(&bits, d->d_err, sizeof(bits), cudaMemcpyDeviceToHost)) != cudaSuccess) return cuda_fail(e);
-    if ((e = cudaMemset(d->d_err, 0, sizeof(unsigned int))) != cudaSuccess) return cuda_fail(e);
+    StreamCtx* c = nullptr;
+    for (StreamCtx& x : d->sctx)
+        if (x.used && x.stream == (cudaStream_t)stream) c = &x;
+    if (!c) return UWSHCU_OK;   // no device-array call on this stream since the last status
+    if ((e = cudaMemcpy(&bits, c->err, sizeof(bits), cudaMemcpyDeviceToHost)) != cudaSuccess) return cuda_fail(e);
+    if ((e = cudaMemset(c->err, 0, sizeof(unsigned int))) != cudaSuccess) return cuda_fail(e);
     return status_from_bits(bits);
 }
 

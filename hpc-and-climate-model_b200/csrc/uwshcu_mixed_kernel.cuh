@@ -577,6 +577,28 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
     A.cnb[i] = CNT(0.0f);
     }
 
+    // ---- non-finite inputs ---------------------------------------------------------------------
+    // No counterpart in the Fortran, where a NaN or Inf input propagates into the column's outputs
+    // or stops the model in findsp: a column with a non-finite value in any input the scheme reads
+    // takes the exit path (label-333 outputs), is marked UW_X_NONFINITE and sets its own status
+    // bit; it runs neither findsp nor conden, so it raises no endrun condition.
+    bool nonfinite = !isfinite(__ldg(&A.pblh[i])) || !isfinite(A.cush[i]);
+    for (int k = 0; k <= mkx; k++)
+        nonfinite |= !isfinite(GI(ps0, k)) || !isfinite(GI(zs0, k)) || !isfinite(GI(tke, k));
+    for (int k = 1; k <= mkx; k++) {
+        nonfinite |= !isfinite(GL(p0, k)) || !isfinite(GL(z0, k)) || !isfinite(GL(dp0, k)) ||
+                     !isfinite(GL(u0, k)) || !isfinite(GL(v0, k)) || !isfinite(GL(qv0, k)) ||
+                     !isfinite(GL(ql0, k)) || !isfinite(GL(qi0, k)) || !isfinite(GL(t0, k)) ||
+                     !isfinite(GL(s0, k));
+        for (int m = 1; m <= ncnst; m++) nonfinite |= !isfinite(GT(m, k));
+    }
+    if (nonfinite) {
+        xflags |= UW_X_NONFINITE;
+        errbits |= UW_ERRBIT_NONFINITE;
+        id_exit = true;
+        stop = true;
+    }
+
     // ---- inputs and findsp (uwshcu.F90:1216-1259) ----------------------------------------------
     for (int k = 0; k <= mkx; k++) {
         ps0[k] = GI(ps0, k);
@@ -594,7 +616,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
         exn0[k] = powf(p0[k] / p00, rovcp);
         qt0[k] = (qv0[k] + ql0[k] + qi0[k]);
         thl0[k] = (t0[k] - xlv * ql0[k] / cp - xls * qi0[k] / cp) / exn0[k];
-        qw0[k] = findsp_point(qv0[k], t0[k], p0[k], errbits, tbld, tblf);
+        qw0[k] = nonfinite ? 0.0f : findsp_point(qv0[k], t0[k], p0[k], errbits, tbld, tblf);
     }
     cush = A.cush[i];
     {
@@ -611,7 +633,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
         }
     }
     // thv0 at layer bottom/top (:1275-1299)
-    for (int k = 1; k <= mkx; k++) {
+    for (int k = 1; k <= mkx && !nonfinite; k++) {
         R thl0bot = thl0[k] + ssthl0[k] * (ps0[k - 1] - p0[k]);
         R qt0bot = qt0[k] + ssqt0[k] * (ps0[k - 1] - p0[k]);
         if (CONDEN(ps0[k - 1], exns0[k - 1], thl0bot, qt0bot, thj, qvj, qlj, qij, tbld, tblf)) {

@@ -23,6 +23,12 @@ extern "C" {
 #define UWSHCU_ERR_MU_INCONSISTENT 1     /* uwshcu.F90:2119-2122 'Critical error in mu calculation' */
 #define UWSHCU_ERR_FINDSP_NONCONVERGED 2 /* uwshcu.F90:5423-5431 'findsp not converging'           */
 #define UWSHCU_ERR_FINDSP_ENTHALPY 3     /* uwshcu.F90:5435-5447 'enthalpy is not conserved'       */
+#define UWSHCU_WARN_NONFINITE_INPUT 4    /* no counterpart in the reference: a column had a NaN or Inf
+                                            input; it took the exit path (zero tendencies, cush = -1,
+                                            exit bit UWSHCU_EXIT_NONFINITE in diag_int row 0) and
+                                            every other column is computed as usual.  Reported
+                                            when none of 1..3 occurred.                          */
+#define UWSHCU_EXIT_NONFINITE (1 << 11)  /* diag_int row 0 (exit flags): the non-finite-input exit */
 #define UWSHCU_ERR_BAD_ARGS (-1)         /* null pointer or dimension out of range                 */
 #define UWSHCU_ERR_NOT_INITIALIZED (-2)  /* uwshcu_init was not called                             */
 #define UWSHCU_ERR_CUDA (-3)             /* CUDA runtime error (uwshcu_last_cuda_error names it)   */
@@ -198,7 +204,13 @@ int bxcompute_uwshcu_inv_(const int *pcols, const int *pver, const int *ncol, co
  * diag_int (8, mix) and diag_real (8, mix) are optional per-column diagnostics (exit/limit flags,
  * kinv, klcl, klfc, krel, kbup, kpen; cin, cinlcl, plcl, plfc, pinv, pbup, ppen, tkeavg).
  * The endrun conditions of the call are collected on the device; uwshcu_device_status(stream)
- * waits for the stream and returns them. */
+ * waits for the stream and returns them.
+ * Streams: the library keeps a worklist, a hand-off region and an endrun word per caller stream
+ * (up to 32 streams per device; a call on a 33rd stream synchronises the device and takes over the
+ * least recently used stream's set, whose uncollected endrun bits are lost), so calls on different
+ * streams may overlap on the GPU (one stream per host thread).  Calls on one stream run in stream
+ * order.  cudaStreamPerThread is one handle for all host threads: order such calls yourself.
+ * The same holds for uwshcu_compute_member, uwshcu_tangent_device and uwshcu_adjoint_device. */
 int uwshcu_compute_device(int mix, int mkx, int iend, int ncnst, double dt, int inv,
                           const double *ps0, const double *zs0, const double *p0,
                           const double *z0, const double *dp0, const double *u0, const double *v0,
@@ -213,8 +225,10 @@ int uwshcu_compute_device(int mix, int mkx, int iend, int ncnst, double dt, int 
                           double *cnt, double *cnb, const double *dpdry0, double *wu,
                           int *diag_int, double *diag_real, void *stream);
 
-/* Wait for `stream` and return the status collected by the device calls enqueued on it since the
- * previous uwshcu_device_status call. */
+/* Wait for `stream` and return the status collected by the device-array calls enqueued on that
+ * stream (uwshcu_compute_device, uwshcu_compute_member, uwshcu_tangent_device) since the previous
+ * uwshcu_device_status call on it; calls on other streams are not reported and not reset.
+ * (uwshcu_compute_device_noalloc reports through its own status_bits instead.) */
 int uwshcu_device_status(void *stream);
 
 /* ---- batched uneven launches ----------------------------------------------------------------- */
@@ -385,10 +399,14 @@ int uwshcu_adjoint_release(void);
  *     give wrong results: order them on one stream or with events.
  *   - status_bits: NULL, or a device pointer to one unsigned int that the call zeroes on `stream`
  *     and into which the kernels OR the endrun conditions of this call (1 mu inconsistency,
- *     2 findsp non-convergence, 4 findsp enthalpy).  uwshcu_device_status does not see them.
- *   - Launching the kernels can make the CUDA driver enlarge the context's local-memory
- *     reservation for their stack frames the first time; make one call during set-up if that
- *     matters. */
+ *     2 findsp non-convergence, 4 findsp enthalpy, 8 non-finite input).  uwshcu_device_status
+ *     does not see them.
+ *   - The first call on a device can still make the CUDA driver allocate device memory: with lazy
+ *     module loading (CUDA_MODULE_LOADING=LAZY, the default since CUDA 12.2) the library's kernels
+ *     and the array itself are loaded when a call first uses them, and the first launches can
+ *     enlarge the context's local-memory reservation for the kernels' stack frames.  Make one call
+ *     per device during set-up, before the host's memory pool claims the GPU (or run with
+ *     CUDA_MODULE_LOADING=EAGER); later calls allocate nothing. */
 int uwshcu_compute_device_noalloc(int mix, int mkx, int iend, int ncnst, double dt, int inv,
                                   const double *ps0, const double *zs0, const double *p0,
                                   const double *z0, const double *dp0, const double *u0,

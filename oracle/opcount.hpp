@@ -6,7 +6,7 @@
 // Fortran scheme (uwshcu.F90) as the oracle states it, statement by statement:
 //   add  : + and - (binary)          mul : *          div : /          sqrt : sqrt
 //   tr   : exp, log, pow, erfc, log10 (one operation each)
-// Comparisons, min/max, fabs, trunc/floor and conversions are not counted.  One thread only: the
+// Comparisons, min/max, fabs, trunc/floor/rint and conversions are not counted.  One thread only: the
 // counters are thread-local and the driver runs the oracle with nthreads = 1.
 #pragma once
 #include <math.h>
@@ -54,6 +54,7 @@ inline cdouble sqrt(cdouble x) { g_ops.sqrt++; return cdouble(std::sqrt(x.v)); }
 inline cdouble fabs(cdouble x) { return cdouble(std::fabs(x.v)); }
 inline cdouble trunc(cdouble x) { return cdouble(std::trunc(x.v)); }
 inline cdouble floor(cdouble x) { return cdouble(std::floor(x.v)); }
+inline cdouble rint(cdouble x) { return cdouble(std::rint(x.v)); }
 inline cdouble copysign(cdouble x, cdouble y) { return cdouble(std::copysign(x.v, y.v)); }
 inline cdouble fma(cdouble a, cdouble b, cdouble c) { g_ops.mul++; g_ops.add++; return cdouble(std::fma(a.v, b.v, c.v)); }
 inline cdouble frexp(cdouble x, int* e) { return cdouble(std::frexp(x.v, e)); }

@@ -14,6 +14,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATHS = {"glibc": os.path.join(HERE, "_build", "libuwshcu_oracle.so"),
              "portable": os.path.join(HERE, "_build", "libuwshcu_oracle_pm.so"),
+             # glibc exp/log/pow with CALERF erfc: the functions a Fortran build of the scheme calls
+             "fortran": os.path.join(HERE, "_build", "libuwshcu_oracle_ftn.so"),
              # operation-counting build (opcount.hpp): same results as "glibc", plus uwo_opcount
              "ops": os.path.join(HERE, "_build", "libuwshcu_oracle_ops.so")}
 LIB_PATH = LIB_PATHS["glibc"]
@@ -41,8 +43,9 @@ def build():
 
 def set_variant(variant):
     """Select the oracle build: 'glibc' (transcendentals from glibc; pinned bit for bit to the
-    reference's drop-in) or 'portable' (the host/device-identical routines of uw_math.h that the
-    CUDA path uses).  Each build keeps its own constants; the selected one is initialised with the
+    reference's drop-in), 'fortran' (glibc exp/log/pow and CAM's CALERF erfc, the functions a
+    Fortran build of uwshcu.F90 calls) or 'portable' (the host/device-identical routines of
+    uw_math.h that the CUDA path uses).  Each build keeps its own constants; the selected one is initialised with the
     default constants on first use."""
     global _lib, LIB_PATH
     LIB_PATH = LIB_PATHS[variant]

@@ -24,6 +24,9 @@
 #include <stdlib.h>
 #include <string.h>
 #include "uwshcu_oracle.h"
+#ifdef UWO_FORTRAN_MATH
+#define UW_ERFC_EXP exp
+#endif
 #include "uw_math.h"
 #ifdef _OPENMP
 #include <omp.h>
@@ -131,13 +134,24 @@ static void gestbl(double tmn, double tmx, double trice, int ip, double epsil, d
     S.pcf[5] = 0.0;
 }
 
-/* The column physics below calls EXP/LOG/POW/ERFC: glibc by default; with UWO_PORTABLE_MATH the
- * host/device-identical routines of uw_math.h (hpc-and-climate-model_b200/csrc), which is how the
- * CUDA path evaluates them.  The saturation table above always uses glibc, as the library does. */
-#ifdef UWO_PORTABLE_MATH
+/* The column physics below calls EXP/LOG/POW/ERFC:
+ *  - default: glibc for all four, which is what the reference's C++ drop-in
+ *    (bxcompute_uwshcu_inv.cpp) calls when built for the host; this build is pinned to it;
+ *  - UWO_FORTRAN_MATH: glibc exp/log/pow and CALERF erfc (uw_math.h, calling glibc exp), the
+ *    functions a Fortran build of uwshcu.F90 calls: the compiler's libm for exp, log and **, and
+ *    CAM's error_function module (Cody's CALERF) for erfc (uwshcu.F90:5);
+ *  - UWO_PORTABLE_MATH: the host/device-identical routines of uw_math.h
+ *    (hpc-and-climate-model_b200/csrc), which is how the CUDA path evaluates them.
+ * The saturation table above always uses glibc, as the library does. */
+#if defined(UWO_PORTABLE_MATH)
 #define EXP(x) uw_exp(x)
 #define LOG(x) uw_log(x)
 #define POW(x, y) uw_pow(x, y)
+#define ERFC(x) uw_erfc(x)
+#elif defined(UWO_FORTRAN_MATH)
+#define EXP(x) exp(x)
+#define LOG(x) log(x)
+#define POW(x, y) pow(x, y)
 #define ERFC(x) uw_erfc(x)
 #else
 #define EXP(x) exp(x)

@@ -23,12 +23,13 @@ def oracle():
     return o
 
 
-class _Portable:
-    """The oracle build with the host/device-identical math routines the CUDA path uses; every
-    call selects that build and switches back to the glibc build afterwards."""
+class _Variant:
+    """Another build of the oracle (oracle.set_variant): every call selects that build and switches
+    back to the glibc build afterwards."""
 
-    def __init__(self, mod):
+    def __init__(self, mod, variant):
         self.m = mod
+        self.variant = variant
 
     def __getattr__(self, name):
         f = getattr(self.m, name)
@@ -36,7 +37,7 @@ class _Portable:
             return f
 
         def call(*a, **k):
-            self.m.set_variant("portable")
+            self.m.set_variant(self.variant)
             try:
                 return f(*a, **k)
             finally:
@@ -46,7 +47,16 @@ class _Portable:
 
 @pytest.fixture(scope="session")
 def oracle_pm(oracle):
-    p = _Portable(oracle)
+    """The oracle build with the host/device-identical math routines the CUDA path uses."""
+    p = _Variant(oracle, "portable")
+    p.init_default()
+    return p
+
+
+@pytest.fixture(scope="session")
+def oracle_ftn(oracle):
+    """The oracle build with the Fortran's own math: glibc exp/log/pow and CAM's CALERF erfc."""
+    p = _Variant(oracle, "fortran")
     p.init_default()
     return p
 

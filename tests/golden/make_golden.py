@@ -50,7 +50,10 @@ def init_oracle_25():
 
 
 def main():
-    subprocess.run(["make", "-s", "-C", os.path.join(REPO, "oracle", "ref")], check=True)
+    # the reference checkout: UWSHCU_REFERENCE_ROOT, else "reference" beside this repository
+    ref_root = os.environ.get("UWSHCU_REFERENCE_ROOT") or os.path.join(os.path.dirname(REPO), "reference")
+    subprocess.run(["make", "-s", "-C", os.path.join(REPO, "oracle", "ref"), "REF_ROOT=" + ref_root],
+                   check=True)
     qmin, wet = init_oracle_25()
     refdropin.init(oracle.consts(), oracle.estbl(), qmin, wet)
     for name, n, seed, rh in CASES:

@@ -111,3 +111,53 @@ def test_batch_rejects_bad_plans_before_touching_the_device(uw):
     assert L.uwshcu_batch_create(ctypes.c_int(1), m, ctypes.byref(h)) == uw.ERR_BAD_ARGS
     assert L.uwshcu_batch_run(None, None) == uw.ERR_BAD_ARGS
     assert L.uwshcu_batch_destroy(None) == uw.ERR_BAD_ARGS
+
+
+# the batched uneven workload at full size: 4 members of 262,144 columns, 1,048,576 in all
+MEMBERS_FULL = ((262_144, 30, (0.55, 0.757)), (262_144, 35, (0.625, 0.86)),
+                (262_144, 51, (0.662, 0.912)), (262_144, 30, (0.75, 0.97)))
+
+
+def _columns(s, idx):
+    """The columns idx of a sounding dict (columns are independent)."""
+    n = s["ncol"]
+    out = {k: (np.ascontiguousarray(v[..., idx]) if isinstance(v, np.ndarray) and v.shape[-1] == n else v)
+           for k, v in s.items()}
+    out["ncol"] = len(idx)
+    return out
+
+
+@pytest.mark.gpu
+def test_full_size_batch_members_match_the_oracle(uw, oracle, oracle_pm, cuda):
+    """One FP64 run of the 1,048,576-column batch (30/35/51/30 levels, about 5/25/45/60 %
+    convecting); 4,096 sampled columns of every member against the oracle: bit for bit against the
+    build with the kernel's math routines, identical trigger, cloud-base and cloud-top decisions
+    against the glibc build (pinned to the reference)."""
+    import torch
+    from util import FIELDS, decisions
+
+    assert uw.init_default() == 0
+    assert uw.set_precision(uw.PREC_FP64) == 0
+    ss = [soundings.make_soundings(n, pver, seed=100 + j, rh_pbl=rh) for j, (n, pver, rh) in enumerate(MEMBERS_FULL)]
+    cases = [uw.DeviceCase(s) for s in ss]
+    plan = uw.BatchPlan(cases)
+    stream = torch.cuda.Stream()
+    try:
+        assert plan.run(stream) == 0, uw.last_cuda_error()
+        assert plan.status(stream) == 0
+    finally:
+        plan.close()
+    rng = np.random.default_rng(0)
+    for j, (s, case) in enumerate(zip(ss, cases)):
+        idx = np.sort(rng.choice(s["ncol"], 4096, replace=False))
+        it = torch.from_numpy(idx).to(case.out["cush"].device)
+        out = {k: v.index_select(v.dim() - 1, it).cpu().numpy() for k, v in case.out.items()}
+        sub = _columns(s, idx)
+        pm = oracle_pm.compute(sub, diag=False)
+        bad = [f for f in FIELDS if not np.array_equal(out[f], pm[f])]
+        assert not bad, (j, bad)
+        g = oracle.compute(sub, diag=False)
+        for name, x, y in zip(("trigger", "cloud base", "cloud top"), decisions(out), decisions(g)):
+            assert np.array_equal(x, y), (j, name)
+    del cases
+    torch.cuda.empty_cache()

@@ -1,48 +1,98 @@
-"""The two oracle builds: glibc transcendentals (pinned bit for bit to the reference's drop-in)
-and the host/device-identical routines of uw_math.h (which the CUDA path reproduces bit for bit).
+"""The three oracle builds and the math routines the CUDA path uses (uw_math.h).
+
+Builds: 'glibc' (exp/log/pow/erfc from glibc, pinned bit for bit to the reference's C++ drop-in),
+'fortran' (glibc exp/log/pow and CAM's CALERF erfc: the functions a Fortran build of uwshcu.F90
+calls) and 'portable' (uw_math.h: correctly rounded exp/log/pow and CALERF erfc, the routines the
+kernels evaluate bit for bit).
 
 The scheme amplifies last-bit differences of exp/log/pow/erfc (1 - thvj/thv0j times
-2 g cridis / wue^2, sqrt of a near-zero wtw, cancellation in the condensate tendencies), so two
-ulp-accurate libraries cannot agree to 1e-11 on every column.  What must hold: identical trigger,
-cloud-base and cloud-top decisions and identical level indices, and values within 1e-6 (floor:
-1e-9 of each field's maximum) on at least 99.9 % of the columns."""
+2 g cridis / wue^2, sqrt of a near-zero wtw, cancellation in the condensate tendencies).  glibc's
+exp/log/pow round correctly in all but about 1 case in 10^3 and its erfc in about 7 in 10, so:
+portable against fortran differs only where glibc misrounds (>= 98 % of the columns within 1e-11 on
+every output); against glibc the erfc difference adds to that (>= 90 %).  Decisions and level
+indices agree on every column in both comparisons."""
+import math
+
 import numpy as np
 import pytest
 
 import soundings
-from util import conditioned_compare
+from util import compare, conditioned_compare
+
+
+def _frac_within(a, b, tol):
+    _, worst = compare(a, b, tol=tol)
+    return float(np.mean(worst <= tol)), float(np.mean(worst == 0.0))
 
 
 @pytest.mark.parametrize("seed", [3, 4])
-def test_math_variants_differ_only_by_conditioning(oracle, oracle_pm, seed):
+def test_math_variants_differ_only_by_conditioning(oracle, oracle_ftn, oracle_pm, seed):
     s = soundings.make_soundings(6000, 30, seed=seed)
     a = oracle_pm.compute(s, diag=True)
+    f = oracle_ftn.compute(s, diag=True)
     b = oracle.compute(s, diag=True)
-    assert np.array_equal(a["diag_int"][2:], b["diag_int"][2:])
-    assert np.array_equal(a["cnt"], b["cnt"]) and np.array_equal(a["cnb"], b["cnb"])
-    w = conditioned_compare(a, b)
-    assert np.mean(w <= 1e-6) >= 0.999, np.mean(w <= 1e-6)
-    assert np.mean(w <= 1e-11) >= 0.7
+    for ref in (f, b):
+        assert np.array_equal(a["diag_int"][2:], ref["diag_int"][2:])
+        assert np.array_equal(a["cnt"], ref["cnt"]) and np.array_equal(a["cnb"], ref["cnb"])
+        assert np.mean(conditioned_compare(a, ref) <= 1e-6) >= 0.999
+    within, exact = _frac_within(a, f, 1e-11)
+    assert within >= 0.98 and exact >= 0.95, (within, exact)     # measured 0.988-0.990, 0.967-0.971
+    within, _ = _frac_within(a, b, 1e-11)
+    assert within >= 0.90, within                                  # measured 0.922-0.928
 
 
-def test_uw_math_accuracy(oracle):
-    import math
+def test_fortran_build_differs_from_glibc_build_only_in_erfc(oracle, oracle_ftn):
+    """Columns that never evaluate erfc (no closure: they leave the scheme before it) are bit for bit
+    the same in the glibc and the Fortran-math builds."""
+    s = soundings.make_soundings(3000, 30, seed=5)
+    f = oracle_ftn.compute(s, diag=True)
+    b = oracle.compute(s, diag=True)
+    # kinv, klcl, klfc of 0 or an exit before the closure: the trigger pass's early exits
+    early = b["diag_real"][2] == 0.0          # plcl never set
+    assert early.sum() > 100
+    _, worst = compare({k: v[..., early] for k, v in f.items() if isinstance(v, np.ndarray) and v.shape[-1] == 3000},
+                       {k: v[..., early] for k, v in b.items() if isinstance(v, np.ndarray) and v.shape[-1] == 3000})
+    assert np.all(worst == 0.0)
+
+
+def test_uw_math_is_correctly_rounded(oracle):
+    """exp, log and pow of uw_math.h return the double nearest to the exact value (mpmath at 200
+    bits), on the argument ranges of the scheme and beyond, and agree with glibc wherever glibc
+    rounds correctly."""
+    mpmath = pytest.importorskip("mpmath")
+    mpmath.mp.prec = 200
     rng = np.random.default_rng(0)
-
-    def ulps(x, y):
-        return np.abs(np.asarray(x).view(np.int64) - np.asarray(y).view(np.int64))
-    x = rng.uniform(-50, 50, 100000)
-    assert ulps(oracle.uwmath(0, x), np.exp(x)).max() <= 1
-    x = np.exp(rng.uniform(-30, 30, 100000))
-    ok = np.abs(np.log(x)) > 1e-3
-    assert ulps(oracle.uwmath(1, x)[ok], np.log(x)[ok]).max() <= 1
-    # the two pow uses of the scheme: (p/p00)**rovcp and PiLCL**(1/rovcp) (uwshcu.F90:52, :4900)
+    n = 3000
     rovcp = oracle.consts()[9]
-    x = rng.uniform(0.003, 1.05, 100000)
-    assert ulps(oracle.uwmath(2, x, np.full_like(x, rovcp)), x ** rovcp).max() <= 2
-    x = rng.uniform(0.7, 1.0, 100000)
-    assert ulps(oracle.uwmath(2, x, np.full_like(x, 1 / rovcp)), x ** (1 / rovcp)).max() <= 2
-    x = rng.uniform(-2, 6, 20000)
+    cases = [(0, rng.uniform(-700, 700, n), None, mpmath.exp, math.exp),
+             (0, rng.uniform(-20, 2, n), None, mpmath.exp, math.exp),
+             (0, rng.uniform(-1e-6, 1e-6, n), None, mpmath.exp, math.exp),
+             (1, np.exp(rng.uniform(-700, 700, n)), None, mpmath.log, math.log),
+             (1, 1.0 + rng.uniform(-0.02, 0.02, n), None, mpmath.log, math.log),
+             # the two pow uses of the scheme: (p/p00)**rovcp and PiLCL**(1/rovcp) (uwshcu.F90:52, :4900)
+             (2, rng.uniform(0.002, 1.05, n), np.full(n, rovcp), mpmath.power, math.pow),
+             (2, rng.uniform(0.5, 1.0, n), np.full(n, 1.0 / rovcp), mpmath.power, math.pow),
+             (2, rng.uniform(0.01, 2.0, n), rng.uniform(-4, 4, n), mpmath.power, math.pow)]
+    for fn, x, y, fm, fg in cases:
+        got = oracle.uwmath(fn, x, y)
+        if y is None:
+            exact = np.array([float(fm(mpmath.mpf(float(v)))) for v in x])
+            glibc = np.array([fg(v) for v in x])
+        else:
+            exact = np.array([float(fm(mpmath.mpf(float(u)), mpmath.mpf(float(v)))) for u, v in zip(x, y)])
+            glibc = np.array([fg(u, v) for u, v in zip(x, y)])
+        assert np.array_equal(got, exact), (fn, int(np.sum(got != exact)))
+        assert np.mean(got == glibc) >= 0.995, fn
+    # special values
+    assert oracle.uwmath(0, np.array([0.0]))[0] == 1.0
+    assert oracle.uwmath(1, np.array([1.0]))[0] == 0.0
+    assert oracle.uwmath(2, np.array([1.0]), np.array([rovcp]))[0] == 1.0
+    assert np.isinf(oracle.uwmath(0, np.array([710.0]))[0])
+    assert oracle.uwmath(0, np.array([-746.0]))[0] == 0.0
+
+
+def test_calerf_accuracy(oracle):
+    x = np.random.default_rng(1).uniform(-2, 6, 20000)
     ref = np.array([math.erfc(v) for v in x])
     assert np.max(np.abs(oracle.uwmath(3, x) - ref) / ref) < 2e-15
 

@@ -2,7 +2,8 @@
 
 The GPU test calls the new entry point twice in a row through the C ABI and checks both results
 against uwshcu_compute_device on the same inputs, with the parity tolerance of the other device
-tests (column error <= 1e-11, identical cloud-top/base decisions).  The CPU test checks the size
+tests (column error <= 1e-11, identical cloud-top/base decisions), and that the second call leaves
+the device's free memory unchanged.  The CPU test checks the size
 limit, which is rejected before any CUDA call."""
 import ctypes
 
@@ -56,9 +57,14 @@ def test_noalloc_matches_device_entry_on_two_calls(uw, cuda):
             case.diag_int.fill_(-7)
             case.diag_real.fill_(-777.0)
             bits.fill_(0x7FFF)
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
         case.reset_cush()
         assert case.launch_noalloc(status_bits=bits) == 0, uw.last_cuda_error()
         torch.cuda.synchronize()
+        if call == 1:
+            # after the first call on the device, a call allocates no device memory
+            assert torch.cuda.mem_get_info()[0] == free_before
         out = case.outputs_numpy()
         assert int(bits.item()) == 0, "endrun bits %#x on call %d" % (int(bits.item()), call)
         for f in ("cnt", "cnb"):
