@@ -21,8 +21,10 @@ def test_overlapping_calls_on_two_streams(uw, cuda):
     for sched in (uw.SCHED_SORTED, uw.SCHED_TWO_PHASE):
         assert uw.set_schedule(sched) == 0
         try:
+            a.reset_cush()
             assert a.launch() == 0 and a.status() == 0
             ra = {k: v.clone() for k, v in a.out.items()}
+            b.reset_cush()
             assert b.launch() == 0 and b.status() == WARN_NONFINITE
             rb = {k: v.clone() for k, v in b.out.items()}
             s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
