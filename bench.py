@@ -14,7 +14,8 @@ call over all columns.  Metric: columns per second.
           device->host copy of its outputs.
   mixed : the mixed-precision path on the same columns: columns/s, speed-up over FP64, relative
           RMS error of column heating, moistening and precipitation against the FP64 path (which is
-          the FP64 oracle bit for bit), and the columns whose decisions change.
+          the FP64 oracle bit for bit), and the columns whose decisions change; fast: the same for
+          the fast-FP64 mode.
   adjoint: the adjoint model against the forward pass on 65,536 x 30 columns (cost ratio, tape).
   parity: the FP64 path on the 259,200 x 30 grid (720 x 360) against the oracle builds: decision
           agreement and the fraction of columns within 1e-11 on every output.
@@ -50,13 +51,15 @@ G = 9.80616
 
 
 # From the ncu capture of the worklist pass on the 65,536-column case of this workload (29,956
-# worklist columns; summary in profiles/uwshcu_fp64_kernel_bench65k.txt): DRAM bytes read + written
-# per worklist column by its two launches (UW_MODE_LIST1 7.362 GB + UW_MODE_RESUME 3.868 GB), and
-# FP64 operations executed per worklist column (2 x DFMA + DADD + DMUL thread instructions per
-# cycle x cycles of each launch: 731.26 x 17,665,035 + 559.94 x 14,018,129; the Newton steps of the
-# IEEE divisions included).  Both scale with the columns a launch processes.
-NCU_DRAM_BYTES_PER_LIST_COLUMN = 11.2301e9 / 29_956
-NCU_FP64_OPS_PER_LIST_COLUMN = (731.26 * 17_665_035 + 559.94 * 14_018_129) / 29_956
+# worklist columns; summary in profiles/uwshcu_fp64_kernel_bench65k.txt, correctly rounded math,
+# non-finite check fused into the loads): DRAM bytes read + written per worklist column by its two
+# launches (UW_MODE_LIST1 7.420 GB + UW_MODE_RESUME 3.876 GB), and FP64 operations executed per
+# worklist column (2 x DFMA + DADD + DMUL thread instructions per cycle x cycles of each launch:
+# 707.70 x 17,051,704 + 561.79 x 14,282,396; the Newton steps of the IEEE divisions included).  Both
+# scale with the columns a launch processes.  Constants of one capture: a change to the column code
+# needs a new capture (the command is in the summary).
+NCU_DRAM_BYTES_PER_LIST_COLUMN = 11.295961e9 / 29_956
+NCU_FP64_OPS_PER_LIST_COLUMN = (707.70 * 17_051_704 + 561.79 * 14_282_396) / 29_956
 FP64_DFMA_PER_CYCLE = 9472    # ncu sm__sass_thread_inst_executed_op_dfma_pred_on.sum.peak_sustained
 # Algorithmic FP64 operations per convecting / other column of each workload, counted by the
 # oracle's operation-counting build (written by oracle/opcount.py; a data file, read as text).
@@ -300,19 +303,23 @@ def column_quantities_dev(case):
             "trigger": o["cush"] != -1.0}
 
 
-def mixed_leg(uw, case, stream, steps, warmup, fp64_ms):
-    """The mixed-precision path on the columns of `case`, whose outputs hold the FP64 path's: speed
-    and the error of column heating, moistening and precipitation against FP64."""
+def precision_leg(uw, case, stream, steps, warmup, fp64_ms, mode):
+    """A reduced-precision mode (uw.PREC_MIXED or uw.PREC_FAST) on the columns of `case`, whose
+    outputs hold the FP64 path's: speed and the error of column heating, moistening and
+    precipitation against FP64.  Every device operation runs on `stream`, in order.  Leaves the
+    FP64 outputs in `case` again."""
     import torch
-    ref = column_quantities_dev(case)
-    assert uw.set_precision(uw.PREC_MIXED) == 0
-    try:
-        def step():
-            case.out["cush"].copy_(case.cush0, non_blocking=True)
-            rc = case.launch(stream=stream)
-            if rc != 0:
-                raise RuntimeError("mixed: %d %s" % (rc, uw.last_cuda_error()))
-        with torch.cuda.stream(stream):
+
+    def step():
+        case.out["cush"].copy_(case.cush0, non_blocking=True)
+        rc = case.launch(stream=stream)
+        if rc != 0:
+            raise RuntimeError("precision %d: %d %s" % (mode, rc, uw.last_cuda_error()))
+
+    with torch.cuda.stream(stream):
+        ref = column_quantities_dev(case)
+        assert uw.set_precision(mode) == 0
+        try:
             for _ in range(warmup):
                 step()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -320,23 +327,29 @@ def mixed_leg(uw, case, stream, steps, warmup, fp64_ms):
             for _ in range(steps):
                 step()
             e1.record(stream)
-        e1.synchronize()
+            q = column_quantities_dev(case)
+        finally:
+            assert uw.set_precision(uw.PREC_FP64) == 0
+            step()                       # the FP64 outputs again, after q is taken
+        stream.synchronize()
         ms = e0.elapsed_time(e1) / steps
-        q = column_quantities_dev(case)
-    finally:
-        assert uw.set_precision(uw.PREC_FP64) == 0
-    err = {}
-    for k in ("heating", "moistening", "precipitation"):
-        a, b = q[k].double(), ref[k].double()
-        err[k] = float(torch.sqrt(torch.mean((a - b) ** 2)) / torch.sqrt(torch.mean(b ** 2)))
+        err, err_kept = {}, {}
+        # the columns whose trigger, cloud-base and cloud-top decisions are the FP64 path's
+        kept = (q["trigger"] == ref["trigger"]) & (q["cnb"] == ref["cnb"]) & (q["cnt"] == ref["cnt"])
+        for k in ("heating", "moistening", "precipitation"):
+            a, b = q[k].double(), ref[k].double()
+            err[k] = float(torch.sqrt(torch.mean((a - b) ** 2)) / torch.sqrt(torch.mean(b ** 2)))
+            err_kept[k] = float(torch.sqrt(torch.mean((a[kept] - b[kept]) ** 2)) / torch.sqrt(torch.mean(b[kept] ** 2)))
+        flips = {"trigger": int((q["trigger"] != ref["trigger"]).sum()),
+                 "cloud_base": int((q["cnb"] != ref["cnb"]).sum()),
+                 "cloud_top": int((q["cnt"] != ref["cnt"]).sum()),
+                 "convecting_columns": int(ref["trigger"].sum())}
+        same = float(kept.double().mean())
     n = case.n
     return {"value": n / (ms * 1e-3), "unit": "columns/s", "ms_per_step": ms,
             "speedup_vs_fp64": fp64_ms / ms, "column_rel_rms_vs_fp64": err,
-            "flips": {"trigger": int((q["trigger"] != ref["trigger"]).sum()),
-                      "cloud_base": int((q["cnb"] != ref["cnb"]).sum()),
-                      "cloud_top": int((q["cnt"] != ref["cnt"]).sum()),
-                      "convecting_columns": int(ref["trigger"].sum())},
-            "targets": "north_star: >= 2x the FP64 path at <= 1e-4 relative RMS"}
+            "column_rel_rms_vs_fp64_same_decisions": err_kept, "columns_with_same_decisions": same,
+            "flips": flips, "targets": "north_star (mixed): >= 2x the FP64 path at <= 1e-4 relative RMS"}
 
 
 def adjoint_leg(uw, steps, warmup, n=65_536):
@@ -762,9 +775,10 @@ def main():
                "field_rel_rms_max": max(v["rel_rms"] for v in rep["fields"].values())}
 
     extras = rank == 0 and world == 1 and not args.no_extras and prec == uw.PREC_FP64
-    mixed = adjoint = None
+    mixed = fast = adjoint = None
     if extras:
-        mixed = mixed_leg(uw, case, stream, args.steps, max(args.warmup, 3), ms)
+        mixed = precision_leg(uw, case, stream, args.steps, max(args.warmup, 3), ms, uw.PREC_MIXED)
+        fast = precision_leg(uw, case, stream, args.steps, max(args.warmup, 3), ms, uw.PREC_FAST)
     if extras or (rank == 0 and world == 1 and not args.no_cpu_baseline):
         # free the large workload before the grid run, the adjoint buffer and the oracle
         del case
@@ -841,6 +855,8 @@ def main():
         line["clocks"] = clk.summary()
     if mixed is not None:
         line["mixed"] = mixed
+    if fast is not None:
+        line["fast"] = fast
     if adjoint is not None:
         line["adjoint"] = adjoint
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -147,6 +147,7 @@ __device__ __forceinline__ Ad uw_div_by(Ad a, Ad b, Ad y)
     const double q = uw_div_by(a.v, b.v, y.v);
     return ad_rec(q, a.i, 1.0 / b.v, b.i, -q / b.v);
 }
+__device__ __forceinline__ bool uw_isfinite(const Ad& x) { return isfinite(x.v); }
 __device__ __forceinline__ Ad uw_exp(Ad x)
 {
     const double e = uw_exp(x.v);

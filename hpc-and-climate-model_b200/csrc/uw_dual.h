@@ -53,6 +53,7 @@ TL_HD Tl uw_div_by(Tl a, Tl b, Tl y)
     const double q = uw_div_by(a.v, b.v, y.v);
     return Tl(q, (a.d - q * b.d) / b.v);
 }
+TL_HD bool uw_isfinite(const Tl& x) { return isfinite(x.v); }
 TL_HD Tl uw_exp(Tl x)
 {
     const double e = uw_exp(x.v);

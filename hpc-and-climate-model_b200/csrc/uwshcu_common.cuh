@@ -75,6 +75,13 @@
 #define UW_L_REI (1 << 8)
 #define UW_L_DELCIN (1 << 9)
 
+// isfinite for the value types of the column code (double, float; the tangent-linear and adjoint
+// value types add their own overloads).
+#if defined(__CUDACC__)
+__host__ __device__ inline bool uw_isfinite(double x) { return isfinite(x); }
+__host__ __device__ inline bool uw_isfinite(float x) { return isfinite(x); }
+#endif
+
 // Device error word bits (set with atomicOr, read back by the host and mapped to status codes).
 #define UW_ERRBIT_MU 1        // 'Critical error in mu calculation' (uwshcu.F90:2119-2122)
 #define UW_ERRBIT_FINDSP 2    // findsp did not converge (uwshcu.F90:5423-5431)

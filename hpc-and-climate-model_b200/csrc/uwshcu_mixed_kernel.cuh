@@ -577,32 +577,17 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
     A.cnb[i] = CNT(0.0f);
     }
 
-    // ---- non-finite inputs ---------------------------------------------------------------------
-    // No counterpart in the Fortran, where a NaN or Inf input propagates into the column's outputs
-    // or stops the model in findsp: a column with a non-finite value in any input the scheme reads
-    // takes the exit path (label-333 outputs), is marked UW_X_NONFINITE and sets its own status
-    // bit; it runs neither findsp nor conden, so it raises no endrun condition.
-    bool nonfinite = !isfinite(__ldg(&A.pblh[i])) || !isfinite(A.cush[i]);
-    for (int k = 0; k <= mkx; k++)
-        nonfinite |= !isfinite(GI(ps0, k)) || !isfinite(GI(zs0, k)) || !isfinite(GI(tke, k));
-    for (int k = 1; k <= mkx; k++) {
-        nonfinite |= !isfinite(GL(p0, k)) || !isfinite(GL(z0, k)) || !isfinite(GL(dp0, k)) ||
-                     !isfinite(GL(u0, k)) || !isfinite(GL(v0, k)) || !isfinite(GL(qv0, k)) ||
-                     !isfinite(GL(ql0, k)) || !isfinite(GL(qi0, k)) || !isfinite(GL(t0, k)) ||
-                     !isfinite(GL(s0, k));
-        for (int m = 1; m <= ncnst; m++) nonfinite |= !isfinite(GT(m, k));
-    }
-    if (nonfinite) {
-        xflags |= UW_X_NONFINITE;
-        errbits |= UW_ERRBIT_NONFINITE;
-        id_exit = true;
-        stop = true;
-    }
-
-    // ---- inputs and findsp (uwshcu.F90:1216-1259) ----------------------------------------------
+    // ---- inputs and findsp (uwshcu.F90:1216-1259), and non-finite inputs ----------------------
+    // Non-finite inputs have no counterpart in the Fortran, where a NaN or Inf propagates into the
+    // column's outputs or stops the model in findsp: a column with a non-finite value in any input
+    // the scheme reads takes the exit path (label-333 outputs), is marked UW_X_NONFINITE and sets
+    // only that status bit (no findsp at or above the bad level, no conden).  The values are checked
+    // as they are loaded; z0 and tke, which the scheme reads later and only at some levels, once here.
+    bool nonfinite = !uw_isfinite(pblh) || !uw_isfinite(A.cush[i]);
     for (int k = 0; k <= mkx; k++) {
         ps0[k] = GI(ps0, k);
         zs0[k] = GI(zs0, k);
+        nonfinite |= !uw_isfinite(ps0[k]) || !uw_isfinite(zs0[k]) || !uw_isfinite(GI(tke, k));
         exns0[k] = powf(ps0[k] / p00, rovcp);
     }
     for (int k = 1; k <= mkx; k++) {
@@ -613,6 +598,8 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
         qi0[k] = GL(qi0, k);
         t0[k] = GL(t0, k);
         s0[k] = GL(s0, k);
+        nonfinite |= !uw_isfinite(p0[k]) || !uw_isfinite(dp0[k]) || !uw_isfinite(qv0[k]) || !uw_isfinite(ql0[k]) ||
+                     !uw_isfinite(qi0[k]) || !uw_isfinite(t0[k]) || !uw_isfinite(s0[k]) || !uw_isfinite(GL(z0, k));
         exn0[k] = powf(p0[k] / p00, rovcp);
         qt0[k] = (qv0[k] + ql0[k] + qi0[k]);
         thl0[k] = (t0[k] - xlv * ql0[k] / cp - xls * qi0[k] / cp) / exn0[k];
@@ -623,14 +610,29 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
         R tmpf[KP];
         slope<KP>(mkx, thl0, p0, ssthl0);
         slope<KP>(mkx, qt0, p0, ssqt0);
-        for (int k = 1; k <= mkx; k++) tmpf[k] = GL(u0, k);
+        for (int k = 1; k <= mkx; k++) {
+            tmpf[k] = GL(u0, k);
+            nonfinite |= !uw_isfinite(tmpf[k]);
+        }
         slope<KP>(mkx, tmpf, p0, ssu0);
-        for (int k = 1; k <= mkx; k++) tmpf[k] = GL(v0, k);
+        for (int k = 1; k <= mkx; k++) {
+            tmpf[k] = GL(v0, k);
+            nonfinite |= !uw_isfinite(tmpf[k]);
+        }
         slope<KP>(mkx, tmpf, p0, ssv0);
         for (int m = 1; m <= ncnst; m++) {
-            for (int k = 1; k <= mkx; k++) tmpf[k] = GT(m, k);
+            for (int k = 1; k <= mkx; k++) {
+                tmpf[k] = GT(m, k);
+                nonfinite |= !uw_isfinite(tmpf[k]);
+            }
             slope<KP>(mkx, tmpf, p0, sstr0[m - 1]);
         }
+    }
+    if (nonfinite) {
+        xflags |= UW_X_NONFINITE;
+        errbits = UW_ERRBIT_NONFINITE;   // findsp of the levels below the bad one reports nothing
+        id_exit = true;
+        stop = true;
     }
     // thv0 at layer bottom/top (:1275-1299)
     for (int k = 1; k <= mkx && !nonfinite; k++) {

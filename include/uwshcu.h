@@ -113,8 +113,10 @@ int uwshcu_profile_read(int *calls, double *trigger_ms, double *list_ms, int *li
 /* Host-array entries (compute_uwshcu_, compute_uwshcu_inv_, bxcompute_uwshcu_inv_): split a call
  * into chunks of chunk_columns columns (0: one chunk) pipelined over `streams` CUDA streams (1..8)
  * of decreasing priority, so that copies in and out and the host-side packing overlap the
- * computation.  Results do not depend on it.  Default: 32768 columns, 4 streams (259,200 columns:
- * 87 ms per call against 157 ms as one chunk; more concurrent chunks compute slower). */
+ * computation.  Results do not depend on it.  Default (and chunk_columns = -1, streams ignored):
+ * the shape follows each call's size, chunks of iend/8 columns rounded up to 1,024 and clamped to
+ * 32,768 .. 262,144, over 4 streams up to 65,536-column chunks and 2 streams above (page-locked
+ * arrays: 259,200 columns in ~75 ms, 1,048,576 in ~220 ms against 272 ms with 32,768 x 4). */
 int uwshcu_set_pipeline(int chunk_columns, int streams);
 
 /* Threads per block of the column kernel (0 = built-in default). */

@@ -153,7 +153,7 @@ def test_pipelined_host_entries_match_one_chunk(uw, cuda):
                 bad = [k for k in o0 if not np.array_equal(o[k], o0[k])]
                 assert not bad, (entry, chunk, streams, bad)
     finally:
-        assert uw.set_pipeline(32768, 4) == 0
+        assert uw.set_pipeline(-1, 0) == 0
 
 
 @pytest.mark.gpu
@@ -200,4 +200,4 @@ def test_page_locked_host_arrays_match_pageable(uw, cuda):
                 bad = [k for k in o0 if not np.array_equal(o[k], o0[k])]
                 assert not bad, (entry, chunk, streams, bad)
     finally:
-        assert uw.set_pipeline(32768, 4) == 0
+        assert uw.set_pipeline(-1, 0) == 0

@@ -37,19 +37,21 @@ def test_fast_fp64_mode_within_precision_bar(uw, cuda):
 
 @pytest.mark.gpu
 def test_mixed_mode_error_is_what_is_stated(uw, cuda):
-    """FP32 bulk with FP64 islands.  Measured on the 259,200-column benchmark workload: column
-    heating / moistening / precipitation relative RMS 8.8e-3 / 8.2e-3 / 9.3e-3, 624 of 104,752
-    convecting columns with another cloud top, 7 trigger flips.  The buoyancy chain in FP32 moves
-    cloud tops across level boundaries, which is an O(1) change for that column; the bar of 1e-4
-    is out of reach for this precision map and the test pins the stated error instead."""
+    """FP32 bulk with FP64 islands.  Measured on the 1,048,576-column benchmark workload: column
+    heating / moistening / precipitation relative RMS 9.2e-3 / 8.5e-3 / 9.4e-3, 2,583 of 423,288
+    convecting columns with another cloud top (0.6 %), 48 trigger flips.  The buoyancy chain in FP32
+    moves cloud tops across level boundaries, which is an O(1) change for that column; the bar of
+    1e-4 is out of reach for this precision map and the test pins the measured error (with the
+    spread of a 16,384-column sample) instead."""
     assert uw.init_default() == 0
     s = soundings.make_soundings(16384, 30, seed=71, rh_pbl=(0.675, 0.93))
     st64, ref = _run(uw, s, uw.PREC_FP64)
     stm, out = _run(uw, s, uw.PREC_MIXED)
     assert st64 == 0 and stm == 0
     rep = errstats.report(out, ref, s["dp0"])
+    print("mixed, 16,384 columns:", {k: v["rel_rms"] for k, v in rep["column"].items()}, rep["flips"])
     for k, v in rep["column"].items():
-        assert v["rel_rms"] <= 3e-2, (k, v)
+        assert v["rel_rms"] <= 1.5e-2, (k, v)
     flips = rep["flips"]
-    assert flips["cloud_top"] <= 0.02 * flips["convecting_columns"], flips
+    assert flips["cloud_top"] <= 0.01 * flips["convecting_columns"], flips
     assert flips["trigger"] <= 1e-3 * rep["columns"], flips

@@ -77,7 +77,7 @@ def test_host_entries_sorted_match_two_phase(uw, cuda):
                 assert not _diff(o0, o), (entry, chunk, streams, slots, _diff(o0, o))
     finally:
         _settings(uw, uw.SCHED_DEFAULT, 0)
-        assert uw.set_pipeline(32768, 4) == 0
+        assert uw.set_pipeline(-1, 0) == 0
 
 
 def test_sorted_schedule_matches_oracle(uw, oracle_pm, cuda):
