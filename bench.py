@@ -17,6 +17,7 @@ call over all columns.  Metric: columns per second.
           the FP64 oracle bit for bit), and the columns whose decisions change; fast: the same for
           the fast-FP64 mode.
   adjoint: the adjoint model against the forward pass on 65,536 x 30 columns (cost ratio, tape).
+  batched: the batched uneven workload (4 x 262,144 columns, 30/35/51/30 levels) as one plan.
   parity: the FP64 path on the 259,200 x 30 grid (720 x 360) against the oracle builds: decision
           agreement and the fraction of columns within 1e-11 on every output.
   --impl reference : the reference algorithm's CPU implementation (the C restatement in
@@ -404,6 +405,53 @@ BATCH_MEMBERS = ((262_144, 30, (0.55, 0.757)), (262_144, 35, (0.625, 0.86)),
                  (262_144, 51, (0.662, 0.912)), (262_144, 30, (0.75, 0.97)))
 
 
+def batched_leg(uw, steps, warmup):
+    """The batched uneven workload in FP64 (4 members of 262,144 columns, 30/35/51/30 levels, ~5/25/
+    45/60 % convecting): one plan, autotuned launch shape, replays of its captured CUDA graph; every
+    device operation on one stream."""
+    import torch
+    import soundings
+    cases = []
+    for j, (n, pver, rh) in enumerate(BATCH_MEMBERS):
+        s = soundings.make_soundings(n, pver, seed=100 + j, rh_pbl=rh)
+        cases.append(uw.DeviceCase(s))
+        del s
+    stream = torch.cuda.Stream()
+    plan = uw.BatchPlan(cases)
+    try:
+        tuned = plan.autotune(stream)
+        assert plan.capture(stream) == 0, uw.last_cuda_error()
+
+        def step():
+            for c in cases:
+                c.out["cush"].copy_(c.cush0, non_blocking=True)
+            rc = plan.run(stream)
+            if rc != 0:
+                raise RuntimeError("uwshcu_batch_run: %d %s" % (rc, uw.last_cuda_error()))
+
+        with torch.cuda.stream(stream):
+            for _ in range(warmup):
+                step()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                step()
+            e1.record(stream)
+            trig = [float((c.out["cush"] != -1.0).double().mean()) for c in cases]
+        e1.synchronize()
+        st = plan.status(stream)
+    finally:
+        plan.close()
+    ms = e0.elapsed_time(e1) / steps
+    ncol = sum(m[0] for m in BATCH_MEMBERS)
+    del cases
+    torch.cuda.empty_cache()
+    return {"value": ncol / (ms * 1e-3), "unit": "columns/s", "ms_per_step": ms, "steps": steps,
+            "workload": "4 members x 262,144 columns, pver 30/35/51/30, FP64, sorted schedule",
+            "trigger_fraction": trig, "status": st,
+            "launch": "CUDA graph replay; autotuned block %d, %d column(s) per lane per task" % (tuned[0], tuned[2])}
+
+
 def run_batched(args):
     """One step = one replay of the captured batch plan over all members, inputs resident in HBM:
     per level class a trigger launch and the worklist pass (sorted schedule, the default: a
@@ -634,7 +682,8 @@ def main():
     ap.add_argument("--ncol", type=int, default=NCOL)
     ap.add_argument("--columns", type=int, default=65536,
                     help="columns of the tangent and adjoint cost configs (65,536 by default)")
-    ap.add_argument("--cpu-sample", type=int, default=65536)
+    ap.add_argument("--cpu-sample", type=int, default=262144,
+                    help="columns of the workload the reference arm computes per step")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the mixed-precision, adjoint and parity legs of the default run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -745,14 +794,17 @@ def main():
         sp = {k: pinned(v) if isinstance(v, np.ndarray) else v for k, v in s.items()}
         outp = {k: pinned(v) for k, v in uw.alloc_outputs(PVER, NCNST, n, s["cush"]).items()}
         sec, rc = host_steps(sp, outp)
-        sec_pg, rc_pg = host_steps(s, uw.alloc_outputs(PVER, NCNST, n, s["cush"]))
         e2e = {"value": job_throughput(world, n, sec), "unit": "columns/s",
                "h2d_bytes_per_step": int(n * (nbytes_in + 8 * PVER)),
                "d2h_bytes_per_step": int(n * nbytes_out), "ms_per_step": sec * 1e3,
-               "host_memory": "page-locked caller arrays (torch pin_memory)", "status": int(rc),
-               "pageable": {"value": job_throughput(world, n, sec_pg), "ms_per_step": sec_pg * 1e3,
-                            "status": int(rc_pg),
-                            "host_memory": "pageable numpy arrays, packed through pinned staging"}}
+               "host_memory": "page-locked caller arrays (torch pin_memory)", "status": int(rc)}
+        if world == 1:
+            # pageable arrays too (one GPU only: eight ranks' extra host copies would not fit the
+            # host's memory beside their page-locked ones)
+            sec_pg, rc_pg = host_steps(s, uw.alloc_outputs(PVER, NCNST, n, s["cush"]))
+            e2e["pageable"] = {"value": job_throughput(world, n, sec_pg), "ms_per_step": sec_pg * 1e3,
+                               "status": int(rc_pg),
+                               "host_memory": "pageable numpy arrays, packed through pinned staging"}
         del keep
 
     # column energy and water budgets of the last step (CAM's check_energy_chng thresholds)
@@ -775,7 +827,7 @@ def main():
                "field_rel_rms_max": max(v["rel_rms"] for v in rep["fields"].values())}
 
     extras = rank == 0 and world == 1 and not args.no_extras and prec == uw.PREC_FP64
-    mixed = fast = adjoint = None
+    mixed = fast = adjoint = batched = None
     if extras:
         mixed = precision_leg(uw, case, stream, args.steps, max(args.warmup, 3), ms, uw.PREC_MIXED)
         fast = precision_leg(uw, case, stream, args.steps, max(args.warmup, 3), ms, uw.PREC_FAST)
@@ -783,9 +835,11 @@ def main():
         # free the large workload before the grid run, the adjoint buffer and the oracle
         del case
         torch.cuda.empty_cache()
-        grid_s, grid_out, grid_rc, grid_st = grid_case(uw)
         if extras:
+            # the adjoint first: its tape buffer takes most of the free device memory
             adjoint = adjoint_leg(uw, args.steps, max(args.warmup, 3))
+            batched = batched_leg(uw, args.steps, max(args.warmup, 3))
+        grid_s, grid_out, grid_rc, grid_st = grid_case(uw)
 
     peak, peak_kind = peaks()
     ncols_dom = phases["worklist_columns"] if phases else n
@@ -859,6 +913,8 @@ def main():
         line["fast"] = fast
     if adjoint is not None:
         line["adjoint"] = adjoint
+    if batched is not None:
+        line["batched"] = batched
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base, parity = cpu_baseline_leg(grid_s, grid_out)
         parity["gpu_status"] = [int(grid_rc), int(grid_st)]
