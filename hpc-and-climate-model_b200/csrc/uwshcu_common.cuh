@@ -94,6 +94,11 @@ struct UwConst {
     double xlv, xlf, xls, cp, zvir, r, g, ep2, p00, rovcp, rpen;
     double rle, rkm, criqc;   // compute_uwshcu parameters (uwshcu.F90:1036, 1038, 1065)
     double rinv;              // 1 / r, correctly rounded (divisions by r in conden)
+    // compute_zwshcu options (zwshcu.F90:30-59, cloud_fraction.F90:52), in force for calls that pass
+    // omega: zmh_shallow_lf, zmh_shallow_ent, zmh_cloud_sh, zmh_shallow_fwcrit, zmh_ent0, zmh_ufrcd,
+    // zmh_ufrc0, zmh_ufrcz
+    int zw_lf, zw_ent, zw_cloud_sh;
+    double zw_fwcrit, zw_ent0, zw_ufrcd, zw_ufrc0, zw_ufrcz;
     // wv_saturation module (wv_saturation.F90:48-59)
     double tmin, tmax, ttrice, epsqs, rgasv, hlatf, hlatv, cpws, tmelt;
     double pcf[6];
@@ -154,6 +159,7 @@ struct UwArgs {
     int *diag_int;       // optional (UW_NDI, mix)
     double *diag_real;   // optional (UW_NDR, mix)
     double *diag_level;  // optional (UW_NDL, mkx + 1, mix)
+    const double *omega; // (mix, mkx) pressure velocity: compute_zwshcu; nullptr: compute_uwshcu
     unsigned int *err;   // device error word
     const UwHand *hand;  // UW_MODE_LIST1 / UW_MODE_RESUME only: device copy of the hand-off region
 };

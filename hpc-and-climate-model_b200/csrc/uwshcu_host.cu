@@ -553,7 +553,8 @@ bool bad_dims(int mix, int mkx, int iend, int ncnst)
            ncnst > UWSHCU_MAX_TRACERS || ncnst != S().k.ncnst;
 }
 
-// Host-pointer call shared by compute_uwshcu_ (inv = 0) and compute_uwshcu_inv_ (inv = 1).
+// Host-pointer call shared by compute_uwshcu_ (inv = 0) and compute_uwshcu_inv_ (inv = 1), and by
+// the compute_zwshcu entries (omega: the pressure velocity (mix, mkx) in the call's level order).
 // Column arrays use leading dimension mix on the host and n = iend on the device.
 int host_call(int inv, int mix, int mkx, int iend, int ncnst, double dt, const double* ps0,
               const double* zs0, const double* p0, const double* z0, const double* dp0,
@@ -564,7 +565,8 @@ int host_call(int inv, int mix, int mkx, int iend, int ncnst, double dt, const d
               double* qiten, double* sten, double* uten, double* vten, double* trten,
               double* qrten, double* qsten, double* precip, double* snow, double* evapc,
               double* cufrc, double* qcu, double* qlu, double* qiu, double* cbmf, double* qc,
-              double* rliq, double* cnt, double* cnb, const double* dpdry0, double* wu)
+              double* rliq, double* cnt, double* cnb, const double* dpdry0, double* wu,
+              const double* omega)
 {
     State& s = S();
     std::lock_guard<std::mutex> lock(s.mu);
@@ -589,7 +591,7 @@ int host_call(int inv, int mix, int mkx, int iend, int ncnst, double dt, const d
     // pipe[c % pipe_streams] once its inputs are in, and the copy-out stream takes its outputs once
     // it is computed.  The host packs chunk c+1 while the GPU works on chunk c and unpacks the
     // chunks in order as they arrive.  Each chunk has its own worklist and endrun word.
-    const size_t per_in = 3 * KI + 11 * KL + KT + 2;     // doubles per column, input block
+    const size_t per_in = 3 * KI + 11 * KL + KT + 2 + (omega ? KL : 0);   // doubles per column, input block
     const size_t per_out = 6 * KI + 14 * KL + KT + 7;    // doubles per column, output block
     // Default shape: chunks of n/8 columns (32,768 .. 262,144, a multiple of 1,024), 4 streams up to
     // 65,536-column chunks and 2 above: enough convecting columns in flight to fill the GPU (a
@@ -619,6 +621,7 @@ int host_call(int inv, int mix, int mkx, int iend, int ncnst, double dt, const d
         static_assert(sizeof(arrays) / sizeof(arrays[0]) == sizeof(rows) / sizeof(rows[0]), "one row count per array");
         for (size_t a = 0; a < sizeof(rows) / sizeof(rows[0]) && direct; a++)
             direct = pinned_range(arrays[a], ((rows[a] - 1) * ld + n) * sizeof(double));
+        if (direct && omega) direct = pinned_range(omega, ((KL - 1) * ld + n) * sizeof(double));
     }
     if ((rc = grow(*d, nin + nout, direct ? 2 * nch : nin + nout + 2 * nch)) != UWSHCU_OK) return rc;
     if ((rc = grow_worklist(*d, n + 2 * nch)) != UWSHCU_OK) return rc;
@@ -686,6 +689,7 @@ int host_call(int inv, int mix, int mkx, int iend, int ncnst, double dt, const d
         A.tr0 = add_in(tr0, KT);   // (mix, mkx, ncnst): mkx*ncnst rows of mix
         A.pblh = add_in(pblh, 1);
         A.cush = const_cast<double*>(add_in(cush, 1));
+        A.omega = omega ? add_in(omega, KL) : nullptr;
         if (!direct) copy_planes(in);
 
         std::vector<Plane>& out = outs[c];
@@ -839,6 +843,15 @@ int uwshcu_init(double xlv, double cp, double xlf, double zvir, double r, double
     k.rle = s.init ? s.k.rle : 0.1;       // uwshcu.F90:1036
     k.rkm = s.init ? s.k.rkm : 14.0;      // uwshcu.F90:1038
     k.criqc = s.init ? s.k.criqc : 0.7e-3; // uwshcu.F90:1065
+    // compute_zwshcu options (zwshcu.F90:31-39, 58; cloud_fraction.F90:52): the reference's defaults
+    k.zw_lf = s.init ? s.k.zw_lf : 1;
+    k.zw_fwcrit = s.init ? s.k.zw_fwcrit : 1.0;
+    k.zw_ent = s.init ? s.k.zw_ent : 0;
+    k.zw_ent0 = s.init ? s.k.zw_ent0 : 0.015;
+    k.zw_cloud_sh = s.init ? s.k.zw_cloud_sh : 0;
+    k.zw_ufrcd = s.init ? s.k.zw_ufrcd : 2.0;
+    k.zw_ufrc0 = s.init ? s.k.zw_ufrc0 : 2.0;
+    k.zw_ufrcz = s.init ? s.k.zw_ufrcz : 2.0;
     // gestbl (wv_saturation.F90:129-138, 181-185); esinti passes latvap, latice, rh2o, cpair
     k.tmin = tmin;
     k.tmax = tmax;
@@ -1080,7 +1093,7 @@ int compute_uwshcu_(const int* mix, const int* mkx, const int* iend, const int* 
                      slflx_out, qtflx_out, flxprc1_out, flxsnow1_out, qvten_out, qlten_out, qiten_out,
                      sten_out, uten_out, vten_out, trten_out, qrten_out, qsten_out, precip_out, snow_out,
                      evapc_out, cufrc_out, qcu_out, qlu_out, qiu_out, cbmf_out, qc_out, rliq_out,
-                     cnt_out, cnb_out, dpdry0_in, wu_out);
+                     cnt_out, cnb_out, dpdry0_in, wu_out, nullptr);
 }
 
 int compute_uwshcu_inv_(const int* mix, const int* mkx, const int* iend, const int* ncnst, const double* dt,
@@ -1113,7 +1126,101 @@ int compute_uwshcu_inv_(const int* mix, const int* mkx, const int* iend, const i
                      umf_inv, slflx_inv, qtflx_inv, flxprc1_inv, flxsnow1_inv, qvten_inv, qlten_inv,
                      qiten_inv, sten_inv, uten_inv, vten_inv, trten_inv, qrten_inv, qsten_inv, precip,
                      snow, evapc_inv, cufrc_inv, qcu_inv, qlu_inv, qiu_inv, cbmf, qc_inv, rliq, cnt_inv,
-                     cnb_inv, dpdry0_inv, wu_inv);
+                     cnb_inv, dpdry0_inv, wu_inv, nullptr);
+}
+
+// ---- compute_zwshcu (zwshcu.F90), the CAS-ESM variant: the same column code with the pressure
+// velocity omega and the options of uwshcu_set_zw_options.
+
+int compute_zwshcu_(const int* mix, const int* mkx, const int* iend, const int* ncnst, const double* dt,
+                    const double* ps0_in, const double* zs0_in, const double* p0_in, const double* z0_in,
+                    const double* dp0_in, const double* u0_in, const double* v0_in, const double* qv0_in,
+                    const double* ql0_in, const double* qi0_in, const double* t0_in, const double* s0_in,
+                    const double* tr0_in, const double* tke_in, const double* cldfrct_in,
+                    const double* concldfrct_in, const double* pblh_in, double* cush_inout,
+                    double* umf_out, double* slflx_out, double* qtflx_out, double* flxprc1_out,
+                    double* flxsnow1_out, double* qvten_out, double* qlten_out, double* qiten_out,
+                    double* sten_out, double* uten_out, double* vten_out, double* trten_out,
+                    double* qrten_out, double* qsten_out, double* precip_out, double* snow_out,
+                    double* evapc_out, double* cufrc_out, double* qcu_out, double* qlu_out,
+                    double* qiu_out, double* cbmf_out, double* qc_out, double* rliq_out,
+                    const double* omega, const double* massflx_sh, const double* tpert2,
+                    double* cnt_out, double* cnb_out, void* qsat, const int* lchnk,
+                    const double* dpdry0_in, double* wu_out)
+{
+    (void)cldfrct_in;
+    (void)concldfrct_in;
+    (void)massflx_sh;
+    (void)tpert2;
+    (void)qsat;
+    (void)lchnk;
+    if (!mix || !mkx || !iend || !ncnst || !dt || !omega) return UWSHCU_ERR_BAD_ARGS;
+    return host_call(0, *mix, *mkx, *iend, *ncnst, *dt, ps0_in, zs0_in, p0_in, z0_in, dp0_in, u0_in, v0_in,
+                     qv0_in, ql0_in, qi0_in, t0_in, s0_in, tr0_in, tke_in, pblh_in, cush_inout, umf_out,
+                     slflx_out, qtflx_out, flxprc1_out, flxsnow1_out, qvten_out, qlten_out, qiten_out,
+                     sten_out, uten_out, vten_out, trten_out, qrten_out, qsten_out, precip_out, snow_out,
+                     evapc_out, cufrc_out, qcu_out, qlu_out, qiu_out, cbmf_out, qc_out, rliq_out,
+                     cnt_out, cnb_out, dpdry0_in, wu_out, omega);
+}
+
+int compute_zwshcu_inv_(const int* mix, const int* mkx, const int* iend, const int* ncnst, const double* dt,
+                        const double* ps0_inv, const double* zs0_inv, const double* p0_inv,
+                        const double* z0_inv, const double* dp0_inv, const double* u0_inv,
+                        const double* v0_inv, const double* qv0_inv, const double* ql0_inv,
+                        const double* qi0_inv, const double* t0_inv, const double* s0_inv,
+                        const double* tr0_inv, const double* tke_inv, const double* cldfrct_inv,
+                        const double* concldfrct_inv, const double* pblh, double* cush,
+                        const double* omega_inv, const double* tpert2, const double* qpert2,
+                        const double* gradt, const double* gradq, const double* landfrac,
+                        const double* lat, const double* lon, const double* massflx_sh,
+                        double* umf_inv, double* slflx_inv, double* qtflx_inv, double* flxprc1_inv,
+                        double* flxsnow1_inv, double* qvten_inv, double* qlten_inv, double* qiten_inv,
+                        double* sten_inv, double* uten_inv, double* vten_inv, double* trten_inv,
+                        double* qrten_inv, double* qsten_inv, double* precip, double* snow,
+                        double* evapc_inv, double* cufrc_inv, double* qcu_inv, double* qlu_inv,
+                        double* qiu_inv, double* cbmf, double* qc_inv, double* rliq, double* cnt_inv,
+                        double* cnb_inv, void* qsat, const int* lchnk, const double* dpdry0_inv,
+                        double* wu_inv)
+{
+    (void)cldfrct_inv;
+    (void)concldfrct_inv;
+    (void)tpert2;
+    (void)qpert2;
+    (void)gradt;
+    (void)gradq;
+    (void)landfrac;
+    (void)lat;
+    (void)lon;
+    (void)massflx_sh;
+    (void)qsat;
+    (void)lchnk;
+    if (!mix || !mkx || !iend || !ncnst || !dt || !omega_inv) return UWSHCU_ERR_BAD_ARGS;
+    return host_call(1, *mix, *mkx, *iend, *ncnst, *dt, ps0_inv, zs0_inv, p0_inv, z0_inv, dp0_inv, u0_inv,
+                     v0_inv, qv0_inv, ql0_inv, qi0_inv, t0_inv, s0_inv, tr0_inv, tke_inv, pblh, cush,
+                     umf_inv, slflx_inv, qtflx_inv, flxprc1_inv, flxsnow1_inv, qvten_inv, qlten_inv,
+                     qiten_inv, sten_inv, uten_inv, vten_inv, trten_inv, qrten_inv, qsten_inv, precip,
+                     snow, evapc_inv, cufrc_inv, qcu_inv, qlu_inv, qiu_inv, cbmf, qc_inv, rliq, cnt_inv,
+                     cnb_inv, dpdry0_inv, wu_inv, omega_inv);
+}
+
+int uwshcu_set_zw_options(int lf, double fwcrit, int ent, double ent0, int cloud_sh, double ufrcd,
+                          double ufrc0, double ufrcz)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    if (!s.init) return UWSHCU_ERR_NOT_INITIALIZED;
+    if (!(fwcrit >= 0.0) || !(ent0 >= 0.0) || !(ufrc0 >= 0.0) || !(ufrcd >= 0.0) || !(ufrcz > -1.0))
+        return UWSHCU_ERR_BAD_ARGS;
+    s.k.zw_lf = lf != 0;
+    s.k.zw_fwcrit = fwcrit;
+    s.k.zw_ent = ent != 0;
+    s.k.zw_ent0 = ent0;
+    s.k.zw_cloud_sh = cloud_sh != 0;
+    s.k.zw_ufrcd = ufrcd;
+    s.k.zw_ufrc0 = ufrc0;
+    s.k.zw_ufrcz = ufrcz;
+    s.gen++;
+    return UWSHCU_OK;
 }
 
 int bxcompute_uwshcu_inv_(const int* pcols, const int* pver, const int* ncol, const int* pcnst,
@@ -1221,6 +1328,48 @@ int uwshcu_compute_device(int mix, int mkx, int iend, int ncnst, double dt, int 
     A.trten = trten; A.qrten = qrten; A.qsten = qsten; A.precip = precip; A.snow = snow; A.evapc = evapc;
     A.cufrc = cufrc; A.qcu = qcu; A.qlu = qlu; A.qiu = qiu; A.cbmf = cbmf; A.qc = qc; A.rliq = rliq;
     A.cnt = cnt; A.cnb = cnb; A.dpdry0 = dpdry0; A.wu = wu; A.diag_int = diag_int; A.diag_real = diag_real;
+    StreamCtx* c = nullptr;
+    if ((rc = stream_ctx(*d, (cudaStream_t)stream, &c)) != UWSHCU_OK) return rc;
+    return enqueue(*d, *c, A, (cudaStream_t)stream);
+}
+
+// compute_zwshcu on device-resident arrays: uwshcu_compute_device plus omega (mix, mkx).
+int compute_zwshcu_device(int mix, int mkx, int iend, int ncnst, double dt, int inv, const double* ps0,
+                          const double* zs0, const double* p0, const double* z0, const double* dp0,
+                          const double* u0, const double* v0, const double* qv0, const double* ql0,
+                          const double* qi0, const double* t0, const double* s0, const double* tr0,
+                          const double* tke, const double* pblh, const double* omega, double* cush, double* umf,
+                          double* slflx, double* qtflx, double* flxprc1, double* flxsnow1,
+                          double* qvten, double* qlten, double* qiten, double* sten, double* uten,
+                          double* vten, double* trten, double* qrten, double* qsten, double* precip,
+                          double* snow, double* evapc, double* cufrc, double* qcu, double* qlu,
+                          double* qiu, double* cbmf, double* qc, double* rliq, double* cnt,
+                          double* cnb, const double* dpdry0, double* wu, int* diag_int,
+                          double* diag_real, void* stream)
+{
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    if (!s.init) return UWSHCU_ERR_NOT_INITIALIZED;
+    if (bad_dims(mix, mkx, iend, ncnst) || (inv != 0 && inv != 1)) return UWSHCU_ERR_BAD_ARGS;
+    const void* need[] = {ps0, zs0, p0, z0, dp0, u0, v0, qv0, ql0, qi0, t0, s0, tr0, tke, pblh, omega, cush,
+                          umf, slflx, qtflx, flxprc1, flxsnow1, qvten, qlten, qiten, sten, uten, vten,
+                          trten, qrten, qsten, precip, snow, evapc, cufrc, qcu, qlu, qiu, cbmf, qc, rliq,
+                          cnt, cnb, dpdry0, wu};
+    for (const void* p : need)
+        if (!p) return UWSHCU_ERR_BAD_ARGS;
+    DeviceState* d = nullptr;
+    int rc = ensure_device(&d);
+    if (rc != UWSHCU_OK) return rc;
+    UwArgs A{};
+    A.mix = mix; A.mkx = mkx; A.iend = iend; A.ncnst = ncnst; A.inv = inv; A.dt = dt;
+    A.ps0 = ps0; A.zs0 = zs0; A.p0 = p0; A.z0 = z0; A.dp0 = dp0; A.u0 = u0; A.v0 = v0; A.qv0 = qv0;
+    A.ql0 = ql0; A.qi0 = qi0; A.t0 = t0; A.s0 = s0; A.tr0 = tr0; A.tke = tke; A.pblh = pblh; A.cush = cush;
+    A.umf = umf; A.slflx = slflx; A.qtflx = qtflx; A.flxprc1 = flxprc1; A.flxsnow1 = flxsnow1;
+    A.qvten = qvten; A.qlten = qlten; A.qiten = qiten; A.sten = sten; A.uten = uten; A.vten = vten;
+    A.trten = trten; A.qrten = qrten; A.qsten = qsten; A.precip = precip; A.snow = snow; A.evapc = evapc;
+    A.cufrc = cufrc; A.qcu = qcu; A.qlu = qlu; A.qiu = qiu; A.cbmf = cbmf; A.qc = qc; A.rliq = rliq;
+    A.cnt = cnt; A.cnb = cnb; A.dpdry0 = dpdry0; A.wu = wu; A.diag_int = diag_int; A.diag_real = diag_real;
+    A.omega = omega;
     StreamCtx* c = nullptr;
     if ((rc = stream_ctx(*d, (cudaStream_t)stream, &c)) != UWSHCU_OK) return rc;
     return enqueue(*d, *c, A, (cudaStream_t)stream);

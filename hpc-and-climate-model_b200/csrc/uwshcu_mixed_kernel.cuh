@@ -1030,14 +1030,24 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
         }
         {
             R wcrit = sqrtf(2.0f * cin * rbuoy);
+            // compute_zwshcu computes rho0inv first and lowers wcrit by the large-scale ascent at
+            // the PBL top (zwshcu.F90:2276, 2295-2303); the same value of rho0inv for both schemes
+            R rho0inv = ps0[kinv - 1] / (r * thv0top[kinv - 1] * exns0[kinv - 1]);
             R sigmaw = sqrtf(rkfre * tkeavg + epsvarw);
+            if (A.omega) {
+                if (c.zw_lf) {
+                    const R tmp1 = MN(MX(-GL(omega, kinv - 1), 0.0f), 3.0f);
+                    wcrit = wcrit - tmp1 / rho0inv / 9.8f;
+                    wcrit = MX(wcrit, 0.0f);
+                }
+                wcrit = wcrit * c.zw_fwcrit;
+            }
             R mu = wcrit / sigmaw / 1.4142f;
             if (mu >= 3.0f) {
                 id_exit = true;
                 stop = true;
             break;
             }
-            R rho0inv = ps0[kinv - 1] / (r * thv0top[kinv - 1] * exns0[kinv - 1]);
             cbmf = (rho0inv * sigmaw / 2.5066f) * expf(-(mu * mu));
             R cbmflimit = 0.9f * dp0[kinv - 1] / g / dt;
             R mumin0 = 0.0f;
@@ -1248,6 +1258,14 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                         if (xc > 0.5f) rei[k] = MN(rei[k], 0.9f * logf(dp0[k] / g / dt / umf[km1] + 1.0f) / dpe / (2.0f * xc - 1.0f));
                         fer[k] = rei[k] * ee2;
                         fdr[k] = rei[k] * ud2;
+                        // compute_zwshcu's entrainment option (zwshcu.F90:2818-2844)
+                        if (A.omega && c.zw_ent) {
+                            bogbot = rbuoy * (thvu[km1] / thvebot - 1.0f) * g;
+                            fer[k] = c.zw_ent0 * bogbot / MX(wue * wue, 1.0e-4f);
+                            R fer_min = 0.0f;
+                            if (bogbot > 1.e-4f) fer_min = 1.e-4f;
+                            fer[k] = MN(MX(fer[k], fer_min), 3.0e-2f);
+                        }
                         umf[k] = umf[km1] * expf(dpe * (fer[k] - fdr[k]));
                         emf[k] = 0.0f;
                         if (fer[k] * dpe < 1.e-4f) {
@@ -1908,6 +1926,16 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                 qcu[k] = 0.5f * (qcubelow + qlj + qij);
                 qlu[k] = 0.5f * (qlubelow + qlj);
                 qiu[k] = 0.5f * (qiubelow + qij);
+                // compute_zwshcu's cloud-fraction option (zwshcu.F90:4415-4431, 4448)
+                R zw_tmp2 = 0.0f, zw_tmp3 = 1.0f;
+                if (A.omega && c.zw_cloud_sh) {
+                    zw_tmp3 = 0.5f * c.zw_ufrc0;
+                    R tmp1 = (GL(z0, k) - GL(z0, krel)) / (GL(z0, kpen) - GL(z0, krel) + 10.0f);
+                    tmp1 = 1.0f + c.zw_ufrcz * tmp1;
+                    zw_tmp3 = zw_tmp3 * tmp1;
+                    zw_tmp2 = fdr[k] * umf[k] * (zs0[k] - zs0[k - 1]) * dt / dp0[k] * 9.8f * c.zw_ufrcd;
+                    zw_tmp2 = MN(1.0f - rmaxfrac, zw_tmp2);
+                }
                 cufrc[k] = (ufrc[k - 1] + ufrc[k]);
                 if (k == krel) {
                     cufrc[k] = (ufrclcl + ufrc[k]) * (prel - ps0[k]) / (ps0[k - 1] - ps0[k]);
@@ -1919,6 +1947,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                         qiu[k] = 0.5f * (qiubelow + criqc * qij / (qlj + qij));
                     }
                 }
+                if (A.omega) cufrc[k] = zw_tmp3 * cufrc[k] + zw_tmp2;
                 qcubelow = qlj + qij;
                 qlubelow = qlj;
                 qiubelow = qij;

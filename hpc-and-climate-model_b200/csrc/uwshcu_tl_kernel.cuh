@@ -1044,14 +1044,24 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
         }
         {
             Tl wcrit = sqrt(2.0 * cin * rbuoy);
+            // compute_zwshcu computes rho0inv first and lowers wcrit by the large-scale ascent at
+            // the PBL top (zwshcu.F90:2276, 2295-2303); the same value of rho0inv for both schemes
+            Tl rho0inv = ps0[kinv - 1] / (r * thv0top[kinv - 1] * exns0[kinv - 1]);
             Tl sigmaw = sqrt(rkfre * tkeavg + epsvarw);
+            if (A.omega) {
+                if (c.zw_lf) {
+                    const Tl tmp1 = MN(MX(-GL(omega, kinv - 1), 0.0), 3.0);
+                    wcrit = wcrit - tmp1 / rho0inv / 9.8;
+                    wcrit = MX(wcrit, 0.0);
+                }
+                wcrit = wcrit * c.zw_fwcrit;
+            }
             Tl mu = wcrit / sigmaw / 1.4142;
             if (mu >= 3.0) {
                 id_exit = true;
                 stop = true;
             break;
             }
-            Tl rho0inv = ps0[kinv - 1] / (r * thv0top[kinv - 1] * exns0[kinv - 1]);
             cbmf = (rho0inv * sigmaw / 2.5066) * uw_exp(-(mu * mu));
             Tl cbmflimit = 0.9 * dp0[kinv - 1] / g / dt;
             Tl mumin0 = 0.0;
@@ -1262,6 +1272,14 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                         if (xc > 0.5) rei[k] = MN(rei[k], 0.9 * uw_log(dp0[k] / g / dt / umf[km1] + 1.0) / dpe / (2.0 * xc - 1.0));
                         fer[k] = rei[k] * ee2;
                         fdr[k] = rei[k] * ud2;
+                        // compute_zwshcu's entrainment option (zwshcu.F90:2818-2844)
+                        if (A.omega && c.zw_ent) {
+                            bogbot = rbuoy * (thvu[km1] / thvebot - 1.0) * g;
+                            fer[k] = c.zw_ent0 * bogbot / MX(wue * wue, 1.0e-4);
+                            Tl fer_min = 0.0;
+                            if (bogbot > 1.e-4) fer_min = 1.e-4;
+                            fer[k] = MN(MX(fer[k], fer_min), 3.0e-2);
+                        }
                         umf[k] = umf[km1] * uw_exp(dpe * (fer[k] - fdr[k]));
                         emf[k] = 0.0;
                         if (fer[k] * dpe < 1.e-4) {
@@ -1918,6 +1936,16 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                 qcu[k] = 0.5 * (qcubelow + qlj + qij);
                 qlu[k] = 0.5 * (qlubelow + qlj);
                 qiu[k] = 0.5 * (qiubelow + qij);
+                // compute_zwshcu's cloud-fraction option (zwshcu.F90:4415-4431, 4448)
+                Tl zw_tmp2 = 0.0, zw_tmp3 = 1.0;
+                if (A.omega && c.zw_cloud_sh) {
+                    zw_tmp3 = 0.5 * c.zw_ufrc0;
+                    Tl tmp1 = (GL(z0, k) - GL(z0, krel)) / (GL(z0, kpen) - GL(z0, krel) + 10.0);
+                    tmp1 = 1.0 + c.zw_ufrcz * tmp1;
+                    zw_tmp3 = zw_tmp3 * tmp1;
+                    zw_tmp2 = fdr[k] * umf[k] * (zs0[k] - zs0[k - 1]) * dt / dp0[k] * 9.8 * c.zw_ufrcd;
+                    zw_tmp2 = MN(1.0 - rmaxfrac, zw_tmp2);
+                }
                 cufrc[k] = (ufrc[k - 1] + ufrc[k]);
                 if (k == krel) {
                     cufrc[k] = (ufrclcl + ufrc[k]) * (prel - ps0[k]) / (ps0[k - 1] - ps0[k]);
@@ -1929,6 +1957,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                         qiu[k] = 0.5 * (qiubelow + criqc * qij / (qlj + qij));
                     }
                 }
+                if (A.omega) cufrc[k] = zw_tmp3 * cufrc[k] + zw_tmp2;
                 qcubelow = qlj + qij;
                 qlubelow = qlj;
                 qiubelow = qij;

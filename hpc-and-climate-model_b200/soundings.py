@@ -144,6 +144,22 @@ def make_soundings(ncol, pver=30, seed=0, rh_pbl=(0.70, 0.95), ncnst=5, dt=1800.
     return out
 
 
+def make_omega(s, seed=0, mean=-0.05, sd=0.3):
+    """Large-scale pressure velocity omega (mkx, ncol) [Pa/s] for compute_zwshcu, bottom-up like the
+    other layer fields: a first-baroclinic-mode profile omega0 sin(pi (ps - p) / (ps - 10 kPa)) below
+    100 hPa (zero above) with omega0 ~ N(mean, sd) per column (negative: ascent), plus N(0, 0.02)
+    per level.  Every column's own surface pressure ps0[0]."""
+    rng = np.random.default_rng(10_000 + seed)
+    n, mkx = s["ncol"], s["mkx"]
+    ps = s["ps0"][0]
+    p = s["p0"]
+    w0 = rng.normal(mean, sd, n)
+    x = np.clip((ps - p) / (ps - 1.0e4), 0.0, 1.0)
+    om = w0 * np.sin(np.pi * x) + rng.normal(0.0, 0.02, (mkx, n))
+    om = np.where(p < 1.0e4, 0.0, om)
+    return np.ascontiguousarray(om, dtype=np.float64)
+
+
 def to_inv(s):
     """Return a copy of a sounding dict in CAM's top-down level order (compute_uwshcu_inv input
     layout, uwshcu.F90:274-297)."""

@@ -47,7 +47,8 @@ EXPORTS = ("uwshcu_init", "uwshcu_set_rpen", "uwshcu_init_default", "uwshcu_set_
            "uwshcu_batch_destroy", "uwshcu_set_pipeline", "uwshcu_set_params",
            "uwshcu_budget_device", "uwshcu_tangent_device", "uwshcu_compute_member",
            "uwshcu_set_hand_slots", "uwshcu_adjoint_device", "uwshcu_adjoint_last_records",
-           "uwshcu_adjoint_release", "uwshcu_set_adjoint_rows")
+           "uwshcu_adjoint_release", "uwshcu_set_adjoint_rows", "compute_zwshcu_",
+           "compute_zwshcu_inv_", "compute_zwshcu_device", "uwshcu_set_zw_options")
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
@@ -95,6 +96,13 @@ PREC_FAST = 2
 def set_params(rpen, rle, rkm, criqc):
     d = ctypes.c_double
     return lib().uwshcu_set_params(d(rpen), d(rle), d(rkm), d(criqc))
+
+
+def set_zw_options(lf=1, fwcrit=1.0, ent=0, ent0=0.015, cloud_sh=0, ufrcd=2.0, ufrc0=2.0, ufrcz=2.0):
+    """uwshcu_set_zw_options: the options of the compute_zwshcu entries (defaults: the reference's)."""
+    d = ctypes.c_double
+    return lib().uwshcu_set_zw_options(ctypes.c_int(lf), d(fwcrit), ctypes.c_int(ent), d(ent0),
+                                       ctypes.c_int(cloud_sh), d(ufrcd), d(ufrc0), d(ufrcz))
 
 
 def set_precision(mode):
@@ -161,10 +169,12 @@ def alloc_outputs(mkx, ncnst, mix, cush_in):
     return out
 
 
-def compute_host(s, entry="compute_uwshcu_", out=None, iend=None):
+def compute_host(s, entry="compute_uwshcu_", out=None, iend=None, omega=None):
     """Call a host entry point on a sounding dict (numpy arrays in the Fortran layout; mix = ncol).
-    entry: 'compute_uwshcu_' (bottom-up arrays), 'compute_uwshcu_inv_' or 'bxcompute_uwshcu_inv_'
-    (CAM top-down arrays, e.g. soundings.to_inv(s)).  Returns (status, outputs)."""
+    entry: 'compute_uwshcu_' or 'compute_zwshcu_' (bottom-up arrays), 'compute_uwshcu_inv_',
+    'compute_zwshcu_inv_' or 'bxcompute_uwshcu_inv_' (CAM top-down arrays, e.g.
+    soundings.to_inv(s)); the compute_zwshcu entries take omega (mkx, ncol) in the same level order.
+    Returns (status, outputs)."""
     L = lib()
     mkx, ncnst, n = s["mkx"], s["ncnst"], s["ncol"]
     if out is None:
@@ -192,6 +202,19 @@ def compute_host(s, entry="compute_uwshcu_", out=None, iend=None):
         rc = L.compute_uwshcu_inv_(ci(n), ci(mkx), ci(ie), ci(ncnst), cd(s["dt"]), *common_in,
                                    _p(z), _p(z), _p(s["massflx_sh"]), *outs1, _p(o["cnt"]),
                                    _p(o["cnb"]), None, lchnk, _p(s["dpdry0"]), _p(o["wu"]))
+    elif entry == "compute_zwshcu_":
+        om = np.ascontiguousarray(omega, dtype=np.float64)
+        z = np.zeros(n)
+        rc = L.compute_zwshcu_(ci(n), ci(mkx), ci(ie), ci(ncnst), cd(s["dt"]), *common_in, *outs1,
+                               _p(om), _p(s["massflx_sh"]), _p(z), _p(o["cnt"]), _p(o["cnb"]), None,
+                               lchnk, _p(s["dpdry0"]), _p(o["wu"]))
+    elif entry == "compute_zwshcu_inv_":
+        om = np.ascontiguousarray(omega, dtype=np.float64)
+        z = np.zeros(n)
+        rc = L.compute_zwshcu_inv_(ci(n), ci(mkx), ci(ie), ci(ncnst), cd(s["dt"]), *common_in,
+                                   _p(om), _p(z), _p(z), _p(z), _p(z), _p(z), _p(z), _p(z),
+                                   _p(s["massflx_sh"]), *outs1, _p(o["cnt"]), _p(o["cnb"]), None, lchnk,
+                                   _p(s["dpdry0"]), _p(o["wu"]))
     elif entry == "bxcompute_uwshcu_inv_":
         rc = L.bxcompute_uwshcu_inv_(ci(n), ci(mkx), ci(ie), ci(ncnst), cd(s["dt"]), *common_in,
                                      *outs1, _p(o["cnt"]), _p(o["cnb"]), lchnk, _p(s["dpdry0"]),
@@ -228,12 +251,28 @@ class DeviceCase:
     def reset_cush(self):
         self.out["cush"].copy_(self.cush0)
 
-    def launch(self, inv=0, stream=None):
-        """Enqueue one call on `stream` (torch stream or None for the current stream)."""
+    def launch(self, inv=0, stream=None, omega=None):
+        """Enqueue one call on `stream` (torch stream or None for the current stream); with omega (a
+        device tensor (mkx, n) of pressure velocity) one compute_zwshcu_device call instead."""
         torch = self.torch
         st = stream if stream is not None else torch.cuda.current_stream()
         P = lambda t: ctypes.c_void_p(t.data_ptr())
         i, o = self.inp, self.out
+        if omega is not None:
+            return lib().compute_zwshcu_device(
+                ctypes.c_int(self.n), ctypes.c_int(self.mkx), ctypes.c_int(self.n),
+                ctypes.c_int(self.ncnst), ctypes.c_double(self.dt), ctypes.c_int(inv),
+                P(i["ps0"]), P(i["zs0"]), P(i["p0"]), P(i["z0"]), P(i["dp0"]), P(i["u0"]), P(i["v0"]),
+                P(i["qv0"]), P(i["ql0"]), P(i["qi0"]), P(i["t0"]), P(i["s0"]), P(i["tr0"]),
+                P(i["tke"]), P(i["pblh"]), P(omega), P(o["cush"]), P(o["umf"]), P(o["slflx"]),
+                P(o["qtflx"]), P(o["flxprc1"]), P(o["flxsnow1"]), P(o["qvten"]), P(o["qlten"]),
+                P(o["qiten"]), P(o["sten"]), P(o["uten"]), P(o["vten"]), P(o["trten"]), P(o["qrten"]),
+                P(o["qsten"]), P(o["precip"]), P(o["snow"]), P(o["evapc"]), P(o["cufrc"]),
+                P(o["qcu"]), P(o["qlu"]), P(o["qiu"]), P(o["cbmf"]), P(o["qc"]), P(o["rliq"]),
+                P(o["cnt"]), P(o["cnb"]), P(i["dpdry0"]), P(o["wu"]),
+                P(self.diag_int) if self.diag_int is not None else None,
+                P(self.diag_real) if self.diag_real is not None else None,
+                ctypes.c_void_p(st.cuda_stream))
         return lib().uwshcu_compute_device(
             ctypes.c_int(self.n), ctypes.c_int(self.mkx), ctypes.c_int(self.n),
             ctypes.c_int(self.ncnst), ctypes.c_double(self.dt), ctypes.c_int(inv),

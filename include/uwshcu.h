@@ -198,6 +198,65 @@ int bxcompute_uwshcu_inv_(const int *pcols, const int *pver, const int *ncol, co
                           double *cnt_inv, double *cnb_inv, const int *lchnk,
                           const double *dpdry0_inv, double *wu_inv);
 
+/* ---- compute_zwshcu: the CAS-ESM variant of the scheme (zwshcu.F90) ----------------------------- */
+
+/* compute_zwshcu (zwshcu.F90:630-644), argument list unchanged: compute_uwshcu's arguments with the
+ * pressure velocity omega (mix, mkx) [Pa/s, negative upwards], massflx_sh and tpert2 between rliq_out
+ * and cnt_out.  Same column code as compute_uwshcu_ plus the variant's options (uwshcu_set_zw_options):
+ * with zmh_shallow_lf the closure lowers wcrit by min(max(-omega, 0), 3) / rho0inv / 9.8 at the
+ * PBL-top layer (zwshcu.F90:2295-2303), and the optional buoyancy-based entrainment
+ * (zwshcu.F90:2818-2844) and cloud-fraction enhancement (zwshcu.F90:4415-4448).  tpert2 is read by the
+ * perturbation options only, which are not built (off in the reference).  rpen and rkm keep the values
+ * of uwshcu_set_params (the variant's namelist defaults are rpen = 15, rkm = 10,
+ * zwshcu.F90:45-46).  omega = 0 everywhere gives compute_uwshcu_'s results bit for bit. */
+int compute_zwshcu_(const int *mix, const int *mkx, const int *iend, const int *ncnst,
+                    const double *dt, const double *ps0_in, const double *zs0_in,
+                    const double *p0_in, const double *z0_in, const double *dp0_in,
+                    const double *u0_in, const double *v0_in, const double *qv0_in,
+                    const double *ql0_in, const double *qi0_in, const double *t0_in,
+                    const double *s0_in, const double *tr0_in, const double *tke_in,
+                    const double *cldfrct_in, const double *concldfrct_in, const double *pblh_in,
+                    double *cush_inout, double *umf_out, double *slflx_out, double *qtflx_out,
+                    double *flxprc1_out, double *flxsnow1_out, double *qvten_out,
+                    double *qlten_out, double *qiten_out, double *sten_out, double *uten_out,
+                    double *vten_out, double *trten_out, double *qrten_out, double *qsten_out,
+                    double *precip_out, double *snow_out, double *evapc_out, double *cufrc_out,
+                    double *qcu_out, double *qlu_out, double *qiu_out, double *cbmf_out,
+                    double *qc_out, double *rliq_out, const double *omega, const double *massflx_sh,
+                    const double *tpert2, double *cnt_out, double *cnb_out, void *qsat,
+                    const int *lchnk, const double *dpdry0_in, double *wu_out);
+
+/* compute_zwshcu_inv (zwshcu.F90:336-628, called from convect_shallow.F90:717-731), argument list
+ * unchanged: CAM's top-down level order, with omega_inv, tpert2, qpert2, gradt, gradq, landfrac, lat,
+ * lon and massflx_sh after cush.  gradt, gradq, landfrac, lat, lon, tpert2 and qpert2 feed the
+ * perturbation options only (zwshcu.F90:511-566, all off in the reference) and are unused. */
+int compute_zwshcu_inv_(const int *mix, const int *mkx, const int *iend, const int *ncnst,
+                        const double *dt, const double *ps0_inv, const double *zs0_inv,
+                        const double *p0_inv, const double *z0_inv, const double *dp0_inv,
+                        const double *u0_inv, const double *v0_inv, const double *qv0_inv,
+                        const double *ql0_inv, const double *qi0_inv, const double *t0_inv,
+                        const double *s0_inv, const double *tr0_inv, const double *tke_inv,
+                        const double *cldfrct_inv, const double *concldfrct_inv,
+                        const double *pblh, double *cush, const double *omega_inv,
+                        const double *tpert2, const double *qpert2, const double *gradt,
+                        const double *gradq, const double *landfrac, const double *lat,
+                        const double *lon, const double *massflx_sh, double *umf_inv,
+                        double *slflx_inv, double *qtflx_inv, double *flxprc1_inv,
+                        double *flxsnow1_inv, double *qvten_inv, double *qlten_inv,
+                        double *qiten_inv, double *sten_inv, double *uten_inv, double *vten_inv,
+                        double *trten_inv, double *qrten_inv, double *qsten_inv, double *precip,
+                        double *snow, double *evapc_inv, double *cufrc_inv, double *qcu_inv,
+                        double *qlu_inv, double *qiu_inv, double *cbmf, double *qc_inv,
+                        double *rliq, double *cnt_inv, double *cnb_inv, void *qsat,
+                        const int *lchnk, const double *dpdry0_inv, double *wu_inv);
+
+/* Options of the compute_zwshcu entries (zwshcu.F90:30-59 namelist uwshcu_nl, cloud_fraction.F90:52):
+ * zmh_shallow_lf, zmh_shallow_fwcrit, zmh_shallow_ent, zmh_ent0, zmh_cloud_sh, zmh_ufrcd, zmh_ufrc0,
+ * zmh_ufrcz.  uwshcu_init sets the reference's defaults 1, 1.0, 0, 0.015, 0, 2.0, 2.0, 2.0; they do not
+ * affect the compute_uwshcu entries. */
+int uwshcu_set_zw_options(int lf, double fwcrit, int ent, double ent0, int cloud_sh, double ufrcd,
+                          double ufrc0, double ufrcz);
+
 /* ---- device-resident entry point -------------------------------------------------------------- */
 
 /* The computation of compute_uwshcu (inv = 0) or compute_uwshcu_inv (inv = 1) on arrays that
@@ -222,6 +281,22 @@ int uwshcu_compute_device(int mix, int mkx, int iend, int ncnst, double dt, int 
                           double *slflx, double *qtflx, double *flxprc1, double *flxsnow1,
                           double *qvten, double *qlten, double *qiten, double *sten, double *uten,
                           double *vten, double *trten, double *qrten, double *qsten,
+                          double *precip, double *snow, double *evapc, double *cufrc, double *qcu,
+                          double *qlu, double *qiu, double *cbmf, double *qc, double *rliq,
+                          double *cnt, double *cnb, const double *dpdry0, double *wu,
+                          int *diag_int, double *diag_real, void *stream);
+
+/* compute_zwshcu on device-resident arrays: uwshcu_compute_device's arguments plus omega (mix, mkx),
+ * in the level order of the call (inv). */
+int compute_zwshcu_device(int mix, int mkx, int iend, int ncnst, double dt, int inv,
+                          const double *ps0, const double *zs0, const double *p0,
+                          const double *z0, const double *dp0, const double *u0, const double *v0,
+                          const double *qv0, const double *ql0, const double *qi0,
+                          const double *t0, const double *s0, const double *tr0,
+                          const double *tke, const double *pblh, const double *omega, double *cush,
+                          double *umf, double *slflx, double *qtflx, double *flxprc1,
+                          double *flxsnow1, double *qvten, double *qlten, double *qiten, double *sten,
+                          double *uten, double *vten, double *trten, double *qrten, double *qsten,
                           double *precip, double *snow, double *evapc, double *cufrc, double *qcu,
                           double *qlu, double *qiu, double *cbmf, double *qc, double *rliq,
                           double *cnt, double *cnb, const double *dpdry0, double *wu,

@@ -63,6 +63,7 @@ def lib():
         _lib.uwo_init_default.restype = ctypes.c_int
         _lib.uwo_compute_uwshcu.restype = ctypes.c_int
         _lib.uwo_compute_uwshcu_inv.restype = ctypes.c_int
+        _lib.uwo_compute_zwshcu.restype = ctypes.c_int
         for name in ("uwo_exnf", "uwo_estblf", "uwo_qsinvert", "uwo_compute_alpha",
                      "uwo_compute_mumin2", "uwo_compute_ppen", "uwo_single_cin"):
             getattr(_lib, name).restype = ctypes.c_double
@@ -110,10 +111,19 @@ def alloc_outputs(mkx, ncnst, mix, cush_in):
     return out
 
 
-def compute(s, nthreads=0, diag=True, inv=False):
+def set_zw_options(lf=1, fwcrit=1.0, ent=0, ent0=0.015, cloud_sh=0, ufrcd=2.0, ufrc0=2.0, ufrcz=2.0):
+    """Options of compute_zwshcu (zmh_shallow_lf, zmh_shallow_fwcrit, zmh_shallow_ent, zmh_ent0,
+    zmh_cloud_sh, zmh_ufrcd, zmh_ufrc0, zmh_ufrcz); the defaults are the reference's."""
+    d = ctypes.c_double
+    return lib().uwo_set_zw_options(ctypes.c_int(lf), d(fwcrit), ctypes.c_int(ent), d(ent0),
+                                    ctypes.c_int(cloud_sh), d(ufrcd), d(ufrc0), d(ufrcz))
+
+
+def compute(s, nthreads=0, diag=True, inv=False, omega=None):
     """Run the oracle on a sounding dict (all columns, mix = iend = ncol).  Returns the output
     dict; with diag=True also 'diag_int' (8, ncol), 'diag_real' (8, ncol) and 'diag_level'
-    (13, mkx + 1, ncol)."""
+    (13, mkx + 1, ncol).  With omega (a (mkx, ncol) array of pressure velocity, bottom-up) it runs
+    compute_zwshcu (zwshcu.F90) instead of compute_uwshcu."""
     L = lib()
     mkx, ncnst, n = s["mkx"], s["ncnst"], s["ncol"]
     o = alloc_outputs(mkx, ncnst, n, s["cush"])
@@ -121,7 +131,24 @@ def compute(s, nthreads=0, diag=True, inv=False):
     dr = np.zeros((NDR, n))
     dl = np.zeros((NDL, mkx + 1, n))
     ci, cd = ctypes.c_int, ctypes.c_double
-    if not inv:
+    if omega is not None:
+        assert not inv
+        om = np.ascontiguousarray(omega, dtype=np.float64)
+        z = np.zeros(n)
+        rc = L.uwo_compute_zwshcu(
+            ci(n), ci(mkx), ci(n), ci(ncnst), cd(s["dt"]),
+            _p(s["ps0"]), _p(s["zs0"]), _p(s["p0"]), _p(s["z0"]), _p(s["dp0"]), _p(s["u0"]),
+            _p(s["v0"]), _p(s["qv0"]), _p(s["ql0"]), _p(s["qi0"]), _p(s["t0"]), _p(s["s0"]),
+            _p(s["tr0"]), _p(s["tke"]), _p(s["cldfrct"]), _p(s["concldfrct"]), _p(s["pblh"]),
+            _p(o["cush"]), _p(o["umf"]), _p(o["slflx"]), _p(o["qtflx"]), _p(o["flxprc1"]),
+            _p(o["flxsnow1"]), _p(o["qvten"]), _p(o["qlten"]), _p(o["qiten"]), _p(o["sten"]),
+            _p(o["uten"]), _p(o["vten"]), _p(o["trten"]), _p(o["qrten"]), _p(o["qsten"]),
+            _p(o["precip"]), _p(o["snow"]), _p(o["evapc"]), _p(o["cufrc"]), _p(o["qcu"]),
+            _p(o["qlu"]), _p(o["qiu"]), _p(o["cbmf"]), _p(o["qc"]), _p(o["rliq"]), _p(om),
+            _p(s["massflx_sh"]), _p(z), _p(o["cnt"]), _p(o["cnb"]), _p(s["dpdry0"]), _p(o["wu"]),
+            di.ctypes.data_as(_I) if diag else None, _p(dr) if diag else None,
+            _p(dl) if diag else None, ci(nthreads))
+    elif not inv:
         rc = L.uwo_compute_uwshcu(
             ci(n), ci(mkx), ci(n), ci(ncnst), cd(s["dt"]),
             _p(s["ps0"]), _p(s["zs0"]), _p(s["p0"]), _p(s["z0"]), _p(s["dp0"]), _p(s["u0"]),

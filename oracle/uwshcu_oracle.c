@@ -53,6 +53,11 @@ typedef struct {
     double qmin[NCMAX];
     int wet[NCMAX];
     int ixnumliq, ixnumice;
+    /* zwshcu options (zwshcu.F90:30-59, cloud_fraction.F90:52), in force when a call passes omega:
+     * zmh_shallow_lf, zmh_shallow_fwcrit, zmh_shallow_ent, zmh_ent0, zmh_cloud_sh, zmh_ufrcd,
+     * zmh_ufrc0, zmh_ufrcz */
+    int zw_lf, zw_ent, zw_cloud_sh;
+    double zw_fwcrit, zw_ent0, zw_ufrcd, zw_ufrc0, zw_ufrcz;
 } uwo_state;
 
 static uwo_state S;
@@ -600,6 +605,7 @@ typedef struct {
     int *diag_int;
     double *diag_real;
     double *diag_level;
+    const double *omega;   /* (mix, mkx) pressure velocity of compute_zwshcu; NULL: compute_uwshcu */
 } uwo_io;
 
 /* Per-level diagnostics (the Fortran's history fields, uwshcu.F90:4383-4433), array
@@ -1244,15 +1250,24 @@ static int uw_column(const uwo_io *A, int i)
             prel = plcl;
             thv0rel = thv0lcl;
         }
-        /* Closure (:2092-2184) */
+        /* Closure (:2092-2184); compute_zwshcu computes rho0inv first (zwshcu.F90:2276) and lowers
+         * wcrit by the large-scale ascent at the PBL top (zwshcu.F90:2295-2303) */
         wcrit = sqrt(2.0 * cin * rbuoy);
+        rho0inv = ps0[kinv - 1] / (r * thv0top[kinv - 1] * exns0[kinv - 1]);
         sigmaw = sqrt(rkfre * tkeavg + epsvarw);
+        if (A->omega) {
+            if (S.zw_lf) {
+                double tmp1 = MN(MX(-AL(A->omega, i, kinv - 1), 0.0), 3.0);
+                wcrit = wcrit - tmp1 / rho0inv / 9.8;
+                wcrit = MX(wcrit, 0.0);
+            }
+            wcrit = wcrit * S.zw_fwcrit;
+        }
         mu = wcrit / sigmaw / 1.4142;
         if (mu >= 3.0) {
             id_exit = 1;
             goto l333;
         }
-        rho0inv = ps0[kinv - 1] / (r * thv0top[kinv - 1] * exns0[kinv - 1]);
         cbmf = (rho0inv * sigmaw / 2.5066) * EXP(-(mu * mu));
         cbmflimit = 0.9 * dp0[kinv - 1] / g / dt;
         mumin0 = 0.0;
@@ -1437,6 +1452,15 @@ static int uw_column(const uwo_io *A, int i)
                     if (xc > 0.5) rei[k] = MN(rei[k], 0.9 * LOG(dp0[k] / g / dt / umf[km1] + 1.0) / dpe / (2.0 * xc - 1.0));
                     fer[k] = rei[k] * ee2;
                     fdr[k] = rei[k] * ud2;
+                    /* compute_zwshcu's entrainment option (zwshcu.F90:2818-2844) */
+                    if (A->omega && S.zw_ent) {
+                        double fer_min;
+                        bogbot = rbuoy * (thvu[km1] / thvebot - 1.0) * g;
+                        fer[k] = S.zw_ent0 * bogbot / MX(wue * wue, 1.0e-4);
+                        fer_min = 0.0;
+                        if (bogbot > 1.e-4) fer_min = 1.e-4;
+                        fer[k] = MN(MX(fer[k], fer_min), 3.0e-2);
+                    }
                     umf[k] = umf[km1] * EXP(dpe * (fer[k] - fdr[k]));
                     emf[k] = 0.0;
                     if (fer[k] * dpe < 1.e-4) {
@@ -2010,7 +2034,7 @@ static int uw_column(const uwo_io *A, int i)
             goto l333;
         }
         {
-            double qcubelow = qlj + qij;
+            double qcubelow = qlj + qij, zw_tmp2, zw_tmp3;
             qlubelow = qlj;
             qiubelow = qij;
             for (k = krel; k <= kpen; k++) {
@@ -2024,6 +2048,18 @@ static int uw_column(const uwo_io *A, int i)
                 qcu[k] = 0.5 * (qcubelow + qlj + qij);
                 qlu[k] = 0.5 * (qlubelow + qlj);
                 qiu[k] = 0.5 * (qiubelow + qij);
+                /* compute_zwshcu's cloud-fraction option (zwshcu.F90:4415-4431) */
+                zw_tmp2 = 0.0;
+                zw_tmp3 = 1.0;
+                if (A->omega && S.zw_cloud_sh) {
+                    double tmp1;
+                    zw_tmp3 = 0.5 * S.zw_ufrc0;
+                    tmp1 = (z0[k] - z0[krel]) / (z0[kpen] - z0[krel] + 10.0);
+                    tmp1 = 1.0 + S.zw_ufrcz * tmp1;
+                    zw_tmp3 = zw_tmp3 * tmp1;
+                    zw_tmp2 = fdr[k] * umf[k] * (zs0[k] - zs0[k - 1]) * dt / dp0[k] * 9.8 * S.zw_ufrcd;
+                    zw_tmp2 = MN(1.0 - rmaxfrac, zw_tmp2);
+                }
                 cufrc[k] = (ufrc[k - 1] + ufrc[k]);
                 if (k == krel) {
                     cufrc[k] = (ufrclcl + ufrc[k]) * (prel - ps0[k]) / (ps0[k - 1] - ps0[k]);
@@ -2035,6 +2071,7 @@ static int uw_column(const uwo_io *A, int i)
                         qiu[k] = 0.5 * (qiubelow + criqc * qij / (qlj + qij));
                     }
                 }
+                if (A->omega) cufrc[k] = zw_tmp3 * cufrc[k] + zw_tmp2;   /* zwshcu.F90:4448 */
                 qcubelow = qlj + qij;
                 qlubelow = qlj;
                 qiubelow = qij;
@@ -2279,6 +2316,7 @@ int uwo_init(double xlv, double cp, double xlf, double zvir, double r, double g,
     /* the Fortran parameter values (uwshcu.F90:1036, 1038, 1065) */
     S.rle = 0.1;
     S.rkm = 14.0;
+    uwo_set_zw_options(1, 1.0, 0, 0.015, 0, 2.0, 2.0, 2.0);
     S.criqc = 0.7e-3;
     /* esinti -> gestbl (esinti.F90:44-51) */
     gestbl(tmn, tmx, trice, icephs, epsqs, xlv, xlf, rgasv, cp, tmelt);
@@ -2339,19 +2377,22 @@ int uwo_findsp(int mix, int ncol, int pver, const double *q, const double *t, co
     return st;
 }
 
-int uwo_compute_uwshcu(int mix, int mkx, int iend, int ncnst, double dt,
-                       const double *ps0, const double *zs0, const double *p0, const double *z0,
-                       const double *dp0, const double *u0, const double *v0, const double *qv0,
-                       const double *ql0, const double *qi0, const double *t0, const double *s0,
-                       const double *tr0, const double *tke, const double *cldfrct,
-                       const double *concldfrct, const double *pblh, double *cush,
-                       double *umf, double *slflx, double *qtflx, double *flxprc1, double *flxsnow1,
-                       double *qvten, double *qlten, double *qiten, double *sten, double *uten,
-                       double *vten, double *trten, double *qrten, double *qsten, double *precip,
-                       double *snow, double *evapc, double *cufrc, double *qcu, double *qlu,
-                       double *qiu, double *cbmf, double *qc, double *rliq, const double *massflx_sh,
-                       double *cnt, double *cnb, const double *dpdry0, double *wu,
-                       int *diag_int, double *diag_real, double *diag_level, int nthreads)
+/* compute_uwshcu (omega NULL) or compute_zwshcu (zwshcu.F90:630-4969, omega (mix, mkx)): the
+ * driver of both, findsp over all (i,k) and the column loop. */
+static int compute_core(int mix, int mkx, int iend, int ncnst, double dt,
+                        const double *ps0, const double *zs0, const double *p0, const double *z0,
+                        const double *dp0, const double *u0, const double *v0, const double *qv0,
+                        const double *ql0, const double *qi0, const double *t0, const double *s0,
+                        const double *tr0, const double *tke, const double *cldfrct,
+                        const double *concldfrct, const double *pblh, double *cush,
+                        double *umf, double *slflx, double *qtflx, double *flxprc1, double *flxsnow1,
+                        double *qvten, double *qlten, double *qiten, double *sten, double *uten,
+                        double *vten, double *trten, double *qrten, double *qsten, double *precip,
+                        double *snow, double *evapc, double *cufrc, double *qcu, double *qlu,
+                        double *qiu, double *cbmf, double *qc, double *rliq, const double *massflx_sh,
+                        double *cnt, double *cnb, const double *dpdry0, double *wu,
+                        int *diag_int, double *diag_real, double *diag_level, int nthreads,
+                        const double *omega)
 {
     int st = 0, i;
     int nthr = nthreads > 0 ? nthreads : UWO_MAXTHREADS();
@@ -2393,13 +2434,77 @@ int uwo_compute_uwshcu(int mix, int mkx, int iend, int ncnst, double dt,
         A.qrten = qrten; A.qsten = qsten; A.precip = precip; A.snow = snow; A.evapc = evapc;
         A.cufrc = cufrc; A.qcu = qcu; A.qlu = qlu; A.qiu = qiu; A.cbmf = cbmf; A.qc = qc;
         A.rliq = rliq; A.cnt = cnt; A.cnb = cnb; A.dpdry0 = dpdry0; A.wu = wu; A.qw0 = qwcol;
-        A.diag_int = diag_int; A.diag_real = diag_real; A.diag_level = diag_level;
+        A.diag_int = diag_int; A.diag_real = diag_real; A.diag_level = diag_level; A.omega = omega;
         s = uw_column(&A, i);
         if (s > st) st = s;
     }
     free(tw0);
     free(qw0);
     return st;
+}
+
+int uwo_compute_uwshcu(int mix, int mkx, int iend, int ncnst, double dt,
+                       const double *ps0, const double *zs0, const double *p0, const double *z0,
+                       const double *dp0, const double *u0, const double *v0, const double *qv0,
+                       const double *ql0, const double *qi0, const double *t0, const double *s0,
+                       const double *tr0, const double *tke, const double *cldfrct,
+                       const double *concldfrct, const double *pblh, double *cush,
+                       double *umf, double *slflx, double *qtflx, double *flxprc1, double *flxsnow1,
+                       double *qvten, double *qlten, double *qiten, double *sten, double *uten,
+                       double *vten, double *trten, double *qrten, double *qsten, double *precip,
+                       double *snow, double *evapc, double *cufrc, double *qcu, double *qlu,
+                       double *qiu, double *cbmf, double *qc, double *rliq, const double *massflx_sh,
+                       double *cnt, double *cnb, const double *dpdry0, double *wu,
+                       int *diag_int, double *diag_real, double *diag_level, int nthreads)
+{
+    return compute_core(mix, mkx, iend, ncnst, dt, ps0, zs0, p0, z0, dp0, u0, v0, qv0, ql0, qi0, t0, s0,
+                        tr0, tke, cldfrct, concldfrct, pblh, cush, umf, slflx, qtflx, flxprc1, flxsnow1,
+                        qvten, qlten, qiten, sten, uten, vten, trten, qrten, qsten, precip, snow, evapc,
+                        cufrc, qcu, qlu, qiu, cbmf, qc, rliq, massflx_sh, cnt, cnb, dpdry0, wu, diag_int,
+                        diag_real, diag_level, nthreads, NULL);
+}
+
+/* compute_zwshcu (zwshcu.F90:630-644): compute_uwshcu's arguments plus the pressure velocity omega
+ * (mix, mkx) [Pa/s]; tpert2 is read only by the perturbation options, which are off here. */
+int uwo_compute_zwshcu(int mix, int mkx, int iend, int ncnst, double dt,
+                       const double *ps0, const double *zs0, const double *p0, const double *z0,
+                       const double *dp0, const double *u0, const double *v0, const double *qv0,
+                       const double *ql0, const double *qi0, const double *t0, const double *s0,
+                       const double *tr0, const double *tke, const double *cldfrct,
+                       const double *concldfrct, const double *pblh, double *cush,
+                       double *umf, double *slflx, double *qtflx, double *flxprc1, double *flxsnow1,
+                       double *qvten, double *qlten, double *qiten, double *sten, double *uten,
+                       double *vten, double *trten, double *qrten, double *qsten, double *precip,
+                       double *snow, double *evapc, double *cufrc, double *qcu, double *qlu,
+                       double *qiu, double *cbmf, double *qc, double *rliq, const double *omega,
+                       const double *massflx_sh, const double *tpert2, double *cnt, double *cnb,
+                       const double *dpdry0, double *wu, int *diag_int, double *diag_real,
+                       double *diag_level, int nthreads)
+{
+    (void)tpert2;
+    if (!omega) return -1;
+    return compute_core(mix, mkx, iend, ncnst, dt, ps0, zs0, p0, z0, dp0, u0, v0, qv0, ql0, qi0, t0, s0,
+                        tr0, tke, cldfrct, concldfrct, pblh, cush, umf, slflx, qtflx, flxprc1, flxsnow1,
+                        qvten, qlten, qiten, sten, uten, vten, trten, qrten, qsten, precip, snow, evapc,
+                        cufrc, qcu, qlu, qiu, cbmf, qc, rliq, massflx_sh, cnt, cnb, dpdry0, wu, diag_int,
+                        diag_real, diag_level, nthreads, omega);
+}
+
+/* The options of compute_zwshcu: zmh_shallow_lf, zmh_shallow_fwcrit, zmh_shallow_ent, zmh_ent0
+ * (zwshcu.F90:31-33, 58) and zmh_cloud_sh, zmh_ufrcd, zmh_ufrc0, zmh_ufrcz (cloud_fraction.F90:52,
+ * zwshcu.F90:37-39).  uwo_init sets the reference's defaults: 1, 1.0, 0, 0.015, 0, 2.0, 2.0, 2.0. */
+int uwo_set_zw_options(int lf, double fwcrit, int ent, double ent0, int cloud_sh, double ufrcd,
+                       double ufrc0, double ufrcz)
+{
+    S.zw_lf = lf != 0;
+    S.zw_fwcrit = fwcrit;
+    S.zw_ent = ent != 0;
+    S.zw_ent0 = ent0;
+    S.zw_cloud_sh = cloud_sh != 0;
+    S.zw_ufrcd = ufrcd;
+    S.zw_ufrc0 = ufrc0;
+    S.zw_ufrcz = ufrcz;
+    return 0;
 }
 
 int uwo_compute_uwshcu_inv(int mix, int mkx, int iend, int ncnst, double dt,

@@ -81,6 +81,31 @@ int uwo_compute_uwshcu(int mix, int mkx, int iend, int ncnst, double dt,
                        double *cnt, double *cnb, const double *dpdry0, double *wu,
                        int *diag_int, double *diag_real, double *diag_level, int nthreads);
 
+/* compute_zwshcu (zwshcu.F90:630-4969), the CAS-ESM variant of the scheme: compute_uwshcu's
+ * arguments plus the pressure velocity omega (mix, mkx) [Pa/s] (and tpert2, read only by the
+ * perturbation options, which are not restated); the options of uwo_set_zw_options apply. */
+int uwo_compute_zwshcu(int mix, int mkx, int iend, int ncnst, double dt,
+                       const double *ps0, const double *zs0, const double *p0, const double *z0,
+                       const double *dp0, const double *u0, const double *v0, const double *qv0,
+                       const double *ql0, const double *qi0, const double *t0, const double *s0,
+                       const double *tr0, const double *tke, const double *cldfrct,
+                       const double *concldfrct, const double *pblh, double *cush,
+                       double *umf, double *slflx, double *qtflx, double *flxprc1, double *flxsnow1,
+                       double *qvten, double *qlten, double *qiten, double *sten, double *uten,
+                       double *vten, double *trten, double *qrten, double *qsten, double *precip,
+                       double *snow, double *evapc, double *cufrc, double *qcu, double *qlu,
+                       double *qiu, double *cbmf, double *qc, double *rliq, const double *omega,
+                       const double *massflx_sh, const double *tpert2, double *cnt, double *cnb,
+                       const double *dpdry0, double *wu, int *diag_int, double *diag_real,
+                       double *diag_level, int nthreads);
+
+/* Options of compute_zwshcu (zwshcu.F90:30-59, cloud_fraction.F90:52): large-scale forcing of the
+ * closure (zmh_shallow_lf), wcrit factor (zmh_shallow_fwcrit), buoyancy-based entrainment
+ * (zmh_shallow_ent, zmh_ent0), cloud-fraction enhancement (zmh_cloud_sh, zmh_ufrcd, zmh_ufrc0,
+ * zmh_ufrcz).  Defaults: 1, 1.0, 0, 0.015, 0, 2.0, 2.0, 2.0. */
+int uwo_set_zw_options(int lf, double fwcrit, int ent, double ent0, int cloud_sh, double ufrcd,
+                       double ufrc0, double ufrcz);
+
 /* compute_uwshcu_inv (uwshcu.F90:251-476): CAM top-down level order in and out. */
 int uwo_compute_uwshcu_inv(int mix, int mkx, int iend, int ncnst, double dt,
                            const double *ps0, const double *zs0, const double *p0, const double *z0,
