@@ -29,6 +29,10 @@ b = src[src.index(marker):]
 cut = b.index('// The fast-FP64 precision mode: same launch shapes as uwshcu_fp64_kernel.')
 b = b[:cut].rstrip() + '\n\n}  // namespace\n'
 b = b.replace('uwshcu_fp64_kernel', 'uwshcu_mixed_kernel')
+# the compute_zwshcu instantiation (ZW) is FP64 only: the mixed kernel is compute_uwshcu's
+b = b.replace('uw_column<KP, NC, MODE, 0, ZW>(A, tbl, i, active, wl, wl_count);',
+              'uw_column<KP, NC, MODE, 0>(A, tbl, i, active, wl, wl_count);')
+b = b.replace('template <int KP, int NC, int MODE, int ZW = 0>\n__global__', 'template <int KP, int NC, int MODE>\n__global__')
 b = b.replace('#define CONDEN(...) (FAST ? conden_fast(__VA_ARGS__) : conden(__VA_ARGS__))', '#define CONDEN(...) conden(__VA_ARGS__)')
 b = re.sub(r'\bdouble\b', 'R', b)
 lit = re.compile(r'(?<![\w.])((?:\d+\.\d*|\.\d+)(?:[eE][-+]?\d+)?|\d+[eE][-+]?\d+)(?![\w.f])')

@@ -83,6 +83,10 @@ def main():
     s = rep(s, "uwshcu_tl_kernel(const __grid_constant__ UwArgs A, int* __restrict__ wl, int* __restrict__ wl_count)",
             "uwshcu_tl_kernel(const __grid_constant__ UwArgs A, int* __restrict__ wl, int* __restrict__ wl_count,\n"
             "                 const __grid_constant__ UwTangent T)")
+    # the compute_zwshcu instantiation (ZW) is FP64 only: the tangent kernel is compute_uwshcu's
+    s = s.replace("uw_column<KP, NC, MODE, 0, ZW>(A, tbl, i, active, wl, wl_count);",
+                  "uw_column<KP, NC, MODE, 0>(A, tbl, i, active, wl, wl_count);")
+    s = s.replace("template <int KP, int NC, int MODE, int ZW = 0>\n__global__", "template <int KP, int NC, int MODE>\n__global__")
     s = rep(s, "uw_column<KP, NC, MODE, 0>(A, tbl, i, active, wl, wl_count);",
             "uw_column<KP, NC, MODE, 0>(A, tbl, i, active, wl, wl_count, T);")
     s = rep(s, "__launch_bounds__(128, UW_LIST_MINB(MODE))", "__launch_bounds__(128)")

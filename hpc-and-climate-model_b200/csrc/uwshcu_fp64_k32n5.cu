@@ -9,18 +9,26 @@ extern "C" cudaError_t uw_fp64_set_constants_k32n5(const UwConst* h, const doubl
     return cudaMemcpyToSymbol(c_estbl, tbl, sizeof(double) * UW_TBL);
 }
 
-// mode: UW_MODE_ALL, UW_MODE_TRIGGER, UW_MODE_LIST, UW_MODE_LIST1 or UW_MODE_RESUME; nthreads: columns (ALL/TRIGGER) or the
+// a->omega: compute_zwshcu's instantiations.  mode: UW_MODE_ALL, UW_MODE_TRIGGER, UW_MODE_LIST, UW_MODE_LIST1 or UW_MODE_RESUME; nthreads: columns (ALL/TRIGGER) or the
 // worklist capacity (LIST).
 extern "C" cudaError_t uw_fp64_launch_k32n5(const UwArgs* a, int mode, int* wl, int* wl_count,
                                                      int nthreads, int block, cudaStream_t stream)
 {
     if (nthreads <= 0) return cudaSuccess;
     dim3 grid((unsigned)((nthreads + block - 1) / block));
-    if (mode == UW_MODE_ALL) uwshcu_fp64_kernel<32, 5, UW_MODE_ALL><<<grid, block, 0, stream>>>(*a, wl, wl_count);
-    else if (mode == UW_MODE_TRIGGER) uwshcu_fp64_kernel<32, 5, UW_MODE_TRIGGER><<<grid, block, 0, stream>>>(*a, wl, wl_count);
-    else if (mode == UW_MODE_LIST1) uwshcu_fp64_kernel<32, 5, UW_MODE_LIST1><<<grid, block, 0, stream>>>(*a, wl, wl_count);
-    else if (mode == UW_MODE_RESUME) uwshcu_fp64_kernel<32, 5, UW_MODE_RESUME><<<grid, block, 0, stream>>>(*a, wl, wl_count);
-    else uwshcu_fp64_kernel<32, 5, UW_MODE_LIST><<<grid, block, 0, stream>>>(*a, wl, wl_count);
+    if (a->omega) {   // compute_zwshcu
+        if (mode == UW_MODE_ALL) uwshcu_fp64_kernel<32, 5, UW_MODE_ALL, 1><<<grid, block, 0, stream>>>(*a, wl, wl_count);
+        else if (mode == UW_MODE_TRIGGER) uwshcu_fp64_kernel<32, 5, UW_MODE_TRIGGER, 1><<<grid, block, 0, stream>>>(*a, wl, wl_count);
+        else if (mode == UW_MODE_LIST1) uwshcu_fp64_kernel<32, 5, UW_MODE_LIST1, 1><<<grid, block, 0, stream>>>(*a, wl, wl_count);
+        else if (mode == UW_MODE_RESUME) uwshcu_fp64_kernel<32, 5, UW_MODE_RESUME, 1><<<grid, block, 0, stream>>>(*a, wl, wl_count);
+        else uwshcu_fp64_kernel<32, 5, UW_MODE_LIST, 1><<<grid, block, 0, stream>>>(*a, wl, wl_count);
+    } else {
+        if (mode == UW_MODE_ALL) uwshcu_fp64_kernel<32, 5, UW_MODE_ALL><<<grid, block, 0, stream>>>(*a, wl, wl_count);
+        else if (mode == UW_MODE_TRIGGER) uwshcu_fp64_kernel<32, 5, UW_MODE_TRIGGER><<<grid, block, 0, stream>>>(*a, wl, wl_count);
+        else if (mode == UW_MODE_LIST1) uwshcu_fp64_kernel<32, 5, UW_MODE_LIST1><<<grid, block, 0, stream>>>(*a, wl, wl_count);
+        else if (mode == UW_MODE_RESUME) uwshcu_fp64_kernel<32, 5, UW_MODE_RESUME><<<grid, block, 0, stream>>>(*a, wl, wl_count);
+        else uwshcu_fp64_kernel<32, 5, UW_MODE_LIST><<<grid, block, 0, stream>>>(*a, wl, wl_count);
+    }
     return cudaGetLastError();
 }
 

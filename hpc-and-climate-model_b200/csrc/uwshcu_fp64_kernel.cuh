@@ -482,7 +482,9 @@ namespace {
 // All 32 lanes of the warp must call it together (it starts with a warp ballot).  `tbl` is the saturation table in shared memory.  In
 // UW_MODE_TRIGGER, convecting columns are appended to wl / *wl_count.
 // FAST = 1: the fast-FP64 precision mode (conden_fast in place of conden), not bit-exact.
-template <int KP, int NC, int MODE, int FAST>
+// ZW = 1: compute_zwshcu (zwshcu.F90), which reads A.omega and the zw_* options; compiled out of the
+// compute_uwshcu instantiations.
+template <int KP, int NC, int MODE, int FAST, int ZW = 0>
 __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restrict__ tbl, const int i_in,
                                           const bool active, int* __restrict__ wl, int* __restrict__ wl_count)
 {
@@ -1066,7 +1068,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
             // the PBL top (zwshcu.F90:2276, 2295-2303); the same value of rho0inv for both schemes
             double rho0inv = ps0[kinv - 1] / (r * thv0top[kinv - 1] * exns0[kinv - 1]);
             double sigmaw = sqrt(rkfre * tkeavg + epsvarw);
-            if (A.omega) {
+            if constexpr (ZW) {
                 if (c.zw_lf) {
                     const double tmp1 = MN(MX(-GL(omega, kinv - 1), 0.0), 3.0);
                     wcrit = wcrit - tmp1 / rho0inv / 9.8;
@@ -1291,7 +1293,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                         fer[k] = rei[k] * ee2;
                         fdr[k] = rei[k] * ud2;
                         // compute_zwshcu's entrainment option (zwshcu.F90:2818-2844)
-                        if (A.omega && c.zw_ent) {
+                        if (ZW && c.zw_ent) {
                             bogbot = rbuoy * (thvu[km1] / thvebot - 1.0) * g;
                             fer[k] = c.zw_ent0 * bogbot / MX(wue * wue, 1.0e-4);
                             double fer_min = 0.0;
@@ -1956,7 +1958,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                 qiu[k] = 0.5 * (qiubelow + qij);
                 // compute_zwshcu's cloud-fraction option (zwshcu.F90:4415-4431, 4448)
                 double zw_tmp2 = 0.0, zw_tmp3 = 1.0;
-                if (A.omega && c.zw_cloud_sh) {
+                if (ZW && c.zw_cloud_sh) {
                     zw_tmp3 = 0.5 * c.zw_ufrc0;
                     double tmp1 = (GL(z0, k) - GL(z0, krel)) / (GL(z0, kpen) - GL(z0, krel) + 10.0);
                     tmp1 = 1.0 + c.zw_ufrcz * tmp1;
@@ -1975,7 +1977,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                         qiu[k] = 0.5 * (qiubelow + criqc * qij / (qlj + qij));
                     }
                 }
-                if (A.omega) cufrc[k] = zw_tmp3 * cufrc[k] + zw_tmp2;
+                if constexpr (ZW) cufrc[k] = zw_tmp3 * cufrc[k] + zw_tmp2;
                 qcubelow = qlj + qij;
                 qlubelow = qlj;
                 qiubelow = qij;
@@ -2189,7 +2191,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
 // UW_MODE_LIST1), the UW_MODE_RESUME launch, which spills less, at 102 (5 blocks: -3.3 % step
 // time against 4, +2.8 % at 6), the trigger pass at 102, the single pass at 168.
 #define UW_LIST_MINB(m) ((m) == UW_MODE_RESUME ? 5 : (UW_MODE_IS_LIST(m) ? 4 : ((m) == UW_MODE_TRIGGER ? 5 : 3)))
-template <int KP, int NC, int MODE>
+template <int KP, int NC, int MODE, int ZW = 0>
 __global__ void __launch_bounds__(128, UW_LIST_MINB(MODE))
 uwshcu_fp64_kernel(const __grid_constant__ UwArgs A, int* __restrict__ wl, int* __restrict__ wl_count)
 {
@@ -2211,7 +2213,7 @@ uwshcu_fp64_kernel(const __grid_constant__ UwArgs A, int* __restrict__ wl, int* 
         active = tid < A.iend;
         i = tid;
     }
-    uw_column<KP, NC, MODE, 0>(A, tbl, i, active, wl, wl_count);
+    uw_column<KP, NC, MODE, 0, ZW>(A, tbl, i, active, wl, wl_count);
 }
 
 // Batched trigger pass: every column of every member of B (members of one level/tracer class).

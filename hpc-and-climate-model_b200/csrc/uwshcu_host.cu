@@ -572,6 +572,7 @@ int host_call(int inv, int mix, int mkx, int iend, int ncnst, double dt, const d
     std::lock_guard<std::mutex> lock(s.mu);
     if (!s.init) return UWSHCU_ERR_NOT_INITIALIZED;
     if (bad_dims(mix, mkx, iend, ncnst)) return UWSHCU_ERR_BAD_ARGS;
+    if (omega && s.precision != UWSHCU_PREC_FP64) return UWSHCU_ERR_BAD_ARGS;   // compute_zwshcu: FP64
     const void* need[] = {ps0, zs0, p0, z0, dp0, u0, v0, qv0, ql0, qi0, t0, s0, tr0, tke, pblh, cush,
                           umf, slflx, qtflx, flxprc1, flxsnow1, qvten, qlten, qiten, sten, uten, vten,
                           trten, qrten, qsten, precip, snow, evapc, cufrc, qcu, qlu, qiu, cbmf, qc, rliq,
@@ -1351,6 +1352,7 @@ int compute_zwshcu_device(int mix, int mkx, int iend, int ncnst, double dt, int 
     std::lock_guard<std::mutex> lock(s.mu);
     if (!s.init) return UWSHCU_ERR_NOT_INITIALIZED;
     if (bad_dims(mix, mkx, iend, ncnst) || (inv != 0 && inv != 1)) return UWSHCU_ERR_BAD_ARGS;
+    if (s.precision != UWSHCU_PREC_FP64) return UWSHCU_ERR_BAD_ARGS;   // compute_zwshcu: FP64 only
     const void* need[] = {ps0, zs0, p0, z0, dp0, u0, v0, qv0, ql0, qi0, t0, s0, tr0, tke, pblh, omega, cush,
                           umf, slflx, qtflx, flxprc1, flxsnow1, qvten, qlten, qiten, sten, uten, vten,
                           trten, qrten, qsten, precip, snow, evapc, cufrc, qcu, qlu, qiu, cbmf, qc, rliq,

@@ -447,7 +447,9 @@ namespace {
 // All 32 lanes of the warp must call it together (it starts with a warp ballot).  `tbl` is the saturation table in shared memory.  In
 // UW_MODE_TRIGGER, convecting columns are appended to wl / *wl_count.
 // FAST = 1: the fast-FP64 precision mode (conden_fast in place of conden), not bit-exact.
-template <int KP, int NC, int MODE, int FAST>
+// ZW = 1: compute_zwshcu (zwshcu.F90), which reads A.omega and the zw_* options; compiled out of the
+// compute_uwshcu instantiations.
+template <int KP, int NC, int MODE, int FAST, int ZW = 0>
 __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restrict__ tbld, const float* __restrict__ tblf, const int i_in,
                                           const bool active, int* __restrict__ wl, int* __restrict__ wl_count)
 {
@@ -1034,7 +1036,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
             // the PBL top (zwshcu.F90:2276, 2295-2303); the same value of rho0inv for both schemes
             R rho0inv = ps0[kinv - 1] / (r * thv0top[kinv - 1] * exns0[kinv - 1]);
             R sigmaw = sqrtf(rkfre * tkeavg + epsvarw);
-            if (A.omega) {
+            if constexpr (ZW) {
                 if (c.zw_lf) {
                     const R tmp1 = MN(MX(-GL(omega, kinv - 1), 0.0f), 3.0f);
                     wcrit = wcrit - tmp1 / rho0inv / 9.8f;
@@ -1259,7 +1261,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                         fer[k] = rei[k] * ee2;
                         fdr[k] = rei[k] * ud2;
                         // compute_zwshcu's entrainment option (zwshcu.F90:2818-2844)
-                        if (A.omega && c.zw_ent) {
+                        if (ZW && c.zw_ent) {
                             bogbot = rbuoy * (thvu[km1] / thvebot - 1.0f) * g;
                             fer[k] = c.zw_ent0 * bogbot / MX(wue * wue, 1.0e-4f);
                             R fer_min = 0.0f;
@@ -1928,7 +1930,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                 qiu[k] = 0.5f * (qiubelow + qij);
                 // compute_zwshcu's cloud-fraction option (zwshcu.F90:4415-4431, 4448)
                 R zw_tmp2 = 0.0f, zw_tmp3 = 1.0f;
-                if (A.omega && c.zw_cloud_sh) {
+                if (ZW && c.zw_cloud_sh) {
                     zw_tmp3 = 0.5f * c.zw_ufrc0;
                     R tmp1 = (GL(z0, k) - GL(z0, krel)) / (GL(z0, kpen) - GL(z0, krel) + 10.0f);
                     tmp1 = 1.0f + c.zw_ufrcz * tmp1;
@@ -1947,7 +1949,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                         qiu[k] = 0.5f * (qiubelow + criqc * qij / (qlj + qij));
                     }
                 }
-                if (A.omega) cufrc[k] = zw_tmp3 * cufrc[k] + zw_tmp2;
+                if constexpr (ZW) cufrc[k] = zw_tmp3 * cufrc[k] + zw_tmp2;
                 qcubelow = qlj + qij;
                 qlubelow = qlj;
                 qiubelow = qij;
