@@ -18,6 +18,8 @@ call over all columns.  Metric: columns per second.
           the fast-FP64 mode.
   adjoint: the adjoint model against the forward pass on 65,536 x 30 columns (cost ratio, tape).
   batched: the batched uneven workload (4 x 262,144 columns, 30/35/51/30 levels) as one plan.
+  zwshcu: compute_zwshcu (zwshcu.F90, the CAS-ESM variant) on the same columns with a synthetic
+          large-scale pressure velocity.
   parity: the FP64 path on the 259,200 x 30 grid (720 x 360) against the oracle builds: decision
           agreement and the fraction of columns within 1e-11 on every output.
   --impl reference : the reference algorithm's CPU implementation (the C restatement in
@@ -351,6 +353,39 @@ def precision_leg(uw, case, stream, steps, warmup, fp64_ms, mode):
             "speedup_vs_fp64": fp64_ms / ms, "column_rel_rms_vs_fp64": err,
             "column_rel_rms_vs_fp64_same_decisions": err_kept, "columns_with_same_decisions": same,
             "flips": flips, "targets": "north_star (mixed): >= 2x the FP64 path at <= 1e-4 relative RMS"}
+
+
+def zwshcu_leg(uw, case, s, stream, steps, warmup):
+    """compute_zwshcu (zwshcu.F90), the CAS-ESM variant, on the columns of `case` with a synthetic
+    large-scale pressure velocity (soundings.make_omega): FP64 columns/s and the trigger fraction.
+    Leaves the compute_uwshcu outputs in `case` again."""
+    import torch
+    import soundings
+    om = torch.from_numpy(soundings.make_omega(s, seed=1)).cuda()
+
+    def step(omega):
+        case.out["cush"].copy_(case.cush0, non_blocking=True)
+        rc = case.launch(stream=stream, omega=omega)
+        if rc != 0:
+            raise RuntimeError("compute_zwshcu_device: %d %s" % (rc, uw.last_cuda_error()))
+
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            step(om)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            step(om)
+        e1.record(stream)
+        trig = float((case.out["cush"] != -1.0).double().mean())
+        step(None)
+    stream.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    return {"value": case.n / (ms * 1e-3), "unit": "columns/s", "ms_per_step": ms, "steps": steps,
+            "trigger_fraction": trig,
+            "workload": "the same columns with omega = omega0 sin(pi (ps - p) / (ps - 10 kPa)), "
+                        "omega0 ~ N(-0.05, 0.3) Pa/s (soundings.make_omega, seed 1); the variant's "
+                        "default options (large-scale forcing on)"}
 
 
 def adjoint_leg(uw, steps, warmup, n=65_536):
@@ -827,10 +862,11 @@ def main():
                "field_rel_rms_max": max(v["rel_rms"] for v in rep["fields"].values())}
 
     extras = rank == 0 and world == 1 and not args.no_extras and prec == uw.PREC_FP64
-    mixed = fast = adjoint = batched = None
+    mixed = fast = adjoint = batched = zw = None
     if extras:
         mixed = precision_leg(uw, case, stream, args.steps, max(args.warmup, 3), ms, uw.PREC_MIXED)
         fast = precision_leg(uw, case, stream, args.steps, max(args.warmup, 3), ms, uw.PREC_FAST)
+        zw = zwshcu_leg(uw, case, s, stream, args.steps, max(args.warmup, 3))
     if extras or (rank == 0 and world == 1 and not args.no_cpu_baseline):
         # free the large workload before the grid run, the adjoint buffer and the oracle
         del case
@@ -915,6 +951,8 @@ def main():
         line["adjoint"] = adjoint
     if batched is not None:
         line["batched"] = batched
+    if zw is not None:
+        line["zwshcu"] = zw
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base, parity = cpu_baseline_leg(grid_s, grid_out)
         parity["gpu_status"] = [int(grid_rc), int(grid_st)]

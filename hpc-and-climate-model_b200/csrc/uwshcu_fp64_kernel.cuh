@@ -1065,7 +1065,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
         {
             double wcrit = sqrt(2.0 * cin * rbuoy);
             // compute_zwshcu computes rho0inv first and lowers wcrit by the large-scale ascent at
-            // the PBL top (zwshcu.F90:2276, 2295-2303); the same value of rho0inv for both schemes
+            // the PBL top (zwshcu.F90:2277, 2295-2303); the same value of rho0inv for both schemes
             double rho0inv = ps0[kinv - 1] / (r * thv0top[kinv - 1] * exns0[kinv - 1]);
             double sigmaw = sqrt(rkfre * tkeavg + epsvarw);
             if constexpr (ZW) {
@@ -1956,7 +1956,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                 qcu[k] = 0.5 * (qcubelow + qlj + qij);
                 qlu[k] = 0.5 * (qlubelow + qlj);
                 qiu[k] = 0.5 * (qiubelow + qij);
-                // compute_zwshcu's cloud-fraction option (zwshcu.F90:4415-4431, 4448)
+                // compute_zwshcu's cloud-fraction option (zwshcu.F90:4413-4431, 4449)
                 double zw_tmp2 = 0.0, zw_tmp3 = 1.0;
                 if (ZW && c.zw_cloud_sh) {
                     zw_tmp3 = 0.5 * c.zw_ufrc0;

@@ -844,7 +844,7 @@ int uwshcu_init(double xlv, double cp, double xlf, double zvir, double r, double
     k.rle = s.init ? s.k.rle : 0.1;       // uwshcu.F90:1036
     k.rkm = s.init ? s.k.rkm : 14.0;      // uwshcu.F90:1038
     k.criqc = s.init ? s.k.criqc : 0.7e-3; // uwshcu.F90:1065
-    // compute_zwshcu options (zwshcu.F90:31-39, 58; cloud_fraction.F90:52): the reference's defaults
+    // compute_zwshcu options (zwshcu.F90:30-57; cloud_fraction.F90:52): the reference's defaults
     k.zw_lf = s.init ? s.k.zw_lf : 1;
     k.zw_fwcrit = s.init ? s.k.zw_fwcrit : 1.0;
     k.zw_ent = s.init ? s.k.zw_ent : 0;

@@ -1033,7 +1033,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
         {
             R wcrit = sqrtf(2.0f * cin * rbuoy);
             // compute_zwshcu computes rho0inv first and lowers wcrit by the large-scale ascent at
-            // the PBL top (zwshcu.F90:2276, 2295-2303); the same value of rho0inv for both schemes
+            // the PBL top (zwshcu.F90:2277, 2295-2303); the same value of rho0inv for both schemes
             R rho0inv = ps0[kinv - 1] / (r * thv0top[kinv - 1] * exns0[kinv - 1]);
             R sigmaw = sqrtf(rkfre * tkeavg + epsvarw);
             if constexpr (ZW) {
@@ -1928,7 +1928,7 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
                 qcu[k] = 0.5f * (qcubelow + qlj + qij);
                 qlu[k] = 0.5f * (qlubelow + qlj);
                 qiu[k] = 0.5f * (qiubelow + qij);
-                // compute_zwshcu's cloud-fraction option (zwshcu.F90:4415-4431, 4448)
+                // compute_zwshcu's cloud-fraction option (zwshcu.F90:4413-4431, 4449)
                 R zw_tmp2 = 0.0f, zw_tmp3 = 1.0f;
                 if (ZW && c.zw_cloud_sh) {
                     zw_tmp3 = 0.5f * c.zw_ufrc0;

@@ -205,10 +205,10 @@ int bxcompute_uwshcu_inv_(const int *pcols, const int *pver, const int *ncol, co
  * and cnt_out.  Same column code as compute_uwshcu_ plus the variant's options (uwshcu_set_zw_options):
  * with zmh_shallow_lf the closure lowers wcrit by min(max(-omega, 0), 3) / rho0inv / 9.8 at the
  * PBL-top layer (zwshcu.F90:2295-2303), and the optional buoyancy-based entrainment
- * (zwshcu.F90:2818-2844) and cloud-fraction enhancement (zwshcu.F90:4415-4448).  tpert2 is read by the
+ * (zwshcu.F90:2818-2844) and cloud-fraction enhancement (zwshcu.F90:4413-4449).  tpert2 is read by the
  * perturbation options only, which are not built (off in the reference).  rpen and rkm keep the values
  * of uwshcu_set_params (the variant's namelist defaults are rpen = 15, rkm = 10,
- * zwshcu.F90:45-46).  omega = 0 everywhere gives compute_uwshcu_'s results bit for bit.  FP64
+ * zwshcu.F90:43-44).  omega = 0 everywhere gives compute_uwshcu_'s results bit for bit.  FP64
  * precision setting only (UWSHCU_ERR_BAD_ARGS otherwise). */
 int compute_zwshcu_(const int *mix, const int *mkx, const int *iend, const int *ncnst,
                     const double *dt, const double *ps0_in, const double *zs0_in,

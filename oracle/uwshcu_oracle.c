@@ -1250,7 +1250,7 @@ static int uw_column(const uwo_io *A, int i)
             prel = plcl;
             thv0rel = thv0lcl;
         }
-        /* Closure (:2092-2184); compute_zwshcu computes rho0inv first (zwshcu.F90:2276) and lowers
+        /* Closure (:2092-2184); compute_zwshcu computes rho0inv first (zwshcu.F90:2277) and lowers
          * wcrit by the large-scale ascent at the PBL top (zwshcu.F90:2295-2303) */
         wcrit = sqrt(2.0 * cin * rbuoy);
         rho0inv = ps0[kinv - 1] / (r * thv0top[kinv - 1] * exns0[kinv - 1]);
@@ -2048,7 +2048,7 @@ static int uw_column(const uwo_io *A, int i)
                 qcu[k] = 0.5 * (qcubelow + qlj + qij);
                 qlu[k] = 0.5 * (qlubelow + qlj);
                 qiu[k] = 0.5 * (qiubelow + qij);
-                /* compute_zwshcu's cloud-fraction option (zwshcu.F90:4415-4431) */
+                /* compute_zwshcu's cloud-fraction option (zwshcu.F90:4413-4431) */
                 zw_tmp2 = 0.0;
                 zw_tmp3 = 1.0;
                 if (A->omega && S.zw_cloud_sh) {
@@ -2071,7 +2071,7 @@ static int uw_column(const uwo_io *A, int i)
                         qiu[k] = 0.5 * (qiubelow + criqc * qij / (qlj + qij));
                     }
                 }
-                if (A->omega) cufrc[k] = zw_tmp3 * cufrc[k] + zw_tmp2;   /* zwshcu.F90:4448 */
+                if (A->omega) cufrc[k] = zw_tmp3 * cufrc[k] + zw_tmp2;   /* zwshcu.F90:4449 */
                 qcubelow = qlj + qij;
                 qlubelow = qlj;
                 qiubelow = qij;
@@ -2491,8 +2491,8 @@ int uwo_compute_zwshcu(int mix, int mkx, int iend, int ncnst, double dt,
 }
 
 /* The options of compute_zwshcu: zmh_shallow_lf, zmh_shallow_fwcrit, zmh_shallow_ent, zmh_ent0
- * (zwshcu.F90:31-33, 58) and zmh_cloud_sh, zmh_ufrcd, zmh_ufrc0, zmh_ufrcz (cloud_fraction.F90:52,
- * zwshcu.F90:37-39).  uwo_init sets the reference's defaults: 1, 1.0, 0, 0.015, 0, 2.0, 2.0, 2.0. */
+ * (zwshcu.F90:30-32, 57) and zmh_cloud_sh, zmh_ufrcd, zmh_ufrc0, zmh_ufrcz (cloud_fraction.F90:52,
+ * zwshcu.F90:36-38).  uwo_init sets the reference's defaults: 1, 1.0, 0, 0.015, 0, 2.0, 2.0, 2.0. */
 int uwo_set_zw_options(int lf, double fwcrit, int ent, double ent0, int cloud_sh, double ufrcd,
                        double ufrc0, double ufrcz)
 {
