@@ -414,8 +414,8 @@ def adjoint_leg(uw, steps, warmup, n=65_536):
         e1.synchronize()
         return e0.elapsed_time(e1) / k
 
-    def adjoint():
-        rc, _ = uw.adjoint_launch(case, cot, stream=stream)
+    def adjoint(defect=False):
+        rc, _ = uw.adjoint_launch(case, cot, stream=stream, defect=defect)
         if rc != 0:
             raise RuntimeError("adjoint: %d %s" % (rc, uw.last_cuda_error()))
 
@@ -423,12 +423,13 @@ def adjoint_leg(uw, steps, warmup, n=65_536):
     ka = max(1, min(steps, 5))
     adj = timed(adjoint, ka)
     rows = uw.adjoint_last_records()
+    checked = timed(lambda: adjoint(True), ka)
     conv = int((case.out["cush"] != -1.0).sum())
     uw.adjoint_release()
     del case, cot
     torch.cuda.empty_cache()
     return {"value": adj / fwd, "unit": "adjoint ms / forward ms", "forward_ms": fwd,
-            "adjoint_ms": adj, "steps": ka, "workload": "%s columns x 30 levels (seed 301)" % f"{n:,}",
+            "adjoint_ms": adj, "checked_adjoint_ms": checked, "steps": ka, "workload": "%s columns x 30 levels (seed 301)" % f"{n:,}",
             "convecting_columns": conv, "tape_rows_per_warp": rows,
             "tape_bytes_per_convecting_column": rows * 32,
             "target": "north_star: <= 4x the forward"}

@@ -76,9 +76,24 @@ __global__ void __launch_bounds__(UW_ADJ_BLOCK) uwshcu_adj_forward(const __grid_
     }
 }
 
+// Fraction r in [1/2, 7/8) for the n-th seed of column i (a hash of both): the split sweeps seed
+// RN(r w) and w - RN(r w), whose sum is w exactly (Sterbenz: RN(r w) lies in [w/2, w]).
+__device__ __forceinline__ double uw_adj_split_frac(unsigned i, unsigned n)
+{
+    unsigned h = i * 0x9E3779B1u ^ (n + 0x7F4A7C15u) * 0x85EBCA77u;
+    h ^= h >> 15;
+    h *= 0x2C1B3C6Du;
+    h ^= h >> 12;
+    h *= 0x297A2D39u;
+    h ^= h >> 15;
+    return 0.5 + 0.375 * (double)(h >> 8) * 0x1p-24;
+}
+
 // Reverse sweep: warp w seeds the indices of its lanes' output-index tables with the cotangents of C,
 // sweeps its tape (uw_adj_sweep) and writes the gradients of its columns.  The adjoints of warp w are
-// zero on entry.
+// zero on entry.  G.split 1 and 2 seed the two parts of a split of every cotangent (uw_adj_split_frac)
+// and store the gradients in G.gsave instead of C; a G.split 0 sweep after them writes, with the
+// gradients, the column's defect of linearity under that split to G.defect.
 template <int KP, int NC>
 __global__ void __launch_bounds__(UW_ADJ_RBLOCK) uwshcu_adj_reverse(const __grid_constant__ UwArgs A,
                                                                     const __grid_constant__ UwAdj G,
@@ -107,10 +122,16 @@ __global__ void __launch_bounds__(UW_ADJ_RBLOCK) uwshcu_adj_reverse(const __grid
 #define SEED_AT(id, w)                                                                                    \
     {                                                                                                     \
         const int id_ = (id), ix_ = id_ & ~AD_NEG;                                                        \
-        if (id_ >= 0 && ix_ < nin + rows) atomicAdd(&af[(size_t)ix_ * 32 + lane], (id_ & AD_NEG) ? -(w) : (w)); \
+        double w_ = (w);                                                                                  \
+        if (G.split) {                                                                                    \
+            const double p_ = uw_adj_split_frac((unsigned)i, nseed++) * w_;                               \
+            w_ = G.split == 1 ? p_ : w_ - p_;                                                             \
+        }                                                                                                 \
+        if (id_ >= 0 && ix_ < nin + rows) atomicAdd(&af[(size_t)ix_ * 32 + lane], (id_ & AD_NEG) ? -w_ : w_); \
     }
 #define SEED(f, k, row)                                                                                   \
     if (C.f) SEED_AT(AID(UW_AO_##f, k), C.f[(size_t)(row) * mix + i])
+    unsigned nseed = 0;
     if (active) {
         for (int k = 0; k <= mkx; k++) {
             SEED(umf, k, RI(k)) SEED(slflx, k, RI(k)) SEED(qtflx, k, RI(k)) SEED(flxprc1, k, RI(k))
@@ -132,6 +153,29 @@ __global__ void __launch_bounds__(UW_ADJ_RBLOCK) uwshcu_adj_reverse(const __grid
                  stage[threadIdx.x >> 5]);
     if (!active) return;
 #define GR(x) __ldcg(&af[(size_t)(x) * 32 + lane])
+#define GS(s, x) G.gsave[((size_t)(s) * nin + (x)) * G.cap + slot]
+    if (G.split) {
+        for (int x = 0; x < nin; x++) GS(G.split - 1, x) = GR(x);
+        return;
+    }
+    if (G.defect) {
+        // per gradient asked for (t0, qv0, tke, pblh, rpen, rle, rkm, criqc): max |g - g1 - g2| over
+        // max (|g1| + |g2|); the column's defect is the largest of them
+        const double* const want[8] = {C.t0, C.qv0, C.tke, C.pblh, C.rpen, C.rle, C.rkm, C.criqc};
+        double worst = 0.0;
+        for (int f = 0; f < 8; f++) {
+            if (!want[f]) continue;
+            const int x0 = f < 3 ? f * mkx : 3 * mkx + f - 2, x1 = f < 2 ? x0 + mkx : (f == 2 ? x0 + mkx + 1 : x0 + 1);
+            double num = 0.0, den = 0.0;
+            for (int x = x0; x < x1; x++) {
+                const double g1 = GS(0, x), g2 = GS(1, x);
+                num = MX(num, fabs(GR(x) - g1 - g2));
+                den = MX(den, fabs(g1) + fabs(g2));
+            }
+            if (den > 0.0) worst = MX(worst, num / den);
+        }
+        G.defect[i] = worst;
+    }
     for (int k = 1; k <= mkx; k++) {
         if (C.t0) C.t0[(size_t)RL(k) * mix + i] = GR(k - 1);
         if (C.qv0) C.qv0[(size_t)RL(k) * mix + i] = GR(mkx + k - 1);
@@ -143,6 +187,7 @@ __global__ void __launch_bounds__(UW_ADJ_RBLOCK) uwshcu_adj_reverse(const __grid
     if (C.rle) C.rle[i] = GR(3 * mkx + 3);
     if (C.rkm) C.rkm[i] = GR(3 * mkx + 4);
     if (C.criqc) C.criqc[i] = GR(3 * mkx + 5);
+#undef GS
 #undef GR
 #undef SEED
 #undef SEED_AT
@@ -239,6 +284,9 @@ def main():
                   "    double* adj;         // warp w's adjoints at adj + w * astride (index x of lane l at x * 32 + l)\n"
                   "    size_t astride;\n"
                   "    unsigned int* status;\n"
+                  "    int split;           // reverse sweep: 0 the cotangents, 1 and 2 the two parts of their split\n"
+                  "    double* gsave;       // gradients of split s at ((s - 1) * (3 mkx + 6) + x) * cap + slot\n"
+                  "    double* defect;      // per column (mix), written by a split-0 sweep; NULL: not computed\n"
                   "};\n" % len(ADJ_OUT), 1)
     s = rep(s, "const bool active, int* __restrict__ wl, int* __restrict__ wl_count)",
             "const bool active, int* __restrict__ wl, int* __restrict__ wl_count,\n"

@@ -25,6 +25,9 @@ static UwAdj to_dev(const UwAdjHost& h)
     g.adj = h.adj;
     g.astride = h.astride;
     g.status = h.status;
+    g.split = h.split;
+    g.gsave = h.gsave;
+    g.defect = h.defect;
     return g;
 }
 

@@ -141,6 +141,9 @@ struct UwAdjHost {
     double* adj;
     size_t astride;      // doubles of adjoints per warp
     unsigned int* status;
+    int split;           // reverse sweep: 0 the cotangents, 1 and 2 the two parts of their split
+    double* gsave;       // the split sweeps' gradients, 2 x (3 mkx + 6) x cap
+    double* defect;      // per column: defect of linearity under the split (NULL: not computed)
 };
 
 // Pointers of one compute_uwshcu call (device addresses), in the Fortran argument order.

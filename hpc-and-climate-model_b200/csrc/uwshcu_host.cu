@@ -1434,7 +1434,10 @@ int uwshcu_tangent_device(const uwshcu_member* m, const uwshcu_tangent* t, void*
 // convecting 30-level columns takes ~1.3e5 rows, of 51-level columns about twice that.
 constexpr int kAdjRows32 = 1 << 18, kAdjRows64 = 1 << 19;
 
-int uwshcu_adjoint_device(const uwshcu_member* m, const uwshcu_adjoint* a, void* stream)
+// The adjoint call; with `defect` (device, mix) each batch runs the reverse sweep three times on its
+// tape: the two parts of a split of the cotangents (their gradients kept in the buffer), then the
+// cotangents themselves, whose sweep writes the gradients and the defect of linearity per column.
+static int adjoint_run(const uwshcu_member* m, const uwshcu_adjoint* a, double* defect, void* stream)
 {
     State& s = S();
     std::lock_guard<std::mutex> lock(s.mu);
@@ -1462,6 +1465,7 @@ int uwshcu_adjoint_device(const uwshcu_member* m, const uwshcu_adjoint* a, void*
                                                 {a->criqc, mix}};
     for (const auto& g : grads)
         if (g.first && (e = cudaMemsetAsync(g.first, 0, g.second * sizeof(double), st)) != cudaSuccess) return cuda_fail(e);
+    if (defect && (e = cudaMemsetAsync(defect, 0, mix * sizeof(double), st)) != cudaSuccess) return cuda_fail(e);
     if (m->iend == 0) return UWSHCU_OK;
     // trigger pass of the FP64 path: the exit columns' outputs and the worklist of the others
     if ((rc = grow_ints(sc->wl, sc->wl_cap, (size_t)m->iend + 1)) != UWSHCU_OK) return rc;
@@ -1496,7 +1500,9 @@ int uwshcu_adjoint_device(const uwshcu_member* m, const uwshcu_adjoint* a, void*
     for (size_t rcap = s.adj_rows > 0 ? std::min((size_t)s.adj_rows, (size_t)full_rows) : (size_t)full_rows;;
          restart = true) {
         const size_t astride = (nin + rcap) * 32;
-        const size_t per_warp = rcap * rowb + astride * sizeof(double) + 32 * nids * sizeof(int) + 2 * sizeof(int) + 1024;
+        const size_t nsave = defect ? 2 * nin : 0;   // the split sweeps' gradients, per slot
+        const size_t per_warp = rcap * rowb + astride * sizeof(double) + 32 * nids * sizeof(int) + 2 * sizeof(int) +
+                                32 * nsave * sizeof(double) + 1024;
         size_t freeb = 0, totalb = 0;
         if ((e = cudaMemGetInfo(&freeb, &totalb)) != cudaSuccess) return cuda_fail(e);
         const size_t avail = (freeb + d->adj_bytes) / 20 * 17;
@@ -1505,7 +1511,8 @@ int uwshcu_adjoint_device(const uwshcu_member* m, const uwshcu_adjoint* a, void*
         const size_t o_ab = 0, o_d = o_ab + up(nw * rcap * 32 * 8), o_adj = o_d + up(nw * rcap * 32 * 16);
         const size_t o_ids = o_adj + up(nw * astride * sizeof(double)), o_nrow = o_ids + up(nb * nids * sizeof(int));
         const size_t o_st = o_nrow + up(2 * nw * sizeof(int)), o_wl = o_st + 256, o_tmp = o_wl + up(ncand * sizeof(int));
-        const size_t o_cush = o_tmp + up(sort_bytes), bytes = o_cush + up((size_t)m->iend * sizeof(double));
+        const size_t o_cush = o_tmp + up(sort_bytes), o_gs = o_cush + up((size_t)m->iend * sizeof(double));
+        const size_t bytes = o_gs + up(nb * nsave * sizeof(double));
         // cush is read and written by the forward sweep: a call that starts again puts back the values
         // the trigger pass left (saved in the buffer before it may be replaced), then saves them anew
         if (restart && (e = cudaMemcpyAsync(m->cush, cush_saved, (size_t)m->iend * sizeof(double),
@@ -1551,13 +1558,20 @@ int uwshcu_adjoint_device(const uwshcu_member* m, const uwshcu_adjoint* a, void*
             h.adj = reinterpret_cast<double*>(base + o_adj);
             h.astride = astride;
             h.status = status;
+            h.gsave = reinterpret_cast<double*>(base + o_gs);
+            h.defect = defect;
             const size_t used = ((size_t)h.nb + 31) / 32;   // warps holding a slot
             if ((e = cudaMemsetAsync(h.ids, 0xff, nb * nids * sizeof(int), st)) != cudaSuccess ||
                 (e = adj_launch(&A, &h, a, 0, st)) != cudaSuccess)
                 return cuda_fail(e);
-            adj_zero_kernel<<<(unsigned)used, 512, 0, st>>>(h.adj, astride, nrow, (int)nin, (int)rcap);
-            if ((e = cudaGetLastError()) != cudaSuccess || (e = adj_launch(&A, &h, a, 1, st)) != cudaSuccess ||
-                (e = cudaMemcpyAsync(counts.data(), nrow, used * sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+            for (int split = defect ? 1 : 0;; split = (split + 1) % 3) {   // 1, 2, 0 or 0
+                h.split = split;
+                adj_zero_kernel<<<(unsigned)used, 512, 0, st>>>(h.adj, astride, nrow, (int)nin, (int)rcap);
+                if ((e = cudaGetLastError()) != cudaSuccess || (e = adj_launch(&A, &h, a, 1, st)) != cudaSuccess)
+                    return cuda_fail(e);
+                if (split == 0) break;
+            }
+            if ((e = cudaMemcpyAsync(counts.data(), nrow, used * sizeof(int), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
                 (e = cudaMemcpyAsync(&bits, status, sizeof(unsigned int), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
                 (e = cudaStreamSynchronize(st)) != cudaSuccess)
                 return cuda_fail(e);
@@ -1577,6 +1591,17 @@ int uwshcu_adjoint_device(const uwshcu_member* m, const uwshcu_adjoint* a, void*
         }
         return UWSHCU_OK;
     }
+}
+
+int uwshcu_adjoint_device(const uwshcu_member* m, const uwshcu_adjoint* a, void* stream)
+{
+    return adjoint_run(m, a, nullptr, stream);
+}
+
+int uwshcu_adjoint_device_checked(const uwshcu_member* m, const uwshcu_adjoint* a, double* defect, void* stream)
+{
+    if (!defect) return UWSHCU_ERR_BAD_ARGS;
+    return adjoint_run(m, a, defect, stream);
 }
 
 int uwshcu_set_adjoint_rows(int rows)

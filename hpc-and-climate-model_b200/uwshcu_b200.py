@@ -46,7 +46,8 @@ EXPORTS = ("uwshcu_init", "uwshcu_set_rpen", "uwshcu_init_default", "uwshcu_set_
            "uwshcu_batch_capture", "uwshcu_batch_autotune", "uwshcu_batch_status",
            "uwshcu_batch_destroy", "uwshcu_set_pipeline", "uwshcu_set_params",
            "uwshcu_budget_device", "uwshcu_tangent_device", "uwshcu_compute_member",
-           "uwshcu_set_hand_slots", "uwshcu_adjoint_device", "uwshcu_adjoint_last_records",
+           "uwshcu_set_hand_slots", "uwshcu_adjoint_device", "uwshcu_adjoint_device_checked",
+           "uwshcu_adjoint_last_records",
            "uwshcu_adjoint_release", "uwshcu_set_adjoint_rows", "compute_zwshcu_",
            "compute_zwshcu_inv_", "compute_zwshcu_device", "uwshcu_set_zw_options")
 
@@ -484,11 +485,13 @@ class Adjoint(ctypes.Structure):
     _fields_ = [(n, ctypes.c_void_p) for n in _TANGENT_OUT] + [(n, ctypes.c_void_p) for n in _ADJ_GRAD]
 
 
-def adjoint_launch(case, cot, inv=0, stream=None):
+def adjoint_launch(case, cot, inv=0, stream=None, defect=False):
     """One uwshcu_adjoint_device call on a DeviceCase: `cot` maps output names to device tensors
     shaped like case.out (the cotangents; missing ones are zero).  Returns (status, gradients): t0,
     qv0 (mkx, n), tke (mkx + 1, n), pblh (n) and the per-column parameter gradients rpen, rle, rkm,
-    criqc (n), as torch tensors; the case's own outputs get the FP64 values."""
+    criqc (n), as torch tensors; the case's own outputs get the FP64 values.  defect=True calls
+    uwshcu_adjoint_device_checked instead and adds the per-column defect of linearity (n) to the
+    gradients as "defect"."""
     import torch
     st = stream if stream is not None else torch.cuda.current_stream()
     dev = case.out["umf"].device
@@ -504,7 +507,13 @@ def adjoint_launch(case, cot, inv=0, stream=None):
     for k in _ADJ_GRAD:
         setattr(a, k, grads[k].data_ptr())
     m = member_of(case, inv)
-    rc = lib().uwshcu_adjoint_device(ctypes.byref(m), ctypes.byref(a), ctypes.c_void_p(st.cuda_stream))
+    if defect:
+        grads["defect"] = torch.full((n,), -1.0, dtype=torch.float64, device=dev)
+        rc = lib().uwshcu_adjoint_device_checked(ctypes.byref(m), ctypes.byref(a),
+                                                 ctypes.c_void_p(grads["defect"].data_ptr()),
+                                                 ctypes.c_void_p(st.cuda_stream))
+    else:
+        rc = lib().uwshcu_adjoint_device(ctypes.byref(m), ctypes.byref(a), ctypes.c_void_p(st.cuda_stream))
     return rc, grads
 
 

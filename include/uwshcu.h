@@ -436,6 +436,20 @@ typedef struct uwshcu_adjoint {
  * 2^18 rows (mkx + 1 <= 32) or 2^19 rows (33 .. 64 levels). */
 int uwshcu_adjoint_device(const uwshcu_member *m, const uwshcu_adjoint *a, void *stream);
 
+/* No counterpart in the reference.  uwshcu_adjoint_device (same outputs and gradients, bit for bit)
+ * that also writes, per column, how far rounding in the reverse sweep moved that column's gradients:
+ * the reverse sweep runs again on the same tape for the two parts w1, w2 of a split of the
+ * cotangents (w1 + w2 = w exactly, a fixed fraction in [1/2, 7/8) per cotangent), and
+ * defect[i] = the largest, over the gradients asked for (non-NULL in `a`), of
+ * max |g(w) - g(w1) - g(w2)| / max (|g(w1)| + |g(w2)|) over that gradient's entries of column i.
+ * The sweep is linear in w, so only rounding makes it non-zero: ~1e-16 .. 1e-14 on a well-
+ * conditioned column; a column whose intermediate adjoints cancel over many orders of magnitude
+ * shows its lost digits here (a gradient with defect 1e-6 has about 6 correct digits fewer than
+ * FP64's 16).  0 for the columns that leave the scheme in the trigger pass.  `defect`: device array
+ * (mix), not NULL.  Costs three reverse sweeps instead of one. */
+int uwshcu_adjoint_device_checked(const uwshcu_member *m, const uwshcu_adjoint *a, double *defect,
+                                  void *stream);
+
 /* Largest tape of the last uwshcu_adjoint_device call, in rows per warp of 32 columns (a sizing
  * aid). */
 int uwshcu_adjoint_last_records(void);

@@ -14,6 +14,11 @@ w = w1 + w2.  Every convecting column must satisfy |<w, TL d> - <ADJ w, d>| <= 1
 (the sum of the two defects), and the median column 1e-13.  The adjoint's forward sweep also
 reproduces the FP64 outputs bit for bit.  The tangent-linear model itself is checked against finite
 differences in test_gpu_tangent.py.
+
+uwshcu_adjoint_device_checked gives the same bits and, per column, the adjoint's defect of linearity
+under its own split of the cotangents (on the same tape): the median convecting column's defect is at
+rounding level, at most 1 % of the columns exceed 1e-8, and every column whose dot products disagree by
+more than 1e-7 of |terms| is among those.
 """
 import numpy as np
 import pytest
@@ -101,6 +106,23 @@ def test_adjoint_dot_product(uw, cuda, inv, pver):
     # the columns that leave the scheme in the trigger pass have zero gradients
     quiet = torch.from_numpy(want["cush"] == -1.0).to(grads["t0"].device)
     assert float(grads["t0"][:, quiet].abs().max()) == 0.0
+    # uwshcu_adjoint_device_checked: the same bits, and a defect per column that flags the columns
+    # whose dot products disagree
+    case_c = uw.DeviceCase(s, inputs=ref.inp)
+    rc, gc = uw.adjoint_launch(case_c, cot, inv=inv, defect=True)
+    assert rc == 0, (rc, uw.last_cuda_error())
+    assert all(torch.equal(gc[k], grads[k]) for k in grads)
+    got_c = case_c.outputs_numpy()
+    assert all(np.array_equal(want[k], got_c[k]) for k in want)
+    defect = gc["defect"]
+    assert bool(torch.isfinite(defect).all()) and float(defect.min()) >= 0.0
+    assert float(defect[quiet].abs().max()) == 0.0
+    dc = defect[conv].cpu().numpy()
+    assert np.median(dc) <= 1e-12, np.median(dc)
+    flagged = int((defect[conv] > 1e-8).sum())
+    assert flagged <= 0.01 * int(conv.sum()), flagged
+    unflagged_bad = torch.nonzero(conv & (err > 1e-7 * scl) & (defect <= 1e-8)).flatten().tolist()
+    assert not unflagged_bad, [(c, float(err[c] / scl[c]), float(defect[c])) for c in unflagged_bad[:8]]
 
 
 def test_adjoint_capacity_and_buffer_reuse(uw, cuda):
