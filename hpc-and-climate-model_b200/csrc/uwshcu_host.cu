@@ -187,6 +187,7 @@ struct State {
     int chunk_columns = 32768;   // host-array calls: columns per pipeline chunk (0: one chunk)
     int pipe_streams = 4;        // host-array calls: streams the chunks alternate over
     bool pipe_auto = true;       // until uwshcu_set_pipeline: the shape follows the call's size
+    bool pipe_ramp = true;       // the auto shape's smaller first and last chunks
     DeviceState dev[kMaxDev];
     char lasterr[256] = "";
 };
@@ -597,15 +598,44 @@ int host_call(int inv, int mix, int mkx, int iend, int ncnst, double dt, const d
     // Default shape: chunks of n/8 columns (32,768 .. 262,144, a multiple of 1,024), 4 streams up to
     // 65,536-column chunks and 2 above: enough convecting columns in flight to fill the GPU (a
     // chunk's worklist pass lasts as long as its deepest columns, whatever its size), few enough
-    // chunks for the copies to overlap.  Measured at 1,048,576 columns (page-locked arrays): 220 ms
-    // with 131,072 x 2 against 272 ms with 32,768 x 4; at 259,200 columns 32,768 x 4 is best.
+    // chunks for the copies to overlap.  Measured at 1,048,576 columns (page-locked arrays): 217 ms
+    // with 131,072 x 2 against 272 ms with 32,768 x 4, 210 ms with the ramped ends below; at
+    // 259,200 columns 32,768 x 4 is best.
     size_t csz = s.chunk_columns > 0 ? (size_t)s.chunk_columns : n;
     size_t nstreams = (size_t)s.pipe_streams;
     if (s.pipe_auto) {
         csz = std::min<size_t>(std::max<size_t>((n / 8 + 1023) / 1024 * 1024, 32768), 262144);
         nstreams = csz > 65536 ? 2 : 4;
     }
-    const size_t nch = (n + csz - 1) / csz;
+    // The chunks: [c0, c0 + nc).  The auto shape ramps at both ends (a quarter, then a half of the
+    // chunk size first and last, 32,768 columns at least): the first chunk's inputs are in, and the
+    // last chunk's outputs are out, sooner.
+    std::vector<std::pair<size_t, size_t>> chunks;
+    {
+        std::vector<size_t> head, tail;
+        size_t rest = n;
+        if (s.pipe_auto && s.pipe_ramp)
+            for (size_t f = 4; f >= 2; f /= 2) {
+                const size_t r = std::max<size_t>(csz / f, 32768);
+                if (r >= csz || rest < 2 * r + 2 * csz) break;
+                head.push_back(r);
+                tail.push_back(r);
+                rest -= 2 * r;
+            }
+        size_t c0 = 0;
+        auto put = [&](size_t nc) {
+            chunks.emplace_back(c0, nc);
+            c0 += nc;
+        };
+        for (size_t nc : head) put(nc);
+        for (size_t body = rest; body > 0;) {
+            const size_t nc = std::min(csz, body);
+            put(nc);
+            body -= nc;
+        }
+        for (size_t j = tail.size(); j-- > 0;) put(tail[j]);
+    }
+    const size_t nch = chunks.size();
     const size_t nin = per_in * n, nout = per_out * n;
     // Page-locked caller arrays: every plane goes straight between them and the device with a
     // strided copy (no host packing, no staging); otherwise through the pinned staging area.
@@ -651,7 +681,7 @@ int host_call(int inv, int mix, int mkx, int iend, int ncnst, double dt, const d
     std::vector<std::vector<Plane>> outs(nch);
     size_t base_in = 0, base_out = 0;
     for (size_t c = 0; c < nch; c++) {
-        const size_t c0 = c * csz, nc = std::min(csz, n - c0);
+        const size_t c0 = chunks[c].first, nc = chunks[c].second;
         double* hin = direct ? nullptr : d->h_buf + base_in;
         double* hout = direct ? nullptr : d->h_buf + nin + base_out;
         double* din = d->d_buf + base_in;

@@ -115,8 +115,11 @@ int uwshcu_profile_read(int *calls, double *trigger_ms, double *list_ms, int *li
  * of decreasing priority, so that copies in and out and the host-side packing overlap the
  * computation.  Results do not depend on it.  Default (and chunk_columns = -1, streams ignored):
  * the shape follows each call's size, chunks of iend/8 columns rounded up to 1,024 and clamped to
- * 32,768 .. 262,144, over 4 streams up to 65,536-column chunks and 2 streams above (page-locked
- * arrays: 259,200 columns in ~75 ms, 1,048,576 in ~220 ms against 272 ms with 32,768 x 4). */
+ * 32,768 .. 262,144, over 4 streams up to 65,536-column chunks and 2 streams above; where the call
+ * holds enough columns the first two and the last two chunks are a quarter and a half of that size
+ * (32,768 at least), so that the computation starts sooner and the last copy out is shorter
+ * (page-locked arrays: 259,200 columns in ~75 ms, 1,048,576 in ~210 ms against 217 ms with uniform
+ * 131,072-column chunks and 272 ms with 32,768 x 4). */
 int uwshcu_set_pipeline(int chunk_columns, int streams);
 
 /* Threads per block of the column kernel (0 = built-in default). */

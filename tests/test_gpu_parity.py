@@ -157,6 +157,23 @@ def test_pipelined_host_entries_match_one_chunk(uw, cuda):
 
 
 @pytest.mark.gpu
+def test_auto_pipeline_with_ramped_chunks_matches_one_chunk(uw, cuda):
+    """The default pipeline shape at 400,000 columns: chunks of 32,768, 32,768, 5 x 50,176, 18,048,
+    32,768 and 32,768 columns over 2 streams; the same bits as one chunk."""
+    s = soundings.make_soundings(400_000, 30, seed=62)
+    try:
+        assert uw.set_pipeline(0, 1) == 0
+        rc0, o0 = uw.compute_host(s)
+        assert uw.set_pipeline(-1, 0) == 0
+        rc, o = uw.compute_host(s)
+        assert rc == rc0 == 0
+        bad = [k for k in o0 if not np.array_equal(o[k], o0[k])]
+        assert not bad, bad
+    finally:
+        assert uw.set_pipeline(-1, 0) == 0
+
+
+@pytest.mark.gpu
 def test_tuning_parameters_match_oracle(uw, oracle_pm, cuda):
     """uwshcu_set_params (rpen, rle, rkm, criqc) against the oracle with the same values."""
     s = soundings.make_soundings(2048, 30, seed=81)
