@@ -187,7 +187,7 @@ struct State {
     int chunk_columns = 32768;   // host-array calls: columns per pipeline chunk (0: one chunk)
     int pipe_streams = 4;        // host-array calls: streams the chunks alternate over
     bool pipe_auto = true;       // until uwshcu_set_pipeline: the shape follows the call's size
-    bool pipe_ramp = true;       // the auto shape's smaller first and last chunks
+    bool pipe_ramp = true;       // smaller first and last chunks (the auto shape, chunk_columns < -1)
     DeviceState dev[kMaxDev];
     char lasterr[256] = "";
 };
@@ -614,7 +614,7 @@ int host_call(int inv, int mix, int mkx, int iend, int ncnst, double dt, const d
     {
         std::vector<size_t> head, tail;
         size_t rest = n;
-        if (s.pipe_auto && s.pipe_ramp)
+        if (s.pipe_ramp && csz < n)
             for (size_t f = 4; f >= 2; f /= 2) {
                 const size_t r = std::max<size_t>(csz / f, 32768);
                 if (r >= csz || rest < 2 * r + 2 * csz) break;
@@ -1029,10 +1029,13 @@ int uwshcu_set_pipeline(int chunk_columns, int streams)
     std::lock_guard<std::mutex> lock(s.mu);
     if (chunk_columns == -1) {   // back to the shape that follows each call's size
         s.pipe_auto = true;
+        s.pipe_ramp = true;
         return UWSHCU_OK;
     }
-    if (chunk_columns < 0 || streams < 1 || streams > DeviceState::kPipe) return UWSHCU_ERR_BAD_ARGS;
-    s.chunk_columns = chunk_columns;
+    if (streams < 1 || streams > DeviceState::kPipe) return UWSHCU_ERR_BAD_ARGS;
+    // below -1: chunks of -chunk_columns columns with the automatic shape's ramped ends
+    s.pipe_ramp = chunk_columns < -1;
+    s.chunk_columns = chunk_columns < -1 ? -chunk_columns : chunk_columns;
     s.pipe_streams = streams;
     s.pipe_auto = false;
     return UWSHCU_OK;

@@ -119,7 +119,8 @@ int uwshcu_profile_read(int *calls, double *trigger_ms, double *list_ms, int *li
  * holds enough columns the first two and the last two chunks are a quarter and a half of that size
  * (32,768 at least), so that the computation starts sooner and the last copy out is shorter
  * (page-locked arrays: 259,200 columns in ~75 ms, 1,048,576 in ~210 ms against 217 ms with uniform
- * 131,072-column chunks and 272 ms with 32,768 x 4). */
+ * 131,072-column chunks and 272 ms with 32,768 x 4).  chunk_columns < -1: chunks of -chunk_columns
+ * columns over `streams` streams with those ramped ends. */
 int uwshcu_set_pipeline(int chunk_columns, int streams);
 
 /* Threads per block of the column kernel (0 = built-in default). */
