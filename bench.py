@@ -343,6 +343,10 @@ def precision_leg(uw, case, stream, steps, warmup, fp64_ms, mode):
             a, b = q[k].double(), ref[k].double()
             err[k] = float(torch.sqrt(torch.mean((a - b) ** 2)) / torch.sqrt(torch.mean(b ** 2)))
             err_kept[k] = float(torch.sqrt(torch.mean((a[kept] - b[kept]) ** 2)) / torch.sqrt(torch.mean(b[kept] ** 2)))
+        import errstats
+        dist = errstats.distribution({k: q[k].double().cpu().numpy() for k in ("heating", "moistening", "precipitation")},
+                                     {k: ref[k].double().cpu().numpy() for k in ("heating", "moistening", "precipitation")},
+                                     (kept & ref["trigger"]).cpu().numpy())
         flips = {"trigger": int((q["trigger"] != ref["trigger"]).sum()),
                  "cloud_base": int((q["cnb"] != ref["cnb"]).sum()),
                  "cloud_top": int((q["cnt"] != ref["cnt"]).sum()),
@@ -352,6 +356,7 @@ def precision_leg(uw, case, stream, steps, warmup, fp64_ms, mode):
     return {"value": n / (ms * 1e-3), "unit": "columns/s", "ms_per_step": ms,
             "speedup_vs_fp64": fp64_ms / ms, "column_rel_rms_vs_fp64": err,
             "column_rel_rms_vs_fp64_same_decisions": err_kept, "columns_with_same_decisions": same,
+            "column_error_distribution": dist,
             "flips": flips, "targets": "north_star (mixed): >= 2x the FP64 path at <= 1e-4 relative RMS"}
 
 

@@ -6,8 +6,8 @@ column heating  H = sum_k sten(k) dp0(k) / g       (W m-2)
 column moistening M = sum_k qvten(k) dp0(k) / g     (kg m-2 s-1)
 precipitation     P = precip                        (m s-1)
 with the relative RMS  sqrt(mean((x - x64)^2)) / sqrt(mean(x64^2))  over all columns, the
-largest relative column error, and the count of columns whose trigger, cloud base or cloud top
-decision differs.
+largest relative column error, the count of columns whose trigger, cloud base or cloud top
+decision differs, and the distribution of the columns' errors behind the RMS.
 """
 import numpy as np
 
@@ -52,4 +52,27 @@ def report(out, ref, dp0):
                     "cloud_top": int(np.sum(out["cnt"] != ref["cnt"])),
                     "convecting_columns": int(np.sum(trig_b))}
     rep["worst_column_rel_rms"] = max(v["rel_rms"] for v in rep["column"].values())
+    same = ((trig_a == trig_b) & (np.asarray(out["cnb"]) == np.asarray(ref["cnb"])) &
+            (np.asarray(out["cnt"]) == np.asarray(ref["cnt"])))
+    rep["distribution"] = distribution(qa, qb, same & trig_b)
     return rep
+
+
+def distribution(qa, qb, sel):
+    """How the relative RMS of each column quantity is made: percentiles (50, 90, 99, 99.9) of the
+    columns' relative errors |x - x64| / max(|x64|, 1e-3 rms(x64)) over the columns in `sel` (the
+    convecting columns whose trigger, cloud base and cloud top are the FP64 path's), and the share
+    of the summed squared error that the worst 0.1 % and 1 % of all columns carry."""
+    res = {}
+    for k in qb:
+        a, b = np.asarray(qa[k], dtype=np.float64), np.asarray(qb[k], dtype=np.float64)
+        rms = float(np.sqrt(np.mean(np.square(b)))) or 1.0
+        rel = np.abs(a - b) / np.maximum(np.abs(b), 1e-3 * rms)
+        d2 = np.sort(np.square(a - b))[::-1]
+        tot = float(d2.sum())
+        n = d2.size
+        res[k] = {"rel_percentiles_same_decisions": [float(np.percentile(rel[sel], p)) if np.any(sel) else 0.0
+                                                     for p in (50, 90, 99, 99.9)],
+                  "sq_error_share_worst_0.1pct": float(d2[: max(1, n // 1000)].sum() / tot) if tot > 0 else 0.0,
+                  "sq_error_share_worst_1pct": float(d2[: max(1, n // 100)].sum() / tot) if tot > 0 else 0.0}
+    return res
