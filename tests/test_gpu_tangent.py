@@ -2,9 +2,10 @@
 
 Objective per column, as the differentiation targets define it: J = precip + sum_k sten(k) dp0(k)/g.
 Directions: relative perturbations of t0, qv0, tke and pblh (uniform in +-1e-3 of each value per
-element), and each tuning parameter rpen, rle, rkm, criqc.  A column is compared only where the
-finite-difference quotients at two step sizes agree to 1e-3 (no branch switch inside the step); the
-scheme's decisions make the others non-differentiable there."""
+element), and each tuning parameter rpen, rle, rkm, criqc.  98 % of the columns whose central
+quotients at two step sizes agree to 1e-3 (no branch switch inside the step) are within 1e-4; and
+every convecting column whose central and one-sided quotients agree to 1 % is within 1e-4 + 5 x
+their disagreement (the rest, at most 5 %, have a jump, a kink or strong curvature inside the step)."""
 import numpy as np
 import pytest
 
@@ -26,11 +27,28 @@ def _run(uw, s):
     return c.outputs_numpy()
 
 
-def _compare(tl, f1, f2, conv):
+def _compare(tl, f1, f2, conv, one_sided, what=""):
+    """f1, f2: central difference quotients at steps h and h/4; one_sided: the forward and backward
+    quotients at h/4.  Returns the columns where the quotients are smooth, the relative error of the
+    tangent against f2, and the columns whose error the difference quotients do not account for.
+
+    The finite differences are their own error bar: where a branch switches inside the step (a jump)
+    the two central quotients disagree, and where the objective has a kink (MX, MN, a limiter) the
+    forward and backward quotients disagree.  A column whose quotients disagree by more than 1 % is
+    not differentiable at this step; every other convecting column must have a tangent within
+    1e-4 + 5 x (that disagreement) of f2."""
     scale = max(float(np.abs(f2[conv]).max()), 1e-300)
-    smooth = conv & (np.abs(f1 - f2) <= 1e-3 * np.maximum(np.abs(f2), 1e-6 * scale))
-    rel = np.abs(tl - f2) / np.maximum(np.abs(f2), 1e-6 * scale)
-    return smooth, rel
+    den = np.maximum(np.abs(f2), 1e-6 * scale)
+    smooth = conv & (np.abs(f1 - f2) <= 1e-3 * den)
+    rel = np.abs(tl - f2) / den
+    fw, bw = one_sided
+    spread = np.maximum(np.abs(f1 - f2), np.abs(fw - bw)) / den
+    rough = conv & (spread > 1e-2)
+    unexplained = conv & ~rough & (rel > 1e-4 + 5.0 * spread)
+    print("%s: %d convecting, %d off by > 1e-4, %d not differentiable at this step, %d unexplained" % (
+        what, int(conv.sum()), int((conv & (rel > 1e-4)).sum()), int(rough.sum()), int(unexplained.sum())))
+    assert rough.sum() <= 0.05 * conv.sum(), (what, int(rough.sum()))
+    return smooth, rel, unexplained
 
 
 @pytest.mark.gpu
@@ -51,13 +69,18 @@ def test_tangent_linear_model(uw, cuda):
     assert all(np.array_equal(vals[k], base[k]) for k in base)
     tl = tout["precip"].cpu().numpy() + (tout["sten"].cpu().numpy() * s["dp0"]).sum(0) / G
 
+    j0 = _J(base, s["dp0"])
+
     def fd(h):
         sp, sm = dict(s), dict(s)
         for k, v in dirs.items():
             sp[k], sm[k] = s[k] + h * v, s[k] - h * v
-        return (_J(_run(uw, sp), s["dp0"]) - _J(_run(uw, sm), s["dp0"])) / (2 * h)
+        jp, jm = _J(_run(uw, sp), s["dp0"]), _J(_run(uw, sm), s["dp0"])
+        return (jp - jm) / (2 * h), ((jp - j0) / h, (j0 - jm) / h)
 
-    smooth, rel = _compare(tl, fd(1e-4), fd(2.5e-5), conv)
+    (f1, _), (f2, sided) = fd(1e-4), fd(2.5e-5)
+    smooth, rel, unexplained = _compare(tl, f1, f2, conv, sided, "inputs")
+    assert not unexplained.any(), np.flatnonzero(unexplained)
     assert smooth.sum() >= 0.9 * conv.sum()
     assert np.mean(rel[smooth] <= 1e-4) >= 0.98, np.percentile(rel[smooth], [50, 90, 99])
 
@@ -79,9 +102,10 @@ def test_tangent_linear_model(uw, cuda):
                 jp = _J(_run(uw, s), s["dp0"])
                 assert uw.set_params(*pm) == 0
                 jm = _J(_run(uw, s), s["dp0"])
-                fds.append((jp - jm) / (2 * h))
+                fds.append(((jp - jm) / (2 * h), ((jp - j0) / h, (j0 - jm) / h)))
             assert uw.set_params(*PARAMS) == 0
-            smooth, rel = _compare(tlp, fds[0], fds[1], conv)
+            smooth, rel, unexplained = _compare(tlp, fds[0][0], fds[1][0], conv, fds[1][1], name)
+            assert not unexplained.any(), (name, np.flatnonzero(unexplained))
             assert smooth.sum() >= 0.9 * conv.sum(), name
             assert np.mean(rel[smooth] <= 1e-4) >= 0.98, (name, np.percentile(rel[smooth], [50, 90, 99]))
     finally:
