@@ -41,6 +41,8 @@ UNITS = {
     "uwshcu_adj_k32n5.cu": ["-fmad=false"],
     "uwshcu_adj_k64n5.cu": ["-fmad=false"],
     "uwshcu_host.cu": [],
+    # measured FP64 throughput (explicit fma: the flag does not matter)
+    "uwshcu_probe.cu": [],
 }
 
 

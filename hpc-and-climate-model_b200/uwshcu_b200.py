@@ -46,7 +46,7 @@ EXPORTS = ("uwshcu_init", "uwshcu_set_rpen", "uwshcu_init_default", "uwshcu_set_
            "uwshcu_batch_capture", "uwshcu_batch_autotune", "uwshcu_batch_status",
            "uwshcu_batch_destroy", "uwshcu_set_pipeline", "uwshcu_set_params",
            "uwshcu_budget_device", "uwshcu_tangent_device", "uwshcu_compute_member",
-           "uwshcu_set_hand_slots", "uwshcu_adjoint_device", "uwshcu_adjoint_device_checked",
+           "uwshcu_set_hand_slots", "uwshcu_adjoint_device", "uwshcu_adjoint_device_checked", "uwshcu_fp64_peak",
            "uwshcu_adjoint_last_records",
            "uwshcu_adjoint_release", "uwshcu_set_adjoint_rows", "compute_zwshcu_",
            "compute_zwshcu_inv_", "compute_zwshcu_device", "uwshcu_set_zw_options")
@@ -515,6 +515,15 @@ def adjoint_launch(case, cot, inv=0, stream=None, defect=False):
     else:
         rc = lib().uwshcu_adjoint_device(ctypes.byref(m), ctypes.byref(a), ctypes.c_void_p(st.cuda_stream))
     return rc, grads
+
+
+def fp64_peak(stream=None):
+    """Measured FP64 throughput of the current device in TFLOP/s (uwshcu_fp64_peak)."""
+    import torch
+    st = stream if stream is not None else torch.cuda.current_stream()
+    v = ctypes.c_double(0.0)
+    rc = lib().uwshcu_fp64_peak(ctypes.byref(v), ctypes.c_void_p(st.cuda_stream))
+    return rc, v.value
 
 
 def adjoint_last_records():

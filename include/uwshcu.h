@@ -519,6 +519,12 @@ int uwshcu_compute_device_noalloc(int mix, int mkx, int iend, int ncnst, double 
                                   int *diag_int, double *diag_real, unsigned int *status_bits,
                                   void *stream);
 
+/* No counterpart in the reference.  Measures the FP64 throughput of the current device in TFLOP/s:
+ * independent chains of fused multiply-adds over two full waves of blocks, best of three timed
+ * launches on `stream` (after a warm-up).  The denominator of the FP64 roofline fractions of the
+ * benchmark; allocates and frees 8 bytes of device memory. */
+int uwshcu_fp64_peak(double *tflops, void *stream);
+
 /* Column energy and water budgets of a call, on device arrays: check_energy_chng
  * (check_energy.F90:321-395) as CAM applies it after the shallow scheme (tphysbc.F90:446-447),
  * for the state before the call (s0, qv0, ql0, qi0, u0, v0, dp0: the call's inputs) and the
