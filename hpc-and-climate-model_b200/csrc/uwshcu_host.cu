@@ -607,9 +607,9 @@ int host_call(int inv, int mix, int mkx, int iend, int ncnst, double dt, const d
         csz = std::min<size_t>(std::max<size_t>((n / 8 + 1023) / 1024 * 1024, 32768), 262144);
         nstreams = csz > 65536 ? 2 : 4;
     }
-    // The chunks: [c0, c0 + nc).  The auto shape ramps at both ends (a quarter, then a half of the
-    // chunk size first and last, 32,768 columns at least): the first chunk's inputs are in, and the
-    // last chunk's outputs are out, sooner.
+    // The chunks: [c0, c0 + nc).  The auto shape (and an explicit chunk_columns below -1) ramps at
+    // both ends (a quarter, then a half of the chunk size first and last, 32,768 columns at least):
+    // the first chunk's inputs are in, and the last chunk's outputs are out, sooner.
     std::vector<std::pair<size_t, size_t>> chunks;
     {
         std::vector<size_t> head, tail;
