@@ -169,6 +169,8 @@ struct DeviceState {
     // adjoint tapes, adjoints and tables, kept between adjoint calls (uwshcu_adjoint_release)
     void* adj_buf = nullptr;
     size_t adj_bytes = 0;
+    void* adj_aux = nullptr;     // the adjoint's ordering pass: level indices, a copy of cush, sort keys
+    size_t adj_aux_bytes = 0;
 };
 
 struct State {
@@ -824,6 +826,20 @@ __global__ void adj_zero_kernel(double* __restrict__ adj, size_t astride, const 
     for (size_t j = threadIdx.x; j < n; j += blockDim.x) p[j] = make_double2(0.0, 0.0);
 }
 
+// The ordering key of candidate j (column wl[j]) from the FP64 path's level indices: the
+// implicit-CIN columns (a second full iteration) after the explicit ones, then the updraft depth
+// kpen - krel, the trip count of the column's updraft level loops.
+__global__ void adj_key_kernel(const int* __restrict__ wl, int n, const int* __restrict__ diag, int mix,
+                               int* __restrict__ key)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const int i = wl[j];
+    const int depth = diag[UW_DI_KPEN * (size_t)mix + i] - diag[UW_DI_KREL * (size_t)mix + i];
+    const int implicit_cin = (diag[UW_DI_LIMIT * (size_t)mix + i] & UW_L_DELCIN) ? 0 : 1;
+    key[j] = implicit_cin * 64 + min(max(depth, 0), 63);
+}
+
 __global__ void eval_math_kernel(int fn, const double* __restrict__ x, const double* __restrict__ y,
                                  double* __restrict__ out, int n)
 {
@@ -1069,7 +1085,7 @@ int uwshcu_finalize(void)
     bool have = cudaGetDevice(&cur) == cudaSuccess;
     for (int dv = 0; dv < kMaxDev; dv++) {
         DeviceState& d = s.dev[dv];
-        if (!d.d_buf && !d.h_buf && !d.stream && !d.pipe[0] && !d.adj_buf && !d.sctx[0].err) continue;
+        if (!d.d_buf && !d.h_buf && !d.stream && !d.pipe[0] && !d.adj_buf && !d.adj_aux && !d.sctx[0].err) continue;
         cudaSetDevice(dv);
         if (d.d_buf) cudaFree(d.d_buf);
         if (d.h_buf) cudaFreeHost(d.h_buf);
@@ -1082,6 +1098,7 @@ int uwshcu_finalize(void)
         for (HandRegion& h : d.hand)
             if (h.base) cudaFree(h.base);
         if (d.adj_buf) cudaFree(d.adj_buf);
+        if (d.adj_aux) cudaFree(d.adj_aux);
         for (int n = 0; n < DeviceState::kSlots; n++)
             for (int j = 0; j < 3; j++)
                 if (d.ev[n][j]) cudaEventDestroy(d.ev[n][j]);
@@ -1511,6 +1528,38 @@ static int adjoint_run(const uwshcu_member* m, const uwshcu_adjoint* a, double* 
         return cuda_fail(e);
     s.adj_records = 0;
     if (ncand == 0) return UWSHCU_OK;
+    auto up = [](size_t x) { return (x + 255) / 256 * 256; };
+    // The candidates' order in the warps: by the FP64 path's implicit-CIN branch and updraft depth
+    // (adj_key_kernel), so that the lanes of a warp climb about as far and the warp's tape holds
+    // fewer rows; ties in ascending column order.  The FP64 worklist pass gives the level indices,
+    // on a copy of cush (which the taped forward sweep reads as the trigger pass left it).
+    size_t pair_bytes = 0;
+    if ((e = cub::DeviceRadixSort::SortPairs(nullptr, pair_bytes, (const int*)nullptr, (int*)nullptr,
+                                             (const int*)nullptr, (int*)nullptr, ncand, 0, 7, st)) != cudaSuccess)
+        return cuda_fail(e);
+    const size_t x_diag = 0, x_cush = x_diag + up(8 * mix * sizeof(int)), x_key = x_cush + up((size_t)m->iend * sizeof(double));
+    const size_t x_keyo = x_key + up((size_t)ncand * sizeof(int)), x_wlo = x_keyo + up((size_t)ncand * sizeof(int));
+    const size_t x_tmp = x_wlo + up((size_t)ncand * sizeof(int)), x_bytes = x_tmp + up(pair_bytes);
+    if (x_bytes > d->adj_aux_bytes) {
+        if (d->adj_aux) cudaFree(d->adj_aux);
+        d->adj_aux = nullptr;
+        d->adj_aux_bytes = 0;
+        if ((e = cudaMalloc(&d->adj_aux, x_bytes + x_bytes / 8)) != cudaSuccess) return cuda_fail(e);
+        d->adj_aux_bytes = x_bytes + x_bytes / 8;
+    }
+    char* const xb = static_cast<char*>(d->adj_aux);
+    int* const x_diag_p = reinterpret_cast<int*>(xb + x_diag);
+    double* const x_cush_p = reinterpret_cast<double*>(xb + x_cush);
+    {
+        UwArgs A2 = A;
+        A2.diag_int = x_diag_p;
+        A2.diag_real = nullptr;
+        A2.diag_level = nullptr;
+        if ((e = cudaMemcpyAsync(x_cush_p, m->cush, (size_t)m->iend * sizeof(double), cudaMemcpyDeviceToDevice, st)) != cudaSuccess ||
+            (e = launch_mode(&A2, UWSHCU_PREC_FP64, kModeList, sc->wl + 1, sc->wl, m->iend, 128, st)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(m->cush, x_cush_p, (size_t)m->iend * sizeof(double), cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
+            return cuda_fail(e);
+    }
     // Batches of warps (32 slots each) whose tapes fit 85 % of the device memory that is free or
     // already held by the adjoint buffer.  The tape capacity is sized from the previous call's largest
     // tape (+1/16); a batch that overflows it makes the call start again at the full capacity.  A
@@ -1519,9 +1568,9 @@ static int adjoint_run(const uwshcu_member* m, const uwshcu_adjoint* a, double* 
     const size_t nin = 3 * mkx + 6, rowb = uw_adj_row_bytes_k32n5();
     const size_t nids = (size_t)(25 + 5) * kp;   // output-index table entries per slot (NC = 5)
     const size_t nw_need = ((size_t)ncand + 31) / 32;
-    auto up = [](size_t x) { return (x + 255) / 256 * 256; };
-    // the candidates in ascending column order: the warps' columns, and with them the tapes and the
-    // order of every reduction, do not depend on the order the trigger pass appended them in
+    // the candidates in ascending column order, then stably by the ordering key: the warps' columns,
+    // and with them the tapes and the order of every reduction, do not depend on the order the
+    // trigger pass appended them in
     int end_bit = 1;
     while (end_bit < 31 && ((size_t)1 << end_bit) < (size_t)m->iend) end_bit++;
     size_t sort_bytes = 0;
@@ -1573,6 +1622,17 @@ static int adjoint_run(const uwshcu_member* m, const uwshcu_adjoint* a, double* 
             (e = cub::DeviceRadixSort::SortKeys(base + o_tmp, tmp_bytes, sc->wl + 1, wl, ncand, 0, end_bit, st)) !=
                 cudaSuccess)
             return cuda_fail(e);
+        {
+            int* const key = reinterpret_cast<int*>(xb + x_key);
+            int* const wl_o = reinterpret_cast<int*>(xb + x_wlo);
+            size_t pb = pair_bytes;
+            adj_key_kernel<<<(unsigned)((ncand + 255) / 256), 256, 0, st>>>(wl, ncand, x_diag_p, m->mix, key);
+            if ((e = cudaGetLastError()) != cudaSuccess ||
+                (e = cub::DeviceRadixSort::SortPairs(xb + x_tmp, pb, key, reinterpret_cast<int*>(xb + x_keyo), wl, wl_o,
+                                                     ncand, 0, 7, st)) != cudaSuccess ||
+                (e = cudaMemcpyAsync(wl, wl_o, (size_t)ncand * sizeof(int), cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
+                return cuda_fail(e);
+        }
         std::vector<int> counts(nw);
         int most = 0;
         unsigned int bits = 0;
@@ -1655,12 +1715,16 @@ int uwshcu_adjoint_release(void)
     cudaError_t e = cudaSuccess;
     for (int dv = 0; dv < kMaxDev; dv++) {
         DeviceState& d = s.dev[dv];
-        if (!d.adj_buf) continue;
+        if (!d.adj_buf && !d.adj_aux) continue;
         cudaSetDevice(dv);
-        const cudaError_t f = cudaFree(d.adj_buf);
-        if (f != cudaSuccess) e = f;
-        d.adj_buf = nullptr;
+        for (void** p : {&d.adj_buf, &d.adj_aux}) {
+            if (!*p) continue;
+            const cudaError_t f = cudaFree(*p);
+            if (f != cudaSuccess) e = f;
+            *p = nullptr;
+        }
         d.adj_bytes = 0;
+        d.adj_aux_bytes = 0;
     }
     if (have) cudaSetDevice(cur);
     return e == cudaSuccess ? UWSHCU_OK : cuda_fail(e);
