@@ -51,3 +51,9 @@ extern "C" cudaError_t uw_adj_launch_k32n5(const UwArgs* a, const void* slots, c
 
 // bytes of one tape row of a warp: 32 records of operand indices and partials
 extern "C" size_t uw_adj_row_bytes_k32n5() { return 32 * (sizeof(int2) + sizeof(double2)); }
+
+// Warps of the forward sweep (one per block) that one SM holds at once.
+extern "C" cudaError_t uw_adj_forward_occupancy_k32n5(int* warps_per_sm)
+{
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(warps_per_sm, uwshcu_adj_forward<32, 5>, UW_ADJ_BLOCK, 0);
+}

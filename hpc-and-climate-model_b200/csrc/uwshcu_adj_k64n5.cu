@@ -48,3 +48,9 @@ extern "C" cudaError_t uw_adj_launch_k64n5(const UwArgs* a, const void* slots, c
     }
     return cudaGetLastError();
 }
+
+// Warps of the forward sweep (one per block) that one SM holds at once.
+extern "C" cudaError_t uw_adj_forward_occupancy_k64n5(int* warps_per_sm)
+{
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(warps_per_sm, uwshcu_adj_forward<64, 5>, UW_ADJ_BLOCK, 0);
+}

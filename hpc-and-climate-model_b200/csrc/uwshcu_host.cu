@@ -52,6 +52,8 @@ extern "C" cudaError_t uw_adj_set_constants_k32n5(const UwConst* h, const double
 extern "C" cudaError_t uw_adj_launch_k32n5(const UwArgs* a, const void* slots, const uwshcu_adjoint* c, int phase,
                                            cudaStream_t stream);
 extern "C" size_t uw_adj_row_bytes_k32n5();   // the same for both units: 32 records per row
+extern "C" cudaError_t uw_adj_forward_occupancy_k32n5(int* warps_per_sm);
+extern "C" cudaError_t uw_adj_forward_occupancy_k64n5(int* warps_per_sm);
 extern "C" cudaError_t uw_adj_set_constants_k64n5(const UwConst* h, const double* tbl);
 extern "C" cudaError_t uw_adj_launch_k64n5(const UwArgs* a, const void* slots, const uwshcu_adjoint* c, int phase,
                                            cudaStream_t stream);
@@ -1564,7 +1566,8 @@ static int adjoint_run(const uwshcu_member* m, const uwshcu_adjoint* a, double* 
     // already held by the adjoint buffer.  The tape capacity is sized from the previous call's largest
     // tape (+1/16); a batch that overflows it makes the call start again at the full capacity.  A
     // batch costs about one warp's forward sweep whatever its size (the sweep is a latency chain per
-    // warp), so one batch for all candidates is what the sizing aims at.
+    // warp), so the sizing aims at one batch for all candidates, or at batches of as many warps as
+    // the GPU holds at once.
     const size_t nin = 3 * mkx + 6, rowb = uw_adj_row_bytes_k32n5();
     const size_t nids = (size_t)(25 + 5) * kp;   // output-index table entries per slot (NC = 5)
     const size_t nw_need = ((size_t)ncand + 31) / 32;
@@ -1588,7 +1591,15 @@ static int adjoint_run(const uwshcu_member* m, const uwshcu_adjoint* a, double* 
         size_t freeb = 0, totalb = 0;
         if ((e = cudaMemGetInfo(&freeb, &totalb)) != cudaSuccess) return cuda_fail(e);
         const size_t avail = (freeb + d->adj_bytes) / 20 * 17;
-        const size_t nw = std::min(nw_need, std::max((size_t)1, avail / per_warp)), nb = 32 * nw;
+        // at most the warps the GPU holds at once: a warp of a batch that waits for a place would
+        // start its chain when the first ones end, and the batch would last two chains
+        int per_sm = 0, nsm = 0, dev = 0;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
+            (e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
+            (e = (k32 ? uw_adj_forward_occupancy_k32n5 : uw_adj_forward_occupancy_k64n5)(&per_sm)) != cudaSuccess)
+            return cuda_fail(e);
+        const size_t resident = std::max<size_t>(1, (size_t)nsm * (size_t)per_sm);
+        const size_t nw = std::min(std::min(nw_need, resident), std::max((size_t)1, avail / per_warp)), nb = 32 * nw;
         // carve the buffer: tapes (operand indices, partials), adjoints, tables, counters, status
         const size_t o_ab = 0, o_d = o_ab + up(nw * rcap * 32 * 8), o_adj = o_d + up(nw * rcap * 32 * 16);
         const size_t o_ids = o_adj + up(nw * astride * sizeof(double)), o_nrow = o_ids + up(nb * nids * sizeof(int));
