@@ -165,6 +165,7 @@ struct UwArgs {
     const double *omega; // (mix, mkx) pressure velocity: compute_zwshcu; nullptr: compute_uwshcu
     unsigned int *err;   // device error word
     const UwHand *hand;  // UW_MODE_LIST1 / UW_MODE_RESUME only: device copy of the hand-off region
+    int *depth_key;      // optional (mix): each computed column's ordering key for the next call
 };
 
 // ---- batched launches --------------------------------------------------------------------------

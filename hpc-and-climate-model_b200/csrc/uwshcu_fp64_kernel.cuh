@@ -2152,6 +2152,12 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
         A.diag_int[UW_DI_KBUP * (size_t)mix + i] = kbup;
         A.diag_int[UW_DI_KPEN * (size_t)mix + i] = kpen;
     }
+    // the column's place in the next call's first worklist launch (uwshcu_set_depth_order): the
+    // explicit-CIN columns first, then by updraft depth
+    if (A.depth_key) {
+        const int depth = kpen - krel;
+        A.depth_key[i] = ((lflags & UW_L_DELCIN) ? 0 : 64) + (depth < 0 ? 0 : (depth > 63 ? 63 : depth));
+    }
     }
     if (errbits) atomicOr(A.err, errbits);
     }  // active

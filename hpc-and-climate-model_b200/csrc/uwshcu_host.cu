@@ -124,6 +124,8 @@ cudaError_t launch_mode(const UwArgs* a, int prec, int mode, int* wl, int* wl_co
 struct HandRegion {
     char* base = nullptr;
     size_t cap = 0, words = 0;
+    char* dsort = nullptr;       // uwshcu_set_depth_order: the keys and the sort of a worklist
+    size_t dsort_bytes = 0;
 };
 
 // What a device-array call (uwshcu_compute_device, uwshcu_compute_member, the tangent-linear and
@@ -136,6 +138,8 @@ struct StreamCtx {
     unsigned int* err = nullptr;   // endrun bits of the calls since the last uwshcu_device_status
     int* wl = nullptr;             // worklist of convecting columns: [0] = count, [1..] = column ids
     size_t wl_cap = 0;
+    int* dkey = nullptr;           // uwshcu_set_depth_order: each column's key from the last call
+    size_t dkey_cap = 0;
     HandRegion hand;               // hand-off region of the sorted schedule
 };
 
@@ -173,6 +177,8 @@ struct DeviceState {
     size_t adj_bytes = 0;
     void* adj_aux = nullptr;     // the adjoint's ordering pass: level indices, a copy of cush, sort keys
     size_t adj_aux_bytes = 0;
+    int* hkey = nullptr;         // uwshcu_set_depth_order, host-array calls: the key of every column
+    size_t hkey_cap = 0;
 };
 
 struct State {
@@ -191,6 +197,7 @@ struct State {
     int chunk_columns = 32768;   // host-array calls: columns per pipeline chunk (0: one chunk)
     int pipe_streams = 4;        // host-array calls: streams the chunks alternate over
     bool pipe_auto = true;       // until uwshcu_set_pipeline: the shape follows the call's size
+    bool depth_order = false;    // uwshcu_set_depth_order
     bool pipe_ramp = true;       // smaller first and last chunks (the auto shape, chunk_columns < -1)
     DeviceState dev[kMaxDev];
     char lasterr[256] = "";
@@ -500,9 +507,67 @@ const UwHand* hand_region(HandRegion& h, int iend, int mkx, int ncnst)
 // The worklist pass over list[0 .. *count): one UW_MODE_LIST launch, or with the sorted schedule
 // the split pass through hand-off region r: UW_MODE_LIST1, the sort of the handed-off
 // columns by iteration-1 updraft depth, UW_MODE_RESUME.
-cudaError_t worklist_pass(HandRegion& h, UwArgs A, int* list, int* count, cudaStream_t st)
+// The key of worklist entry j for the ordering by the last call's depth (list entries beyond the
+// count sort last).
+__global__ void depth_list_key_kernel(const int* __restrict__ list, const int* __restrict__ count, int n,
+                                      const int* __restrict__ dkey, int* __restrict__ key)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    key[j] = j < *count ? dkey[list[j]] : 255;
+}
+
+// A key array of at least n entries, zero where new (the keys of columns no call has computed yet).
+int grow_keys(int*& buf, size_t& cap, size_t n)
+{
+    if (n <= cap) return UWSHCU_OK;
+    cudaError_t e;
+    if (buf && (e = cudaFree(buf)) != cudaSuccess) return cuda_fail(e);
+    buf = nullptr;
+    cap = 0;
+    if ((e = cudaMalloc(&buf, n * sizeof(int))) != cudaSuccess) return cuda_fail(e);
+    if ((e = cudaMemset(buf, 0, n * sizeof(int))) != cudaSuccess || (e = cudaDeviceSynchronize()) != cudaSuccess)
+        return cuda_fail(e);
+    cap = n;
+    return UWSHCU_OK;
+}
+
+// list[0 .. *count) in ascending order of dkey[column] (stable), through the region's sort buffers.
+cudaError_t order_by_depth(HandRegion& h, int* list, const int* count, int n, const int* dkey, cudaStream_t st)
+{
+    cudaError_t e;
+    size_t pb = 0;
+    if ((e = cub::DeviceRadixSort::SortPairs(nullptr, pb, (const int*)nullptr, (int*)nullptr, (const int*)nullptr,
+                                             (int*)nullptr, n, 0, 8, st)) != cudaSuccess)
+        return e;
+    const size_t seg = ((size_t)n * sizeof(int) + 255) / 256 * 256, need = 3 * seg + pb;
+    if (need > h.dsort_bytes) {
+        if (h.dsort && (e = cudaFree(h.dsort)) != cudaSuccess) return e;
+        h.dsort = nullptr;
+        h.dsort_bytes = 0;
+        if ((e = cudaMalloc(&h.dsort, need + need / 8)) != cudaSuccess) return e;
+        h.dsort_bytes = need + need / 8;
+    }
+    int* key = reinterpret_cast<int*>(h.dsort);
+    int* key_o = reinterpret_cast<int*>(h.dsort + seg);
+    int* list_o = reinterpret_cast<int*>(h.dsort + 2 * seg);
+    depth_list_key_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(list, count, n, dkey, key);
+    if ((e = cudaGetLastError()) != cudaSuccess ||
+        (e = cub::DeviceRadixSort::SortPairs(h.dsort + 3 * seg, pb, key, key_o, list, list_o, n, 0, 8, st)) != cudaSuccess)
+        return e;
+    return cudaMemcpyAsync(list, list_o, (size_t)n * sizeof(int), cudaMemcpyDeviceToDevice, st);
+}
+
+// dkey (optional): each column's ordering key, read to order list[] before the first worklist
+// launch and rewritten by it for the next call (uwshcu_set_depth_order).
+cudaError_t worklist_pass(HandRegion& h, UwArgs A, int* list, int* count, cudaStream_t st, int* dkey)
 {
     State& s = S();
+    if (dkey) {
+        A.depth_key = dkey;
+        const cudaError_t e = order_by_depth(h, list, count, A.iend, dkey, st);
+        if (e != cudaSuccess) return e;
+    }
     const UwHand* H = nullptr;
     if (s.schedule == UWSHCU_SCHED_SORTED) H = hand_region(h, A.iend, A.mkx, A.ncnst);
     if (!H) return launch_mode(&A, s.precision, kModeList, list, count, A.iend, s.block, st);
@@ -546,7 +611,12 @@ int enqueue(DeviceState& d, StreamCtx& c, UwArgs A, cudaStream_t st)
     if (ev && (e = cudaEventRecord(ev[0], st)) != cudaSuccess) return cuda_fail(e);
     if ((e = launch_mode(&A, s.precision, kModeTrigger, list, count, A.iend, s.block, st)) != cudaSuccess) return cuda_fail(e);
     if (ev && (e = cudaEventRecord(ev[1], st)) != cudaSuccess) return cuda_fail(e);
-    if ((e = worklist_pass(c.hand, A, list, count, st)) != cudaSuccess) return cuda_fail(e);
+    int* dkey = nullptr;
+    if (s.depth_order) {
+        if ((rc = grow_keys(c.dkey, c.dkey_cap, (size_t)A.iend)) != UWSHCU_OK) return rc;
+        dkey = c.dkey;
+    }
+    if ((e = worklist_pass(c.hand, A, list, count, st, dkey)) != cudaSuccess) return cuda_fail(e);
     if (ev && (e = cudaEventRecord(ev[2], st)) != cudaSuccess) return cuda_fail(e);
     return UWSHCU_OK;
 }
@@ -660,6 +730,7 @@ int host_call(int inv, int mix, int mkx, int iend, int ncnst, double dt, const d
     }
     if ((rc = grow(*d, nin + nout, direct ? 2 * nch : nin + nout + 2 * nch)) != UWSHCU_OK) return rc;
     if ((rc = grow_worklist(*d, n + 2 * nch)) != UWSHCU_OK) return rc;
+    if (s.depth_order && (rc = grow_keys(d->hkey, d->hkey_cap, n)) != UWSHCU_OK) return rc;
     cudaError_t e;
     if (!d->pipe[0]) {
         int least = 0, greatest = 0;
@@ -788,7 +859,8 @@ int host_call(int inv, int mix, int mkx, int iend, int ncnst, double dt, const d
         } else {
             if ((e = launch_mode(&A, s.precision, kModeTrigger, wreg + 2, wreg, A.iend, s.block, st)) != cudaSuccess)
                 return cuda_fail(e);
-            if ((e = worklist_pass(d->hand[1 + c % nstreams], A, wreg + 2, wreg, st)) != cudaSuccess)
+            if ((e = worklist_pass(d->hand[1 + c % nstreams], A, wreg + 2, wreg, st,
+                                   s.depth_order ? d->hkey + c0 : nullptr)) != cudaSuccess)
                 return cuda_fail(e);
         }
         if ((e = cudaEventRecord(d->ev_comp[c], st)) != cudaSuccess) return cuda_fail(e);
@@ -1059,6 +1131,15 @@ int uwshcu_set_pipeline(int chunk_columns, int streams)
     return UWSHCU_OK;
 }
 
+int uwshcu_set_depth_order(int on)
+{
+    if (on != 0 && on != 1) return UWSHCU_ERR_BAD_ARGS;
+    State& s = S();
+    std::lock_guard<std::mutex> lock(s.mu);
+    s.depth_order = on != 0;
+    return UWSHCU_OK;
+}
+
 int uwshcu_set_block(int threads)
 {
     State& s = S();
@@ -1096,9 +1177,14 @@ int uwshcu_finalize(void)
             if (c.err) cudaFree(c.err);
             if (c.wl) cudaFree(c.wl);
             if (c.hand.base) cudaFree(c.hand.base);
+            if (c.hand.dsort) cudaFree(c.hand.dsort);
+            if (c.dkey) cudaFree(c.dkey);
         }
-        for (HandRegion& h : d.hand)
+        for (HandRegion& h : d.hand) {
             if (h.base) cudaFree(h.base);
+            if (h.dsort) cudaFree(h.dsort);
+        }
+        if (d.hkey) cudaFree(d.hkey);
         if (d.adj_buf) cudaFree(d.adj_buf);
         if (d.adj_aux) cudaFree(d.adj_aux);
         for (int n = 0; n < DeviceState::kSlots; n++)

@@ -47,6 +47,7 @@ EXPORTS = ("uwshcu_init", "uwshcu_set_rpen", "uwshcu_init_default", "uwshcu_set_
            "uwshcu_batch_destroy", "uwshcu_set_pipeline", "uwshcu_set_params",
            "uwshcu_budget_device", "uwshcu_tangent_device", "uwshcu_compute_member",
            "uwshcu_set_hand_slots", "uwshcu_adjoint_device", "uwshcu_adjoint_device_checked", "uwshcu_fp64_peak",
+           "uwshcu_set_depth_order",
            "uwshcu_adjoint_last_records",
            "uwshcu_adjoint_release", "uwshcu_set_adjoint_rows", "compute_zwshcu_",
            "compute_zwshcu_inv_", "compute_zwshcu_device", "uwshcu_set_zw_options")
@@ -135,6 +136,10 @@ def profile_read():
 
 def set_pipeline(chunk_columns, streams):
     return lib().uwshcu_set_pipeline(ctypes.c_int(chunk_columns), ctypes.c_int(streams))
+
+
+def set_depth_order(on):
+    return lib().uwshcu_set_depth_order(ctypes.c_int(1 if on else 0))
 
 
 def set_hand_slots(slots):

@@ -123,6 +123,17 @@ int uwshcu_profile_read(int *calls, double *trigger_ms, double *list_ms, int *li
  * columns over `streams` streams with those ramped ends. */
 int uwshcu_set_pipeline(int chunk_columns, int streams);
 
+/* No counterpart in the reference.  on = 1: every worklist pass (device-array calls per caller
+ * stream, host-array calls per device) orders its convecting columns by the updraft the same
+ * column index had in the previous call (explicit-CIN columns first, then by cloud-top depth above
+ * the release level), so that the lanes of a warp climb about as far.  A model that calls with the
+ * same column layout every time step (CAM's chunks) gets warps of like columns, as the weather
+ * changes slowly from step to step; results do not depend on it.  Measured on 1,048,576 columns
+ * whose state evolves by the computed tendencies each step: 2-6 % less time per step; on repeated
+ * identical inputs (the upper bound) 8 %.  Costs one sort of the worklist per pass and an int per
+ * column.  on = 0 (default): trigger order. */
+int uwshcu_set_depth_order(int on);
+
 /* Threads per block of the column kernel (0 = built-in default). */
 int uwshcu_set_block(int threads);
 
