@@ -131,7 +131,8 @@ int uwshcu_set_pipeline(int chunk_columns, int streams);
  * changes slowly from step to step; results do not depend on it.  Measured on 1,048,576 columns
  * whose state evolves by the computed tendencies each step: 2-6 % less time per step; on repeated
  * identical inputs (the upper bound) 8 %.  Costs one sort of the worklist per pass and an int per
- * column.  on = 0 (default): trigger order. */
+ * column (uwshcu_compute_device_noalloc, which allocates nothing, keeps trigger order).  on = 0
+ * (default): trigger order. */
 int uwshcu_set_depth_order(int on);
 
 /* Threads per block of the column kernel (0 = built-in default). */
