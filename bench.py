@@ -357,7 +357,7 @@ def precision_leg(uw, case, stream, steps, warmup, fp64_ms, mode):
             "speedup_vs_fp64": fp64_ms / ms, "column_rel_rms_vs_fp64": err,
             "column_rel_rms_vs_fp64_same_decisions": err_kept, "columns_with_same_decisions": same,
             "column_error_distribution": dist,
-            "flips": flips, "targets": "north_star (mixed): >= 2x the FP64 path at <= 1e-4 relative RMS"}
+            "flips": flips, "targets": "mixed precision: >= 2x the FP64 path at <= 1e-4 relative RMS"}
 
 
 def depth_order_leg(uw, case, stream, nsteps=4, dt=1800.0, cp=1004.64):
@@ -474,7 +474,7 @@ def adjoint_leg(uw, steps, warmup, n=65_536):
             "adjoint_ms": adj, "checked_adjoint_ms": checked, "steps": ka, "workload": "%s columns x 30 levels (seed 301)" % f"{n:,}",
             "convecting_columns": conv, "tape_rows_per_warp": rows,
             "tape_bytes_per_convecting_column": rows * 32,
-            "target": "north_star: <= 4x the forward"}
+            "target": "adjoint: <= 4x the forward"}
 
 
 # Batched uneven workload: 4 members of 262,144 columns (1,048,576 in all) with 30, 35, 51 and 30
