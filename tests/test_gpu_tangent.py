@@ -5,7 +5,9 @@ Directions: relative perturbations of t0, qv0, tke and pblh (uniform in +-1e-3 o
 element), and each tuning parameter rpen, rle, rkm, criqc.  98 % of the columns whose central
 quotients at two step sizes agree to 1e-3 (no branch switch inside the step) are within 1e-4; and
 every convecting column whose central and one-sided quotients agree to 1 % is within 1e-4 + 5 x
-their disagreement (the rest, at most 5 %, have a jump, a kink or strong curvature inside the step)."""
+their disagreement (the rest, at most 5 % at 30 levels and 15 % at 51, have a jump, a kink or strong
+curvature inside the step).  At 51 levels (the 64-level unit) the input steps are 10x smaller: a
+column makes more saturation evaluations, so a step crosses more of their kinks."""
 import numpy as np
 import pytest
 
@@ -47,15 +49,19 @@ def _compare(tl, f1, f2, conv, one_sided, what=""):
     unexplained = conv & ~rough & (rel > 1e-4 + 5.0 * spread)
     print("%s: %d convecting, %d off by > 1e-4, %d not differentiable at this step, %d unexplained" % (
         what, int(conv.sum()), int((conv & (rel > 1e-4)).sum()), int(rough.sum()), int(unexplained.sum())))
-    assert rough.sum() <= 0.05 * conv.sum(), (what, int(rough.sum()))
-    return smooth, rel, unexplained
+    return smooth, rel, unexplained, rough
 
 
 @pytest.mark.gpu
-def test_tangent_linear_model(uw, cuda):
+# (levels, the two relative steps of the input direction, the share of the convecting columns allowed
+# to be non-differentiable at that step): 51 levels make more saturation evaluations per column, so
+# they take smaller steps
+@pytest.mark.parametrize("pver,steps,rough_max,smooth_min", [(30, (1e-4, 2.5e-5), 0.05, 0.9),
+                                                             (51, (1e-5, 2.5e-6), 0.15, 0.85)])
+def test_tangent_linear_model(uw, cuda, pver, steps, rough_max, smooth_min):
     import torch
     assert uw.init_default() == 0
-    s = soundings.make_soundings(4096, 30, seed=201, rh_pbl=(0.675, 0.93))
+    s = soundings.make_soundings(4096, pver, seed=201, rh_pbl=(0.675, 0.93))
     rng = np.random.default_rng(5)
     dirs = {k: s[k] * rng.uniform(-1e-3, 1e-3, s[k].shape) for k in ("t0", "qv0", "tke", "pblh")}
     base = _run(uw, s)
@@ -78,11 +84,22 @@ def test_tangent_linear_model(uw, cuda):
         jp, jm = _J(_run(uw, sp), s["dp0"]), _J(_run(uw, sm), s["dp0"])
         return (jp - jm) / (2 * h), ((jp - j0) / h, (j0 - jm) / h)
 
-    (f1, _), (f2, sided) = fd(1e-4), fd(2.5e-5)
-    smooth, rel, unexplained = _compare(tl, f1, f2, conv, sided, "inputs")
-    assert not unexplained.any(), np.flatnonzero(unexplained)
-    assert smooth.sum() >= 0.9 * conv.sum()
-    assert np.mean(rel[smooth] <= 1e-4) >= 0.98, np.percentile(rel[smooth], [50, 90, 99])
+    (f1, _), (f2, sided) = fd(steps[0]), fd(steps[1])
+    fails = []
+
+    def judge(name, smooth, rel, unexplained, rough):
+        within = float(np.mean(rel[smooth] <= 1e-4))
+        print("   %s: smooth %d, within 1e-4 on them %.4f" % (name, int(smooth.sum()), within))
+        if unexplained.any():
+            fails.append((name, "unexplained", np.flatnonzero(unexplained)[:8]))
+        if rough.sum() > rough_max * conv.sum():
+            fails.append((name, "not differentiable", int(rough.sum())))
+        if smooth.sum() < smooth_min * conv.sum():
+            fails.append((name, "smooth", int(smooth.sum())))
+        if within < 0.98:
+            fails.append((name, "within 1e-4", within, np.percentile(rel[smooth], [50, 90, 99])))
+
+    judge("inputs", *_compare(tl, f1, f2, conv, sided, "inputs %d levels" % pver))
 
     # tuning parameters, one at a time
     try:
@@ -104,9 +121,7 @@ def test_tangent_linear_model(uw, cuda):
                 jm = _J(_run(uw, s), s["dp0"])
                 fds.append(((jp - jm) / (2 * h), ((jp - j0) / h, (j0 - jm) / h)))
             assert uw.set_params(*PARAMS) == 0
-            smooth, rel, unexplained = _compare(tlp, fds[0][0], fds[1][0], conv, fds[1][1], name)
-            assert not unexplained.any(), (name, np.flatnonzero(unexplained))
-            assert smooth.sum() >= 0.9 * conv.sum(), name
-            assert np.mean(rel[smooth] <= 1e-4) >= 0.98, (name, np.percentile(rel[smooth], [50, 90, 99]))
+            judge(name, *_compare(tlp, fds[0][0], fds[1][0], conv, fds[1][1], name))
     finally:
         assert uw.init_default() == 0
+    assert not fails, fails
