@@ -2163,12 +2163,10 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
 
 // ---- kernels ---------------------------------------------------------------------------------------
 
-// Register caps (resident blocks of 128 per SM): the worklist launches at 128 registers (4 blocks
-// instead of 3 at their natural 168; the extra warps hide more FP64 and local-memory latency than
-// the added spills cost, -10 % time on the benchmark workload; 5 blocks cost +1.5f % for
-// UW_MODE_LIST1), the UW_MODE_RESUME launch, which spills less, at 102 (5 blocks: -3.3f % step
-// time against 4, +2.8f % at 6), the trigger pass at 102, the single pass at 168.f
-#define UW_LIST_MINB(m) ((m) == UW_MODE_RESUME ? 5 : (UW_MODE_IS_LIST(m) ? 4 : ((m) == UW_MODE_TRIGGER ? 5 : 3)))
+// Register caps (resident blocks of 128 per SM): the worklist launches at 72 registers (7 blocks;
+// 1,048,576 x 30 columns: 103.9 ms against 115.6 ms at the FP64 kernel's 4 and 5 blocks, 109.8 ms
+// at 6, 104.5 ms at 8), the trigger pass at 102, the single pass at 168.
+#define UW_LIST_MINB(m) ((m) == UW_MODE_RESUME ? 7 : (UW_MODE_IS_LIST(m) ? 7 : ((m) == UW_MODE_TRIGGER ? 5 : 3)))
 template <int KP, int NC, int MODE>
 __global__ void __launch_bounds__(128, UW_LIST_MINB(MODE))
 uwshcu_mixed_kernel(const __grid_constant__ UwArgs A, int* __restrict__ wl, int* __restrict__ wl_count)

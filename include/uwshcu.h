@@ -43,7 +43,7 @@ extern "C" {
 #define UWSHCU_PREC_FP64 0               /* FP64 throughout, Fortran evaluation order, no FMA      */
 #define UWSHCU_PREC_MIXED 1              /* FP32 bulk, FP64 conden/roots/qsinvert/implicit CIN/
                                             positive_moisture, Kahan vertical sums (ncnst <= 5).
-                                            1.5x the FP64 path; column heating/moistening/precip
+                                            1.7x the FP64 path; column heating/moistening/precip
                                             ~0.9 % relative RMS (cloud tops of ~0.6 % of the
                                             convecting columns move)                            */
 #define UWSHCU_PREC_FAST 2               /* FP64 throughout with a Newton conden that stops each
