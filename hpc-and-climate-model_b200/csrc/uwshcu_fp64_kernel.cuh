@@ -2194,9 +2194,10 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
 // Register caps (resident blocks of 128 per SM): the worklist launches at 128 registers (4 blocks
 // instead of 3 at their natural 168; the extra warps hide more FP64 and local-memory latency than
 // the added spills cost, -10 % time on the benchmark workload; 5 blocks cost +1.5 % for
-// UW_MODE_LIST1), the UW_MODE_RESUME launch, which spills less, at 102 (5 blocks: -3.3 % step
-// time against 4, +2.8 % at 6), the trigger pass at 102, the single pass at 168.
-#define UW_LIST_MINB(m) ((m) == UW_MODE_RESUME ? 5 : (UW_MODE_IS_LIST(m) ? 4 : ((m) == UW_MODE_TRIGGER ? 5 : 3)))
+// UW_MODE_LIST1), the UW_MODE_RESUME launch, which spills less, at 85 (6 blocks: 177.1-177.4 ms
+// per 1,048,576-column step against 178.7-178.8 at 5 with the correctly rounded math routines),
+// the trigger pass at 102 (6 blocks: no change), the single pass at 168.
+#define UW_LIST_MINB(m) ((m) == UW_MODE_RESUME ? 6 : (UW_MODE_IS_LIST(m) ? 4 : ((m) == UW_MODE_TRIGGER ? 5 : 3)))
 template <int KP, int NC, int MODE, int ZW = 0>
 __global__ void __launch_bounds__(128, UW_LIST_MINB(MODE))
 uwshcu_fp64_kernel(const __grid_constant__ UwArgs A, int* __restrict__ wl, int* __restrict__ wl_count)
