@@ -105,8 +105,9 @@ i0 = b.index("// Register caps (resident blocks of 128 per SM)")
 i1 = b.index("\n", b.index("#define UW_LIST_MINB(m)", i0))
 b = b[:i0] + """// Register caps (resident blocks of 128 per SM): the worklist launches at 72 registers (7 blocks;
 // 1,048,576 x 30 columns: 103.9 ms against 115.6 ms at the FP64 kernel's 4 and 5 blocks, 109.8 ms
-// at 6, 104.5 ms at 8), the trigger pass at 102, the single pass at 168.
-#define UW_LIST_MINB(m) ((m) == UW_MODE_RESUME ? 7 : (UW_MODE_IS_LIST(m) ? 7 : ((m) == UW_MODE_TRIGGER ? 5 : 3)))""" + b[i1:]
+// at 6, 104.5 ms at 8), the trigger pass at 72 too (7 blocks: 103.1-103.4 ms against 104.8 ms at 5),
+// the single pass at 168.
+#define UW_LIST_MINB(m) ((m) == UW_MODE_RESUME ? 7 : (UW_MODE_IS_LIST(m) ? 7 : ((m) == UW_MODE_TRIGGER ? 7 : 3)))""" + b[i1:]
 start = b.index("        // positive_moisture_single (uwshcu.F90:5096-5162 via :3995-4001); state after the tendencies")
 end = b.index("        for (int k = 1; k <= mkx; k++) {\n            qtten[k] = qvten[k] + qlten[k] + qiten[k];", start)
 pm = open(D + 'mixed_positive_moisture.inc').read()

@@ -2165,8 +2165,9 @@ __device__ __forceinline__ void uw_column(const UwArgs& A, const double* __restr
 
 // Register caps (resident blocks of 128 per SM): the worklist launches at 72 registers (7 blocks;
 // 1,048,576 x 30 columns: 103.9 ms against 115.6 ms at the FP64 kernel's 4 and 5 blocks, 109.8 ms
-// at 6, 104.5 ms at 8), the trigger pass at 102, the single pass at 168.
-#define UW_LIST_MINB(m) ((m) == UW_MODE_RESUME ? 7 : (UW_MODE_IS_LIST(m) ? 7 : ((m) == UW_MODE_TRIGGER ? 5 : 3)))
+// at 6, 104.5 ms at 8), the trigger pass at 72 too (7 blocks: 103.1-103.4 ms against 104.8 ms at 5),
+// the single pass at 168.
+#define UW_LIST_MINB(m) ((m) == UW_MODE_RESUME ? 7 : (UW_MODE_IS_LIST(m) ? 7 : ((m) == UW_MODE_TRIGGER ? 7 : 3)))
 template <int KP, int NC, int MODE>
 __global__ void __launch_bounds__(128, UW_LIST_MINB(MODE))
 uwshcu_mixed_kernel(const __grid_constant__ UwArgs A, int* __restrict__ wl, int* __restrict__ wl_count)
