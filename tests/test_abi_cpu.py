@@ -63,6 +63,12 @@ def test_bad_arguments_are_rejected(uw):
     assert uw.set_adjoint_rows(-1) == uw.ERR_BAD_ARGS and uw.set_adjoint_rows((1 << 19) + 1) == uw.ERR_BAD_ARGS
     assert uw.set_adjoint_rows(0) == 0
     assert uw.adjoint_release() == 0
+    assert L.uwshcu_adjoint_device_checked(None, None, None, None) == uw.ERR_BAD_ARGS
+    assert L.uwshcu_set_depth_order(ctypes.c_int(2)) == uw.ERR_BAD_ARGS
+    assert uw.set_depth_order(True) == 0 and uw.set_depth_order(False) == 0
+    assert L.uwshcu_set_pipeline(ctypes.c_int(-2), ctypes.c_int(0)) == uw.ERR_BAD_ARGS   # streams 1..8
+    assert uw.set_pipeline(-65536, 2) == 0 and uw.set_pipeline(-1, 0) == 0
+    assert L.uwshcu_fp64_peak(None, None) == uw.ERR_BAD_ARGS
 
 
 def test_init_rejects_bad_tracer_metadata(uw):
